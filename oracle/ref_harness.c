@@ -1,0 +1,337 @@
+/*
+ * Reference harness: runs the reference's own s-mode full-wave HDDM solver
+ * (lib/hddm, lib/fem, lib/mymt_aij_solver, main/fullwave/fullwave.c), built
+ * from its sources by oracle/Makefile.ref, on a synthetic model written by
+ * adventure_fullwave_b200.meshgen.write_hddm_model.  TEST INFRASTRUCTURE ONLY:
+ * it is the oracle the CUDA path is checked against and the CPU baseline it
+ * is timed against; the product never links or runs it.
+ *
+ * The flow is the reference's main() (main/fullwave/main.c:34-124) with one
+ * change made through the reference's own plug-in table (HDDM_FUNC,
+ * lib/std/types.h:629-730): the table from set_hddm_func_fullwave
+ * (main/fullwave/fullwave.c:23-146) gets
+ *   - make_TMP_AIJ wrapped to add the edge current source of <dir>/source.txt
+ *     to the assembled right-hand side of the subdomain that owns the edge
+ *     (the lowest-numbered subdomain holding it), and
+ *   - solve_dom_1st / iteration_s / solve_dom_last wrapped to record timings
+ *     and, on request, dump the reference's intermediate data.
+ * The correction-Jo pre-solve of main.c:92-98 runs only for antennas, which
+ * synthetic models do not define.
+ *
+ * Usage: fw_ref_harness [reference options] <model_dir>
+ * Environment:
+ *   FW_HARNESS_OUT   output prefix (default <model_dir>/ref)
+ *   FW_HARNESS_DUMP  0: timings + solution, 1: + integer maps,
+ *                    2: + assembled TMP_AIJ and skyline factors
+ * Outputs: <prefix>.json (timings, counts), <prefix>.sol (solution),
+ *          <prefix>.ints, <prefix>.aij, <prefix>.fac (dumps), and the
+ *          reference's own residual log under <model_dir>/calc_log/.
+ */
+#include "advfullwave_lib.h"
+#include "libfem.h"
+#include "libhddm.h"
+
+#include "fullwave.h"
+
+#include <stdint.h>
+
+/* the program identity the reference's fullwave driver passes to its
+   option parser (main/fullwave/main.c:13-19) */
+#define LOCAL_MODULE_NAME "Full-Wave analysis with HDDM"
+#define LOCAL_VERSION ADVFW_VERSION
+#define LOCAL_WORK WORK_HDDM_ANALYSIS
+#define LOCAL_FIELD FIELD_ELECTROMAGNETIC
+#define LOCAL_ANALYSIS ANALYSIS_FULL_WAVECURRENT
+#define LOCAL_N_ARGUMENT 0
+#define LOCAL_USAGE ""
+#include <time.h>
+
+extern COM_WLD_ID COM_ID;
+extern COM_GRP_ID COM_GID;
+extern int nstart;
+extern int nend;
+extern int nrepeat;
+extern HDDM_SW hddm_sw;
+extern WORK_TIMES work_times;
+extern double s_time;
+
+static int g_dump = 0;
+static char g_prefix[FILENAME_MAX];
+static PartMesh *g_pm = NULL;
+
+/* source edges owned per subdomain: (local edge id, value) */
+typedef struct {
+  int n;
+  int *edge;
+  double *re;
+  double *im;
+} SubSource;
+static SubSource *g_src = NULL;
+
+static double t_now(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+static double t_assemble = 0.0, t_first = 0.0, t_last = 0.0, t_iter_total = 0.0;
+static double t_iter_mark = -1.0;
+static int n_iter = 0;
+static FILE *f_aij = NULL, *f_fac = NULL;
+
+/* the reference's fullwave table entries this harness wraps */
+static void (*ref_make_TMP_AIJ)(DomMesh *, MTRL) = NULL;
+static void (*ref_solve_dom_1st)(DomMesh *, HDDM_Opt, SolvOpt, int (*)(AIJ_MAT *, SolvOpt, FILE *),
+                                 HDDM_DOM_VEC *, int (*)(TMP_AIJ, HDDM_DOM_VEC *), FILE *) = NULL;
+static void (*ref_iteration_s)(PartMesh *, HDDM_VEC *, HDDM_Opt, int (*)(HDDM_VEC *)) = NULL;
+static void (*ref_solve_dom_last)(DomMesh *, SolvOpt, int (*)(AIJ_MAT *, SolvOpt, FILE *), HDDM_DOM_VEC *,
+                                  FILE *) = NULL;
+
+static void w_i32(FILE *f, int v) { fwrite(&v, 4, 1, f); }
+
+static void harness_make_TMP_AIJ(DomMesh *dm, MTRL mtrl) {
+  double t0 = t_now();
+  ref_make_TMP_AIJ(dm, mtrl);
+  SubSource *s = &g_src[dm->domid];
+  for (int k = 0; k < s->n; k++) {
+    Complex *b = &dm->tmp_aij.tmp_b_c[s->edge[k]];
+    b->re += s->re[k];
+    b->im += s->im[k];
+  }
+  t_assemble += t_now() - t0;
+  if (g_dump >= 2 && f_aij) {
+    TMP_AIJ *a = &dm->tmp_aij;
+    w_i32(f_aij, a->nf);
+    for (int i = 0; i < a->nf; i++) {
+      w_i32(f_aij, a->tmp_ai[i]);
+      fwrite(a->tmp_aij[i], 4, a->tmp_ai[i], f_aij);
+      fwrite(a->tmp_vij_c[i], sizeof(Complex), a->tmp_ai[i], f_aij);
+    }
+    fwrite(a->tmp_b_c, sizeof(Complex), a->nf, f_aij);
+  }
+}
+
+static void harness_solve_dom_1st(DomMesh *dm, HDDM_Opt hddm_opt, SolvOpt solvopt,
+                                  int (*dom_solver)(AIJ_MAT *, SolvOpt, FILE *), HDDM_DOM_VEC *v,
+                                  int (*makePC)(TMP_AIJ, HDDM_DOM_VEC *), FILE *fp_log) {
+  double t0 = t_now();
+  ref_solve_dom_1st(dm, hddm_opt, solvopt, dom_solver, v, makePC, fp_log);
+  t_first += t_now() - t0;
+  if (g_dump >= 2 && f_fac) {
+    DMatrix *d = &dm->dmat;
+    w_i32(f_fac, d->ndim);
+    w_i32(f_fac, d->nlen);
+    fwrite(d->idx1, 4, d->ndim, f_fac);
+    fwrite(d->idx2, 4, d->ndim, f_fac);
+    fwrite(d->mat_dc, sizeof(double _Complex), d->nlen, f_fac);
+  }
+}
+
+static void harness_iteration_s(PartMesh *pm, HDDM_VEC *hv, HDDM_Opt hddm_opt, int (*setPC)(HDDM_VEC *)) {
+  ref_iteration_s(pm, hv, hddm_opt, setPC);
+  double t = t_now();
+  if (t_iter_mark >= 0.0) t_iter_total += t - t_iter_mark;
+  t_iter_mark = t;
+  n_iter++;
+}
+
+static void harness_solve_dom_last(DomMesh *dm, SolvOpt solvopt, int (*s)(AIJ_MAT *, SolvOpt, FILE *),
+                                   HDDM_DOM_VEC *v, FILE *fp_log) {
+  double t0 = t_now();
+  ref_solve_dom_last(dm, solvopt, s, v, fp_log);
+  t_last += t_now() - t0;
+}
+
+static void set_hddm_func_harness(HDDM_FUNC *f, OPTIONS options) {
+  set_hddm_func_fullwave(f, options);
+  ref_make_TMP_AIJ = f->make_TMP_AIJ;
+  ref_solve_dom_1st = f->solve_dom_1st;
+  ref_iteration_s = f->iteration_s;
+  ref_solve_dom_last = f->solve_dom_last;
+  f->make_TMP_AIJ = harness_make_TMP_AIJ;
+  f->solve_dom_1st = harness_solve_dom_1st;
+  f->iteration_s = harness_iteration_s;
+  f->solve_dom_last = harness_solve_dom_last;
+}
+
+/* global node id of each subdomain-local edge DOF */
+static int *edge_gnid(PartMesh *pm, DomMesh *dm) {
+  int *g = (int *)malloc(sizeof(int) * (dm->nmp > 0 ? dm->nmp : 1));
+  for (int e = 0; e < dm->nmp; e++) g[e] = pm->pnid2gnid[dm->snid2pnid[dm->mpid2snid[e]]];
+  return g;
+}
+
+static void load_sources(const char *dir, PartMesh *pm) {
+  char path[FILENAME_MAX];
+  snprintf(path, sizeof(path), "%s/source.txt", dir);
+  g_src = (SubSource *)calloc(pm->ndomain, sizeof(SubSource));
+  FILE *f = fopen(path, "r");
+  if (!f) return;
+  int nrhs = 0, n = 0;
+  if (fscanf(f, "%d", &nrhs) != 1 || nrhs < 1 || fscanf(f, "%d", &n) != 1) {
+    fclose(f);
+    return;
+  }
+  /* only the first right-hand side drives the reference run */
+  for (int k = 0; k < n; k++) {
+    int gnid;
+    double re, im;
+    if (fscanf(f, "%d %lf %lf", &gnid, &re, &im) != 3) break;
+    for (int d = 0; d < pm->ndomain; d++) {
+      DomMesh *dm = &pm->dm[d];
+      int *g = edge_gnid(pm, dm);
+      int found = -1;
+      for (int e = 0; e < dm->nmp; e++)
+        if (g[e] == gnid) {
+          found = e;
+          break;
+        }
+      free(g);
+      if (found >= 0) {
+        SubSource *s = &g_src[d];
+        s->edge = (int *)realloc(s->edge, sizeof(int) * (s->n + 1));
+        s->re = (double *)realloc(s->re, sizeof(double) * (s->n + 1));
+        s->im = (double *)realloc(s->im, sizeof(double) * (s->n + 1));
+        s->edge[s->n] = found;
+        s->re[s->n] = re;
+        s->im[s->n] = im;
+        s->n++;
+        break;
+      }
+    }
+  }
+  fclose(f);
+}
+
+static void dump_ints(PartMesh *pm) {
+  char path[FILENAME_MAX];
+  snprintf(path, sizeof(path), "%s.ints", g_prefix);
+  FILE *f = fopen(path, "wb");
+  if (!f) return;
+  w_i32(f, pm->ndomain);
+  w_i32(f, pm->infree);
+  w_i32(f, pm->outfree);
+  w_i32(f, pm->total_free);
+  for (int d = 0; d < pm->ndomain; d++) {
+    DomMesh *dm = &pm->dm[d];
+    w_i32(f, dm->nmp);
+    w_i32(f, dm->nap);
+    w_i32(f, dm->nel);
+    fwrite(dm->nop, 4, dm->nel * dm->nd_elem, f);
+    w_i32(f, dm->dbc_Axn0.nbc);
+    fwrite(dm->dbc_Axn0.ibc, 4, dm->dbc_Axn0.nbc, f);
+    w_i32(f, dm->ninbc);
+    for (int i = 0; i < dm->ninbc; i++) {
+      w_i32(f, dm->inbc[i].nfid);
+      w_i32(f, dm->inbc[i].ln_part);
+    }
+    int *g = edge_gnid(pm, dm);
+    fwrite(g, 4, dm->nmp, f);
+    free(g);
+  }
+  fclose(f);
+}
+
+static void dump_solution(PartMesh *pm) {
+  char path[FILENAME_MAX];
+  snprintf(path, sizeof(path), "%s.sol", g_prefix);
+  FILE *f = fopen(path, "wb");
+  if (!f) return;
+  w_i32(f, pm->ndomain);
+  for (int d = 0; d < pm->ndomain; d++) {
+    DomMesh *dm = &pm->dm[d];
+    w_i32(f, dm->nmp);
+    int *g = edge_gnid(pm, dm);
+    fwrite(g, 4, dm->nmp, f);
+    free(g);
+    fwrite(dm->x_c, sizeof(Complex), dm->nmp, f);
+  }
+  fclose(f);
+}
+
+int main(int argc, char **argv) {
+  OPTIONS options;
+  double t0 = t_now();
+  const char *model_dir = argc > 1 ? argv[argc - 1] : ".";
+  const char *out = getenv("FW_HARNESS_OUT");
+  const char *dump = getenv("FW_HARNESS_DUMP");
+  g_dump = dump ? atoi(dump) : 0;
+  if (out)
+    snprintf(g_prefix, sizeof(g_prefix), "%s", out);
+  else
+    snprintf(g_prefix, sizeof(g_prefix), "%s/ref", model_dir);
+
+  hddm_time_Init();
+  /* the solver selection main() hard-codes (main/fullwave/main.c:46-60) */
+  options.solvopt.solver_dom = SOLVER_LU;
+  options.solvopt.solver_pc = SOLVER_PC_ICC;
+  options.solvopt.solver_eps = 1.0e-09;
+  options.solvopt.solver_log = NO_NEED;
+  options.solvopt.coJo_sol = SOLVER_CGMETHOD;
+  options.solvopt.coJo_sol_pc = SOLVER_PC_ICC;
+  options.solvopt.coJo_sol_log = NO_NEED;
+  options.hddm_opt.hddm_solver = HDDM_COCG;
+  options.hddm_opt.hddm_pc = HDDM_PC_DIAG;
+  options.hddm_opt.hddm_log = NEED;
+  options.hddm_opt.coJo_hddm_sol = HDDM_CGMETHOD;
+  options.hddm_opt.coJo_hddm_pc = HDDM_PC_DIAG;
+  options.hddm_opt.coJo_hddm_log = NEED;
+  main_Init(argc, argv, &options);
+  if (make_outdata_directory(options.datasw) > 0) return 1;
+  if (make_calclog_directory(options.datasw) > 0) return 1;
+
+  /* hddm_Init (lib/hddm/make_PartMesh.c:58-117) in s-mode, calling
+     make_PartMesh_FW directly: make_PartMesh's material check
+     (make_MESH_check_flag_2nd, lib/fem/make_MESH.c:78-130) insists on an
+     antenna definition, and synthetic models drive the solve through an edge
+     current instead. */
+  {
+    char fname[FILENAME_MAX];
+    nstart = 0;
+    nend = COM_GID.nparent;
+    nrepeat = COM_GID.nparent;
+    g_pm = (PartMesh *)Malloc(sizeof(PartMesh), nrepeat);
+    for (int i = nstart, j = 0; i < nend; i++, j++) {
+      init_PartMesh(&g_pm[j], options);
+      make_modeldata_filename(fname, options.datasw, i);
+      read_modeldata_file(fname, &g_pm[j], options);
+    }
+    make_mtrldat_filename(fname, options.datasw, 0);
+    read_mtrldat_file(fname, &g_pm[0].mtrl, options);
+    for (int i = 1; i < COM_GID.nparent; i++) Copy_MTRL(&g_pm[i].mtrl, g_pm[0].mtrl);
+    make_PartMesh_FW(g_pm, options);
+  }
+  double t_init = t_now() - t0;
+  load_sources(model_dir, &g_pm[0]);
+  if (g_dump >= 1) dump_ints(&g_pm[0]);
+  if (g_dump >= 2) {
+    char path[FILENAME_MAX];
+    snprintf(path, sizeof(path), "%s.aij", g_prefix);
+    f_aij = fopen(path, "wb");
+    snprintf(path, sizeof(path), "%s.fac", g_prefix);
+    f_fac = fopen(path, "wb");
+  }
+
+  hddm_sw.t_loop = -2;
+  hddm_sw.antenna = -1;
+  double t1 = t_now();
+  hddm_solver_CS(g_pm, options, set_hddm_func_harness);
+  double t_solve = t_now() - t1;
+  if (f_aij) fclose(f_aij);
+  if (f_fac) fclose(f_fac);
+  dump_solution(&g_pm[0]);
+
+  char path[FILENAME_MAX];
+  snprintf(path, sizeof(path), "%s.json", g_prefix);
+  FILE *f = fopen(path, "w");
+  if (f) {
+    fprintf(f,
+            "{\"ndomain\": %d, \"total_free\": %d, \"iterations\": %d, \"t_init_s\": %.6f, "
+            "\"t_assemble_s\": %.6f, \"t_first_s\": %.6f, \"t_iter_total_s\": %.6f, "
+            "\"t_iter_count\": %d, \"t_last_s\": %.6f, \"t_solve_s\": %.6f}\n",
+            g_pm[0].ndomain, g_pm[0].total_free, n_iter, t_init, t_assemble, t_first, t_iter_total,
+            n_iter > 0 ? n_iter - 1 : 0, t_last, t_solve);
+    fclose(f);
+  }
+  return 0;
+}
