@@ -1,0 +1,130 @@
+"""ctypes binding of the C ABI in ``include/fwgpu.h`` (``libfwgpu.so``).
+
+The library is loaded from this package directory.  There is no fallback:
+if the shared library is missing the import of the solver fails loudly, and
+without a CUDA device every call that needs the GPU returns
+``FWGPU_ERR_CUDA``, which is raised as ``FwgpuError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfwgpu.so")
+
+OK = 0
+ERR_ARG = -1
+ERR_CUDA = -2
+ERR_STATE = -3
+ERR_NOT_CONVERGED = -4
+ERR_BREAKDOWN = -5
+ERR_NOMEM = -6
+ERR_MESH = -7
+
+PREC_FP64 = 0
+PREC_FP32_IR = 1
+
+c_i32 = ctypes.c_int32
+c_i64 = ctypes.c_int64
+c_dbl = ctypes.c_double
+P = ctypes.POINTER
+
+
+class FwMesh(ctypes.Structure):
+    _fields_ = [
+        ("n_vertices", c_i32), ("vertex_crd", P(c_dbl)),
+        ("n_tets", c_i32), ("tet_vertices", P(c_i32)), ("tet_edges", P(c_i32)), ("tet_flag", P(c_i32)),
+        ("n_edges", c_i32), ("pec_edge", P(ctypes.c_uint8)),
+        ("n_subdomains", c_i32), ("sub_of_tet", P(c_i32)),
+    ]
+
+
+class FwMaterial(ctypes.Structure):
+    _fields_ = [
+        ("n_eps", c_i32), ("eps_flag", P(c_i32)), ("eps", P(c_dbl)),
+        ("n_sigma", c_i32), ("sigma_flag", P(c_i32)), ("sigma", P(c_dbl)),
+        ("omega", c_dbl),
+    ]
+
+
+class FwSource(ctypes.Structure):
+    _fields_ = [("n_entries", c_i32), ("edge", P(c_i32)), ("value", P(c_dbl))]
+
+
+class FwOptions(ctypes.Structure):
+    _fields_ = [
+        ("hddm_eps", c_dbl), ("hddm_max_loop", c_i32), ("precision", c_i32), ("ir_max_steps", c_i32),
+        ("ir_tol", c_dbl), ("graph_iterations", c_i32), ("device", c_i32),
+    ]
+
+
+class FwSizes(ctypes.Structure):
+    _fields_ = [
+        ("n_subdomains", c_i32), ("total_free", c_i32), ("total_dofs", c_i64), ("total_interior", c_i64),
+        ("nlen_reference", c_i64), ("nlen_interior", c_i64), ("nnz_lower", c_i64),
+        ("nnz_interface_rows", c_i64), ("nnz_coupling", c_i64), ("nnz_interior", c_i64),
+        ("max_local_dofs", c_i32), ("max_interior", c_i32),
+    ]
+
+
+class FwResult(ctypes.Structure):
+    _fields_ = [
+        ("iterations", c_i32), ("converged", c_i32), ("initial_norm", c_dbl), ("final_resi", c_dbl),
+        ("final_resi_l2", c_dbl), ("t_setup_ms", c_dbl), ("t_iterate_ms", c_dbl), ("t_last_ms", c_dbl),
+    ]
+
+
+# every symbol the header declares, with its argument types
+SIGNATURES = {
+    "fwgpu_create": [P(FwMesh), P(FwMaterial), P(FwOptions), P(ctypes.c_void_p)],
+    "fwgpu_destroy": [ctypes.c_void_p],
+    "fwgpu_get_sizes": [ctypes.c_void_p, P(FwSizes)],
+    "fwgpu_last_error": [],
+    "fwgpu_abi_version": [],
+    "fwgpu_make_tmp_aij": [ctypes.c_void_p, P(FwSource)],
+    "fwgpu_solve_dom_1st": [ctypes.c_void_p],
+    "fwgpu_iteration_s_1st": [ctypes.c_void_p, P(c_i32)],
+    "fwgpu_iteration_s": [ctypes.c_void_p, P(c_i32)],
+    "fwgpu_solve_dom_last": [ctypes.c_void_p],
+    "fwgpu_hddm_solve": [ctypes.c_void_p, P(FwSource), P(FwResult)],
+    "fwgpu_hddm_resolve": [ctypes.c_void_p, P(FwSource), P(FwResult)],
+    "fwgpu_get_edge_solution": [ctypes.c_void_p, P(c_dbl)],
+    "fwgpu_get_history": [ctypes.c_void_p, P(c_dbl), c_i32, P(c_i32)],
+    "fwgpu_get_subdomain_maps": [ctypes.c_void_p, c_i32, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32),
+                                 P(c_i32), P(c_i32), P(c_i32), P(c_i32)],
+    "fwgpu_get_skyline_profile": [ctypes.c_void_p, c_i32, P(c_i32), P(c_i32), P(c_i32)],
+    "fwgpu_get_tmp_aij": [ctypes.c_void_p, c_i32, P(c_i32), P(c_i32), P(c_i32), P(c_dbl), P(c_dbl)],
+    "fwgpu_get_factor": [ctypes.c_void_p, c_i32, P(c_dbl)],
+}
+
+
+class FwgpuError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"fwgpu error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load ``libfwgpu.so`` (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with adventure_fullwave_b200.build.build()")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_char_p if name == "fwgpu_last_error" else ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def check(rc: int, allow=()) -> int:
+    if rc != OK and rc not in allow:
+        raise FwgpuError(rc, load().fwgpu_last_error().decode())
+    return rc

@@ -1,0 +1,774 @@
+// C ABI of the HDDM hot path (include/fwgpu.h): context, uploads and the
+// host orchestration of the device kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fw_internal.h"
+#include "fw_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error = "";
+
+int set_error(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define FW_CUDA(call)                                                                                \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess) {                                                                         \
+      return set_error(e_ == cudaErrorMemoryAllocation ? FWGPU_ERR_NOMEM : FWGPU_ERR_CUDA,           \
+                       std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+    }                                                                                                \
+  } while (0)
+
+}  // namespace
+
+struct fwgpu_context {
+  fw::Model m;
+  fw::Plan p;
+  fwgpu_options opts{};
+  cudaStream_t stream = nullptr;
+  std::vector<void *> allocs;
+  int stage = 0;  // 0 created, 1 assembled, 2 first solve, 3 interface iteration, 4 last step
+
+  // static device data
+  int32_t *d_tv = nullptr, *d_el_order = nullptr, *d_mesh_status = nullptr;
+  double *d_crd = nullptr, *d_el_eps = nullptr, *d_el_sigma = nullptr;
+  int64_t *d_cptr = nullptr, *d_contrib = nullptr;
+  double2 *d_aval = nullptr;
+  int32_t *d_row_ptr = nullptr, *d_col = nullptr, *d_idx1 = nullptr;
+  uint8_t *d_isbc = nullptr;
+  int64_t *d_dof_off = nullptr, *d_nnz_off = nullptr;
+  // envelope
+  std::vector<int32_t> h_idx1;
+  std::vector<int32_t> h_env_lo;
+  std::vector<int64_t> h_env_ptr;
+  int64_t nlen_int = 0;
+  int64_t nlen_ref = 0;
+  double2 *d_L64 = nullptr;
+  float2 *d_L32 = nullptr;
+  int32_t *d_env_lo = nullptr;
+  int64_t *d_env_ptr = nullptr;
+  // operators and right-hand sides
+  std::vector<double2> h_b_local;  // TMP_B per local DOF (concatenated)
+  double2 *d_cpl_val = nullptr, *d_ifr_val = nullptr, *d_aii_val = nullptr, *d_pcloc = nullptr;
+  double2 *d_fI = nullptr, *d_fG = nullptr;
+  int64_t *d_edge_src = nullptr;
+  double2 *d_xedge = nullptr;
+  fw::DevProblem dp{};
+  fw::CocgScalars *d_sc = nullptr;
+  fw::CocgScalars *h_sc = nullptr;  // pinned
+  double *d_hist = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_iters = 0;
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool factor_bad = false;
+
+  template <typename T>
+  int alloc(T **ptr, size_t count) {
+    *ptr = nullptr;
+    if (count == 0) count = 1;
+    void *raw = nullptr;
+    cudaError_t e = cudaMalloc(&raw, count * sizeof(T));
+    if (e != cudaSuccess)
+      return set_error(FWGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(raw);
+    *ptr = (T *)raw;
+    return FWGPU_OK;
+  }
+  template <typename T>
+  int upload(T **ptr, const std::vector<T> &v) {
+    int rc = alloc(ptr, v.size());
+    if (rc) return rc;
+    if (!v.empty()) FW_CUDA(cudaMemcpyAsync(*ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    return FWGPU_OK;
+  }
+  void release(void *ptr) {
+    if (!ptr) return;
+    auto it = std::find(allocs.begin(), allocs.end(), ptr);
+    if (it != allocs.end()) {
+      cudaFree(*it);
+      allocs.erase(it);
+    }
+  }
+};
+
+namespace {
+
+#define FW_TRY(expr)           \
+  do {                         \
+    int rc_ = (expr);          \
+    if (rc_ != FWGPU_OK) return rc_; \
+  } while (0)
+
+std::vector<int64_t> offsets_from_rel(const std::vector<int32_t> &rel_ptr, const std::vector<int64_t> &count_off,
+                                      int nsub) {
+  // rel_ptr holds (n_s + 1) relative entries per subdomain; returns the
+  // cumulative base of each subdomain's entry arrays
+  std::vector<int64_t> off(nsub + 1, 0);
+  for (int s = 0; s < nsub; s++) {
+    const int64_t n = count_off[s + 1] - count_off[s];
+    off[s + 1] = off[s] + rel_ptr[count_off[s] + s + n];
+  }
+  return off;
+}
+
+int resolve_material(fw::Model &m, const fwgpu_mesh *mesh, const fwgpu_material *mt) {
+  m.el_eps.assign(m.nt, 0.0);
+  m.el_sigma.assign(m.nt, 0.0);
+  // the reference searches the tables linearly and takes the first match
+  // (lib/fem/make_elem_em.c:98-109); absent flags leave eps = sigma = 0
+  for (int t = 0; t < m.nt; t++) {
+    const int f = mesh->tet_flag[t];
+    for (int i = 0; i < mt->n_eps; i++)
+      if (mt->eps_flag[i] == f) {
+        m.el_eps[t] = mt->eps[i];
+        break;
+      }
+    for (int i = 0; i < mt->n_sigma; i++)
+      if (mt->sigma_flag[i] == f) {
+        m.el_sigma[t] = mt->sigma[i];
+        break;
+      }
+  }
+  return FWGPU_OK;
+}
+
+int build_rhs(fwgpu_context *c, const fwgpu_source *src) {
+  const fw::Plan &p = c->p;
+  const int nsub = c->m.nsub;
+  std::vector<double2> fI(p.sub_int_off[nsub], make_double2(0.0, 0.0));
+  std::vector<double2> fG(p.sub_if_off[nsub], make_double2(0.0, 0.0));
+  c->h_b_local.assign(p.sub_dof_off[nsub], make_double2(0.0, 0.0));
+  if (src && src->n_entries > 0) {
+    if (!src->edge || !src->value) return set_error(FWGPU_ERR_ARG, "source without edges or values");
+    // owner subdomain and local DOF of every edge: the first subdomain holding it
+    std::vector<int32_t> owner(c->m.ne, -1), local(c->m.ne, -1);
+    for (int s = 0; s < nsub; s++) {
+      const fw::SubHost &h = p.subs[s];
+      for (int r = 0; r < h.nmp; r++) {
+        const int e = h.edge_gid[r];
+        if (owner[e] < 0) {
+          owner[e] = s;
+          local[e] = r;
+        }
+      }
+    }
+    for (int k = 0; k < src->n_entries; k++) {
+      const int e = src->edge[k];
+      if (e < 0 || e >= c->m.ne) return set_error(FWGPU_ERR_ARG, "source edge out of range");
+      const int s = owner[e], r = local[e];
+      if (s < 0) continue;
+      const double2 val = make_double2(src->value[2 * k], src->value[2 * k + 1]);
+      double2 &b = c->h_b_local[p.sub_dof_off[s] + r];
+      b.x += val.x;
+      b.y += val.y;
+      const fw::SubHost &h = p.subs[s];
+      if (h.cidx[r] >= 0) {
+        fI[p.sub_int_off[s] + h.cidx[r]] = b;
+      } else if (h.slot[r] >= 0) {
+        fG[p.sub_if_off[s] + h.slot[r]] = b;
+      }
+    }
+  }
+  if (!c->d_fI) {
+    FW_TRY(c->alloc(&c->d_fI, fI.size()));
+    FW_TRY(c->alloc(&c->d_fG, fG.size()));
+  }
+  if (!fI.empty())
+    FW_CUDA(cudaMemcpyAsync(c->d_fI, fI.data(), fI.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  if (!fG.empty())
+    FW_CUDA(cudaMemcpyAsync(c->d_fG, fG.data(), fG.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  c->dp.fI = c->d_fI;
+  c->dp.fG = c->d_fG;
+  return FWGPU_OK;
+}
+
+int read_status(fwgpu_context *c, int32_t *status) {
+  FW_CUDA(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(fw::CocgScalars), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  if (status) *status = c->h_sc->status;
+  return FWGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fwgpu_last_error(void) { return g_last_error.c_str(); }
+int fwgpu_abi_version(void) { return FWGPU_ABI_VERSION; }
+
+int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_options *opts, fwgpu_context **out) {
+  if (!mesh || !mt || !opts || !out) return set_error(FWGPU_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (mesh->n_vertices <= 0 || mesh->n_tets <= 0 || mesh->n_edges <= 0 || mesh->n_subdomains <= 0 ||
+      !mesh->vertex_crd || !mesh->tet_vertices || !mesh->tet_edges || !mesh->tet_flag || !mesh->pec_edge ||
+      !mesh->sub_of_tet)
+    return set_error(FWGPU_ERR_ARG, "incomplete mesh");
+  if (opts->precision != FWGPU_PREC_FP64 && opts->precision != FWGPU_PREC_FP32_IR)
+    return set_error(FWGPU_ERR_ARG, "unknown precision");
+  if (opts->hddm_max_loop < 0) return set_error(FWGPU_ERR_ARG, "negative hddm_max_loop");
+  for (int64_t k = 0; k < 4 * (int64_t)mesh->n_tets; k++)
+    if (mesh->tet_vertices[k] < 0 || mesh->tet_vertices[k] >= mesh->n_vertices)
+      return set_error(FWGPU_ERR_ARG, "tet_vertices out of range");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(FWGPU_ERR_CUDA, "no CUDA device");
+  if (opts->device < 0 || opts->device >= ndev) return set_error(FWGPU_ERR_ARG, "bad device ordinal");
+
+  fwgpu_context *c = new fwgpu_context();
+  c->opts = *opts;
+  if (c->opts.graph_iterations <= 0) c->opts.graph_iterations = 16;
+  if (c->opts.ir_max_steps <= 0) c->opts.ir_max_steps = 1;
+  fw::Model &m = c->m;
+  m.nv = mesh->n_vertices;
+  m.nt = mesh->n_tets;
+  m.ne = mesh->n_edges;
+  m.nsub = mesh->n_subdomains;
+  m.crd.assign(mesh->vertex_crd, mesh->vertex_crd + 3 * (int64_t)m.nv);
+  m.tv.assign(mesh->tet_vertices, mesh->tet_vertices + 4 * (int64_t)m.nt);
+  m.te.assign(mesh->tet_edges, mesh->tet_edges + 6 * (int64_t)m.nt);
+  m.flag.assign(mesh->tet_flag, mesh->tet_flag + m.nt);
+  m.sub_of_tet.assign(mesh->sub_of_tet, mesh->sub_of_tet + m.nt);
+  m.pec.assign(mesh->pec_edge, mesh->pec_edge + m.ne);
+  m.omega = mt->omega;
+  resolve_material(m, mesh, mt);
+  std::string err = fw::build_plan(m, c->p);
+  if (!err.empty()) {
+    delete c;
+    return set_error(FWGPU_ERR_ARG, err);
+  }
+  cudaError_t e = cudaSetDevice(opts->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return set_error(FWGPU_ERR_CUDA, std::string("device setup: ") + cudaGetErrorString(e));
+  }
+  for (auto &ev : c->ev) cudaEventCreate(&ev);
+  *out = c;
+
+  const fw::Plan &p = c->p;
+  const int nsub = m.nsub;
+  FW_TRY(c->upload(&c->d_crd, m.crd));
+  FW_TRY(c->upload(&c->d_tv, m.tv));
+  FW_TRY(c->upload(&c->d_el_order, p.el_order));
+  FW_TRY(c->upload(&c->d_el_eps, m.el_eps));
+  FW_TRY(c->upload(&c->d_el_sigma, m.el_sigma));
+  FW_TRY(c->upload(&c->d_cptr, p.contrib_ptr));
+  FW_TRY(c->upload(&c->d_contrib, p.contrib));
+  FW_TRY(c->upload(&c->d_row_ptr, p.csr_row_ptr));
+  FW_TRY(c->upload(&c->d_col, p.csr_col));
+  FW_TRY(c->upload(&c->d_isbc, p.isbc));
+  FW_TRY(c->upload(&c->d_dof_off, p.sub_dof_off));
+  FW_TRY(c->upload(&c->d_nnz_off, p.sub_nnz_off));
+  FW_TRY(c->alloc(&c->d_mesh_status, 4));
+  FW_CUDA(cudaMemsetAsync(c->d_mesh_status, 0, 4 * sizeof(int32_t), c->stream));
+
+  // subdomains largest first (by interior DOFs, then local DOFs)
+  std::vector<int32_t> order(nsub);
+  for (int s = 0; s < nsub; s++) order[s] = s;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const fw::SubHost &x = p.subs[a], &y = p.subs[b];
+    return x.nI != y.nI ? x.nI > y.nI : x.nmp > y.nmp;
+  });
+  fw::DevProblem &dp = c->dp;
+  dp.nsub = nsub;
+  dp.nfree = p.total_free;
+  int32_t *d_order = nullptr;
+  int64_t *d_int_off = nullptr, *d_if_off = nullptr;
+  FW_TRY(c->upload(&d_order, order));
+  FW_TRY(c->upload(&d_int_off, p.sub_int_off));
+  FW_TRY(c->upload(&d_if_off, p.sub_if_off));
+  dp.sub_order = d_order;
+  dp.int_off = d_int_off;
+  dp.if_off = d_if_off;
+  // operator structures
+  auto cpl_off = offsets_from_rel(p.cpl_ptr, p.sub_int_off, nsub);
+  auto ifr_off = offsets_from_rel(p.ifr_ptr, p.sub_if_off, nsub);
+  auto aii_off = offsets_from_rel(p.aii_ptr, p.sub_int_off, nsub);
+  int32_t *ip = nullptr;
+  int64_t *lp = nullptr;
+  FW_TRY(c->upload(&ip, p.cpl_ptr));
+  dp.cpl_ptr = ip;
+  FW_TRY(c->upload(&lp, cpl_off));
+  dp.cpl_off = lp;
+  FW_TRY(c->upload(&ip, p.cpl_col));
+  dp.cpl_col = ip;
+  FW_TRY(c->upload(&ip, p.ifr_ptr));
+  dp.ifr_ptr = ip;
+  FW_TRY(c->upload(&lp, ifr_off));
+  dp.ifr_off = lp;
+  FW_TRY(c->upload(&ip, p.ifr_col));
+  dp.ifr_col = ip;
+  FW_TRY(c->upload(&ip, p.aii_ptr));
+  dp.aii_ptr = ip;
+  FW_TRY(c->upload(&lp, aii_off));
+  dp.aii_off = lp;
+  FW_TRY(c->upload(&ip, p.aii_col));
+  dp.aii_col = ip;
+  FW_TRY(c->upload(&ip, p.if_ln));
+  dp.if_ln = ip;
+  FW_TRY(c->upload(&ip, p.gq_ptr));
+  dp.gq_ptr = ip;
+  FW_TRY(c->upload(&lp, p.gq_slot));
+  dp.gq_slot = lp;
+  FW_TRY(c->alloc(&c->d_cpl_val, p.cpl_src.size()));
+  FW_TRY(c->alloc(&c->d_ifr_val, p.ifr_src.size()));
+  FW_TRY(c->alloc(&c->d_pcloc, p.if_diag_src.size()));
+  dp.cpl_val = c->d_cpl_val;
+  dp.ifr_val = c->d_ifr_val;
+  if (opts->precision == FWGPU_PREC_FP32_IR) {
+    FW_TRY(c->alloc(&c->d_aii_val, p.aii_src.size()));
+    dp.aii_val = c->d_aii_val;
+  }
+  const int64_t nI_tot = p.sub_int_off[nsub], nG_tot = p.sub_if_off[nsub];
+  FW_TRY(c->alloc(&dp.Y, nI_tot));
+  FW_TRY(c->alloc(&dp.V, nG_tot));
+  FW_TRY(c->alloc(&dp.qloc, nG_tot));
+  if (opts->precision == FWGPU_PREC_FP32_IR) {
+    FW_TRY(c->alloc(&dp.B, nI_tot));
+    FW_TRY(c->alloc(&dp.Y32, nI_tot));
+  }
+  const int64_t nf = std::max<int64_t>(1, p.total_free);
+  FW_TRY(c->alloc(&dp.P, nf));
+  FW_TRY(c->alloc(&dp.Q, nf));
+  FW_TRY(c->alloc(&dp.R, nf));
+  FW_TRY(c->alloc(&dp.Z, nf));
+  FW_TRY(c->alloc(&dp.U, nf));
+  FW_TRY(c->alloc(&dp.PC, nf));
+  int nb = (int)std::min<int64_t>((p.total_free + 255) / 256, 1184);
+  if (nb < 1) nb = 1;
+  dp.n_part_blocks = nb;
+  FW_TRY(c->alloc(&dp.part, 8 * (size_t)nb));
+  FW_TRY(c->alloc(&c->d_sc, 1));
+  dp.sc = c->d_sc;
+  FW_CUDA(cudaMallocHost(&c->h_sc, sizeof(fw::CocgScalars)));
+  FW_TRY(c->alloc(&c->d_hist, (size_t)std::max(1, opts->hddm_max_loop) + 2));
+  dp.hist = c->d_hist;
+  dp.ir_steps = c->opts.ir_max_steps;
+  dp.ir_tol = c->opts.ir_tol;
+  // per-edge solution source: the first subdomain holding each edge
+  std::vector<int64_t> esrc(m.ne, -1);
+  std::vector<uint8_t> seen(m.ne, 0);
+  for (int s = 0; s < nsub; s++) {
+    const fw::SubHost &h = p.subs[s];
+    for (int r = 0; r < h.nmp; r++) {
+      const int e = h.edge_gid[r];
+      if (seen[e]) continue;
+      seen[e] = 1;
+      if (h.cidx[r] >= 0)
+        esrc[e] = p.sub_int_off[s] + h.cidx[r];
+      else if (h.slot[r] >= 0)
+        esrc[e] = -(p.sub_if_off[s] + h.slot[r]) - 2;
+      else
+        esrc[e] = -1;
+    }
+  }
+  FW_TRY(c->upload(&c->d_edge_src, esrc));
+  FW_TRY(c->alloc(&c->d_xedge, m.ne));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  return FWGPU_OK;
+}
+
+int fwgpu_destroy(fwgpu_context *c) {
+  if (!c) return FWGPU_OK;
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->h_sc) cudaFreeHost(c->h_sc);
+  for (auto &ev : c->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return FWGPU_OK;
+}
+
+int fwgpu_get_sizes(const fwgpu_context *c, fwgpu_sizes *sz) {
+  if (!c || !sz) return set_error(FWGPU_ERR_ARG, "null argument");
+  const fw::Plan &p = c->p;
+  const int nsub = c->m.nsub;
+  sz->n_subdomains = nsub;
+  sz->total_free = p.total_free;
+  sz->total_dofs = p.sub_dof_off[nsub];
+  sz->total_interior = p.sub_int_off[nsub];
+  sz->nlen_reference = c->nlen_ref;
+  sz->nlen_interior = c->nlen_int;
+  sz->nnz_lower = p.nnz_total;
+  sz->nnz_interface_rows = (int64_t)p.ifr_src.size();
+  sz->nnz_coupling = (int64_t)p.cpl_src.size();
+  sz->nnz_interior = (int64_t)p.aii_src.size();
+  sz->max_local_dofs = p.max_local;
+  sz->max_interior = p.max_interior;
+  return FWGPU_OK;
+}
+
+int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  const fw::Plan &p = c->p;
+  FW_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  double *d_elmat = nullptr;
+  FW_TRY(c->alloc(&d_elmat, (size_t)c->m.nt * 72));
+  fw::launch_element_matrices(c->m.nt, c->d_el_order, c->d_tv, c->d_crd, c->d_el_eps, c->d_el_sigma, c->m.omega,
+                              d_elmat, c->d_mesh_status, c->stream);
+  if (!c->d_aval) FW_TRY(c->alloc(&c->d_aval, p.nnz_total));
+  fw::launch_gather_values(p.nnz_total, c->d_cptr, c->d_contrib, (const double2 *)d_elmat, c->d_aval, c->stream);
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  c->release(d_elmat);
+  int32_t mesh_status = 0;
+  FW_CUDA(cudaMemcpy(&mesh_status, c->d_mesh_status, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (mesh_status) return set_error(FWGPU_ERR_MESH, "non-positive element volume or degenerate edge");
+  FW_TRY(build_rhs(c, src));
+  // operators gathered from the assembled values
+  {
+    int64_t *tmp = nullptr;
+    FW_TRY(c->upload(&tmp, p.cpl_src));
+    fw::launch_gather_ops((int64_t)p.cpl_src.size(), tmp, c->d_aval, c->d_cpl_val, c->stream);
+    FW_CUDA(cudaStreamSynchronize(c->stream));
+    c->release(tmp);
+    FW_TRY(c->upload(&tmp, p.ifr_src));
+    fw::launch_gather_ops((int64_t)p.ifr_src.size(), tmp, c->d_aval, c->d_ifr_val, c->stream);
+    FW_CUDA(cudaStreamSynchronize(c->stream));
+    c->release(tmp);
+    if (c->d_aii_val) {
+      FW_TRY(c->upload(&tmp, p.aii_src));
+      fw::launch_gather_ops((int64_t)p.aii_src.size(), tmp, c->d_aval, c->d_aii_val, c->stream);
+      FW_CUDA(cudaStreamSynchronize(c->stream));
+      c->release(tmp);
+    }
+    FW_TRY(c->upload(&tmp, p.if_diag_src));
+    fw::launch_diag_pc((int64_t)p.if_diag_src.size(), tmp, c->d_aval, c->d_pcloc, c->stream);
+    FW_CUDA(cudaStreamSynchronize(c->stream));
+    c->release(tmp);
+  }
+  FW_CUDA(cudaGetLastError());
+  c->stage = 1;
+  return FWGPU_OK;
+}
+
+int fwgpu_solve_dom_1st(fwgpu_context *c) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->stage < 1) return set_error(FWGPU_ERR_STATE, "solve_dom_1st before make_tmp_aij");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  const fw::Plan &p = c->p;
+  const int nsub = c->m.nsub;
+  const int64_t ndof = p.sub_dof_off[nsub];
+  if (!c->d_L64) {
+    // skyline profile on the device, envelope layout on the host
+    FW_TRY(c->alloc(&c->d_idx1, ndof));
+    fw::launch_profile(nsub, c->d_dof_off, c->d_nnz_off, c->d_row_ptr, c->d_col, c->d_aval, c->d_isbc, c->d_idx1,
+                       c->stream);
+    c->h_idx1.resize(ndof);
+    FW_CUDA(cudaMemcpyAsync(c->h_idx1.data(), c->d_idx1, ndof * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    FW_CUDA(cudaStreamSynchronize(c->stream));
+    const int64_t nI_tot = p.sub_int_off[nsub];
+    c->h_env_lo.assign(nI_tot, 0);
+    c->h_env_ptr.assign(nI_tot, 0);
+    std::vector<int64_t> dst(p.nnz_total, -1);
+    int64_t pos = 0, nref = 0;
+    for (int s = 0; s < nsub; s++) {
+      const fw::SubHost &h = p.subs[s];
+      const int32_t *idx1 = c->h_idx1.data() + p.sub_dof_off[s];
+      // reference skyline length (advlas_skyline.c:20-24)
+      int64_t idx2 = 0;
+      for (int i = 1; i < h.nmp; i++) idx2 += i - idx1[i];
+      nref += idx2 + h.nmp;
+      const int64_t io = p.sub_int_off[s];
+      for (int r = 0; r < h.nmp; r++) {
+        const int cI = h.cidx[r];
+        if (cI < 0) continue;
+        const int lo = h.cidx[idx1[r]];
+        c->h_env_lo[io + cI] = lo;
+        c->h_env_ptr[io + cI] = pos;
+        pos += cI - lo + 1;
+      }
+      const int64_t z0 = p.sub_nnz_off[s];
+      for (int r = 0; r < h.nmp; r++) {
+        const int cI = h.cidx[r];
+        if (cI < 0) continue;
+        const int lo = c->h_env_lo[io + cI];
+        for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++) {
+          const int j = h.col[q];
+          const int cj = h.cidx[j];
+          if (cj < 0 || cj < lo) continue;
+          dst[z0 + q] = c->h_env_ptr[io + cI] + (cj - lo);
+        }
+      }
+    }
+    c->nlen_int = pos;
+    c->nlen_ref = nref;
+    FW_TRY(c->upload(&c->d_env_lo, c->h_env_lo));
+    FW_TRY(c->upload(&c->d_env_ptr, c->h_env_ptr));
+    int64_t *d_dst = nullptr;
+    FW_TRY(c->upload(&d_dst, dst));
+    FW_TRY(c->alloc(&c->d_L64, pos));
+    FW_CUDA(cudaMemsetAsync(c->d_L64, 0, std::max<int64_t>(1, pos) * sizeof(double2), c->stream));
+    fw::launch_scatter_envelope(p.nnz_total, d_dst, c->d_aval, c->d_L64, c->stream);
+    FW_CUDA(cudaStreamSynchronize(c->stream));
+    c->release(d_dst);
+    c->dp.env_lo = c->d_env_lo;
+    c->dp.env_ptr = c->d_env_ptr;
+    c->dp.L64 = c->d_L64;
+    // factor
+    FW_CUDA(cudaMemsetAsync(c->d_mesh_status + 1, 0, sizeof(int32_t), c->stream));
+    fw::launch_factor(c->dp, c->dp.int_off, c->d_env_lo, c->d_env_ptr, c->d_L64, c->d_mesh_status + 1, c->stream);
+    FW_CUDA(cudaGetLastError());
+    if (c->opts.precision == FWGPU_PREC_FP32_IR) {
+      FW_TRY(c->alloc(&c->d_L32, pos));
+      fw::launch_to_fp32(pos, c->d_L64, c->d_L32, c->stream);
+      c->dp.L32 = c->d_L32;
+      c->dp.L64 = nullptr;
+    }
+    int32_t fstat = 0;
+    FW_CUDA(cudaMemcpyAsync(&fstat, c->d_mesh_status + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    FW_CUDA(cudaStreamSynchronize(c->stream));
+    c->factor_bad = fstat != 0;
+    if (c->opts.precision == FWGPU_PREC_FP32_IR) {
+      // the FP64 factor is only kept for introspection of small problems
+      if (pos > (int64_t)64 * 1024 * 1024) {
+        c->release(c->d_L64);
+        c->d_L64 = nullptr;
+      }
+    }
+  }
+  fw::launch_subsolve(c->dp, fw::kModeFirst, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
+  FW_CUDA(cudaGetLastError());
+  c->stage = 2;
+  if (c->factor_bad) return set_error(FWGPU_ERR_BREAKDOWN, "zero or non-finite pivot in a subdomain factor");
+  return FWGPU_OK;
+}
+
+int fwgpu_iteration_s_1st(fwgpu_context *c, int32_t *status) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "iteration_s_1st before solve_dom_1st");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  fw::launch_set_status(c->d_sc, c->opts.hddm_eps, c->opts.hddm_max_loop, c->stream);
+  fw::launch_cocg_first(c->dp, c->d_pcloc, c->stream);
+  FW_CUDA(cudaGetLastError());
+  FW_TRY(read_status(c, status));
+  c->stage = 3;
+  return FWGPU_OK;
+}
+
+int fwgpu_iteration_s(fwgpu_context *c, int32_t *status) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "iteration_s outside the interface loop");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  fw::launch_cocg_iteration(c->dp, c->stream);
+  FW_CUDA(cudaGetLastError());
+  FW_TRY(read_status(c, status));
+  return FWGPU_OK;
+}
+
+int fwgpu_solve_dom_last(fwgpu_context *c) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->stage < 3) return set_error(FWGPU_ERR_STATE, "solve_dom_last before the interface loop");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  fw::launch_subsolve(c->dp, fw::kModeLast, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
+  fw::launch_edge_solution(c->m.ne, c->d_edge_src, c->dp.Y, c->dp.V, c->d_xedge, c->stream);
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  c->stage = 4;
+  return FWGPU_OK;
+}
+
+static int run_loop(fwgpu_context *c, fwgpu_result *res) {
+  // interface iterations captured in a CUDA graph, graph_iterations per launch
+  if (!c->graph) {
+    cudaGraph_t g;
+    FW_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < c->opts.graph_iterations; k++) fw::launch_cocg_iteration(c->dp, c->stream);
+    FW_CUDA(cudaStreamEndCapture(c->stream, &g));
+    FW_CUDA(cudaGraphInstantiate(&c->graph, g, 0));
+    cudaGraphDestroy(g);
+    c->graph_iters = c->opts.graph_iterations;
+  }
+  int32_t st = c->h_sc->status;
+  while (st == 0) {
+    FW_CUDA(cudaGraphLaunch(c->graph, c->stream));
+    FW_TRY(read_status(c, &st));
+  }
+  (void)res;
+  return FWGPU_OK;
+}
+
+static int fill_result(fwgpu_context *c, fwgpu_result *res) {
+  FW_TRY(read_status(c, nullptr));
+  const fw::CocgScalars &sc = *c->h_sc;
+  if (res) {
+    res->iterations = sc.loop - 1;
+    res->converged = sc.converged;
+    res->initial_norm = sc.norm0;
+    res->final_resi = sc.resi;
+    res->final_resi_l2 = sc.resi_l2;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    res->t_setup_ms = ms;
+    cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]);
+    res->t_iterate_ms = ms;
+    cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
+    res->t_last_ms = ms;
+  }
+  return sc.converged ? FWGPU_OK : set_error(FWGPU_ERR_NOT_CONVERGED, "hddm_max_loop reached before hddm_eps");
+}
+
+int fwgpu_hddm_solve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *res) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->opts.hddm_max_loop == 0) return set_error(FWGPU_ERR_ARG, "hddm_max_loop is 0");
+  FW_TRY(fwgpu_make_tmp_aij(c, src));
+  FW_TRY(fwgpu_solve_dom_1st(c));
+  int32_t st = 0;
+  FW_TRY(fwgpu_iteration_s_1st(c, &st));
+  FW_CUDA(cudaEventRecord(c->ev[1], c->stream));
+  FW_TRY(run_loop(c, res));
+  FW_CUDA(cudaEventRecord(c->ev[2], c->stream));
+  FW_TRY(fwgpu_solve_dom_last(c));
+  FW_CUDA(cudaEventRecord(c->ev[3], c->stream));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  return fill_result(c, res);
+}
+
+int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *res) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "resolve before the factors exist");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  FW_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  FW_TRY(build_rhs(c, src));
+  fw::launch_subsolve(c->dp, fw::kModeFirst, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
+  int32_t st = 0;
+  FW_TRY(fwgpu_iteration_s_1st(c, &st));
+  FW_CUDA(cudaEventRecord(c->ev[1], c->stream));
+  FW_TRY(run_loop(c, res));
+  FW_CUDA(cudaEventRecord(c->ev[2], c->stream));
+  FW_TRY(fwgpu_solve_dom_last(c));
+  FW_CUDA(cudaEventRecord(c->ev[3], c->stream));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  return fill_result(c, res);
+}
+
+int fwgpu_get_edge_solution(fwgpu_context *c, double *x) {
+  if (!c || !x) return set_error(FWGPU_ERR_ARG, "null argument");
+  if (c->stage < 4) return set_error(FWGPU_ERR_STATE, "no solution yet");
+  FW_CUDA(cudaMemcpy(x, c->d_xedge, (size_t)c->m.ne * sizeof(double2), cudaMemcpyDeviceToHost));
+  return FWGPU_OK;
+}
+
+int fwgpu_get_history(fwgpu_context *c, double *resi, int32_t max_n, int32_t *n_out) {
+  if (!c || !n_out) return set_error(FWGPU_ERR_ARG, "null argument");
+  FW_TRY(read_status(c, nullptr));
+  int n = std::max(0, c->h_sc->loop - 1);
+  n = std::min(n, std::max(1, c->opts.hddm_max_loop));
+  *n_out = n;
+  if (resi && max_n > 0) FW_CUDA(cudaMemcpy(resi, c->d_hist, std::min(n, max_n) * sizeof(double), cudaMemcpyDeviceToHost));
+  return FWGPU_OK;
+}
+
+int fwgpu_get_subdomain_maps(const fwgpu_context *c, int32_t s, int32_t *nel, int32_t *nmp, int32_t *nbc,
+                             int32_t *ninbc, int32_t *nop, int32_t *ibc, int32_t *inbc_nfid, int32_t *inbc_ln_part,
+                             int32_t *edge_gid) {
+  if (!c || s < 0 || s >= c->m.nsub) return set_error(FWGPU_ERR_ARG, "bad subdomain");
+  const fw::SubHost &h = c->p.subs[s];
+  if (nel) *nel = (int32_t)h.els.size();
+  if (nmp) *nmp = h.nmp;
+  if (nbc) *nbc = (int32_t)h.ibc.size();
+  if (ninbc) *ninbc = h.nG;
+  if (nop) std::copy(h.nop.begin(), h.nop.end(), nop);
+  if (ibc) std::copy(h.ibc.begin(), h.ibc.end(), ibc);
+  if (inbc_nfid) std::copy(h.inbc_nfid.begin(), h.inbc_nfid.end(), inbc_nfid);
+  if (inbc_ln_part) std::copy(h.inbc_ln.begin(), h.inbc_ln.end(), inbc_ln_part);
+  if (edge_gid) std::copy(h.edge_gid.begin(), h.edge_gid.end(), edge_gid);
+  return FWGPU_OK;
+}
+
+int fwgpu_get_skyline_profile(fwgpu_context *c, int32_t s, int32_t *idx1, int32_t *idx2, int32_t *nlen) {
+  if (!c || s < 0 || s >= c->m.nsub) return set_error(FWGPU_ERR_ARG, "bad subdomain");
+  if (c->h_idx1.empty()) return set_error(FWGPU_ERR_STATE, "no profile yet");
+  const fw::SubHost &h = c->p.subs[s];
+  const int32_t *src = c->h_idx1.data() + c->p.sub_dof_off[s];
+  int32_t acc = 0;
+  for (int i = 0; i < h.nmp; i++) {
+    if (idx1) idx1[i] = src[i];
+    if (i > 0) acc += i - src[i];
+    if (idx2) idx2[i] = acc;
+  }
+  if (nlen) *nlen = acc + h.nmp;
+  return FWGPU_OK;
+}
+
+int fwgpu_get_tmp_aij(fwgpu_context *c, int32_t s, int32_t *nnz, int32_t *row_ptr, int32_t *col, double *val,
+                      double *b) {
+  if (!c || s < 0 || s >= c->m.nsub || !nnz) return set_error(FWGPU_ERR_ARG, "bad argument");
+  if (c->stage < 1) return set_error(FWGPU_ERR_STATE, "not assembled");
+  const fw::Plan &p = c->p;
+  const fw::SubHost &h = p.subs[s];
+  const int64_t z0 = p.sub_nnz_off[s];
+  const int64_t n = p.sub_nnz_off[s + 1] - z0;
+  std::vector<double2> v(n);
+  FW_CUDA(cudaMemcpy(v.data(), c->d_aval + z0, n * sizeof(double2), cudaMemcpyDeviceToHost));
+  // rows after DeleteZero (aij_matrix_func.h:342-391)
+  int32_t k = 0;
+  if (row_ptr) row_ptr[0] = 0;
+  for (int r = 0; r < h.nmp; r++) {
+    for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++) {
+      if (v[q].x == 0.0 && v[q].y == 0.0) continue;
+      if (col) col[k] = h.col[q];
+      if (val) {
+        val[2 * k] = v[q].x;
+        val[2 * k + 1] = v[q].y;
+      }
+      k++;
+    }
+    if (row_ptr) row_ptr[r + 1] = k;
+  }
+  *nnz = k;
+  if (b) {
+    for (int r = 0; r < h.nmp; r++) {
+      const double2 bb = c->h_b_local[p.sub_dof_off[s] + r];
+      b[2 * r] = bb.x;
+      b[2 * r + 1] = bb.y;
+    }
+  }
+  return FWGPU_OK;
+}
+
+int fwgpu_get_factor(fwgpu_context *c, int32_t s, double *mat) {
+  if (!c || s < 0 || s >= c->m.nsub || !mat) return set_error(FWGPU_ERR_ARG, "bad argument");
+  if (c->stage < 2 || !c->d_L64) return set_error(FWGPU_ERR_STATE, "no FP64 factor");
+  const fw::Plan &p = c->p;
+  const fw::SubHost &h = p.subs[s];
+  const int64_t io = p.sub_int_off[s];
+  const int64_t b0 = h.nI > 0 ? c->h_env_ptr[io] : 0;
+  const int64_t b1 = h.nI > 0 ? c->h_env_ptr[io + h.nI - 1] + (h.nI - 1 - c->h_env_lo[io + h.nI - 1]) + 1 : 0;
+  std::vector<double2> L(b1 - b0);
+  if (b1 > b0) FW_CUDA(cudaMemcpy(L.data(), c->d_L64 + b0, (b1 - b0) * sizeof(double2), cudaMemcpyDeviceToHost));
+  const int32_t *idx1 = c->h_idx1.data() + p.sub_dof_off[s];
+  int64_t idx2 = 0;
+  for (int i = 0; i < h.nmp; i++) {
+    if (i > 0) idx2 += i - idx1[i];
+    for (int j = idx1[i]; j <= i; j++) {
+      double2 val = make_double2(0.0, 0.0);
+      if (h.cidx[i] < 0) {
+        if (j == i) val = make_double2(1.0, 0.0);
+      } else if (h.cidx[j] >= 0) {
+        const int cI = h.cidx[i];
+        val = L[c->h_env_ptr[io + cI] - b0 + (h.cidx[j] - c->h_env_lo[io + cI])];
+      }
+      mat[2 * (idx2 + j)] = val.x;
+      mat[2 * (idx2 + j) + 1] = val.y;
+    }
+  }
+  return FWGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,103 @@
+// Internal host-side data structures of the HDDM hot path.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fwgpu.h"
+
+namespace fw {
+
+// Element edge table of the reference (lib/fem/tetrahedral.h:19-24):
+// slot i joins vertices kTetN[i][0] and kTetN[i][1]; kTetN[i][2..3] is the
+// opposite edge.
+constexpr int kTetN[6][4] = {{0, 1, 2, 3}, {0, 2, 3, 1}, {0, 3, 1, 2}, {1, 2, 0, 3}, {1, 3, 2, 0}, {2, 3, 0, 1}};
+// File order of the 6 mid-nodes is 01,02,03,12,23,13; the reference swaps
+// node slots 8 and 9 (lib/fem/make_MESH.c:573-584), so element slot i reads
+// file mid-node kFileSlot[i].
+constexpr int kFileSlot[6] = {0, 1, 2, 3, 5, 4};
+
+// Per-subdomain integer data, the state make_PartMesh_FW leaves in DomMesh.
+struct SubHost {
+  std::vector<int32_t> els;       // global element ids, ascending
+  int32_t nap = 0;                // local vertices
+  int32_t nmp = 0;                // local edge DOFs
+  std::vector<int32_t> nop;       // 10*nel: 4 local vertex ids, 6 local edge ids (tet_n order)
+  std::vector<int32_t> edge_gid;  // nmp: global edge id of each local edge DOF
+  std::vector<int32_t> ibc;       // Dirichlet list: sorted PEC edge ids then interface nfids
+  int32_t npec = 0;
+  std::vector<int32_t> inbc_nfid; // sorted
+  std::vector<int32_t> inbc_ln;   // global interface id of each inbc entry
+  std::vector<uint8_t> isbc;      // nmp
+  std::vector<int32_t> cidx;      // nmp: interior (compressed) index, -1 for Dirichlet DOFs
+  std::vector<int32_t> slot;      // nmp: interface slot (position in inbc), -1 otherwise
+  int32_t nI = 0;                 // interior DOFs
+  int32_t nG = 0;                 // interface DOFs
+  // structural lower-triangle rows (sorted columns), local DOF ids
+  std::vector<int32_t> row_ptr;   // nmp+1
+  std::vector<int32_t> col;       // nnz
+};
+
+struct Model {
+  int32_t nv = 0, nt = 0, ne = 0, nsub = 0;
+  std::vector<double> crd;
+  std::vector<int32_t> tv, te, flag, sub_of_tet;
+  std::vector<uint8_t> pec;
+  // material resolved per element (the reference's first-match linear search
+  // over the flag tables, lib/fem/make_elem_em.c:98-109)
+  std::vector<double> el_eps, el_sigma;
+  double omega = 0.0;
+};
+
+// Host plan: integer maps and index lists for the device gathers.
+struct Plan {
+  std::vector<SubHost> subs;
+  int32_t total_free = 0;            // interface DOFs
+  std::vector<int32_t> iface_gid;    // global edge id of each interface DOF
+  std::vector<int32_t> iface_owner_sub;
+  // concatenated over subdomains (sub-major, elements in sub order)
+  std::vector<int32_t> el_order;     // global element id of each element slot
+  std::vector<int64_t> sub_el_off;   // nsub+1
+  std::vector<int64_t> sub_dof_off;  // nsub+1, offsets of local DOF arrays
+  std::vector<int64_t> sub_nnz_off;  // nsub+1, offsets of lower CSR entries
+  std::vector<int64_t> sub_int_off;  // nsub+1, offsets of interior arrays
+  std::vector<int64_t> sub_if_off;   // nsub+1, offsets of interface slot arrays
+  // lower CSR (local rows, concatenated), row_ptr relative to sub_nnz_off
+  std::vector<int32_t> csr_row_ptr;  // sum(nmp+1)
+  std::vector<int32_t> csr_col;      // local col
+  std::vector<int64_t> contrib_ptr;  // nnz_total+1
+  std::vector<int64_t> contrib;      // element-slot*36 + (i*6+j)
+  std::vector<uint8_t> isbc;         // sum(nmp)
+  // per-iteration operators (positions into the global lower-CSR value array)
+  // coupling: interior row c -> interface slots   (b_I = -A_IG v)
+  std::vector<int32_t> cpl_ptr;      // sum(nI+1), relative
+  std::vector<int32_t> cpl_col;      // interface slot
+  std::vector<int64_t> cpl_src;      // lower-CSR position
+  // interface rows: slot k -> (interior c) or (interface slot)
+  std::vector<int32_t> ifr_ptr;      // sum(nG+1), relative
+  std::vector<int32_t> ifr_col;      // >=0 interior index, <0: -(slot+1)
+  std::vector<int64_t> ifr_src;
+  // interior operator (both triangles), for FP64 refinement residuals
+  std::vector<int32_t> aii_ptr;      // sum(nI+1), relative
+  std::vector<int32_t> aii_col;
+  std::vector<int64_t> aii_src;
+  // interface slot data
+  std::vector<int32_t> if_ln;        // sum(nG): global interface id
+  std::vector<int64_t> if_diag_src;  // sum(nG): lower-CSR position of the diagonal, -1 if absent
+  std::vector<int32_t> if_local;     // sum(nG): local DOF id
+  // interior data
+  std::vector<int32_t> int_local;    // sum(nI): local DOF id
+  std::vector<int64_t> int_diag_src; // sum(nI): lower-CSR position of the diagonal
+  // gather of q into Q: for each interface DOF g, the (sub-major) slots in sub order
+  std::vector<int32_t> gq_ptr;       // total_free+1
+  std::vector<int64_t> gq_slot;      // global slot index (sub_if_off + k)
+  int64_t nnz_total = 0;
+  int64_t nlen_reference = 0;
+  int32_t max_local = 0, max_interior = 0, max_iface = 0;
+};
+
+// Builds the plan; returns an empty string on success or an error message.
+std::string build_plan(const Model &m, Plan &p);
+
+}  // namespace fw

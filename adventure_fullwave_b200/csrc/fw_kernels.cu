@@ -1,0 +1,653 @@
+// Device kernels of the HDDM hot path: value gather into the assembled
+// lower rows, skyline profile, envelope scatter, batched LDL^T factor, the
+// per-iteration subdomain solves and the interface COCG.
+//
+// Layout.  Subdomains are concatenated.  Each subdomain's non-Dirichlet
+// ("interior") DOFs keep the reference's order and form a compressed
+// envelope: interior row c stores columns env_lo[c]..c contiguously from
+// env_ptr[c], the diagonal last.  The reference's envelope
+// (advlas_skyline.c:12-25) also spans Dirichlet columns, whose factor entries
+// are exactly zero (their rows are identity after SetBC,
+// aij_matrix_func.h:83-104), so leaving them out changes no result and
+// removes those bytes from every substitution pass.
+//
+// One warp works on one subdomain; warps take subdomains largest first.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fw_kernels.cuh"
+
+namespace fw {
+
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kThreads = 32 * kWarpsPerBlock;
+constexpr double kNearlyZero = 1.0e-60;  // NEARLY_ZERO, lib/std/defs.h:105
+
+__device__ __forceinline__ double2 cz() { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double cabs_ref(double2 a) { return sqrt(a.x * a.x + a.y * a.y); }  // ComplexAbs
+__device__ __forceinline__ bool ciszero(double2 a) { return a.x == 0.0 && a.y == 0.0; }           // ISZERO
+// ComplexReciprocal / ComplexDivide (lib/std/complex_adv.c:39-52,133-137)
+__device__ __forceinline__ double2 crecip_ref(double2 a) {
+  const double d = 1.0 / (a.x * a.x + a.y * a.y);
+  return make_double2(a.x * d, -(a.y * d));
+}
+__device__ __forceinline__ double2 cdiv_ref(double2 a, double2 b) { return cmul(a, crecip_ref(b)); }
+// 1/b by Smith's algorithm (R. L. Smith, CACM 5(8), 1962): the pivot
+// reciprocal of the skyline factor, which the reference takes with C99
+// complex division.
+__device__ __forceinline__ double2 crecip_smith(double2 b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    const double r = b.y / b.x;
+    const double den = b.x + b.y * r;
+    return make_double2(1.0 / den, -r / den);
+  }
+  const double r = b.x / b.y;
+  const double den = b.x * r + b.y;
+  return make_double2(r / den, -1.0 / den);
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_xor(T v, int o);
+template <>
+__device__ __forceinline__ double2 shfl_xor(double2 v, int o) {
+  return make_double2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
+}
+template <>
+__device__ __forceinline__ float2 shfl_xor(float2 v, int o) {
+  return make_float2(__shfl_xor_sync(0xffffffffu, v.x, o), __shfl_xor_sync(0xffffffffu, v.y, o));
+}
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = cadd(v, shfl_xor(v, o));
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T czero();
+template <>
+__device__ __forceinline__ double2 czero<double2>() {
+  return make_double2(0.0, 0.0);
+}
+template <>
+__device__ __forceinline__ float2 czero<float2>() {
+  return make_float2(0.0f, 0.0f);
+}
+
+__device__ __forceinline__ int warp_id_global() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
+
+// ----------------------------------------------------------------------------
+// assembly
+
+// aval[q] = sum of the element-matrix contributions of lower entry q in
+// element order (aij_matrix_func.h:289-322 adds them in element order into a
+// zero-initialised slot; zero contributions leave the sum unchanged).
+__global__ void gather_values_kernel(int64_t nnz, const int64_t *__restrict__ cptr, const int64_t *__restrict__ contrib,
+                                     const double2 *__restrict__ elmat, double2 *__restrict__ aval) {
+  int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nnz) return;
+  double re = 0.0, im = 0.0;
+  for (int64_t t = cptr[q]; t < cptr[q + 1]; t++) {
+    const double2 v = elmat[contrib[t]];
+    re = re + v.x;
+    im = im + v.y;
+  }
+  aval[q] = make_double2(re, im);
+}
+
+// Skyline profile after Dirichlet elimination and DeleteZero: the first
+// column of each sorted row (advlas_copy_nzindex_to_skyindex,
+// advlas_skyline.c:12-25); Dirichlet rows keep only their unit diagonal
+// (aij_matrix_func.h:98-103) and Dirichlet columns are zeroed and deleted
+// (:107-135).
+__global__ void profile_kernel(int32_t nsub, const int64_t *__restrict__ dof_off, const int64_t *__restrict__ nnz_off,
+                               const int32_t *__restrict__ row_ptr_rel, const int32_t *__restrict__ col,
+                               const double2 *__restrict__ aval, const uint8_t *__restrict__ isbc,
+                               int32_t *__restrict__ idx1) {
+  const int s = warp_id_global();
+  if (s >= nsub) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t d0 = dof_off[s];
+  const int n = (int)(dof_off[s + 1] - d0);
+  const int32_t *rp = row_ptr_rel + d0 + s;  // n+1 entries per subdomain
+  const int64_t z0 = nnz_off[s];
+  for (int r = lane; r < n; r += 32) {
+    int first = r;
+    if (!isbc[d0 + r]) {
+      for (int q = rp[r]; q < rp[r + 1]; q++) {
+        const int c = col[z0 + q];
+        if (isbc[d0 + c]) continue;
+        if (ciszero(aval[z0 + q])) continue;
+        first = c;
+        break;
+      }
+    }
+    idx1[d0 + r] = first;
+  }
+}
+
+__global__ void scatter_envelope_kernel(int64_t nnz, const int64_t *__restrict__ dst, const double2 *__restrict__ aval,
+                                        double2 *__restrict__ L) {
+  int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nnz) return;
+  const int64_t d = dst[q];
+  if (d >= 0) L[d] = aval[q];
+}
+
+__global__ void gather_ops_kernel(int64_t n, const int64_t *__restrict__ src, const double2 *__restrict__ aval,
+                                  double2 *__restrict__ dst) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  dst[t] = aval[src[t]];
+}
+
+// DIAG_MAKE (lib/hddm/hddm_pc.h:52-86) at the interface DOFs: the diagonal
+// of the unmodified matrix, 1 where it is absent or zero.
+__global__ void diag_pc_kernel(int64_t n, const int64_t *__restrict__ diag_src, const double2 *__restrict__ aval,
+                               double2 *__restrict__ pcloc) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  double2 v = make_double2(1.0, 0.0);
+  const int64_t q = diag_src[t];
+  if (q >= 0 && !ciszero(aval[q])) v = aval[q];
+  pcloc[t] = v;
+}
+
+__global__ void to_fp32_kernel(int64_t n, const double2 *__restrict__ src, float2 *__restrict__ dst) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double2 v = src[t];
+  dst[t] = make_float2((float)v.x, (float)v.y);
+}
+
+// ----------------------------------------------------------------------------
+// LDL^T factor (advlas_skyline_ldl_decomposite, advlas_skyline.c:79-128),
+// row-Crout without pivoting, in place: off-diagonals become L (unit lower),
+// the diagonal becomes 1/d.  One warp per subdomain; the dot products of each
+// (i, j) step are split across the lanes.
+__global__ void factor_kernel(int32_t nsub, const int32_t *__restrict__ sub_order, const int64_t *__restrict__ int_off,
+                              const int32_t *__restrict__ env_lo, const int64_t *__restrict__ env_ptr,
+                              double2 *L, int32_t *status) {
+  const int w = warp_id_global();
+  if (w >= nsub) return;
+  const int s = sub_order[w];
+  const int lane = threadIdx.x & 31;
+  const int64_t o = int_off[s];
+  const int nI = (int)(int_off[s + 1] - o);
+  const int32_t *lo = env_lo + o;
+  const int64_t *ptr = env_ptr + o;
+  bool bad = false;
+  for (int i = 0; i < nI; i++) {
+    const int lo_i = lo[i];
+    double2 *Gi = L + ptr[i] - lo_i;  // Gi[k]: entry (i, k)
+    for (int j = lo_i; j < i; j++) {
+      const int lo_j = lo[j];
+      const double2 *Lj = L + ptr[j] - lo_j;
+      const int k0 = lo_i > lo_j ? lo_i : lo_j;
+      double2 acc = cz();
+      for (int k = k0 + lane; k < j; k += 32) acc = cadd(acc, cmul(Gi[k], Lj[k]));
+      acc = warp_sum(acc);
+      if (lane == 0) Gi[j] = csub(Gi[j], acc);
+      __syncwarp();
+    }
+    double2 acc = cz();
+    for (int k = lo_i + lane; k < i; k += 32) {
+      const double2 g = Gi[k];
+      const double2 dk = L[ptr[k] + (k - lo[k])];
+      acc = cadd(acc, cmul(cmul(g, g), dk));
+      Gi[k] = cmul(g, dk);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      const double2 d = csub(Gi[i], acc);
+      const double2 r = crecip_smith(d);
+      if (!(isfinite(r.x) && isfinite(r.y)) || ciszero(d)) bad = true;
+      Gi[i] = r;
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && bad) atomicMax(status, 1);
+}
+
+// ----------------------------------------------------------------------------
+// Envelope substitutions (advlas_skyline_ldl_solve, advlas_skyline.c:134-167):
+// forward row dot products with unit L, scaling by the stored 1/d, backward
+// column updates with L^T.  In place on y.
+template <typename T>
+__device__ __forceinline__ void env_solve(int nI, const int32_t *__restrict__ lo, const int64_t *__restrict__ ptr,
+                                          const T *__restrict__ L, T *y, int lane) {
+  for (int i = 1; i < nI; i++) {
+    const int lo_i = lo[i];
+    const T *row = L + ptr[i] - lo_i;
+    T acc = czero<T>();
+    for (int k = lo_i + lane; k < i; k += 32) acc = cadd(acc, cmul(row[k], y[k]));
+    acc = warp_sum(acc);
+    if (lane == 0) y[i] = csub(y[i], acc);
+    __syncwarp();
+  }
+  for (int i = lane; i < nI; i += 32) y[i] = cmul(y[i], L[ptr[i] + (i - lo[i])]);
+  __syncwarp();
+  for (int i = nI - 1; i >= 1; i--) {
+    const int lo_i = lo[i];
+    const T *row = L + ptr[i] - lo_i;
+    const T xi = y[i];
+    for (int k = lo_i + lane; k < i; k += 32) y[k] = csub(y[k], cmul(row[k], xi));
+    __syncwarp();
+  }
+}
+
+// One subdomain solve of the HDDM loop per warp:
+//   first (solve_dom_1st_d, hddm_solver.h:461-555):  v = 0, b = f
+//   iteration (solve_dom_d, :559-622):                v = P, b = 0
+//   last (solve_dom_last_d, :626-693):                v = P, b = f
+// Dirichlet elimination gives the interior right-hand side f_I - A_IG v
+// (aij_matrix_func.h:60-136, the PEC values are zero); after the solve,
+// q = A_G. x (- f_G when b = f) is the subdomain's contribution to Q at its
+// interface DOFs (MxV_TMP_AIJ, aij_matrix_func.h:624-658, restricted to the
+// interface rows that COM_RES_SP_FUNC reads, hddm_solver_sp.h:41-54).
+template <bool kFp32>
+__global__ void __launch_bounds__(kThreads) subsolve_kernel(DevProblem p, int mode) {
+  if (p.sc->status != 0 && mode == kModeIter) return;
+  const int w = warp_id_global();
+  if (w >= p.nsub) return;
+  const int s = p.sub_order[w];
+  const int lane = threadIdx.x & 31;
+  const int64_t io = p.int_off[s], go = p.if_off[s];
+  const int nI = (int)(p.int_off[s + 1] - io);
+  const int nG = (int)(p.if_off[s + 1] - go);
+  const bool with_bc = mode != kModeFirst;
+  const bool with_f = mode != kModeIter;
+  double2 *y = p.Y + io;
+  double2 *v = p.V + go;
+  for (int k = lane; k < nG; k += 32) v[k] = with_bc ? p.P[p.if_ln[go + k]] : cz();
+  __syncwarp();
+  const int32_t *cptr = p.cpl_ptr + io + s;
+  const int64_t cbase = p.cpl_off[s];
+  double2 *b = kFp32 ? p.B + io : y;
+  for (int c = lane; c < nI; c += 32) {
+    double2 acc = with_f ? p.fI[io + c] : cz();
+    for (int q = cptr[c]; q < cptr[c + 1]; q++) acc = csub(acc, cmul(p.cpl_val[cbase + q], v[p.cpl_col[cbase + q]]));
+    b[c] = acc;
+  }
+  __syncwarp();
+  const int32_t *lo = p.env_lo + io;
+  const int64_t *ptr = p.env_ptr + io;
+  if (!kFp32) {
+    env_solve<double2>(nI, lo, ptr, p.L64, y, lane);
+  } else {
+    // FP32 factor with FP64 iterative refinement: x0 = solve32(b);
+    // repeat r = b - A_II x (FP64), x += solve32(r).
+    float2 *y32 = p.Y32 + io;
+    for (int c = lane; c < nI; c += 32) y32[c] = make_float2((float)b[c].x, (float)b[c].y);
+    __syncwarp();
+    env_solve<float2>(nI, lo, ptr, p.L32, y32, lane);
+    for (int c = lane; c < nI; c += 32) y[c] = make_double2((double)y32[c].x, (double)y32[c].y);
+    __syncwarp();
+    const int32_t *aptr = p.aii_ptr + io + s;
+    const int64_t abase = p.aii_off[s];
+    double bnorm = 0.0;
+    if (p.ir_tol > 0.0) {
+      for (int c = lane; c < nI; c += 32) bnorm = fmax(bnorm, fabs(b[c].x) + fabs(b[c].y));
+      for (int o2 = 16; o2 > 0; o2 >>= 1) bnorm = fmax(bnorm, __shfl_xor_sync(0xffffffffu, bnorm, o2));
+    }
+    for (int step = 0; step < p.ir_steps; step++) {
+      double rnorm = 0.0;
+      for (int c = lane; c < nI; c += 32) {
+        double2 r = b[c];
+        for (int q = aptr[c]; q < aptr[c + 1]; q++) r = csub(r, cmul(p.aii_val[abase + q], y[p.aii_col[abase + q]]));
+        y32[c] = make_float2((float)r.x, (float)r.y);
+        rnorm = fmax(rnorm, fabs(r.x) + fabs(r.y));
+      }
+      if (p.ir_tol > 0.0) {
+        for (int o2 = 16; o2 > 0; o2 >>= 1) rnorm = fmax(rnorm, __shfl_xor_sync(0xffffffffu, rnorm, o2));
+        if (rnorm <= p.ir_tol * bnorm) break;
+      }
+      __syncwarp();
+      env_solve<float2>(nI, lo, ptr, p.L32, y32, lane);
+      for (int c = lane; c < nI; c += 32)
+        y[c] = cadd(y[c], make_double2((double)y32[c].x, (double)y32[c].y));
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  const int32_t *rptr = p.ifr_ptr + go + s;
+  const int64_t rbase = p.ifr_off[s];
+  for (int k = lane; k < nG; k += 32) {
+    double2 acc = cz();
+    for (int q = rptr[k]; q < rptr[k + 1]; q++) {
+      const int c = p.ifr_col[rbase + q];
+      const double2 xv = c >= 0 ? y[c] : v[-c - 1];
+      acc = cadd(acc, cmul(p.ifr_val[rbase + q], xv));
+    }
+    if (with_f) acc = csub(acc, p.fG[go + k]);
+    p.qloc[go + k] = acc;
+  }
+}
+
+// ----------------------------------------------------------------------------
+// interface COCG (ITERATION_S_1ST / ITERATION_S, hddm_solver_s.h:158-400)
+
+constexpr int kRedThreads = 256;
+enum { kFPqRe = 0, kFPqIm, kFMax, kFRzRe, kFRzIm, kFL2, kNFields };
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) r += sh[i];
+  return r;  // valid in thread 0
+}
+__device__ __forceinline__ double block_max(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) r = fmax(r, sh[i]);
+  return r;
+}
+
+// reduce the per-block partials of field f in a fixed order (one block)
+__device__ double reduce_partials(const double *part, int nb, int f, bool is_max, double *sh) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    const double x = part[f * nb + i];
+    v = is_max ? fmax(v, x) : v + x;
+  }
+  double r = is_max ? block_max(v, sh) : block_sum(v, sh);
+  __syncthreads();
+  if (threadIdx.x == 0) sh[32] = r;
+  __syncthreads();
+  r = sh[32];
+  __syncthreads();
+  return r;
+}
+
+__device__ __forceinline__ double2 gather_q(const DevProblem &p, int g) {
+  double2 q = cz();
+  for (int t = p.gq_ptr[g]; t < p.gq_ptr[g + 1]; t++) q = cadd(q, p.qloc[p.gq_slot[t]]);
+  return q;
+}
+
+// first step: Q and PC gathered over subdomains (hddm_solver_s.h:174-181),
+// PC reciprocal (hddm_pc.h:128-135), r = Q, z = r pc, p = z, max|r|, (r, z)
+__global__ void cocg_first_kernel(DevProblem p, const double2 *__restrict__ pcloc) {
+  __shared__ double sh[40];
+  double mx = 0.0, rzr = 0.0, rzi = 0.0, l2 = 0.0;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
+    const double2 q = gather_q(p, g);
+    double2 pc = cz();
+    for (int t = p.gq_ptr[g]; t < p.gq_ptr[g + 1]; t++) pc = cadd(pc, pcloc[p.gq_slot[t]]);
+    pc = ciszero(pc) ? make_double2(1.0, 0.0) : cdiv_ref(make_double2(1.0, 0.0), pc);
+    p.PC[g] = pc;
+    p.Q[g] = q;
+    p.R[g] = q;
+    const double2 z = cmul(q, pc);
+    p.Z[g] = z;
+    p.P[g] = z;
+    p.U[g] = cz();
+    mx = fmax(mx, cabs_ref(q));
+    const double2 rz = cmul(q, z);
+    rzr += rz.x;
+    rzi += rz.y;
+    l2 += q.x * q.x + q.y * q.y;
+  }
+  const int nb = p.n_part_blocks;
+  double r;
+  r = block_max(mx, sh);
+  if (threadIdx.x == 0) p.part[kFMax * nb + blockIdx.x] = r;
+  r = block_sum(rzr, sh);
+  if (threadIdx.x == 0) p.part[kFRzRe * nb + blockIdx.x] = r;
+  r = block_sum(rzi, sh);
+  if (threadIdx.x == 0) p.part[kFRzIm * nb + blockIdx.x] = r;
+  r = block_sum(l2, sh);
+  if (threadIdx.x == 0) p.part[kFL2 * nb + blockIdx.x] = r;
+}
+
+__global__ void cocg_first_scalars_kernel(DevProblem p) {
+  __shared__ double sh[40];
+  const int nb = p.n_part_blocks;
+  const double mx = reduce_partials(p.part, nb, kFMax, true, sh);
+  const double rzr = reduce_partials(p.part, nb, kFRzRe, false, sh);
+  const double rzi = reduce_partials(p.part, nb, kFRzIm, false, sh);
+  const double l2 = reduce_partials(p.part, nb, kFL2, false, sh);
+  if (threadIdx.x == 0) {
+    CocgScalars *sc = p.sc;
+    sc->norm0 = mx;
+    sc->l2_0 = sqrt(l2);
+    sc->status = mx < kNearlyZero ? 1 : 0;
+    sc->r0inv = 1.0 / mx;
+    sc->rz = make_double2(rzr, rzi);
+    sc->resi = 1.0;
+    sc->resi_l2 = 1.0;
+    sc->loop = 1;
+    sc->converged = mx < kNearlyZero ? 1 : 0;
+  }
+}
+
+__global__ void cocg_begin_kernel(CocgScalars *sc) {
+  if (sc->status == 1) sc->status = 2;
+}
+
+// Q gathered over subdomains (hddm_solver_s.h:273 with COM_RES_SP) and (p, q)
+__global__ void cocg_gather_pq_kernel(DevProblem p) {
+  if (p.sc->status != 0) return;
+  __shared__ double sh[40];
+  double re = 0.0, im = 0.0;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
+    const double2 q = gather_q(p, g);
+    p.Q[g] = q;
+    const double2 t = cmul(p.P[g], q);
+    re += t.x;
+    im += t.y;
+  }
+  const int nb = p.n_part_blocks;
+  double r = block_sum(re, sh);
+  if (threadIdx.x == 0) p.part[kFPqRe * nb + blockIdx.x] = r;
+  r = block_sum(im, sh);
+  if (threadIdx.x == 0) p.part[kFPqIm * nb + blockIdx.x] = r;
+}
+
+// -alpha = -(r, z) / (p, q)  (hddm_solver_s.h:282-295)
+__global__ void cocg_alpha_kernel(DevProblem p) {
+  if (p.sc->status != 0) return;
+  __shared__ double sh[40];
+  const int nb = p.n_part_blocks;
+  const double pr = reduce_partials(p.part, nb, kFPqRe, false, sh);
+  const double pi = reduce_partials(p.part, nb, kFPqIm, false, sh);
+  if (threadIdx.x == 0) {
+    CocgScalars *sc = p.sc;
+    const double2 pq = make_double2(pr, pi);
+    if (cabs_ref(sc->rz) < kNearlyZero && cabs_ref(pq) < kNearlyZero) {
+      sc->malpha = cz();
+    } else {
+      sc->malpha = csub(cz(), cdiv_ref(sc->rz, pq));
+    }
+  }
+}
+
+// u += -alpha p, r += -alpha q, max|r|, z = r pc, (r, z)  (hddm_solver_s.h:297-344)
+__global__ void cocg_update_kernel(DevProblem p) {
+  if (p.sc->status != 0) return;
+  __shared__ double sh[40];
+  const double2 ma = p.sc->malpha;
+  double mx = 0.0, rzr = 0.0, rzi = 0.0, l2 = 0.0;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
+    p.U[g] = cadd(p.U[g], cmul(ma, p.P[g]));
+    const double2 r = cadd(p.R[g], cmul(ma, p.Q[g]));
+    p.R[g] = r;
+    mx = fmax(mx, cabs_ref(r));
+    const double2 z = cmul(r, p.PC[g]);
+    p.Z[g] = z;
+    const double2 rz = cmul(r, z);
+    rzr += rz.x;
+    rzi += rz.y;
+    l2 += r.x * r.x + r.y * r.y;
+  }
+  const int nb = p.n_part_blocks;
+  double r;
+  r = block_max(mx, sh);
+  if (threadIdx.x == 0) p.part[kFMax * nb + blockIdx.x] = r;
+  r = block_sum(rzr, sh);
+  if (threadIdx.x == 0) p.part[kFRzRe * nb + blockIdx.x] = r;
+  r = block_sum(rzi, sh);
+  if (threadIdx.x == 0) p.part[kFRzIm * nb + blockIdx.x] = r;
+  r = block_sum(l2, sh);
+  if (threadIdx.x == 0) p.part[kFL2 * nb + blockIdx.x] = r;
+}
+
+// resi, beta = (r', z') / (r, z), convergence and loop count
+// (hddm_solver_s.h:318-379, hddm_solver.h:125-143)
+__global__ void cocg_beta_kernel(DevProblem p) {
+  if (p.sc->status != 0) return;
+  __shared__ double sh[40];
+  const int nb = p.n_part_blocks;
+  const double mx = reduce_partials(p.part, nb, kFMax, true, sh);
+  const double rzr = reduce_partials(p.part, nb, kFRzRe, false, sh);
+  const double rzi = reduce_partials(p.part, nb, kFRzIm, false, sh);
+  const double l2 = reduce_partials(p.part, nb, kFL2, false, sh);
+  if (threadIdx.x == 0) {
+    CocgScalars *sc = p.sc;
+    const double resi = mx * sc->r0inv;
+    sc->resi = resi;
+    sc->resi_l2 = sqrt(l2) / sc->l2_0;
+    p.hist[sc->loop - 1] = resi;
+    const double2 rz = make_double2(rzr, rzi);
+    if (cabs_ref(rz) < kNearlyZero && cabs_ref(sc->rz) < kNearlyZero) {
+      sc->beta = cz();
+    } else {
+      sc->beta = cdiv_ref(rz, sc->rz);
+    }
+    sc->rz = rz;
+    if (resi < sc->eps) {
+      sc->status = 1;
+      sc->converged = 1;
+    } else if (sc->loop >= sc->max_loop) {
+      sc->status = 1;
+    }
+    sc->loop += 1;
+  }
+}
+
+// p = z + beta p, or p = u after the last iteration (hddm_solver_s.h:356-376)
+__global__ void cocg_pupdate_kernel(DevProblem p) {
+  const int st = p.sc->status;
+  if (st == 2) return;
+  const double2 be = p.sc->beta;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
+    p.P[g] = st == 1 ? p.U[g] : cadd(p.Z[g], cmul(be, p.P[g]));
+  }
+}
+
+__global__ void edge_solution_kernel(int64_t ne, const int64_t *__restrict__ src, const double2 *__restrict__ Y,
+                                     const double2 *__restrict__ V, double2 *__restrict__ x) {
+  int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int64_t s = src[e];
+  x[e] = s >= 0 ? Y[s] : (s < -1 ? V[-s - 2] : make_double2(0.0, 0.0));
+}
+
+__global__ void set_status_kernel(CocgScalars *sc, double eps, int32_t max_loop) {
+  sc->eps = eps;
+  sc->max_loop = max_loop;
+  sc->status = 0;
+  sc->converged = 0;
+}
+
+unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+}  // namespace
+
+void launch_gather_values(int64_t nnz, const int64_t *contrib_ptr, const int64_t *contrib, const double2 *elmat,
+                          double2 *aval, cudaStream_t stream) {
+  if (nnz <= 0) return;
+  gather_values_kernel<<<blocks_for(nnz, 256), 256, 0, stream>>>(nnz, contrib_ptr, contrib, elmat, aval);
+}
+
+void launch_profile(int32_t nsub, const int64_t *dof_off, const int64_t *nnz_off, const int32_t *row_ptr_rel,
+                    const int32_t *col, const double2 *aval, const uint8_t *isbc, int32_t *idx1,
+                    cudaStream_t stream) {
+  profile_kernel<<<blocks_for((int64_t)nsub * 32, kThreads), kThreads, 0, stream>>>(nsub, dof_off, nnz_off,
+                                                                                      row_ptr_rel, col, aval, isbc,
+                                                                                      idx1);
+}
+
+void launch_scatter_envelope(int64_t nnz, const int64_t *dst, const double2 *aval, double2 *L, cudaStream_t stream) {
+  if (nnz <= 0) return;
+  scatter_envelope_kernel<<<blocks_for(nnz, 256), 256, 0, stream>>>(nnz, dst, aval, L);
+}
+
+void launch_gather_ops(int64_t n, const int64_t *src, const double2 *aval, double2 *dst, cudaStream_t stream) {
+  if (n <= 0) return;
+  gather_ops_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, src, aval, dst);
+}
+
+void launch_diag_pc(int64_t n, const int64_t *diag_src, const double2 *aval, double2 *pcloc, cudaStream_t stream) {
+  if (n <= 0) return;
+  diag_pc_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, diag_src, aval, pcloc);
+}
+
+void launch_factor(const DevProblem &p, const int64_t *int_off, const int32_t *env_lo, const int64_t *env_ptr,
+                   double2 *L, int32_t *status, cudaStream_t stream) {
+  factor_kernel<<<blocks_for((int64_t)p.nsub * 32, kThreads), kThreads, 0, stream>>>(p.nsub, p.sub_order, int_off,
+                                                                                       env_lo, env_ptr, L, status);
+}
+
+void launch_to_fp32(int64_t n, const double2 *src, float2 *dst, cudaStream_t stream) {
+  if (n <= 0) return;
+  to_fp32_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, src, dst);
+}
+
+void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stream) {
+  const unsigned nb = blocks_for((int64_t)p.nsub * 32, kThreads);
+  if (fp32)
+    subsolve_kernel<true><<<nb, kThreads, 0, stream>>>(p, mode);
+  else
+    subsolve_kernel<false><<<nb, kThreads, 0, stream>>>(p, mode);
+}
+
+void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream) {
+  cocg_first_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p, pcloc);
+  cocg_first_scalars_kernel<<<1, kRedThreads, 0, stream>>>(p);
+}
+
+void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream) {
+  cocg_begin_kernel<<<1, 1, 0, stream>>>(p.sc);
+  launch_subsolve(p, kModeIter, p.L32 != nullptr, stream);
+  cocg_gather_pq_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
+  cocg_alpha_kernel<<<1, kRedThreads, 0, stream>>>(p);
+  cocg_update_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
+  cocg_beta_kernel<<<1, kRedThreads, 0, stream>>>(p);
+  cocg_pupdate_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
+}
+
+void launch_edge_solution(int64_t ne, const int64_t *edge_src, const double2 *Y, const double2 *V, double2 *x,
+                          cudaStream_t stream) {
+  if (ne <= 0) return;
+  edge_solution_kernel<<<blocks_for(ne, 256), 256, 0, stream>>>(ne, edge_src, Y, V, x);
+}
+
+void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream) {
+  set_status_kernel<<<1, 1, 0, stream>>>(sc, eps, max_loop);
+}
+
+}  // namespace fw

@@ -1,0 +1,101 @@
+// Device kernels of the HDDM hot path (declarations shared by fw_capi.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace fw {
+
+// COCG scalars of one interface problem, resident on the device.  Mirrors the
+// scalars of ITERATION_S / ITERATION_S_1ST (lib/hddm/hddm_solver_s.h:158-400)
+// and hddm_sw (lib/std/types.h:732-741).
+struct CocgScalars {
+  double2 rz;        // (r, z) bilinear
+  double2 rz_new;
+  double2 malpha;    // -alpha
+  double2 beta;
+  double norm0;      // max|r0|
+  double r0inv;      // 1 / max|r0|
+  double l2_0;       // ||r0||_2
+  double resi;       // max|r| / max|r0|
+  double resi_l2;    // ||r||_2 / ||r0||_2
+  double eps;        // hddm_eps
+  int32_t status;    // 0 iterating, 1 last iteration done (p := u), 2 finished
+  int32_t loop;      // hddm_sw.loop
+  int32_t max_loop;  // hddm_max_loop
+  int32_t converged;
+  int32_t factor_status;  // non-zero: a pivot was zero or not finite
+  int32_t pad;
+};
+
+// Per-problem device pointers used by the iteration kernels.
+struct DevProblem {
+  int32_t nsub;
+  int32_t nfree;                 // interface DOFs
+  const int32_t *sub_order;      // warps take subdomains in this order
+  const int64_t *int_off;        // nsub+1
+  const int64_t *if_off;         // nsub+1
+  // interior envelope (compressed)
+  const int32_t *env_lo;         // sum nI: first stored column (interior index)
+  const int64_t *env_ptr;        // sum nI: position of column env_lo in the value arrays
+  const double2 *L64;
+  const float2 *L32;
+  // operators
+  const int32_t *cpl_ptr;        // sum(nI+1) relative
+  const int64_t *cpl_off;        // nsub+1 base of cpl arrays
+  const int32_t *cpl_col;
+  const double2 *cpl_val;
+  const int32_t *ifr_ptr;        // sum(nG+1) relative
+  const int64_t *ifr_off;
+  const int32_t *ifr_col;
+  const double2 *ifr_val;
+  const int32_t *aii_ptr;        // sum(nI+1) relative
+  const int64_t *aii_off;
+  const int32_t *aii_col;
+  const double2 *aii_val;
+  const int32_t *if_ln;          // sum nG
+  const double2 *fI;             // sum nI, interior right-hand side
+  const double2 *fG;             // sum nG, interface right-hand side
+  // work
+  double2 *Y;                    // sum nI, interior solution
+  double2 *B;                    // sum nI, right-hand side copy (refinement)
+  float2 *Y32;                   // sum nI, FP32 work (refinement)
+  double2 *V;                    // sum nG, interface values
+  double2 *qloc;                 // sum nG
+  // interface vectors
+  double2 *P, *Q, *R, *Z, *U, *PC;
+  const int32_t *gq_ptr;         // nfree+1
+  const int64_t *gq_slot;
+  CocgScalars *sc;
+  double *hist;                  // residual history
+  double *part;                  // reduction partials, 4 * n_part_blocks
+  int32_t n_part_blocks;
+  int32_t ir_steps;
+  double ir_tol;
+};
+
+enum SolveMode { kModeFirst = 0, kModeIter = 1, kModeLast = 2 };
+
+void launch_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
+                             const double *el_eps, const double *el_sigma, double omega, double *out,
+                             int32_t *status, cudaStream_t stream);
+void launch_gather_values(int64_t nnz, const int64_t *contrib_ptr, const int64_t *contrib, const double2 *elmat,
+                          double2 *aval, cudaStream_t stream);
+void launch_profile(int32_t nsub, const int64_t *dof_off, const int64_t *nnz_off, const int32_t *row_ptr_rel,
+                    const int32_t *col, const double2 *aval, const uint8_t *isbc, int32_t *idx1,
+                    cudaStream_t stream);
+void launch_scatter_envelope(int64_t nnz, const int64_t *dst, const double2 *aval, double2 *L, cudaStream_t stream);
+void launch_gather_ops(int64_t n, const int64_t *src, const double2 *aval, double2 *dst, cudaStream_t stream);
+void launch_diag_pc(int64_t n, const int64_t *diag_src, const double2 *aval, double2 *pcloc, cudaStream_t stream);
+void launch_factor(const DevProblem &p, const int64_t *int_off, const int32_t *env_lo, const int64_t *env_ptr,
+                   double2 *L, int32_t *status, cudaStream_t stream);
+void launch_to_fp32(int64_t n, const double2 *src, float2 *dst, cudaStream_t stream);
+void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stream);
+void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream);
+void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream);
+void launch_edge_solution(int64_t ne, const int64_t *edge_src, const double2 *Y, const double2 *V, double2 *x,
+                          cudaStream_t stream);
+void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream);
+
+}  // namespace fw

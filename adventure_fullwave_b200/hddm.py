@@ -1,0 +1,233 @@
+"""Host API of the B200 HDDM hot path, shaped after the reference's solver
+interface.
+
+The reference drives one full-wave solve through ``hddm_solver_CS(pm,
+options, set_hddm_func_fullwave)`` (``lib/hddm/hddm_solver.h:25-183``), which
+walks the plug-in table ``HDDM_FUNC`` (``lib/std/types.h:629-730``) slot by
+slot for every (part, subdomain).  ``HddmSolver`` exposes the same slots,
+each batched over all subdomains on the GPU (``make_tmp_aij``,
+``solve_dom_1st``, ``iteration_s_1st``, ``iteration_s``, ``solve_dom_last``),
+and ``hddm_solver_CS`` runs the whole loop like the reference's driver.
+
+Options keep the reference's names and meaning: ``hddm_eps`` is the
+max-norm relative interface residual at which COCG stops (``-hddm-eps``,
+default 1e-3), ``hddm_max_loop`` caps the iterations (``-hddm-max-loop``,
+default 4000).  Errors are raised as ``FwgpuError`` instead of the
+reference's print-and-exit.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import FwgpuError  # noqa: F401  (re-exported)
+
+P = ctypes.POINTER
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(P(ctype))
+
+
+@dataclass
+class HddmResult:
+    iterations: int
+    converged: bool
+    initial_norm: float
+    final_resi: float
+    final_resi_l2: float
+    t_setup_ms: float
+    t_iterate_ms: float
+    t_last_ms: float
+
+
+class HddmSolver:
+    """All subdomains of one full-wave model resident on one GPU.
+
+    ``model`` is an ``adventure_fullwave_b200.meshgen.Model`` (or any object
+    with the same fields).  ``precision`` is ``"fp64"`` (the reference's
+    complex FP64 skyline factors) or ``"fp32_ir"`` (factors stored and
+    applied in complex FP32, FP64 iterative refinement of every subdomain
+    solve).
+    """
+
+    def __init__(self, model, hddm_eps: float = 1e-3, hddm_max_loop: int = 4000, precision: str = "fp64",
+                 ir_max_steps: int = 1, ir_tol: float = 0.0, graph_iterations: int = 16, device: int = 0):
+        lib = _lib.load()
+        self._lib = lib
+        self.model = model
+        self.hddm_eps = float(hddm_eps)
+        self.hddm_max_loop = int(hddm_max_loop)
+        a = {}
+        a["crd"] = np.ascontiguousarray(model.vertex_crd, dtype=np.float64)
+        a["tv"] = np.ascontiguousarray(model.tets, dtype=np.int32)
+        a["te"] = np.ascontiguousarray(model.tet_edges, dtype=np.int32)
+        a["flag"] = np.ascontiguousarray(model.flag, dtype=np.int32)
+        a["pec"] = np.ascontiguousarray(model.pec_edge, dtype=np.uint8)
+        a["sub"] = np.ascontiguousarray(model.sub_of_tet, dtype=np.int32)
+        a["mf"] = np.ascontiguousarray(model.mat_flag, dtype=np.int32)
+        a["me"] = np.ascontiguousarray(model.mat_eps, dtype=np.float64)
+        a["ms"] = np.ascontiguousarray(model.mat_sigma, dtype=np.float64)
+        mesh = _lib.FwMesh(
+            int(a["crd"].shape[0]), _ptr(a["crd"], ctypes.c_double), int(a["tv"].shape[0]),
+            _ptr(a["tv"], ctypes.c_int32), _ptr(a["te"], ctypes.c_int32), _ptr(a["flag"], ctypes.c_int32),
+            int(a["pec"].shape[0]), _ptr(a["pec"], ctypes.c_uint8), int(model.nsub), _ptr(a["sub"], ctypes.c_int32))
+        mt = _lib.FwMaterial(int(a["mf"].shape[0]), _ptr(a["mf"], ctypes.c_int32), _ptr(a["me"], ctypes.c_double),
+                             int(a["mf"].shape[0]), _ptr(a["mf"], ctypes.c_int32), _ptr(a["ms"], ctypes.c_double),
+                             float(model.omega))
+        prec = {"fp64": _lib.PREC_FP64, "fp32_ir": _lib.PREC_FP32_IR}[precision]
+        self.precision = precision
+        opts = _lib.FwOptions(self.hddm_eps, self.hddm_max_loop, prec, int(ir_max_steps), float(ir_tol),
+                              int(graph_iterations), int(device))
+        handle = ctypes.c_void_p()
+        _lib.check(lib.fwgpu_create(ctypes.byref(mesh), ctypes.byref(mt), ctypes.byref(opts), ctypes.byref(handle)))
+        self._h = handle
+        self.n_edges = int(model.n_edges)
+
+    # -- lifecycle --------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.fwgpu_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- sources -----------------------------------------------------------
+    def _source(self, source) -> Tuple[_lib.FwSource, tuple]:
+        if source is None:
+            return _lib.FwSource(0, None, None), ()
+        if isinstance(source, int):
+            edges, vals = self.model.sources[source]
+        else:
+            edges, vals = source
+        e = np.ascontiguousarray(edges, dtype=np.int32)
+        v = np.ascontiguousarray(np.stack([np.real(vals), np.imag(vals)], axis=1).ravel(), dtype=np.float64)
+        return _lib.FwSource(int(e.shape[0]), _ptr(e, ctypes.c_int32), _ptr(v, ctypes.c_double)), (e, v)
+
+    # -- the reference's plug-in slots, batched ----------------------------
+    def make_tmp_aij(self, source=0) -> None:
+        src, keep = self._source(source)
+        _lib.check(self._lib.fwgpu_make_tmp_aij(self._h, ctypes.byref(src)))
+
+    def solve_dom_1st(self) -> None:
+        _lib.check(self._lib.fwgpu_solve_dom_1st(self._h))
+
+    def iteration_s_1st(self) -> int:
+        st = ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_iteration_s_1st(self._h, ctypes.byref(st)))
+        return st.value
+
+    def iteration_s(self) -> int:
+        st = ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_iteration_s(self._h, ctypes.byref(st)))
+        return st.value
+
+    def solve_dom_last(self) -> None:
+        _lib.check(self._lib.fwgpu_solve_dom_last(self._h))
+
+    # -- batched driver ----------------------------------------------------
+    def solve(self, source=0, raise_not_converged: bool = False) -> HddmResult:
+        src, keep = self._source(source)
+        res = _lib.FwResult()
+        allow = () if raise_not_converged else (_lib.ERR_NOT_CONVERGED,)
+        _lib.check(self._lib.fwgpu_hddm_solve(self._h, ctypes.byref(src), ctypes.byref(res)), allow=allow)
+        return self._result(res)
+
+    def resolve(self, source, raise_not_converged: bool = False) -> HddmResult:
+        src, keep = self._source(source)
+        res = _lib.FwResult()
+        allow = () if raise_not_converged else (_lib.ERR_NOT_CONVERGED,)
+        _lib.check(self._lib.fwgpu_hddm_resolve(self._h, ctypes.byref(src), ctypes.byref(res)), allow=allow)
+        return self._result(res)
+
+    @staticmethod
+    def _result(r: _lib.FwResult) -> HddmResult:
+        return HddmResult(int(r.iterations), bool(r.converged), float(r.initial_norm), float(r.final_resi),
+                          float(r.final_resi_l2), float(r.t_setup_ms), float(r.t_iterate_ms), float(r.t_last_ms))
+
+    # -- results -----------------------------------------------------------
+    def edge_solution(self) -> np.ndarray:
+        x = np.zeros(2 * self.n_edges, dtype=np.float64)
+        _lib.check(self._lib.fwgpu_get_edge_solution(self._h, _ptr(x, ctypes.c_double)))
+        return x[0::2] + 1j * x[1::2]
+
+    def history(self) -> np.ndarray:
+        n = ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_get_history(self._h, None, 0, ctypes.byref(n)))
+        h = np.zeros(max(1, n.value), dtype=np.float64)
+        _lib.check(self._lib.fwgpu_get_history(self._h, _ptr(h, ctypes.c_double), n.value, ctypes.byref(n)))
+        return h[: n.value]
+
+    def sizes(self) -> dict:
+        s = _lib.FwSizes()
+        _lib.check(self._lib.fwgpu_get_sizes(self._h, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in _lib.FwSizes._fields_}
+
+    # -- introspection -----------------------------------------------------
+    def subdomain_maps(self, s: int) -> dict:
+        nel, nmp, nbc, ninbc = (ctypes.c_int32() for _ in range(4))
+        lib = self._lib
+        _lib.check(lib.fwgpu_get_subdomain_maps(self._h, s, ctypes.byref(nel), ctypes.byref(nmp), ctypes.byref(nbc),
+                                                ctypes.byref(ninbc), None, None, None, None, None))
+        nop = np.zeros(10 * nel.value, np.int32)
+        ibc = np.zeros(max(1, nbc.value), np.int32)
+        nf = np.zeros(max(1, ninbc.value), np.int32)
+        ln = np.zeros(max(1, ninbc.value), np.int32)
+        gid = np.zeros(max(1, nmp.value), np.int32)
+        i32 = ctypes.c_int32
+        _lib.check(lib.fwgpu_get_subdomain_maps(self._h, s, None, None, None, None, _ptr(nop, i32), _ptr(ibc, i32),
+                                                _ptr(nf, i32), _ptr(ln, i32), _ptr(gid, i32)))
+        return dict(nel=nel.value, nmp=nmp.value, nop=nop, ibc=ibc[: nbc.value], inbc_nfid=nf[: ninbc.value],
+                    inbc_ln_part=ln[: ninbc.value], edge_gid=gid[: nmp.value])
+
+    def skyline_profile(self, s: int) -> Tuple[np.ndarray, np.ndarray, int]:
+        nmp = self.subdomain_maps(s)["nmp"]
+        idx1 = np.zeros(nmp, np.int32)
+        idx2 = np.zeros(nmp, np.int32)
+        nlen = ctypes.c_int32()
+        i32 = ctypes.c_int32
+        _lib.check(self._lib.fwgpu_get_skyline_profile(self._h, s, _ptr(idx1, i32), _ptr(idx2, i32),
+                                                       ctypes.byref(nlen)))
+        return idx1, idx2, nlen.value
+
+    def tmp_aij(self, s: int):
+        nmp = self.subdomain_maps(s)["nmp"]
+        nnz = ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_get_tmp_aij(self._h, s, ctypes.byref(nnz), None, None, None, None))
+        rp = np.zeros(nmp + 1, np.int32)
+        col = np.zeros(max(1, nnz.value), np.int32)
+        val = np.zeros(2 * max(1, nnz.value), np.float64)
+        b = np.zeros(2 * nmp, np.float64)
+        i32 = ctypes.c_int32
+        _lib.check(self._lib.fwgpu_get_tmp_aij(self._h, s, ctypes.byref(nnz), _ptr(rp, i32), _ptr(col, i32),
+                                               _ptr(val, ctypes.c_double), _ptr(b, ctypes.c_double)))
+        n = nnz.value
+        return rp, col[:n], val[0:2 * n:2] + 1j * val[1:2 * n:2], b[0::2] + 1j * b[1::2]
+
+    def factor(self, s: int) -> np.ndarray:
+        idx1, idx2, nlen = self.skyline_profile(s)
+        m = np.zeros(2 * nlen, np.float64)
+        _lib.check(self._lib.fwgpu_get_factor(self._h, s, _ptr(m, ctypes.c_double)))
+        return m[0::2] + 1j * m[1::2]
+
+
+def hddm_solver_CS(model, source=0, **opts) -> Tuple[np.ndarray, HddmResult]:
+    """One full-wave HDDM solve (the reference's ``hddm_solver_CS`` with
+    ``set_hddm_func_fullwave``); returns the edge solution and the result."""
+    with HddmSolver(model, **opts) as s:
+        r = s.solve(source)
+        return s.edge_solution(), r

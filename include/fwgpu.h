@@ -1,0 +1,219 @@
+/*
+ * fwgpu.h -- C ABI of the B200 HDDM hot path of ADVENTURE_FullWave.
+ *
+ * One context holds every part and subdomain of a full-wave HDDM problem
+ * resident on one GPU.  The reference's per-subdomain loops over
+ * (part, subdomain) in lib/hddm/hddm_solver_s.h become one batched call each;
+ * every entry point below replaces one slot of the reference's plug-in table
+ * HDDM_FUNC (lib/std/types.h:629-730) as filled by set_hddm_func_fullwave
+ * (main/fullwave/fullwave.c:23-146), or the driver that walks it
+ * (hddm_solver_CS, lib/hddm/hddm_solver.h:25-183).
+ *
+ * Conventions
+ *   - plain C types only; complex numbers are interleaved (re, im) doubles,
+ *     the layout of the reference's Complex (lib/std/types.h).
+ *   - every function returns FWGPU_OK (0) or a negative FWGPU_ERR_* code and
+ *     never exits the process (the reference calls emessage()/exit()).
+ *   - the caller owns every buffer passed in; the library owns device state
+ *     behind the opaque context.  A context is used by one host thread at a
+ *     time and runs on its own CUDA stream.
+ *   - there is no CPU fallback: without a CUDA device every call that needs
+ *     the GPU returns FWGPU_ERR_CUDA.
+ */
+#ifndef FWGPU_H
+#define FWGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FWGPU_ABI_VERSION 1
+
+enum {
+  FWGPU_OK = 0,
+  FWGPU_ERR_ARG = -1,           /* invalid argument or inconsistent sizes */
+  FWGPU_ERR_CUDA = -2,          /* CUDA runtime error or no device */
+  FWGPU_ERR_STATE = -3,         /* call out of order (e.g. solve before factor) */
+  FWGPU_ERR_NOT_CONVERGED = -4, /* COCG hit hddm_max_loop before hddm_eps */
+  FWGPU_ERR_BREAKDOWN = -5,     /* zero or non-finite pivot in a subdomain factor */
+  FWGPU_ERR_NOMEM = -6,         /* device allocation failed */
+  FWGPU_ERR_MESH = -7           /* degenerate or negatively oriented element */
+};
+
+/* precision of the subdomain factors */
+enum {
+  FWGPU_PREC_FP64 = 0,    /* factor stored and applied in complex FP64 (the reference) */
+  FWGPU_PREC_FP32_IR = 1  /* factor stored and applied in complex FP32, FP64 iterative
+                             refinement of every subdomain solve */
+};
+
+/* Model input: the fullwave driver's mesh, material flags, PEC wall and
+ * partition, i.e. what lib/hddm/make_PartMesh.c:58-117 (hddm_Init) reads
+ * from the part files, for one part.  Global numbering: vertices
+ * 0..n_vertices-1, edges 0..n_edges-1. */
+typedef struct {
+  int32_t n_vertices;
+  const double *vertex_crd;   /* 3*n_vertices */
+  int32_t n_tets;
+  const int32_t *tet_vertices; /* 4*n_tets, positively oriented (tet_Volume6 > 0) */
+  const int32_t *tet_edges;    /* 6*n_tets global edge ids in file order 01,02,03,12,23,13 */
+  const int32_t *tet_flag;     /* n_tets material flags */
+  int32_t n_edges;
+  const uint8_t *pec_edge;     /* n_edges, 1 = edge on the PEC wall (DirichletBCs_Axn0) */
+  int32_t n_subdomains;
+  const int32_t *sub_of_tet;   /* n_tets, subdomain of each element */
+} fwgpu_mesh;
+
+/* Material table: the reference's MTRL (lib/std/types.h:257-279) as read
+ * from mtrl.dat by read_mtrldat_file (lib/std/fileio.c:3474-3572). */
+typedef struct {
+  int32_t n_eps;
+  const int32_t *eps_flag;   /* Permittivity flags */
+  const double *eps;         /* absolute permittivity [F/m] per flag */
+  int32_t n_sigma;
+  const int32_t *sigma_flag; /* Conductor flags */
+  const double *sigma;       /* conductivity [S/m] per flag */
+  double omega;              /* AntennaOmega [rad/s] */
+} fwgpu_material;
+
+/* Right-hand side: edge currents added to the assembled right-hand side of
+ * the lowest-numbered subdomain holding each edge. */
+typedef struct {
+  int32_t n_entries;
+  const int32_t *edge;     /* global edge ids */
+  const double *value;     /* 2*n_entries (re, im) */
+} fwgpu_source;
+
+typedef struct {
+  double hddm_eps;       /* -hddm-eps, max-norm relative residual (default 1e-3) */
+  int32_t hddm_max_loop; /* -hddm-max-loop (default 4000) */
+  int32_t precision;     /* FWGPU_PREC_* */
+  int32_t ir_max_steps;  /* FP32_IR: refinement steps per subdomain solve (>=1) */
+  double ir_tol;         /* FP32_IR: stop refining when the subdomain residual drops below
+                            ir_tol * |rhs| (0 = always ir_max_steps) */
+  int32_t graph_iterations; /* COCG iterations captured per CUDA graph launch */
+  int32_t device;        /* CUDA device ordinal */
+} fwgpu_options;
+
+typedef struct fwgpu_context fwgpu_context;
+
+/* Sizes a caller needs to allocate result buffers and to compute the
+ * roofline of the substitution kernels. */
+typedef struct {
+  int32_t n_subdomains;
+  int32_t total_free;       /* interface DOFs ("DOF on interface", hddm_solver.h:90) */
+  int64_t total_dofs;       /* sum over subdomains of local edge DOFs */
+  int64_t total_interior;   /* sum of non-Dirichlet local DOFs */
+  int64_t nlen_reference;   /* sum of the reference's skyline lengths (advlas_skyline.c:24) */
+  int64_t nlen_interior;    /* sum of stored interior envelope lengths */
+  int64_t nnz_lower;        /* sum of stored lower-triangle entries of the assembled matrices */
+  int64_t nnz_interface_rows; /* entries of the interface-row operator used per iteration */
+  int64_t nnz_coupling;     /* entries of the interior-interface coupling used per iteration */
+  int64_t nnz_interior;     /* entries of the interior operator used by refinement */
+  int32_t max_local_dofs;
+  int32_t max_interior;
+} fwgpu_sizes;
+
+typedef struct {
+  int32_t iterations;      /* COCG iterations done (hddm_sw.loop - 1 at exit) */
+  int32_t converged;       /* 1 if resi < hddm_eps */
+  double initial_norm;     /* max|r0| ("# Norm", hddm_solver_s.h:205) */
+  double final_resi;       /* max|r|/max|r0| at exit */
+  double final_resi_l2;    /* ||r||_2/||r0||_2 at exit */
+  double t_setup_ms;       /* assembly + factor + first solve, device time */
+  double t_iterate_ms;     /* COCG loop, device time */
+  double t_last_ms;        /* final subdomain solves, device time */
+} fwgpu_result;
+
+/* -- lifecycle ----------------------------------------------------------- */
+
+/* Builds every subdomain's local numbering, Dirichlet list and interface maps
+ * on the host (make_PartMesh_FW, lib/hddm/make_PartMesh.c:1201-1241, with
+ * make_PartMesh_FW_TetQ :1628-1707 and the inner-BC renumbering :158-858 for
+ * one part) and uploads mesh and material to the device. */
+int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mtrl, const fwgpu_options *opts,
+                 fwgpu_context **out);
+int fwgpu_destroy(fwgpu_context *ctx);
+int fwgpu_get_sizes(const fwgpu_context *ctx, fwgpu_sizes *sizes);
+/* Last CUDA/library error as text (never NULL). */
+const char *fwgpu_last_error(void);
+int fwgpu_abi_version(void);
+
+/* -- reference plug-in slots, batched over all subdomains ----------------- */
+
+/* make_TMP_AIJ: HDDM_make_TMP_AIJ_em_E (main/fullwave/fullwave.c:221-259):
+ * element matrices tet_MakeElement_EM_E (lib/fem/make_elem_em.c:14-400)
+ * summed into each subdomain's lower-triangle rows in element order, exact
+ * zeros removed (aij_matrix_func.h:260-391), plus the source right-hand side. */
+int fwgpu_make_tmp_aij(fwgpu_context *ctx, const fwgpu_source *src);
+
+/* solve_dom_1st: hddm_solver_CS_solve_dom_1st_d (lib/hddm/hddm_solver.h:461-555)
+ * for every subdomain: Dirichlet elimination, skyline envelope
+ * (advlas_skyline.c:12-60), LDL^T factor (advlas_skyline.c:79-128), first
+ * solve, vec = A x - b, the diagonal preconditioner (hddm_pc.h:52-86), and
+ * the scatter-add into Q and PC (hddm_solver_sp.h:8-25). */
+int fwgpu_solve_dom_1st(fwgpu_context *ctx);
+
+/* iteration_s_1st: ITERATION_S_1ST (lib/hddm/hddm_solver_s.h:158-256) with
+ * DIAG_GATHER_S (hddm_pc.h:108-137). */
+int fwgpu_iteration_s_1st(fwgpu_context *ctx, int32_t *status);
+
+/* One HDDM step: renewal_bc_sp + solve_dom + COM_res_sp for every subdomain
+ * (hddm_solver_s.h:69-112, hddm_solver.h:559-622, hddm_solver_sp.h:28-69)
+ * followed by iteration_s (hddm_solver_s.h:260-400).  status receives 1 when
+ * the residual reached hddm_eps. */
+int fwgpu_iteration_s(fwgpu_context *ctx, int32_t *status);
+
+/* solve_dom_last: hddm_solver_CS_solve_dom_last_d (hddm_solver.h:626-693)
+ * with the converged interface values, then get_result_sp
+ * (main/fullwave/fullwave.c:500-514). */
+int fwgpu_solve_dom_last(fwgpu_context *ctx);
+
+/* -- batched driver ------------------------------------------------------- */
+
+/* hddm_solver_CS (lib/hddm/hddm_solver.h:25-183, s-mode loop
+ * hddm_solver_s.h): make_tmp_aij, solve_dom_1st, iteration_s_1st, iterations
+ * captured in CUDA graphs until hddm_eps or hddm_max_loop, solve_dom_last.
+ * Returns FWGPU_ERR_NOT_CONVERGED (with the result filled) when the loop
+ * hits hddm_max_loop. */
+int fwgpu_hddm_solve(fwgpu_context *ctx, const fwgpu_source *src, fwgpu_result *result);
+
+/* Re-run only the interface iteration and last step for a new right-hand side
+ * on the existing factors (multi-source runs). */
+int fwgpu_hddm_resolve(fwgpu_context *ctx, const fwgpu_source *src, fwgpu_result *result);
+
+/* -- results -------------------------------------------------------------- */
+
+/* Edge solution per global edge (2*n_edges doubles).  Every subdomain holding
+ * an edge computes the same value; the lowest-numbered one is returned. */
+int fwgpu_get_edge_solution(fwgpu_context *ctx, double *x_edges);
+/* Residual history: resi per iteration (hddm_solver_s.h:319-323),
+ * up to max_n entries; n_out receives the count. */
+int fwgpu_get_history(fwgpu_context *ctx, double *resi, int32_t max_n, int32_t *n_out);
+
+/* -- introspection for parity tests -------------------------------------- */
+
+/* Integer maps of subdomain s as the reference's make_PartMesh leaves them:
+ * nop (10*nel, after make_MESH_change_nop), Dirichlet list ibc (nbc, PEC
+ * then interface), inbc (nfid, ln_part pairs), and the global edge id of each
+ * local edge DOF.  Pass NULL buffers to query the counts. */
+int fwgpu_get_subdomain_maps(const fwgpu_context *ctx, int32_t s, int32_t *nel, int32_t *nmp, int32_t *nbc,
+                             int32_t *ninbc, int32_t *nop, int32_t *ibc, int32_t *inbc_nfid,
+                             int32_t *inbc_ln_part, int32_t *edge_gid);
+/* The reference's skyline profile of subdomain s after Dirichlet elimination:
+ * idx1[n], idx2[n] and nlen (advlas_skyline.c:12-25). */
+int fwgpu_get_skyline_profile(fwgpu_context *ctx, int32_t s, int32_t *idx1, int32_t *idx2, int32_t *nlen);
+/* Assembled lower rows of subdomain s (row_ptr[n+1], col[nnz], val[2*nnz]) and
+ * right-hand side b[2n]; pass NULL to query nnz through *nnz. */
+int fwgpu_get_tmp_aij(fwgpu_context *ctx, int32_t s, int32_t *nnz, int32_t *row_ptr, int32_t *col, double *val,
+                      double *b);
+/* FP64 factor of subdomain s in the reference's skyline layout
+ * (mat[idx2[i]+j], 1/d on the diagonal); nlen complex values. */
+int fwgpu_get_factor(fwgpu_context *ctx, int32_t s, double *mat);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FWGPU_H */

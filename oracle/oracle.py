@@ -1,0 +1,233 @@
+"""CPU oracle of the full-wave HDDM hot path.
+
+TEST INFRASTRUCTURE ONLY: used by tests/, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` as the checker; the product never
+imports it.  Two parts:
+
+* ``partition`` restates, in numpy, the integer setup the reference's
+  ``make_PartMesh_FW`` (``lib/hddm/make_PartMesh.c:1201-1241``) performs for
+  one part: subdomain-local vertex and edge numbering in subdomain node order
+  (``make_MESH_make_ap``/``change_ap``, ``lib/fem/make_MESH.c:237-272,539-552``),
+  the slot-8/9 swap of ``nop`` (``make_MESH.c:556-585``), the interface DOFs
+  (mid-nodes shared by subdomains, PEC ones excluded, part-interface order,
+  ``make_PartMesh.c:158-748``) and the Dirichlet list with the interface DOFs
+  last (``make_PartMesh.c:1068-1194``).
+* ``hddm`` runs ``oracle/fw_oracle.c`` (built into ``oracle/liboracle.so``),
+  the C restatement of the reference's assembly, skyline LDL^T and s-mode
+  COCG, on those arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+from typing import List
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+FILE_SLOT = np.array([0, 1, 2, 3, 5, 4])  # tet_n slot -> file mid-node
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "fw_oracle.c")
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+        # gcc -O2 as the reference's Makefile.in:33
+        subprocess.run(["gcc", "-O2", "-shared", "-fPIC", "-o", LIB, src, "-lm"], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(LIB)
+    return _lib
+
+
+@dataclass
+class SubData:
+    els: np.ndarray        # global element ids
+    nop: np.ndarray        # (nel, 10) local ids after the slot swap
+    crd: np.ndarray        # (nap, 3) local vertex coordinates
+    eps: np.ndarray        # (nel,)
+    sigma: np.ndarray      # (nel,)
+    edge_gid: np.ndarray   # (nmp,) global edge id of each local edge
+    ibc: np.ndarray        # Dirichlet list: PEC (sorted) then interface (sorted)
+    inbc_nfid: np.ndarray  # sorted local ids of interface DOFs
+    inbc_ln: np.ndarray    # their part-interface numbers
+    b: np.ndarray          # (nmp,) complex assembled source right-hand side
+
+
+@dataclass
+class Partition:
+    subs: List[SubData]
+    tfree: int
+    iface_gid: np.ndarray
+
+
+def material_per_element(model) -> tuple:
+    """First match of each element flag in the Permittivity and Conductor
+    tables (``lib/fem/make_elem_em.c:98-109``)."""
+    eps = np.zeros(model.n_tets)
+    sig = np.zeros(model.n_tets)
+    # the tables have unique flags, so a dictionary lookup is the first match
+    emap = {}
+    for f, e in zip(model.mat_flag.tolist(), model.mat_eps.tolist()):
+        emap.setdefault(f, e)
+    smap = {}
+    for f, s in zip(model.mat_flag.tolist(), model.mat_sigma.tolist()):
+        smap.setdefault(f, s)
+    fl = model.flag.tolist()
+    eps[:] = [emap.get(f, 0.0) for f in fl]
+    sig[:] = [smap.get(f, 0.0) for f in fl]
+    return eps, sig
+
+
+def partition(model, source=0) -> Partition:
+    nv = model.n_vertices
+    ne = model.n_edges
+    nsub = model.nsub
+    order = np.argsort(model.sub_of_tet, kind="stable")
+    counts = np.bincount(model.sub_of_tet, minlength=nsub)
+    starts = np.concatenate([[0], np.cumsum(counts)])
+    eps, sig = material_per_element(model)
+    held = np.zeros(ne, dtype=np.int64)
+    owner = np.full(ne, -1, dtype=np.int64)
+    sub_edges = []
+    for s in range(nsub):
+        els = order[starts[s]:starts[s + 1]]
+        e = np.unique(model.tet_edges[els])
+        sub_edges.append(e)
+        held[e] += 1
+        new = owner[e] < 0
+        owner[e[new]] = s
+    iface = (held >= 2) & ~model.pec_edge
+    iface_gid = np.nonzero(iface)[0]
+    ln_of = np.full(ne, -1, dtype=np.int64)
+    ln_of[iface_gid] = np.arange(iface_gid.shape[0])
+    if source is None:
+        src_e, src_v = np.zeros(0, np.int64), np.zeros(0, np.complex128)
+    elif isinstance(source, int):
+        src_e, src_v = model.sources[source]
+    else:
+        src_e, src_v = source
+    subs = []
+    for s in range(nsub):
+        els = order[starts[s]:starts[s + 1]]
+        e = sub_edges[s]
+        v = np.unique(model.tets[els])
+        eloc = {int(g): i for i, g in enumerate(e.tolist())}
+        vloc = np.full(nv, -1, dtype=np.int64)
+        vloc[v] = np.arange(v.shape[0])
+        nop = np.empty((els.shape[0], 10), dtype=np.int32)
+        nop[:, :4] = vloc[model.tets[els]]
+        te = model.tet_edges[els][:, FILE_SLOT]
+        nop[:, 4:] = np.searchsorted(e, te)
+        pec_l = np.nonzero(model.pec_edge[e])[0]
+        if_l = np.nonzero(iface[e])[0]
+        b = np.zeros(e.shape[0], dtype=np.complex128)
+        for g, val in zip(np.asarray(src_e).tolist(), np.asarray(src_v).tolist()):
+            if owner[g] == s:
+                b[eloc[g]] += val
+        subs.append(SubData(els=els, nop=nop, crd=model.vertex_crd[v], eps=eps[els], sigma=sig[els], edge_gid=e,
+                            ibc=np.concatenate([pec_l, if_l]).astype(np.int32), inbc_nfid=if_l.astype(np.int32),
+                            inbc_ln=ln_of[e[if_l]].astype(np.int32), b=b))
+    return Partition(subs=subs, tfree=int(iface_gid.shape[0]), iface_gid=iface_gid)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def hddm(model, part: Partition, hddm_eps: float = 1e-3, hddm_max_loop: int = 4000):
+    """The reference's s-mode HDDM solve on ``part``.  Returns
+    (per-edge solution (global edge ids, lowest subdomain's value),
+    per-subdomain solutions, residual history, initial norm)."""
+    lib = load()
+    subs = part.subs
+    nsub = len(subs)
+    i32, f64 = ctypes.c_int32, ctypes.c_double
+    nel = np.array([s.nop.shape[0] for s in subs], np.int32)
+    nap = np.array([s.crd.shape[0] for s in subs], np.int32)
+    nmp = np.array([s.edge_gid.shape[0] for s in subs], np.int32)
+    nbc = np.array([s.ibc.shape[0] for s in subs], np.int32)
+    nin = np.array([s.inbc_nfid.shape[0] for s in subs], np.int32)
+    nop = np.ascontiguousarray(np.concatenate([s.nop for s in subs]), np.int32)
+    crd = np.ascontiguousarray(np.concatenate([s.crd for s in subs]), np.float64)
+    eps = np.ascontiguousarray(np.concatenate([s.eps for s in subs]), np.float64)
+    sig = np.ascontiguousarray(np.concatenate([s.sigma for s in subs]), np.float64)
+    ibc = np.ascontiguousarray(np.concatenate([s.ibc for s in subs]), np.int32)
+    nf = np.ascontiguousarray(np.concatenate([s.inbc_nfid for s in subs]), np.int32)
+    ln = np.ascontiguousarray(np.concatenate([s.inbc_ln for s in subs]), np.int32)
+    bb = np.concatenate([s.b for s in subs])
+    b = np.ascontiguousarray(np.stack([bb.real, bb.imag], 1).ravel(), np.float64)
+    x = np.zeros(2 * int(nmp.sum()), np.float64)
+    hist = np.zeros(max(1, hddm_max_loop) + 1, np.float64)
+    norm0 = ctypes.c_double()
+    lib.orc_hddm.restype = ctypes.c_int
+    it = lib.orc_hddm(nsub, _p(nel, i32), _p(nop, i32), _p(nap, i32), _p(crd, f64), _p(eps, f64), _p(sig, f64),
+                      _p(nmp, i32), _p(nbc, i32), _p(ibc, i32), _p(nin, i32), _p(nf, i32), _p(ln, i32), _p(b, f64),
+                      int(part.tfree), ctypes.c_double(model.omega), ctypes.c_double(hddm_eps), int(hddm_max_loop),
+                      _p(x, f64), _p(hist, f64), ctypes.byref(norm0))
+    if it < 0:
+        raise RuntimeError(f"oracle failed with {it}")
+    xs = x[0::2] + 1j * x[1::2]
+    per_sub = np.split(xs, np.cumsum(nmp)[:-1])
+    xe = np.zeros(model.n_edges, dtype=np.complex128)
+    seen = np.zeros(model.n_edges, dtype=bool)
+    for s, xv in zip(subs, per_sub):
+        new = ~seen[s.edge_gid]
+        xe[s.edge_gid[new]] = xv[new]
+        seen[s.edge_gid] = True
+    return xe, per_sub, hist[:it], norm0.value
+
+
+def assemble_sub(model, sub: SubData):
+    lib = load()
+    i32, f64 = ctypes.c_int32, ctypes.c_double
+    nmp = sub.edge_gid.shape[0]
+    nop = np.ascontiguousarray(sub.nop, np.int32)
+    crd = np.ascontiguousarray(sub.crd, np.float64)
+    eps = np.ascontiguousarray(sub.eps, np.float64)
+    sig = np.ascontiguousarray(sub.sigma, np.float64)
+    b = np.ascontiguousarray(np.stack([sub.b.real, sub.b.imag], 1).ravel(), np.float64)
+    cap = 64 * nmp + 64
+    rp = np.zeros(nmp + 1, np.int32)
+    col = np.zeros(cap, np.int32)
+    val = np.zeros(2 * cap, np.float64)
+    bo = np.zeros(2 * nmp, np.float64)
+    lib.orc_assemble_sub.restype = ctypes.c_int
+    n = lib.orc_assemble_sub(int(nop.shape[0]), _p(nop, i32), _p(crd, f64), _p(eps, f64), _p(sig, f64), nmp,
+                             _p(b, f64), ctypes.c_double(model.omega), cap, _p(rp, i32), _p(col, i32), _p(val, f64),
+                             _p(bo, f64))
+    if n < 0:
+        raise RuntimeError("assembly buffer too small")
+    return rp, col[:n], val[0:2 * n:2] + 1j * val[1:2 * n:2], bo[0::2] + 1j * bo[1::2]
+
+
+def factor_sub(model, sub: SubData):
+    lib = load()
+    i32, f64 = ctypes.c_int32, ctypes.c_double
+    nmp = sub.edge_gid.shape[0]
+    nop = np.ascontiguousarray(sub.nop, np.int32)
+    crd = np.ascontiguousarray(sub.crd, np.float64)
+    eps = np.ascontiguousarray(sub.eps, np.float64)
+    sig = np.ascontiguousarray(sub.sigma, np.float64)
+    ibc = np.ascontiguousarray(sub.ibc, np.int32)
+    idx1 = np.zeros(nmp, np.int32)
+    idx2 = np.zeros(nmp, np.int32)
+    lib.orc_factor_sub.restype = ctypes.c_int
+    cap = nmp * (nmp + 1) // 2 + 1
+    mat = np.zeros(2 * cap, np.float64)
+    n = lib.orc_factor_sub(int(nop.shape[0]), _p(nop, i32), _p(crd, f64), _p(eps, f64), _p(sig, f64), nmp,
+                           int(ibc.shape[0]), _p(ibc, i32), ctypes.c_double(model.omega), cap, _p(idx1, i32),
+                           _p(idx2, i32), _p(mat, f64))
+    if n < 0:
+        raise RuntimeError("factor buffer too small")
+    return idx1, idx2, n, mat[0:2 * n:2] + 1j * mat[1:2 * n:2]
