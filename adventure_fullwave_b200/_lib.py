@@ -82,6 +82,11 @@ SIGNATURES = {
     "fwgpu_get_sizes": [ctypes.c_void_p, P(FwSizes)],
     "fwgpu_last_error": [],
     "fwgpu_abi_version": [],
+    "fwgpu_partition_build": [P(FwMesh), P(ctypes.c_void_p)],
+    "fwgpu_partition_destroy": [ctypes.c_void_p],
+    "fwgpu_partition_info": [ctypes.c_void_p, P(c_i32), P(c_i32)],
+    "fwgpu_partition_maps": [ctypes.c_void_p, c_i32, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32),
+                             P(c_i32), P(c_i32), P(c_i32), P(c_i32)],
     "fwgpu_make_tmp_aij": [ctypes.c_void_p, P(FwSource)],
     "fwgpu_solve_dom_1st": [ctypes.c_void_p],
     "fwgpu_iteration_s_1st": [ctypes.c_void_p, P(c_i32)],

@@ -203,34 +203,35 @@ int read_status(fwgpu_context *c, int32_t *status) {
 
 }  // namespace
 
-extern "C" {
+struct fwgpu_partition {
+  fw::Model m;
+  fw::Plan p;
+};
 
-const char *fwgpu_last_error(void) { return g_last_error.c_str(); }
-int fwgpu_abi_version(void) { return FWGPU_ABI_VERSION; }
+static int copy_maps(const fw::Plan &p, int32_t s, int32_t *nel, int32_t *nmp, int32_t *nbc, int32_t *ninbc,
+                     int32_t *nop, int32_t *ibc, int32_t *inbc_nfid, int32_t *inbc_ln_part, int32_t *edge_gid) {
+  if (s < 0 || s >= (int32_t)p.subs.size()) return set_error(FWGPU_ERR_ARG, "bad subdomain");
+  const fw::SubHost &h = p.subs[s];
+  if (nel) *nel = (int32_t)h.els.size();
+  if (nmp) *nmp = h.nmp;
+  if (nbc) *nbc = (int32_t)h.ibc.size();
+  if (ninbc) *ninbc = h.nG;
+  if (nop) std::copy(h.nop.begin(), h.nop.end(), nop);
+  if (ibc) std::copy(h.ibc.begin(), h.ibc.end(), ibc);
+  if (inbc_nfid) std::copy(h.inbc_nfid.begin(), h.inbc_nfid.end(), inbc_nfid);
+  if (inbc_ln_part) std::copy(h.inbc_ln.begin(), h.inbc_ln.end(), inbc_ln_part);
+  if (edge_gid) std::copy(h.edge_gid.begin(), h.edge_gid.end(), edge_gid);
+  return FWGPU_OK;
+}
 
-int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_options *opts, fwgpu_context **out) {
-  if (!mesh || !mt || !opts || !out) return set_error(FWGPU_ERR_ARG, "null argument");
-  *out = nullptr;
-  if (mesh->n_vertices <= 0 || mesh->n_tets <= 0 || mesh->n_edges <= 0 || mesh->n_subdomains <= 0 ||
+static int model_from_mesh(const fwgpu_mesh *mesh, fw::Model &m) {
+  if (!mesh || mesh->n_vertices <= 0 || mesh->n_tets <= 0 || mesh->n_edges <= 0 || mesh->n_subdomains <= 0 ||
       !mesh->vertex_crd || !mesh->tet_vertices || !mesh->tet_edges || !mesh->tet_flag || !mesh->pec_edge ||
       !mesh->sub_of_tet)
     return set_error(FWGPU_ERR_ARG, "incomplete mesh");
-  if (opts->precision != FWGPU_PREC_FP64 && opts->precision != FWGPU_PREC_FP32_IR)
-    return set_error(FWGPU_ERR_ARG, "unknown precision");
-  if (opts->hddm_max_loop < 0) return set_error(FWGPU_ERR_ARG, "negative hddm_max_loop");
   for (int64_t k = 0; k < 4 * (int64_t)mesh->n_tets; k++)
     if (mesh->tet_vertices[k] < 0 || mesh->tet_vertices[k] >= mesh->n_vertices)
       return set_error(FWGPU_ERR_ARG, "tet_vertices out of range");
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
-    return set_error(FWGPU_ERR_CUDA, "no CUDA device");
-  if (opts->device < 0 || opts->device >= ndev) return set_error(FWGPU_ERR_ARG, "bad device ordinal");
-
-  fwgpu_context *c = new fwgpu_context();
-  c->opts = *opts;
-  if (c->opts.graph_iterations <= 0) c->opts.graph_iterations = 16;
-  if (c->opts.ir_max_steps <= 0) c->opts.ir_max_steps = 1;
-  fw::Model &m = c->m;
   m.nv = mesh->n_vertices;
   m.nt = mesh->n_tets;
   m.ne = mesh->n_edges;
@@ -241,6 +242,34 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   m.flag.assign(mesh->tet_flag, mesh->tet_flag + m.nt);
   m.sub_of_tet.assign(mesh->sub_of_tet, mesh->sub_of_tet + m.nt);
   m.pec.assign(mesh->pec_edge, mesh->pec_edge + m.ne);
+  return FWGPU_OK;
+}
+
+extern "C" {
+
+const char *fwgpu_last_error(void) { return g_last_error.c_str(); }
+int fwgpu_abi_version(void) { return FWGPU_ABI_VERSION; }
+
+int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_options *opts, fwgpu_context **out) {
+  if (!mesh || !mt || !opts || !out) return set_error(FWGPU_ERR_ARG, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(FWGPU_ERR_CUDA, "no CUDA device");
+  if (opts->device < 0 || opts->device >= ndev) return set_error(FWGPU_ERR_ARG, "bad device ordinal");
+
+  fwgpu_context *c = new fwgpu_context();
+  c->opts = *opts;
+  if (c->opts.graph_iterations <= 0) c->opts.graph_iterations = 16;
+  if (c->opts.ir_max_steps <= 0) c->opts.ir_max_steps = 1;
+  fw::Model &m = c->m;
+  {
+    int rc = model_from_mesh(mesh, m);
+    if (rc != FWGPU_OK) {
+      delete c;
+      return rc;
+    }
+  }
   m.omega = mt->omega;
   resolve_material(m, mesh, mt);
   std::string err = fw::build_plan(m, c->p);
@@ -357,6 +386,11 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   dp.hist = c->d_hist;
   dp.ir_steps = c->opts.ir_max_steps;
   dp.ir_tol = c->opts.ir_tol;
+  {
+    const bool fp32 = opts->precision == FWGPU_PREC_FP32_IR;
+    const size_t smem = fw::subsolve_smem_bytes(p.max_interior, p.max_iface, fp32);
+    dp.cta_smem = fw::configure_subsolve(smem) == 0 ? (int32_t)smem : 0;
+  }
   // per-edge solution source: the first subdomain holding each edge
   std::vector<int64_t> esrc(m.ne, -1);
   std::vector<uint8_t> seen(m.ne, 0);
@@ -378,6 +412,43 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   FW_TRY(c->alloc(&c->d_xedge, m.ne));
   FW_CUDA(cudaStreamSynchronize(c->stream));
   return FWGPU_OK;
+}
+
+int fwgpu_partition_build(const fwgpu_mesh *mesh, fwgpu_partition **out) {
+  if (!out) return set_error(FWGPU_ERR_ARG, "null argument");
+  *out = nullptr;
+  fwgpu_partition *part = new fwgpu_partition();
+  int rc = model_from_mesh(mesh, part->m);
+  if (rc != FWGPU_OK) {
+    delete part;
+    return rc;
+  }
+  std::string err = fw::build_plan(part->m, part->p);
+  if (!err.empty()) {
+    delete part;
+    return set_error(FWGPU_ERR_ARG, err);
+  }
+  *out = part;
+  return FWGPU_OK;
+}
+
+int fwgpu_partition_destroy(fwgpu_partition *part) {
+  delete part;
+  return FWGPU_OK;
+}
+
+int fwgpu_partition_info(const fwgpu_partition *part, int32_t *n_subdomains, int32_t *total_free) {
+  if (!part) return set_error(FWGPU_ERR_ARG, "null partition");
+  if (n_subdomains) *n_subdomains = part->m.nsub;
+  if (total_free) *total_free = part->p.total_free;
+  return FWGPU_OK;
+}
+
+int fwgpu_partition_maps(const fwgpu_partition *part, int32_t s, int32_t *nel, int32_t *nmp, int32_t *nbc,
+                         int32_t *ninbc, int32_t *nop, int32_t *ibc, int32_t *inbc_nfid, int32_t *inbc_ln_part,
+                         int32_t *edge_gid) {
+  if (!part) return set_error(FWGPU_ERR_ARG, "null partition");
+  return copy_maps(part->p, s, nel, nmp, nbc, ninbc, nop, ibc, inbc_nfid, inbc_ln_part, edge_gid);
 }
 
 int fwgpu_destroy(fwgpu_context *c) {
@@ -677,18 +748,8 @@ int fwgpu_get_history(fwgpu_context *c, double *resi, int32_t max_n, int32_t *n_
 int fwgpu_get_subdomain_maps(const fwgpu_context *c, int32_t s, int32_t *nel, int32_t *nmp, int32_t *nbc,
                              int32_t *ninbc, int32_t *nop, int32_t *ibc, int32_t *inbc_nfid, int32_t *inbc_ln_part,
                              int32_t *edge_gid) {
-  if (!c || s < 0 || s >= c->m.nsub) return set_error(FWGPU_ERR_ARG, "bad subdomain");
-  const fw::SubHost &h = c->p.subs[s];
-  if (nel) *nel = (int32_t)h.els.size();
-  if (nmp) *nmp = h.nmp;
-  if (nbc) *nbc = (int32_t)h.ibc.size();
-  if (ninbc) *ninbc = h.nG;
-  if (nop) std::copy(h.nop.begin(), h.nop.end(), nop);
-  if (ibc) std::copy(h.ibc.begin(), h.ibc.end(), ibc);
-  if (inbc_nfid) std::copy(h.inbc_nfid.begin(), h.inbc_nfid.end(), inbc_nfid);
-  if (inbc_ln_part) std::copy(h.inbc_ln.begin(), h.inbc_ln.end(), inbc_ln_part);
-  if (edge_gid) std::copy(h.edge_gid.begin(), h.edge_gid.end(), edge_gid);
-  return FWGPU_OK;
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  return copy_maps(c->p, s, nel, nmp, nbc, ninbc, nop, ibc, inbc_nfid, inbc_ln_part, edge_gid);
 }
 
 int fwgpu_get_skyline_profile(fwgpu_context *c, int32_t s, int32_t *idx1, int32_t *idx2, int32_t *nlen) {

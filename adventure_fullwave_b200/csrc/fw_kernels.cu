@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "fw_kernels.cuh"
 
@@ -338,6 +339,279 @@ __global__ void __launch_bounds__(kThreads) subsolve_kernel(DevProblem p, int mo
 }
 
 // ----------------------------------------------------------------------------
+// Block-row envelope substitutions, one CTA per subdomain.
+//
+// Rows are taken in blocks of 32.  Forward: the rectangle left of the block
+// (columns < r0) is a set of independent dot products, spread over all warps;
+// the 32x32 triangle inside the block is then resolved by one warp with
+// shuffles from a padded shared-memory tile (row stride 33 keeps both the
+// column-wise forward reads and the row-wise backward reads free of bank
+// conflicts).  Backward: the block's triangle first, then the transposed
+// rectangle update of the columns left of the block, spread over all threads.
+// The interior vector, the interface values and the row metadata of the
+// subdomain stay in shared memory; the factor streams from global memory.
+constexpr int kRB = 32;       // rows per block
+constexpr int kTriStride = 33;
+constexpr int kCtaThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ T shfl_idx(T v, int src);
+template <>
+__device__ __forceinline__ double2 shfl_idx(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+template <>
+__device__ __forceinline__ float2 shfl_idx(float2 v, int src) {
+  return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+template <typename T>
+__device__ __forceinline__ T from_d2(double2 a);
+template <>
+__device__ __forceinline__ double2 from_d2<double2>(double2 a) {
+  return a;
+}
+template <>
+__device__ __forceinline__ float2 from_d2<float2>(double2 a) {
+  return make_float2((float)a.x, (float)a.y);
+}
+
+struct CtaMeta {
+  const int32_t *lo;   // shared: first stored column of each interior row
+  const int32_t *pr;   // shared: row start (column lo) relative to the subdomain base
+  const int32_t *bmin; // shared: smallest lo of each row block
+  int nI;
+};
+
+template <typename T>
+__device__ void cta_forward(const CtaMeta &m, const T *__restrict__ L, T *y, T *tri, T *rect) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  for (int r0 = 0; r0 < m.nI; r0 += kRB) {
+    const int nb = min(kRB, m.nI - r0);
+    for (int t = warp; t < nb; t += nw) {
+      const int i = r0 + t;
+      const int lo_i = m.lo[i];
+      const T *row = L + m.pr[i] - lo_i;
+      T acc = czero<T>();
+      for (int k = lo_i + lane; k < r0; k += 32) acc = cadd(acc, cmul(row[k], y[k]));
+      acc = warp_sum(acc);
+      if (lane == 0) rect[t] = acc;
+      const int col = r0 + lane;
+      tri[t * kTriStride + lane] = (col < i && col >= lo_i) ? row[col] : czero<T>();
+    }
+    __syncthreads();
+    if (warp == 0) {
+      T acc = lane < nb ? csub(y[r0 + lane], rect[lane]) : czero<T>();
+      for (int j = 0; j < nb - 1; j++) {
+        const T yj = shfl_idx(acc, j);
+        if (lane > j) acc = csub(acc, cmul(tri[lane * kTriStride + j], yj));
+      }
+      if (lane < nb) y[r0 + lane] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__device__ void cta_diag(const CtaMeta &m, const T *__restrict__ L, T *y) {
+  for (int i = threadIdx.x; i < m.nI; i += blockDim.x) y[i] = cmul(y[i], L[m.pr[i] + (i - m.lo[i])]);
+  __syncthreads();
+}
+
+template <typename T>
+__device__ void cta_backward(const CtaMeta &m, const T *__restrict__ L, T *y, T *tri) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  const int nblk = (m.nI + kRB - 1) / kRB;
+  for (int blk = nblk - 1; blk >= 0; blk--) {
+    const int r0 = blk * kRB;
+    const int nb = min(kRB, m.nI - r0);
+    for (int t = warp; t < nb; t += nw) {
+      const int i = r0 + t;
+      const int lo_i = m.lo[i];
+      const T *row = L + m.pr[i] - lo_i;
+      const int col = r0 + lane;
+      tri[t * kTriStride + lane] = (col < i && col >= lo_i) ? row[col] : czero<T>();
+    }
+    __syncthreads();
+    if (warp == 0) {
+      T val = lane < nb ? y[r0 + lane] : czero<T>();
+      for (int i = nb - 1; i >= 1; i--) {
+        const T xi = shfl_idx(val, i);
+        if (lane < i) val = csub(val, cmul(tri[i * kTriStride + lane], xi));
+      }
+      if (lane < nb) y[r0 + lane] = val;
+    }
+    __syncthreads();
+    const int kmin = m.bmin[blk];
+    for (int k = kmin + tid; k < r0; k += blockDim.x) {
+      T acc = czero<T>();
+      for (int t = 0; t < nb; t++) {
+        const int i = r0 + t;
+        const int lo_i = m.lo[i];
+        if (k >= lo_i) acc = cadd(acc, cmul(L[m.pr[i] + (k - lo_i)], y[i]));
+      }
+      y[k] = csub(y[k], acc);
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void cta_solve(const CtaMeta &m, const T *__restrict__ L, T *y, T *tri, T *rect) {
+  cta_forward<T>(m, L, y, tri, rect);
+  cta_diag<T>(m, L, y);
+  cta_backward<T>(m, L, y, tri);
+}
+
+// Shared-memory bytes of one subdomain CTA.
+__host__ __device__ inline size_t cta_smem_bytes(int nI, int nG, bool fp32) {
+  const int nblk = (nI + kRB - 1) / kRB;
+  size_t b = 0;
+  b += (size_t)nI * 8 + (size_t)nblk * 4;        // lo, pr, bmin
+  b = (b + 15) & ~(size_t)15;
+  b += (size_t)nG * 16;                           // v
+  if (fp32) {
+    b += (size_t)nI * 32;                         // x, b (FP64)
+    b += (size_t)nI * 8;                          // y (FP32)
+    b += (size_t)kRB * kTriStride * 8 + kRB * 8;  // tri, rect
+  } else {
+    b += (size_t)nI * 16;                         // y
+    b += (size_t)kRB * kTriStride * 16 + kRB * 16;
+  }
+  return b + 64;
+}
+
+template <bool kFp32>
+__global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p, int mode) {
+  using LT = typename std::conditional<kFp32, float2, double2>::type;
+  if (mode == kModeIter && p.sc->status != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s = p.sub_order[blockIdx.x];
+  const int64_t io = p.int_off[s], go = p.if_off[s];
+  const int nI = (int)(p.int_off[s + 1] - io);
+  const int nG = (int)(p.if_off[s + 1] - go);
+  const int nblk = (nI + kRB - 1) / kRB;
+  const int tid = threadIdx.x;
+  // shared layout
+  int32_t *lo = (int32_t *)smem_raw;
+  int32_t *pr = lo + nI;
+  int32_t *bmin = pr + nI;
+  size_t off = ((size_t)nI * 8 + (size_t)nblk * 4 + 15) & ~(size_t)15;
+  double2 *v = (double2 *)(smem_raw + off);
+  off += (size_t)nG * 16;
+  double2 *xd = nullptr, *bd = nullptr;
+  if (kFp32) {
+    xd = (double2 *)(smem_raw + off);
+    off += (size_t)nI * 16;
+    bd = (double2 *)(smem_raw + off);
+    off += (size_t)nI * 16;
+  }
+  LT *y = (LT *)(smem_raw + off);
+  off += (size_t)nI * sizeof(LT);
+  LT *tri = (LT *)(smem_raw + off);
+  off += (size_t)kRB * kTriStride * sizeof(LT);
+  LT *rect = (LT *)(smem_raw + off);
+
+  const int64_t base = nI > 0 ? p.env_ptr[io] : 0;
+  for (int i = tid; i < nI; i += blockDim.x) {
+    lo[i] = p.env_lo[io + i];
+    pr[i] = (int32_t)(p.env_ptr[io + i] - base);
+  }
+  const bool with_bc = mode != kModeFirst;
+  const bool with_f = mode != kModeIter;
+  for (int k = tid; k < nG; k += blockDim.x) v[k] = with_bc ? p.P[p.if_ln[go + k]] : cz();
+  __syncthreads();
+  for (int b = tid; b < nblk; b += blockDim.x) {
+    int mn = b * kRB;
+    const int e = min(nI, (b + 1) * kRB);
+    for (int i = b * kRB; i < e; i++) mn = min(mn, lo[i]);
+    bmin[b] = mn;
+  }
+  // Dirichlet elimination: interior right-hand side f_I - A_IG v
+  const int32_t *cptr = p.cpl_ptr + io + s;
+  const int64_t cbase = p.cpl_off[s];
+  for (int c = tid; c < nI; c += blockDim.x) {
+    double2 acc = with_f ? p.fI[io + c] : cz();
+    for (int q = cptr[c]; q < cptr[c + 1]; q++) acc = csub(acc, cmul(p.cpl_val[cbase + q], v[p.cpl_col[cbase + q]]));
+    if (kFp32) bd[c] = acc;
+    y[c] = from_d2<LT>(acc);
+  }
+  __syncthreads();
+  CtaMeta m{lo, pr, bmin, nI};
+  if (!kFp32) {
+    cta_solve<LT>(m, (const LT *)p.L64 + base, y, tri, rect);
+  } else {
+    const LT *L = (const LT *)p.L32 + base;
+    cta_solve<LT>(m, L, y, tri, rect);
+    for (int c = tid; c < nI; c += blockDim.x) xd[c] = make_double2((double)y[c].x, (double)y[c].y);
+    __syncthreads();
+    const int32_t *aptr = p.aii_ptr + io + s;
+    const int64_t abase = p.aii_off[s];
+    __shared__ double red[kCtaThreads / 32];
+    __shared__ int stop;
+    for (int step = 0; step < p.ir_steps; step++) {
+      // FP64 residual of the subdomain system, rounded into the FP32 work vector
+      double rn = 0.0;
+      for (int c = tid; c < nI; c += blockDim.x) {
+        double2 r = bd[c];
+        for (int q = aptr[c]; q < aptr[c + 1]; q++) r = csub(r, cmul(p.aii_val[abase + q], xd[p.aii_col[abase + q]]));
+        y[c] = from_d2<LT>(r);
+        rn = fmax(rn, fabs(r.x) + fabs(r.y));
+      }
+      if (p.ir_tol > 0.0) {
+        double bn = 0.0;
+        for (int c = tid; c < nI; c += blockDim.x) bn = fmax(bn, fabs(bd[c].x) + fabs(bd[c].y));
+        for (int o2 = 16; o2 > 0; o2 >>= 1) {
+          rn = fmax(rn, __shfl_xor_sync(0xffffffffu, rn, o2));
+          bn = fmax(bn, __shfl_xor_sync(0xffffffffu, bn, o2));
+        }
+        if ((tid & 31) == 0) red[tid >> 5] = rn <= p.ir_tol * bn ? 1.0 : 0.0;
+        __syncthreads();
+        if (tid == 0) {
+          int all = 1;
+          for (int w = 0; w < (int)(blockDim.x >> 5); w++) all &= red[w] > 0.5;
+          stop = all;
+        }
+        __syncthreads();
+        if (stop) break;
+      }
+      __syncthreads();
+      cta_solve<LT>(m, L, y, tri, rect);
+      for (int c = tid; c < nI; c += blockDim.x)
+        xd[c] = cadd(xd[c], make_double2((double)y[c].x, (double)y[c].y));
+      __syncthreads();
+    }
+  }
+  // q = A_G. x (- f_G)
+  const int32_t *rptr = p.ifr_ptr + go + s;
+  const int64_t rbase = p.ifr_off[s];
+  double2 *yout = p.Y + io;
+  for (int k = tid; k < nG; k += blockDim.x) {
+    double2 acc = cz();
+    for (int q = rptr[k]; q < rptr[k + 1]; q++) {
+      const int c = p.ifr_col[rbase + q];
+      double2 xv;
+      if (c >= 0) {
+        if (kFp32)
+          xv = xd[c];
+        else
+          xv = make_double2((double)y[c].x, (double)y[c].y);
+      } else {
+        xv = v[-c - 1];
+      }
+      acc = cadd(acc, cmul(p.ifr_val[rbase + q], xv));
+    }
+    if (with_f) acc = csub(acc, p.fG[go + k]);
+    p.qloc[go + k] = acc;
+  }
+  if (mode == kModeLast) {
+    for (int c = tid; c < nI; c += blockDim.x)
+      yout[c] = kFp32 ? xd[c] : make_double2((double)y[c].x, (double)y[c].y);
+    for (int k = tid; k < nG; k += blockDim.x) p.V[go + k] = v[k];
+  }
+}
+
+// ----------------------------------------------------------------------------
 // interface COCG (ITERATION_S_1ST / ITERATION_S, hddm_solver_s.h:158-400)
 
 constexpr int kRedThreads = 256;
@@ -617,12 +891,31 @@ void launch_to_fp32(int64_t n, const double2 *src, float2 *dst, cudaStream_t str
   to_fp32_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(n, src, dst);
 }
 
+size_t subsolve_smem_bytes(int max_interior, int max_iface, bool fp32) {
+  return cta_smem_bytes(max_interior, max_iface, fp32);
+}
+
 void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stream) {
+  if (p.cta_smem > 0) {
+    if (fp32)
+      subsolve_cta_kernel<true><<<p.nsub, kCtaThreads, p.cta_smem, stream>>>(p, mode);
+    else
+      subsolve_cta_kernel<false><<<p.nsub, kCtaThreads, p.cta_smem, stream>>>(p, mode);
+    return;
+  }
+  // subdomains too large for one CTA's shared memory: one warp each, vectors in global memory
   const unsigned nb = blocks_for((int64_t)p.nsub * 32, kThreads);
   if (fp32)
     subsolve_kernel<true><<<nb, kThreads, 0, stream>>>(p, mode);
   else
     subsolve_kernel<false><<<nb, kThreads, 0, stream>>>(p, mode);
+}
+
+int configure_subsolve(size_t smem) {
+  if (smem > 227 * 1024) return -1;
+  cudaError_t e1 = cudaFuncSetAttribute(subsolve_cta_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e2 = cudaFuncSetAttribute(subsolve_cta_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return (e1 == cudaSuccess && e2 == cudaSuccess) ? 0 : -2;
 }
 
 void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream) {

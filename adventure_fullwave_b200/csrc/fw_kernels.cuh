@@ -73,6 +73,7 @@ struct DevProblem {
   int32_t n_part_blocks;
   int32_t ir_steps;
   double ir_tol;
+  int32_t cta_smem;              // dynamic shared bytes of the CTA-per-subdomain solve (0: warp path)
 };
 
 enum SolveMode { kModeFirst = 0, kModeIter = 1, kModeLast = 2 };
@@ -92,6 +93,8 @@ void launch_factor(const DevProblem &p, const int64_t *int_off, const int32_t *e
                    double2 *L, int32_t *status, cudaStream_t stream);
 void launch_to_fp32(int64_t n, const double2 *src, float2 *dst, cudaStream_t stream);
 void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stream);
+size_t subsolve_smem_bytes(int max_interior, int max_iface, bool fp32);
+int configure_subsolve(size_t smem);
 void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream);
 void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream);
 void launch_edge_solution(int64_t ne, const int64_t *edge_src, const double2 *Y, const double2 *V, double2 *x,

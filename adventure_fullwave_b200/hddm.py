@@ -45,6 +45,68 @@ class HddmResult:
     t_last_ms: float
 
 
+def _mesh_struct(model):
+    a = {}
+    a["crd"] = np.ascontiguousarray(model.vertex_crd, dtype=np.float64)
+    a["tv"] = np.ascontiguousarray(model.tets, dtype=np.int32)
+    a["te"] = np.ascontiguousarray(model.tet_edges, dtype=np.int32)
+    a["flag"] = np.ascontiguousarray(model.flag, dtype=np.int32)
+    a["pec"] = np.ascontiguousarray(model.pec_edge, dtype=np.uint8)
+    a["sub"] = np.ascontiguousarray(model.sub_of_tet, dtype=np.int32)
+    mesh = _lib.FwMesh(
+        int(a["crd"].shape[0]), _ptr(a["crd"], ctypes.c_double), int(a["tv"].shape[0]),
+        _ptr(a["tv"], ctypes.c_int32), _ptr(a["te"], ctypes.c_int32), _ptr(a["flag"], ctypes.c_int32),
+        int(a["pec"].shape[0]), _ptr(a["pec"], ctypes.c_uint8), int(model.nsub), _ptr(a["sub"], ctypes.c_int32))
+    return mesh, a
+
+
+def _maps(fn, handle, s: int) -> dict:
+    nel, nmp, nbc, ninbc = (ctypes.c_int32() for _ in range(4))
+    _lib.check(fn(handle, s, ctypes.byref(nel), ctypes.byref(nmp), ctypes.byref(nbc), ctypes.byref(ninbc), None,
+                  None, None, None, None))
+    nop = np.zeros(10 * nel.value, np.int32)
+    ibc = np.zeros(max(1, nbc.value), np.int32)
+    nf = np.zeros(max(1, ninbc.value), np.int32)
+    ln = np.zeros(max(1, ninbc.value), np.int32)
+    gid = np.zeros(max(1, nmp.value), np.int32)
+    i32 = ctypes.c_int32
+    _lib.check(fn(handle, s, None, None, None, None, _ptr(nop, i32), _ptr(ibc, i32), _ptr(nf, i32), _ptr(ln, i32),
+                  _ptr(gid, i32)))
+    return dict(nel=nel.value, nmp=nmp.value, nop=nop.reshape(-1, 10), ibc=ibc[: nbc.value],
+                inbc_nfid=nf[: ninbc.value], inbc_ln_part=ln[: ninbc.value], edge_gid=gid[: nmp.value])
+
+
+class Partition:
+    """Host-only integer setup (the reference's make_PartMesh_FW for one
+    part): subdomain-local numbering, Dirichlet lists and interface maps.
+    Needs no GPU."""
+
+    def __init__(self, model):
+        self._lib = _lib.load()
+        mesh, keep = _mesh_struct(model)
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.fwgpu_partition_build(ctypes.byref(mesh), ctypes.byref(h)))
+        self._h = h
+        ns, tf = ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_partition_info(h, ctypes.byref(ns), ctypes.byref(tf)))
+        self.n_subdomains = ns.value
+        self.total_free = tf.value
+
+    def maps(self, s: int) -> dict:
+        return _maps(self._lib.fwgpu_partition_maps, self._h, s)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.fwgpu_partition_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class HddmSolver:
     """All subdomains of one full-wave model resident on one GPU.
 
@@ -179,20 +241,7 @@ class HddmSolver:
 
     # -- introspection -----------------------------------------------------
     def subdomain_maps(self, s: int) -> dict:
-        nel, nmp, nbc, ninbc = (ctypes.c_int32() for _ in range(4))
-        lib = self._lib
-        _lib.check(lib.fwgpu_get_subdomain_maps(self._h, s, ctypes.byref(nel), ctypes.byref(nmp), ctypes.byref(nbc),
-                                                ctypes.byref(ninbc), None, None, None, None, None))
-        nop = np.zeros(10 * nel.value, np.int32)
-        ibc = np.zeros(max(1, nbc.value), np.int32)
-        nf = np.zeros(max(1, ninbc.value), np.int32)
-        ln = np.zeros(max(1, ninbc.value), np.int32)
-        gid = np.zeros(max(1, nmp.value), np.int32)
-        i32 = ctypes.c_int32
-        _lib.check(lib.fwgpu_get_subdomain_maps(self._h, s, None, None, None, None, _ptr(nop, i32), _ptr(ibc, i32),
-                                                _ptr(nf, i32), _ptr(ln, i32), _ptr(gid, i32)))
-        return dict(nel=nel.value, nmp=nmp.value, nop=nop, ibc=ibc[: nbc.value], inbc_nfid=nf[: ninbc.value],
-                    inbc_ln_part=ln[: ninbc.value], edge_gid=gid[: nmp.value])
+        return _maps(self._lib.fwgpu_get_subdomain_maps, self._h, s)
 
     def skyline_profile(self, s: int) -> Tuple[np.ndarray, np.ndarray, int]:
         nmp = self.subdomain_maps(s)["nmp"]

@@ -141,6 +141,21 @@ int fwgpu_get_sizes(const fwgpu_context *ctx, fwgpu_sizes *sizes);
 const char *fwgpu_last_error(void);
 int fwgpu_abi_version(void);
 
+/* -- host-only integer setup --------------------------------------------- */
+
+/* The integer part of fwgpu_create without any device work:
+ * make_PartMesh_FW for one part (lib/hddm/make_PartMesh.c:1201-1241).  Lets a
+ * host without a GPU inspect the subdomain numbering. */
+typedef struct fwgpu_partition fwgpu_partition;
+int fwgpu_partition_build(const fwgpu_mesh *mesh, fwgpu_partition **out);
+int fwgpu_partition_destroy(fwgpu_partition *part);
+/* n_subdomains and total_free (interface DOFs) */
+int fwgpu_partition_info(const fwgpu_partition *part, int32_t *n_subdomains, int32_t *total_free);
+/* Same layout as fwgpu_get_subdomain_maps. */
+int fwgpu_partition_maps(const fwgpu_partition *part, int32_t s, int32_t *nel, int32_t *nmp, int32_t *nbc,
+                         int32_t *ninbc, int32_t *nop, int32_t *ibc, int32_t *inbc_nfid, int32_t *inbc_ln_part,
+                         int32_t *edge_gid);
+
 /* -- reference plug-in slots, batched over all subdomains ----------------- */
 
 /* make_TMP_AIJ: HDDM_make_TMP_AIJ_em_E (main/fullwave/fullwave.c:221-259):

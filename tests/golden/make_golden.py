@@ -1,0 +1,79 @@
+"""Generates the golden fixtures of tests/golden/ by running the reference
+itself (built from its sources by oracle/Makefile.ref into oracle/_ref/) on
+synthetic models.
+
+    make -f oracle/Makefile.ref
+    python tests/golden/make_golden.py
+
+Every fixture is one ``.npz`` holding the model parameters it was made from
+and the reference's outputs: the integer maps of make_PartMesh_FW, the
+assembled TMP_AIJ rows, the skyline profile and LDL^T factor of every
+subdomain, the residual history and the converged edge solution.  The C1
+fixture keeps the residual history, the iteration count and a strided
+sample of the solution.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
+sys.path.insert(0, HERE)
+
+from adventure_fullwave_b200 import meshgen  # noqa: E402
+import refdump  # noqa: E402
+
+# name -> (make_model kwargs, hddm_eps, hddm_max_loop, full dump)
+CASES = {
+    "tiny": (dict(name="tiny", n=4, size=1.0, npml=1, layers=None, nleaves=4, leaf_cap=None, jitter=None, seed=0),
+             1e-12, 2000, True),
+    "layered": (dict(name="layered", n=6, size=1.5, npml=1, layers=2, nleaves=None, leaf_cap=200,
+                     jitter=(0.3, 0.7), seed=3), 1e-10, 4000, True),
+    "c1": (dict(name="c1", seed=0), 1e-6, 20000, False),
+}
+
+
+def make_case(name: str) -> str:
+    kw, eps, maxloop, full = CASES[name]
+    model = meshgen.make_model(**kw)
+    meshgen.round_trip_material(model)
+    out = refdump.run_harness(model, eps, maxloop, dump=2 if full else 0)
+    arrays = {
+        "params": np.frombuffer(json.dumps(dict(kw=kw, eps=eps, max_loop=maxloop)).encode(), dtype=np.uint8),
+        "hist": out["hist"],
+        "norm0": np.array([out["norm0"]]),
+        "iterations": np.array([out["json"]["iterations"]]),
+        "total_free": np.array([out["json"]["total_free"]]),
+    }
+    if full:
+        arrays["x"] = out["x"]
+        for s, (im, am, fm) in enumerate(zip(out["ints"], out["aij"], out["fac"])):
+            for k, v in im.items():
+                arrays[f"s{s}_{k}"] = v
+            for k, v in am.items():
+                arrays[f"s{s}_aij_{k}"] = v
+            arrays[f"s{s}_idx1"] = fm["idx1"]
+            arrays[f"s{s}_idx2"] = fm["idx2"]
+            arrays[f"s{s}_fac"] = fm["mat"]
+    else:
+        stride = 97
+        arrays["x_sample_stride"] = np.array([stride])
+        arrays["x_sample"] = out["x"][::stride]
+        arrays["x_sum"] = np.array([out["x"].sum()])
+        arrays["x_abs2"] = np.array([np.sum(np.abs(out["x"]) ** 2)])
+    path = os.path.join(HERE, f"ref_{name}.npz")
+    np.savez_compressed(path, **arrays)
+    return path
+
+
+def params_of(npz) -> dict:
+    return json.loads(bytes(npz["params"]).decode())
+
+
+if __name__ == "__main__":
+    for name in (sys.argv[1:] or CASES):
+        print(make_case(name), os.path.getsize(os.path.join(HERE, f"ref_{name}.npz")))

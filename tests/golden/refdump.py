@@ -1,0 +1,140 @@
+"""Readers for the dump files the reference harness (oracle/ref_harness.c)
+writes, and a runner for it.  Used by make_golden.py (run where the
+reference is built) and by the tests that re-run the reference harness when
+its binary is present."""
+from __future__ import annotations
+
+import json
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+REPO = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
+HARNESS = os.path.join(REPO, "oracle", "_ref", "fw_ref_harness")
+
+
+def read_ints(path: str, nv: int):
+    a = np.frombuffer(open(path, "rb").read(), dtype="<i4")
+    nsub, infree = int(a[0]), int(a[1])
+    o = 4
+    subs = []
+    for _ in range(nsub):
+        nmp, nap, nel = (int(v) for v in a[o:o + 3])
+        o += 3
+        nop = a[o:o + 10 * nel].reshape(nel, 10).copy()
+        o += 10 * nel
+        nbc = int(a[o])
+        o += 1
+        ibc = a[o:o + nbc].copy()
+        o += nbc
+        nin = int(a[o])
+        o += 1
+        inb = a[o:o + 2 * nin].reshape(nin, 2).copy()
+        o += 2 * nin
+        gid = a[o:o + nmp] - nv
+        o += nmp
+        subs.append(dict(nop=nop, ibc=ibc, inbc_nfid=inb[:, 0].copy(), inbc_ln=inb[:, 1].copy(), edge_gid=gid))
+    return infree, subs
+
+
+def read_aij(path: str):
+    b = open(path, "rb").read()
+    o = 0
+    out = []
+    while o < len(b):
+        nf = struct.unpack_from("<i", b, o)[0]
+        o += 4
+        rp = [0]
+        cols, vals = [], []
+        for _ in range(nf):
+            n = struct.unpack_from("<i", b, o)[0]
+            o += 4
+            cols.append(np.frombuffer(b, "<i4", n, o))
+            o += 4 * n
+            vals.append(np.frombuffer(b, "<c16", n, o))
+            o += 16 * n
+            rp.append(rp[-1] + n)
+        bb = np.frombuffer(b, "<c16", nf, o).copy()
+        o += 16 * nf
+        out.append(dict(row_ptr=np.array(rp, np.int32), col=np.concatenate(cols).astype(np.int32),
+                        val=np.concatenate(vals), b=bb))
+    return out
+
+
+def read_fac(path: str):
+    b = open(path, "rb").read()
+    o = 0
+    out = []
+    while o < len(b):
+        nd, nl = struct.unpack_from("<ii", b, o)
+        o += 8
+        i1 = np.frombuffer(b, "<i4", nd, o).copy()
+        o += 4 * nd
+        i2 = np.frombuffer(b, "<i4", nd, o).copy()
+        o += 4 * nd
+        mat = np.frombuffer(b, "<c16", nl, o).copy()
+        o += 16 * nl
+        out.append(dict(idx1=i1, idx2=i2, nlen=nl, mat=mat))
+    return out
+
+
+def read_sol(path: str, nv: int, n_edges: int):
+    b = open(path, "rb").read()
+    nsub = struct.unpack_from("<i", b, 0)[0]
+    o = 4
+    xe = np.zeros(n_edges, np.complex128)
+    seen = np.zeros(n_edges, bool)
+    for _ in range(nsub):
+        n = struct.unpack_from("<i", b, o)[0]
+        o += 4
+        g = np.frombuffer(b, "<i4", n, o) - nv
+        o += 4 * n
+        x = np.frombuffer(b, "<c16", n, o)
+        o += 16 * n
+        new = ~seen[g]
+        xe[g[new]] = x[new]
+        seen[g] = True
+    return xe
+
+
+def read_log(path: str):
+    """Residual history of the full-wave solve from the reference's calc_log
+    (hddm_solver_s.h:203-207, :319-323): returns (norm0, resi per iteration)."""
+    norm0 = None
+    hist = []
+    for line in open(path):
+        t = line.split()
+        if len(t) >= 4 and t[0] == "0" and t[2] == "#" and t[3] == "Norm":
+            norm0 = float(t[4])
+        elif len(t) == 2 and not line.startswith("#"):
+            hist.append(float(t[1]))
+    return norm0, np.array(hist)
+
+
+def run_harness(model, hddm_eps: float, hddm_max_loop: int, dump: int = 2, workdir: str = None, timeout=3600):
+    """Write ``model`` in the reference's part-file layout and run the
+    reference on it.  Returns a dict of the parsed outputs."""
+    from adventure_fullwave_b200 import meshgen
+
+    own = workdir is None
+    wd = tempfile.mkdtemp(prefix="fwref_") if own else workdir
+    mdir = os.path.join(wd, "MODEL")
+    meshgen.write_hddm_model(model, mdir)
+    env = dict(os.environ, FW_HARNESS_DUMP=str(dump), FW_HARNESS_OUT=os.path.join(mdir, "ref"))
+    cmd = [HARNESS, "-memlimit", "60000", "-hddm-eps", repr(hddm_eps), "-hddm-max-loop", str(hddm_max_loop), "MODEL"]
+    subprocess.run(cmd, cwd=wd, env=env, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                   timeout=timeout)
+    nv = model.n_vertices
+    out = dict(json=json.load(open(os.path.join(mdir, "ref.json"))))
+    out["x"] = read_sol(os.path.join(mdir, "ref.sol"), nv, model.n_edges)
+    out["norm0"], out["hist"] = read_log(os.path.join(mdir, "calc_log", "log_g_HDDM_Full_Wave"))
+    if dump >= 1:
+        out["infree"], out["ints"] = read_ints(os.path.join(mdir, "ref.ints"), nv)
+    if dump >= 2:
+        out["aij"] = read_aij(os.path.join(mdir, "ref.aij"))
+        out["fac"] = read_fac(os.path.join(mdir, "ref.fac"))
+    out["workdir"] = wd
+    return out

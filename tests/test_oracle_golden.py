@@ -1,0 +1,46 @@
+"""The oracle restatement (oracle/fw_oracle.c) against the reference's own
+outputs (golden fixtures made by tests/golden/make_golden.py from the
+reference built from its sources): bit for bit."""
+import numpy as np
+import pytest
+
+from helpers import golden
+from oracle import oracle
+
+
+@pytest.mark.parametrize("name", ["tiny", "layered"])
+def test_assembly_and_factor_bitwise(name):
+    z, params, model = golden(name)
+    part = oracle.partition(model)
+    for s, sub in enumerate(part.subs):
+        rp, col, val, b = oracle.assemble_sub(model, sub)
+        assert np.array_equal(rp, z[f"s{s}_aij_row_ptr"])
+        assert np.array_equal(col, z[f"s{s}_aij_col"])
+        assert np.array_equal(val, z[f"s{s}_aij_val"])
+        idx1, idx2, nlen, mat = oracle.factor_sub(model, sub)
+        assert np.array_equal(idx1, z[f"s{s}_idx1"]) and np.array_equal(idx2, z[f"s{s}_idx2"])
+        assert nlen == z[f"s{s}_fac"].shape[0]
+        assert np.array_equal(mat, z[f"s{s}_fac"])
+
+
+@pytest.mark.parametrize("name", ["tiny", "layered"])
+def test_hddm_bitwise(name):
+    z, params, model = golden(name)
+    part = oracle.partition(model)
+    xe, per_sub, hist, norm0 = oracle.hddm(model, part, params["eps"], params["max_loop"])
+    assert len(hist) == int(z["iterations"][0])
+    assert norm0 == pytest.approx(float(z["norm0"][0]), rel=1e-6)
+    # the reference prints the history with 7 digits
+    assert np.allclose(hist, z["hist"], rtol=5e-7, atol=0)
+    assert np.array_equal(xe, z["x"])
+
+
+def test_c1_history_and_solution():
+    z, params, model = golden("c1")
+    part = oracle.partition(model)
+    xe, per_sub, hist, norm0 = oracle.hddm(model, part, params["eps"], params["max_loop"])
+    assert len(hist) == int(z["iterations"][0]) == 450
+    assert np.allclose(hist, z["hist"], rtol=5e-7, atol=0)
+    stride = int(z["x_sample_stride"][0])
+    assert np.array_equal(xe[::stride], z["x_sample"])
+    assert xe.sum() == z["x_sum"][0]
