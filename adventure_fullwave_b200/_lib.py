@@ -64,7 +64,7 @@ class FwSizes(ctypes.Structure):
         ("n_subdomains", c_i32), ("total_free", c_i32), ("total_dofs", c_i64), ("total_interior", c_i64),
         ("nlen_reference", c_i64), ("nlen_interior", c_i64), ("nnz_lower", c_i64),
         ("nnz_interface_rows", c_i64), ("nnz_coupling", c_i64), ("nnz_interior", c_i64),
-        ("max_local_dofs", c_i32), ("max_interior", c_i32),
+        ("total_iface_slots", c_i64), ("max_local_dofs", c_i32), ("max_interior", c_i32),
     ]
 
 
@@ -72,7 +72,12 @@ class FwResult(ctypes.Structure):
     _fields_ = [
         ("iterations", c_i32), ("converged", c_i32), ("initial_norm", c_dbl), ("final_resi", c_dbl),
         ("final_resi_l2", c_dbl), ("t_setup_ms", c_dbl), ("t_iterate_ms", c_dbl), ("t_last_ms", c_dbl),
+        ("kernel_launches", c_i64),
     ]
+
+
+class FwKernelProfile(ctypes.Structure):
+    _fields_ = [("subsolve_ms", c_dbl), ("interface_ms", c_dbl), ("iteration_ms", c_dbl), ("reps", c_i32)]
 
 
 # every symbol the header declares, with its argument types
@@ -94,6 +99,7 @@ SIGNATURES = {
     "fwgpu_solve_dom_last": [ctypes.c_void_p],
     "fwgpu_hddm_solve": [ctypes.c_void_p, P(FwSource), P(FwResult)],
     "fwgpu_hddm_resolve": [ctypes.c_void_p, P(FwSource), P(FwResult)],
+    "fwgpu_profile_iteration": [ctypes.c_void_p, c_i32, P(FwKernelProfile)],
     "fwgpu_get_edge_solution": [ctypes.c_void_p, P(c_dbl)],
     "fwgpu_get_history": [ctypes.c_void_p, P(c_dbl), c_i32, P(c_i32)],
     "fwgpu_get_subdomain_maps": [ctypes.c_void_p, c_i32, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32),

@@ -72,6 +72,9 @@ struct fwgpu_context {
   int graph_iters = 0;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool factor_bad = false;
+  bool factor_fresh = false;       // factor matches the assembled values
+  int64_t launches = 0;            // kernels launched since the last reset
+  int64_t *d_env_dst = nullptr;    // lower entry -> envelope position (-1: outside)
 
   template <typename T>
   int alloc(T **ptr, size_t count) {
@@ -384,6 +387,7 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   FW_CUDA(cudaMallocHost(&c->h_sc, sizeof(fw::CocgScalars)));
   FW_TRY(c->alloc(&c->d_hist, (size_t)std::max(1, opts->hddm_max_loop) + 2));
   dp.hist = c->d_hist;
+  dp.hist_cap = std::max(1, opts->hddm_max_loop) + 2;
   dp.ir_steps = c->opts.ir_max_steps;
   dp.ir_tol = c->opts.ir_tol;
   {
@@ -478,6 +482,7 @@ int fwgpu_get_sizes(const fwgpu_context *c, fwgpu_sizes *sz) {
   sz->nnz_interface_rows = (int64_t)p.ifr_src.size();
   sz->nnz_coupling = (int64_t)p.cpl_src.size();
   sz->nnz_interior = (int64_t)p.aii_src.size();
+  sz->total_iface_slots = p.sub_if_off[nsub];
   sz->max_local_dofs = p.max_local;
   sz->max_interior = p.max_interior;
   return FWGPU_OK;
@@ -490,6 +495,7 @@ int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
   FW_CUDA(cudaEventRecord(c->ev[0], c->stream));
   double *d_elmat = nullptr;
   FW_TRY(c->alloc(&d_elmat, (size_t)c->m.nt * 72));
+  c->launches += 2;
   fw::launch_element_matrices(c->m.nt, c->d_el_order, c->d_tv, c->d_crd, c->d_el_eps, c->d_el_sigma, c->m.omega,
                               d_elmat, c->d_mesh_status, c->stream);
   if (!c->d_aval) FW_TRY(c->alloc(&c->d_aval, p.nnz_total));
@@ -505,6 +511,7 @@ int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
   {
     int64_t *tmp = nullptr;
     FW_TRY(c->upload(&tmp, p.cpl_src));
+    c->launches += c->d_aii_val ? 4 : 3;
     fw::launch_gather_ops((int64_t)p.cpl_src.size(), tmp, c->d_aval, c->d_cpl_val, c->stream);
     FW_CUDA(cudaStreamSynchronize(c->stream));
     c->release(tmp);
@@ -525,6 +532,7 @@ int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
   }
   FW_CUDA(cudaGetLastError());
   c->stage = 1;
+  c->factor_fresh = false;
   return FWGPU_OK;
 }
 
@@ -538,6 +546,7 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
   if (!c->d_L64) {
     // skyline profile on the device, envelope layout on the host
     FW_TRY(c->alloc(&c->d_idx1, ndof));
+    c->launches += 1;
     fw::launch_profile(nsub, c->d_dof_off, c->d_nnz_off, c->d_row_ptr, c->d_col, c->d_aval, c->d_isbc, c->d_idx1,
                        c->stream);
     c->h_idx1.resize(ndof);
@@ -581,22 +590,23 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     c->nlen_ref = nref;
     FW_TRY(c->upload(&c->d_env_lo, c->h_env_lo));
     FW_TRY(c->upload(&c->d_env_ptr, c->h_env_ptr));
-    int64_t *d_dst = nullptr;
-    FW_TRY(c->upload(&d_dst, dst));
+    FW_TRY(c->upload(&c->d_env_dst, dst));
     FW_TRY(c->alloc(&c->d_L64, pos));
-    FW_CUDA(cudaMemsetAsync(c->d_L64, 0, std::max<int64_t>(1, pos) * sizeof(double2), c->stream));
-    fw::launch_scatter_envelope(p.nnz_total, d_dst, c->d_aval, c->d_L64, c->stream);
-    FW_CUDA(cudaStreamSynchronize(c->stream));
-    c->release(d_dst);
     c->dp.env_lo = c->d_env_lo;
     c->dp.env_ptr = c->d_env_ptr;
+    if (c->opts.precision == FWGPU_PREC_FP32_IR) FW_TRY(c->alloc(&c->d_L32, pos));
+  }
+  if (!c->factor_fresh) {
+    // envelope values and LDL^T factor (the layout is fixed by the model)
+    const int64_t pos = c->nlen_int;
+    FW_CUDA(cudaMemsetAsync(c->d_L64, 0, std::max<int64_t>(1, pos) * sizeof(double2), c->stream));
+    c->launches += c->opts.precision == FWGPU_PREC_FP32_IR ? 3 : 2;
+    fw::launch_scatter_envelope(p.nnz_total, c->d_env_dst, c->d_aval, c->d_L64, c->stream);
     c->dp.L64 = c->d_L64;
-    // factor
     FW_CUDA(cudaMemsetAsync(c->d_mesh_status + 1, 0, sizeof(int32_t), c->stream));
     fw::launch_factor(c->dp, c->dp.int_off, c->d_env_lo, c->d_env_ptr, c->d_L64, c->d_mesh_status + 1, c->stream);
     FW_CUDA(cudaGetLastError());
     if (c->opts.precision == FWGPU_PREC_FP32_IR) {
-      FW_TRY(c->alloc(&c->d_L32, pos));
       fw::launch_to_fp32(pos, c->d_L64, c->d_L32, c->stream);
       c->dp.L32 = c->d_L32;
       c->dp.L64 = nullptr;
@@ -605,15 +615,10 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     FW_CUDA(cudaMemcpyAsync(&fstat, c->d_mesh_status + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     FW_CUDA(cudaStreamSynchronize(c->stream));
     c->factor_bad = fstat != 0;
-    if (c->opts.precision == FWGPU_PREC_FP32_IR) {
-      // the FP64 factor is only kept for introspection of small problems
-      if (pos > (int64_t)64 * 1024 * 1024) {
-        c->release(c->d_L64);
-        c->d_L64 = nullptr;
-      }
-    }
+    c->factor_fresh = true;
   }
   fw::launch_subsolve(c->dp, fw::kModeFirst, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
+  c->launches += 1;
   FW_CUDA(cudaGetLastError());
   c->stage = 2;
   if (c->factor_bad) return set_error(FWGPU_ERR_BREAKDOWN, "zero or non-finite pivot in a subdomain factor");
@@ -626,6 +631,7 @@ int fwgpu_iteration_s_1st(fwgpu_context *c, int32_t *status) {
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_set_status(c->d_sc, c->opts.hddm_eps, c->opts.hddm_max_loop, c->stream);
   fw::launch_cocg_first(c->dp, c->d_pcloc, c->stream);
+  c->launches += 3;
   FW_CUDA(cudaGetLastError());
   FW_TRY(read_status(c, status));
   c->stage = 3;
@@ -637,6 +643,7 @@ int fwgpu_iteration_s(fwgpu_context *c, int32_t *status) {
   if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "iteration_s outside the interface loop");
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_cocg_iteration(c->dp, c->stream);
+  c->launches += 7;
   FW_CUDA(cudaGetLastError());
   FW_TRY(read_status(c, status));
   return FWGPU_OK;
@@ -648,6 +655,7 @@ int fwgpu_solve_dom_last(fwgpu_context *c) {
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_subsolve(c->dp, fw::kModeLast, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
   fw::launch_edge_solution(c->m.ne, c->d_edge_src, c->dp.Y, c->dp.V, c->d_xedge, c->stream);
+  c->launches += 2;
   FW_CUDA(cudaGetLastError());
   FW_CUDA(cudaStreamSynchronize(c->stream));
   c->stage = 4;
@@ -668,6 +676,7 @@ static int run_loop(fwgpu_context *c, fwgpu_result *res) {
   int32_t st = c->h_sc->status;
   while (st == 0) {
     FW_CUDA(cudaGraphLaunch(c->graph, c->stream));
+    c->launches += 7 * (int64_t)c->graph_iters;
     FW_TRY(read_status(c, &st));
   }
   (void)res;
@@ -690,6 +699,7 @@ static int fill_result(fwgpu_context *c, fwgpu_result *res) {
     res->t_iterate_ms = ms;
     cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
     res->t_last_ms = ms;
+    res->kernel_launches = c->launches;
   }
   return sc.converged ? FWGPU_OK : set_error(FWGPU_ERR_NOT_CONVERGED, "hddm_max_loop reached before hddm_eps");
 }
@@ -697,6 +707,7 @@ static int fill_result(fwgpu_context *c, fwgpu_result *res) {
 int fwgpu_hddm_solve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *res) {
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (c->opts.hddm_max_loop == 0) return set_error(FWGPU_ERR_ARG, "hddm_max_loop is 0");
+  c->launches = 0;
   FW_TRY(fwgpu_make_tmp_aij(c, src));
   FW_TRY(fwgpu_solve_dom_1st(c));
   int32_t st = 0;
@@ -715,6 +726,7 @@ int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *
   if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "resolve before the factors exist");
   FW_CUDA(cudaSetDevice(c->opts.device));
   FW_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  c->launches = 1;
   FW_TRY(build_rhs(c, src));
   fw::launch_subsolve(c->dp, fw::kModeFirst, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
   int32_t st = 0;
@@ -726,6 +738,45 @@ int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *
   FW_CUDA(cudaEventRecord(c->ev[3], c->stream));
   FW_CUDA(cudaStreamSynchronize(c->stream));
   return fill_result(c, res);
+}
+
+int fwgpu_profile_iteration(fwgpu_context *c, int32_t reps, fwgpu_kernel_profile *out) {
+  if (!c || !out || reps <= 0) return set_error(FWGPU_ERR_ARG, "bad argument");
+  if (c->stage < 3 || !c->graph) return set_error(FWGPU_ERR_STATE, "profile needs a finished solve");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
+  cudaEvent_t a, b;
+  FW_CUDA(cudaEventCreate(&a));
+  FW_CUDA(cudaEventCreate(&b));
+  fw::launch_profile_reset(c->d_sc, c->stream);
+  // warm-up
+  fw::launch_cocg_iteration(c->dp, c->stream);
+  float ms = 0.f;
+  FW_CUDA(cudaEventRecord(a, c->stream));
+  for (int r = 0; r < reps; r++) fw::launch_subsolve(c->dp, fw::kModeIter, fp32, c->stream);
+  FW_CUDA(cudaEventRecord(b, c->stream));
+  FW_CUDA(cudaEventSynchronize(b));
+  FW_CUDA(cudaEventElapsedTime(&ms, a, b));
+  out->subsolve_ms = ms / reps;
+  FW_CUDA(cudaEventRecord(a, c->stream));
+  for (int r = 0; r < reps; r++) fw::launch_cocg_iteration(c->dp, c->stream);
+  FW_CUDA(cudaEventRecord(b, c->stream));
+  FW_CUDA(cudaEventSynchronize(b));
+  FW_CUDA(cudaEventElapsedTime(&ms, a, b));
+  out->interface_ms = ms / reps - out->subsolve_ms;
+  const int launches = std::max(1, reps / std::max(1, c->graph_iters));
+  FW_CUDA(cudaEventRecord(a, c->stream));
+  for (int r = 0; r < launches; r++) FW_CUDA(cudaGraphLaunch(c->graph, c->stream));
+  FW_CUDA(cudaEventRecord(b, c->stream));
+  FW_CUDA(cudaEventSynchronize(b));
+  FW_CUDA(cudaEventElapsedTime(&ms, a, b));
+  out->iteration_ms = ms / (launches * c->graph_iters);
+  out->reps = reps;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  FW_CUDA(cudaGetLastError());
+  c->stage = 2;
+  return FWGPU_OK;
 }
 
 int fwgpu_get_edge_solution(fwgpu_context *c, double *x) {

@@ -804,7 +804,7 @@ __global__ void cocg_beta_kernel(DevProblem p) {
     const double resi = mx * sc->r0inv;
     sc->resi = resi;
     sc->resi_l2 = sqrt(l2) / sc->l2_0;
-    p.hist[sc->loop - 1] = resi;
+    if (sc->loop - 1 < p.hist_cap) p.hist[sc->loop - 1] = resi;
     const double2 rz = make_double2(rzr, rzi);
     if (cabs_ref(rz) < kNearlyZero && cabs_ref(sc->rz) < kNearlyZero) {
       sc->beta = cz();
@@ -845,6 +845,14 @@ __global__ void set_status_kernel(CocgScalars *sc, double eps, int32_t max_loop)
   sc->max_loop = max_loop;
   sc->status = 0;
   sc->converged = 0;
+}
+
+// iteration state for kernel timing: never converges, no loop limit
+__global__ void profile_reset_kernel(CocgScalars *sc) {
+  sc->status = 0;
+  sc->eps = -1.0;
+  sc->max_loop = 0x7fffffff;
+  sc->loop = 1;
 }
 
 unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
@@ -938,6 +946,8 @@ void launch_edge_solution(int64_t ne, const int64_t *edge_src, const double2 *Y,
   if (ne <= 0) return;
   edge_solution_kernel<<<blocks_for(ne, 256), 256, 0, stream>>>(ne, edge_src, Y, V, x);
 }
+
+void launch_profile_reset(CocgScalars *sc, cudaStream_t stream) { profile_reset_kernel<<<1, 1, 0, stream>>>(sc); }
 
 void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream) {
   set_status_kernel<<<1, 1, 0, stream>>>(sc, eps, max_loop);

@@ -74,6 +74,7 @@ struct DevProblem {
   int32_t ir_steps;
   double ir_tol;
   int32_t cta_smem;              // dynamic shared bytes of the CTA-per-subdomain solve (0: warp path)
+  int32_t hist_cap;              // entries of hist
 };
 
 enum SolveMode { kModeFirst = 0, kModeIter = 1, kModeLast = 2 };
@@ -100,5 +101,6 @@ void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream);
 void launch_edge_solution(int64_t ne, const int64_t *edge_src, const double2 *Y, const double2 *V, double2 *x,
                           cudaStream_t stream);
 void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream);
+void launch_profile_reset(CocgScalars *sc, cudaStream_t stream);
 
 }  // namespace fw

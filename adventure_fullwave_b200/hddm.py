@@ -43,6 +43,7 @@ class HddmResult:
     t_setup_ms: float
     t_iterate_ms: float
     t_last_ms: float
+    kernel_launches: int = 0
 
 
 def _mesh_struct(model):
@@ -219,7 +220,17 @@ class HddmSolver:
     @staticmethod
     def _result(r: _lib.FwResult) -> HddmResult:
         return HddmResult(int(r.iterations), bool(r.converged), float(r.initial_norm), float(r.final_resi),
-                          float(r.final_resi_l2), float(r.t_setup_ms), float(r.t_iterate_ms), float(r.t_last_ms))
+                          float(r.final_resi_l2), float(r.t_setup_ms), float(r.t_iterate_ms), float(r.t_last_ms),
+                          int(r.kernel_launches))
+
+    def profile_iteration(self, reps: int = 50) -> dict:
+        """Average device time of the kernels of one interface iteration
+        (CUDA events on the solver's stream).  Overwrites the iteration
+        state: call ``resolve`` afterwards for a solution."""
+        prof = _lib.FwKernelProfile()
+        _lib.check(self._lib.fwgpu_profile_iteration(self._h, int(reps), ctypes.byref(prof)))
+        return dict(subsolve_ms=prof.subsolve_ms, interface_ms=prof.interface_ms, iteration_ms=prof.iteration_ms,
+                    reps=prof.reps)
 
     # -- results -----------------------------------------------------------
     def edge_solution(self) -> np.ndarray:

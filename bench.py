@@ -1,0 +1,358 @@
+"""Benchmark of the B200 HDDM hot path: time to reach a 1e-6 max-norm
+relative interface residual (the reference's COCG criterion,
+lib/hddm/hddm_solver_s.h:311-318,370) on a synthetic layered-PML model.
+
+One step = one full HDDM solve with the model resident in HBM: element
+assembly into the subdomain envelopes, LDL^T factors, first solve, COCG to
+``--eps``, final solves.  ``value`` is seconds per solve on the device
+(CUDA events on the solver's stream, max over ranks); ``e2e`` is the same
+solve through the public API from host arrays (subdomain setup, uploads,
+solve, download of the edge solution) timed per step.
+
+    python bench.py [--gpus N --steps K --warmup W] [--config c2] [--precision fp64|fp32_ir]
+    python bench.py --impl reference ...   # the reference's own CPU solver
+
+Under torchrun (N > 1) every rank solves its own copy of the model (replicas;
+the multi-GPU interface exchange is not in this run), and rank 0 prints the
+line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+import numpy as np  # noqa: E402
+
+from adventure_fullwave_b200 import meshgen  # noqa: E402
+
+METRIC = "time-to-1e-6 HDDM residual (max-norm relative, interface COCG), 1 B200"
+WORKLOADS = {
+    "c1": "C1: [0,1]^3 16^3 hexes x 6 Kuhn tets (24,576 tets), vacuum, 4-cell PML, PEC wall, 300 MHz, "
+          "centre z-dipole, RCB 1 part x 64 subdomains",
+    "c2": "C2: [0,1.5]^3 48^3 hexes x 6 tets (663,552 tets), 8 random layers, 6-cell PML, PEC wall, 300 MHz, "
+          "centre z-dipole, jittered RCB (leaf cap 600) 1 part x 1654 subdomains",
+    "c3": "C3: [0,1.5]^3 96^3 hexes x 6 tets (5,308,416 tets), 8 random layers, 8-cell PML, PEC wall, 300 MHz, "
+          "centre z-dipole, jittered RCB (leaf cap 900)",
+}
+# COCG iterations to 1e-6 of the FP64 GPU solve on each model (B200, this
+# code); the reference's CPU time is extrapolated with them where running the
+# reference to convergence would take hours (C2: ~7,800 iterations).
+ITERS_FP64 = {"c1": 450, "c2": 7790}
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            t = [x.strip() for x in line.split(",")]
+            if len(t) < 9:
+                continue
+            try:
+                sm.append(float(t[1]))
+                mx = max(mx, float(t[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, t[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(sz: dict, precision: str, ir_steps: int) -> int:
+    """Bytes one batched subdomain-solve launch must move at least: one pass
+    over the interior envelope, the interface-row and coupling operators
+    (value + column), row metadata and the interface values in and out."""
+    elem = 16 if precision == "fp64" else 8
+    b = sz["nlen_interior"] * elem
+    b += (sz["nnz_interface_rows"] + sz["nnz_coupling"]) * 20
+    b += sz["total_interior"] * (4 + 8 + 4) + sz["total_iface_slots"] * (4 + 4)
+    b += sz["total_iface_slots"] * 32
+    if precision != "fp64":
+        b += ir_steps * sz["nnz_interior"] * 20
+    return int(b)
+
+
+def ncu_traffic(config: str, precision: str):
+    """DRAM bytes per launch of the substitution kernel from the committed
+    ncu summary, when it covers this workload."""
+    path = os.path.join(REPO, "profiles", "subsolve_dram_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(f"{config}_{precision}")
+    except Exception:
+        return None
+
+
+def make_model(config: str):
+    model = meshgen.make_model(config)
+    meshgen.round_trip_material(model)
+    return model
+
+
+def cpu_baseline_reference(model, config: str, sample_iters: int, n_iters: int):
+    """The reference itself (oracle/_ref/fw_ref_harness, built from its
+    sources, single thread) on a bounded sample of the workload: setup plus
+    ``sample_iters`` COCG iterations, extrapolated to ``n_iters``."""
+    sys.path.insert(0, os.path.join(REPO, "tests", "golden"))
+    import refdump
+
+    if not os.path.exists(refdump.HARNESS):
+        return None
+    wd = tempfile.mkdtemp(prefix="fwbench_")
+    try:
+        t0 = time.time()
+        out = refdump.run_harness(model, 1e-6, sample_iters, dump=0, workdir=wd, timeout=1800)
+        wall = time.time() - t0
+        j = out["json"]
+        per_iter = j["t_iter_total_s"] / max(1, j["t_iter_count"])
+        setup = j["t_init_s"] + j["t_first_s"]
+        total = setup + n_iters * per_iter + j["t_last_s"]
+        return {"value": total, "unit": "s", "cores": 1, "kind": "reference",
+                "sample": f"reference s-mode solver on the {config} model: setup + {sample_iters} COCG iterations "
+                          f"({wall:.1f} s wall), {per_iter:.3f} s/iteration extrapolated to {n_iters} iterations",
+                "setup_s": setup, "per_iteration_s": per_iter, "iterations_assumed": n_iters}
+    finally:
+        shutil.rmtree(wd, ignore_errors=True)
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    model = make_model(args.config)
+    n_iters = ITERS_FP64.get(args.config, 5000)
+    vals = []
+    last = None
+    for step in range(args.warmup + args.steps):
+        r = cpu_baseline_reference(model, args.config, args.ref_iters, n_iters)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/fw_ref_harness is not built"}))
+            return 0
+        if step >= args.warmup:
+            vals.append(r["value"])
+        last = r
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": WORKLOADS.get(args.config, args.config), "precision": "fp64",
+                       "hddm_eps": args.eps},
+            "cpu_baseline": {k: last[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["cpu_baseline"]["value"] = value
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    rank, world, local = env_rank()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_mod
+
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist = dist_mod
+    from adventure_fullwave_b200 import hddm
+
+    model = make_model(args.config)
+    solver = hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
+                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, graph_iterations=args.graph_iters,
+                             device=local)
+    for _ in range(args.warmup):
+        solver.solve(0)
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    clocks.start()
+    times, iters, launches, results = [], [], [], []
+    for _ in range(args.steps):
+        r = solver.solve(0)
+        results.append(r)
+        times.append((r.t_setup_ms + r.t_iterate_ms + r.t_last_ms) / 1e3)
+        iters.append(r.iterations)
+        launches.append(r.kernel_launches)
+    clk = clocks.stop()
+    total = float(np.sum(times))
+    if dist:
+        import torch
+
+        t = torch.tensor([total], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+        dist.barrier()
+    value = total / args.steps
+    sz = solver.sizes()
+    x_check = solver.edge_solution()
+
+    # kernel timing of the dominant kernel for the roofline
+    prof = solver.profile_iteration(reps=args.prof_reps)
+    solver.resolve(0)
+    peak, peak_kind = load_peaks()
+    alg = algorithmic_bytes(sz, args.precision, args.ir_steps)
+    achieved = alg / (prof["subsolve_ms"] * 1e-3) / 1e9
+    traffic = ncu_traffic(args.config, args.precision)
+    roofline = {"bound": "hbm", "kernel": "subsolve_cta_kernel (one batched subdomain solve)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic, "algorithmic_bytes": alg,
+                "kernel_ms": prof["subsolve_ms"], "interface_kernels_ms": prof["interface_ms"],
+                "iteration_ms_graph": prof["iteration_ms"]}
+
+    # end to end through the public API from host arrays
+    solver.close()
+    e2e_times = []
+    h2d = sum(a.nbytes for a in (model.vertex_crd, model.tets, model.tet_edges, model.flag, model.pec_edge,
+                                 model.sub_of_tet, model.mat_flag, model.mat_eps, model.mat_sigma))
+    d2h = model.n_edges * 16
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
+                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, graph_iterations=args.graph_iters,
+                             device=local) as s2:
+            s2.solve(0)
+            xe = s2.edge_solution()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e = float(np.mean(e2e_times))
+    if dist:
+        import torch
+
+        t = torch.tensor([e2e], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_reference(model, args.config, args.ref_iters,
+                                     int(np.mean(iters)) if args.precision == "fp64" else
+                                     ITERS_FP64.get(args.config, int(np.mean(iters))))
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128" if args.precision == "fp64" else "c64 factor, c128 refinement and COCG",
+        "data": "synthetic (seeded generator; no dataset)",
+        "config": {"workload": WORKLOADS.get(args.config, args.config), "precision": args.precision,
+                   "hddm_eps": args.eps, "n_tets": model.n_tets, "n_subdomains": model.nsub,
+                   "interface_dofs": sz["total_free"], "ir_steps": args.ir_steps if args.precision != "fp64" else 0,
+                   "l2": "inputs larger than L2 (envelope %.0f MB)" % (
+                       sz["nlen_interior"] * (16 if args.precision == "fp64" else 8) / 1e6),
+                   "parallelism": f"{world} replica(s)"},
+        "iterations": int(np.mean(iters)), "setup_ms": float(np.mean([r.t_setup_ms for r in results])),
+        "iterate_ms": float(np.mean([r.t_iterate_ms for r in results])),
+        "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": int(np.sum(launches)),
+        "solution_check": {"finite": bool(np.all(np.isfinite(x_check))), "final_resi": results[-1].final_resi},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ncu_case(args):
+    """A short run for ncu captures: setup, the first solve and
+    ``--ncu-iters`` interface iterations, launched one by one."""
+    from adventure_fullwave_b200 import hddm
+
+    model = make_model(args.config)
+    with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
+                         ir_max_steps=args.ir_steps, ir_tol=args.ir_tol) as s:
+        s.make_tmp_aij(0)
+        s.solve_dom_1st()
+        s.iteration_s_1st()
+        for _ in range(args.ncu_iters):
+            s.iteration_s()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_ir"])
+    ap.add_argument("--eps", type=float, default=1e-6)
+    ap.add_argument("--max-loop", type=int, default=50000)
+    ap.add_argument("--ir-steps", type=int, default=1)
+    ap.add_argument("--ir-tol", type=float, default=0.0)
+    ap.add_argument("--graph-iters", type=int, default=32)
+    ap.add_argument("--prof-reps", type=int, default=50)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--ref-iters", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="bench", choices=["bench", "ncu"])
+    ap.add_argument("--ncu-iters", type=int, default=20)
+    args = ap.parse_args()
+    if args.mode == "ncu":
+        return run_ncu_case(args)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

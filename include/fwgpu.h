@@ -112,6 +112,7 @@ typedef struct {
   int64_t nnz_interface_rows; /* entries of the interface-row operator used per iteration */
   int64_t nnz_coupling;     /* entries of the interior-interface coupling used per iteration */
   int64_t nnz_interior;     /* entries of the interior operator used by refinement */
+  int64_t total_iface_slots; /* sum over subdomains of interface DOFs */
   int32_t max_local_dofs;
   int32_t max_interior;
 } fwgpu_sizes;
@@ -125,6 +126,7 @@ typedef struct {
   double t_setup_ms;       /* assembly + factor + first solve, device time */
   double t_iterate_ms;     /* COCG loop, device time */
   double t_last_ms;        /* final subdomain solves, device time */
+  int64_t kernel_launches; /* kernels this library launched for the call */
 } fwgpu_result;
 
 /* -- lifecycle ----------------------------------------------------------- */
@@ -198,6 +200,22 @@ int fwgpu_hddm_solve(fwgpu_context *ctx, const fwgpu_source *src, fwgpu_result *
 /* Re-run only the interface iteration and last step for a new right-hand side
  * on the existing factors (multi-source runs). */
 int fwgpu_hddm_resolve(fwgpu_context *ctx, const fwgpu_source *src, fwgpu_result *result);
+
+/* -- measurement ---------------------------------------------------------- */
+
+typedef struct {
+  double subsolve_ms;   /* one batched subdomain-solve launch of the interface iteration, average */
+  double interface_ms;  /* the interface (COCG) kernels of one iteration, average */
+  double iteration_ms;  /* one iteration replayed from the CUDA graph, average */
+  int32_t reps;
+} fwgpu_kernel_profile;
+
+/* Times the kernels of one interface iteration with CUDA events on the
+ * context's stream.  Needs factors (after fwgpu_hddm_solve); overwrites the
+ * iteration state, so the solution must be recomputed with
+ * fwgpu_hddm_resolve afterwards.  No reference counterpart (the reference
+ * times whole phases with gettimeofday, lib/std/timefunc.c:17-111). */
+int fwgpu_profile_iteration(fwgpu_context *ctx, int32_t reps, fwgpu_kernel_profile *out);
 
 /* -- results -------------------------------------------------------------- */
 
