@@ -383,30 +383,68 @@ struct CtaMeta {
   int nI;
 };
 
+// rows of a block handled by one warp (rows w, w+nw, ...); kRowsPerWarp
+// independent accumulators keep several loads in flight per lane
+constexpr int kRowsPerWarp = kRB / (kCtaThreads / 32);
+
 template <typename T>
 __device__ void cta_forward(const CtaMeta &m, const T *__restrict__ L, T *y, T *tri, T *rect) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
   for (int r0 = 0; r0 < m.nI; r0 += kRB) {
     const int nb = min(kRB, m.nI - r0);
-    for (int t = warp; t < nb; t += nw) {
+    int lo_u[kRowsPerWarp], len_u[kRowsPerWarp];
+    const T *row_u[kRowsPerWarp];
+    int maxlen = 0;
+#pragma unroll
+    for (int u = 0; u < kRowsPerWarp; u++) {
+      const int t = warp + u * nw;
       const int i = r0 + t;
-      const int lo_i = m.lo[i];
-      const T *row = L + m.pr[i] - lo_i;
-      T acc = czero<T>();
-      for (int k = lo_i + lane; k < r0; k += 32) acc = cadd(acc, cmul(row[k], y[k]));
-      acc = warp_sum(acc);
-      if (lane == 0) rect[t] = acc;
-      const int col = r0 + lane;
-      tri[t * kTriStride + lane] = (col < i && col >= lo_i) ? row[col] : czero<T>();
+      if (t < nb) {
+        lo_u[u] = m.lo[i];
+        row_u[u] = L + m.pr[i] - lo_u[u];
+        len_u[u] = max(0, r0 - lo_u[u]);
+      } else {
+        lo_u[u] = 0;
+        row_u[u] = L;
+        len_u[u] = 0;
+      }
+      maxlen = max(maxlen, len_u[u]);
+    }
+    T acc[kRowsPerWarp];
+#pragma unroll
+    for (int u = 0; u < kRowsPerWarp; u++) acc[u] = czero<T>();
+    for (int k = lane; k < maxlen; k += 32) {
+#pragma unroll
+      for (int u = 0; u < kRowsPerWarp; u++) {
+        if (k < len_u[u]) {
+          const int col = lo_u[u] + k;
+          acc[u] = cadd(acc[u], cmul(row_u[u][col], y[col]));
+        }
+      }
+    }
+    // stage the block's triangle: tri[t][j] = L[r0+t][r0+j]
+#pragma unroll
+    for (int u = 0; u < kRowsPerWarp; u++) {
+      const int t = warp + u * nw;
+      if (t < nb) {
+        const int col = r0 + lane;
+        tri[t * kTriStride + lane] = (col < r0 + t && col >= lo_u[u]) ? row_u[u][col] : czero<T>();
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kRowsPerWarp; u++) {
+      const T a = warp_sum(acc[u]);
+      const int t = warp + u * nw;
+      if (lane == 0 && t < nb) rect[t] = a;
     }
     __syncthreads();
     if (warp == 0) {
-      T acc = lane < nb ? csub(y[r0 + lane], rect[lane]) : czero<T>();
+      T val = lane < nb ? csub(y[r0 + lane], rect[lane]) : czero<T>();
       for (int j = 0; j < nb - 1; j++) {
-        const T yj = shfl_idx(acc, j);
-        if (lane > j) acc = csub(acc, cmul(tri[lane * kTriStride + j], yj));
+        const T yj = shfl_idx(val, j);
+        if (lane > j) val = csub(val, cmul(tri[lane * kTriStride + j], yj));
       }
-      if (lane < nb) y[r0 + lane] = acc;
+      if (lane < nb) y[r0 + lane] = val;
     }
     __syncthreads();
   }
@@ -425,12 +463,16 @@ __device__ void cta_backward(const CtaMeta &m, const T *__restrict__ L, T *y, T 
   for (int blk = nblk - 1; blk >= 0; blk--) {
     const int r0 = blk * kRB;
     const int nb = min(kRB, m.nI - r0);
-    for (int t = warp; t < nb; t += nw) {
-      const int i = r0 + t;
-      const int lo_i = m.lo[i];
-      const T *row = L + m.pr[i] - lo_i;
-      const int col = r0 + lane;
-      tri[t * kTriStride + lane] = (col < i && col >= lo_i) ? row[col] : czero<T>();
+#pragma unroll
+    for (int u = 0; u < kRowsPerWarp; u++) {
+      const int t = warp + u * nw;
+      if (t < nb) {
+        const int i = r0 + t;
+        const int lo_i = m.lo[i];
+        const T *row = L + m.pr[i] - lo_i;
+        const int col = r0 + lane;
+        tri[t * kTriStride + lane] = (col < i && col >= lo_i) ? row[col] : czero<T>();
+      }
     }
     __syncthreads();
     if (warp == 0) {
@@ -442,13 +484,17 @@ __device__ void cta_backward(const CtaMeta &m, const T *__restrict__ L, T *y, T 
       if (lane < nb) y[r0 + lane] = val;
     }
     __syncthreads();
+    // columns left of the block: y_k -= sum_i L_ik x_i, loads issued
+    // unconditionally (clamped index, zero weight outside the row)
     const int kmin = m.bmin[blk];
     for (int k = kmin + tid; k < r0; k += blockDim.x) {
       T acc = czero<T>();
+#pragma unroll 8
       for (int t = 0; t < nb; t++) {
         const int i = r0 + t;
-        const int lo_i = m.lo[i];
-        if (k >= lo_i) acc = cadd(acc, cmul(L[m.pr[i] + (k - lo_i)], y[i]));
+        const int d = k - m.lo[i];
+        const T lv = L[m.pr[i] + max(d, 0)];
+        if (d >= 0) acc = cadd(acc, cmul(lv, y[i]));
       }
       y[k] = csub(y[k], acc);
     }
