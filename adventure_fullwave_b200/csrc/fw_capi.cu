@@ -201,6 +201,8 @@ int read_status(fwgpu_context *c, int32_t *status) {
   FW_CUDA(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(fw::CocgScalars), cudaMemcpyDeviceToHost, c->stream));
   FW_CUDA(cudaStreamSynchronize(c->stream));
   if (status) *status = c->h_sc->status;
+  if (c->h_sc->pad != 0)
+    return set_error(FWGPU_ERR_CUDA, "subdomain solve gave up waiting for a TMA copy");
   return FWGPU_OK;
 }
 
@@ -560,6 +562,7 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     for (int s = 0; s < nsub; s++) {
       const fw::SubHost &h = p.subs[s];
       const int32_t *idx1 = c->h_idx1.data() + p.sub_dof_off[s];
+      pos = (pos + 1) & ~(int64_t)1;  // every subdomain's envelope starts 16-byte aligned in FP32 too
       // reference skyline length (advlas_skyline.c:20-24)
       int64_t idx2 = 0;
       for (int i = 1; i < h.nmp; i++) idx2 += i - idx1[i];
@@ -591,15 +594,16 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     FW_TRY(c->upload(&c->d_env_lo, c->h_env_lo));
     FW_TRY(c->upload(&c->d_env_ptr, c->h_env_ptr));
     FW_TRY(c->upload(&c->d_env_dst, dst));
-    FW_TRY(c->alloc(&c->d_L64, pos));
+    // padding: bulk copies of a block may read up to 16 bytes past its end
+    FW_TRY(c->alloc(&c->d_L64, pos + 64));
     c->dp.env_lo = c->d_env_lo;
     c->dp.env_ptr = c->d_env_ptr;
-    if (c->opts.precision == FWGPU_PREC_FP32_IR) FW_TRY(c->alloc(&c->d_L32, pos));
+    if (c->opts.precision == FWGPU_PREC_FP32_IR) FW_TRY(c->alloc(&c->d_L32, pos + 64));
   }
   if (!c->factor_fresh) {
     // envelope values and LDL^T factor (the layout is fixed by the model)
     const int64_t pos = c->nlen_int;
-    FW_CUDA(cudaMemsetAsync(c->d_L64, 0, std::max<int64_t>(1, pos) * sizeof(double2), c->stream));
+    FW_CUDA(cudaMemsetAsync(c->d_L64, 0, (pos + 64) * sizeof(double2), c->stream));
     c->launches += c->opts.precision == FWGPU_PREC_FP32_IR ? 3 : 2;
     fw::launch_scatter_envelope(p.nnz_total, c->d_env_dst, c->d_aval, c->d_L64, c->stream);
     c->dp.L64 = c->d_L64;
@@ -607,7 +611,7 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     fw::launch_factor(c->dp, c->dp.int_off, c->d_env_lo, c->d_env_ptr, c->d_L64, c->d_mesh_status + 1, c->stream);
     FW_CUDA(cudaGetLastError());
     if (c->opts.precision == FWGPU_PREC_FP32_IR) {
-      fw::launch_to_fp32(pos, c->d_L64, c->d_L32, c->stream);
+      fw::launch_to_fp32(pos + 64, c->d_L64, c->d_L32, c->stream);
       c->dp.L32 = c->d_L32;
       c->dp.L64 = nullptr;
     }
