@@ -341,24 +341,18 @@ __global__ void __launch_bounds__(kThreads) subsolve_kernel(DevProblem p, int mo
 // ----------------------------------------------------------------------------
 // Block-row envelope substitutions, one CTA per subdomain.
 //
-// Rows are taken in blocks of kRB.  A block's rows are contiguous in the
-// envelope, so the whole block is brought into shared memory by one TMA bulk
-// copy (cp.async.bulk, completion on an mbarrier), double-buffered: block
-// b+1 is in flight while block b is computed.  Forward: the rectangle left
-// of the block (columns < r0) is a set of independent dot products spread
-// over the warps; the kRB x kRB triangle is then resolved by one warp with
-// shuffles from a padded shared tile (row stride kRB+1 keeps the column-wise
-// forward reads and the row-wise backward reads free of bank conflicts).
-// Backward: the block's triangle first, then the transposed rectangle update
-// of the columns left of the block, spread over all threads.  Blocks larger
-// than a staging buffer read the factor from global memory instead.  Every
-// mbarrier wait is bounded; on a timeout the CTA records an error, waits
-// (bounded) for its copies in flight and leaves at the next block boundary.
-constexpr int kRB = 16;            // rows per block
-constexpr int kTriStride = kRB + 1;
+// Rows are taken in blocks of 32.  Forward: the rectangle left of the block
+// (columns < r0) is a set of independent dot products, spread over all warps;
+// the 32x32 triangle inside the block is then resolved by one warp with
+// shuffles from a padded shared-memory tile (row stride 33 keeps both the
+// column-wise forward reads and the row-wise backward reads free of bank
+// conflicts).  Backward: the block's triangle first, then the transposed
+// rectangle update of the columns left of the block, spread over all threads.
+// The interior vector, the interface values and the row metadata of the
+// subdomain stay in shared memory; the factor streams from global memory.
+constexpr int kRB = 32;       // rows per block
+constexpr int kTriStride = 33;
 constexpr int kCtaThreads = 256;
-constexpr int kRowsPerWarp = (kRB + kCtaThreads / 32 - 1) / (kCtaThreads / 32);
-constexpr uint32_t kWaitTries = 1u << 20;
 
 template <typename T>
 __device__ __forceinline__ T shfl_idx(T v, int src);
@@ -382,119 +376,36 @@ __device__ __forceinline__ float2 from_d2<float2>(double2 a) {
   return make_float2((float)a.x, (float)a.y);
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-// 1D bulk copy global -> shared through the TMA unit (no multicast)
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// staging state of one CTA, in shared memory
-template <typename T>
-struct Staging {
-  T *buf[2];
-  uint64_t *bar;     // [2]
-  int32_t *ok;       // [2] block staged in buffer k
-  int32_t *e0;       // [2] first element held by buffer k
-  uint32_t *uses;    // [2] copies issued into buffer k
-  int32_t *abort;    // CTA gave up waiting
-  int32_t cap;       // elements per buffer
-};
-
 struct CtaMeta {
   const int32_t *lo;   // shared: first stored column of each interior row
   const int32_t *pr;   // shared: row start (column lo) relative to the subdomain base
   const int32_t *bmin; // shared: smallest lo of each row block
   int nI;
-  int nlen;            // stored entries of the subdomain
 };
 
-__device__ __forceinline__ int block_end(const CtaMeta &m, int r1) { return r1 < m.nI ? m.pr[r1] : m.nlen; }
-
-// thread 0: start the copy of rows [r0, r1) into buffer k
-template <typename T>
-__device__ void stage_issue(Staging<T> &st, const CtaMeta &m, const T *L, int k, int r0, int r1) {
-  constexpr int kAlign = 16 / (int)sizeof(T);
-  const int e_begin = m.pr[r0];
-  const int a0 = e_begin - (e_begin % kAlign);
-  int n = block_end(m, r1) - a0;
-  n = (n + kAlign - 1) / kAlign * kAlign;
-  if (n > 0 && n <= st.cap) {
-    fence_proxy_async();
-    mbar_arrive_expect_tx(&st.bar[k], (uint32_t)(n * sizeof(T)));
-    bulk_g2s(st.buf[k], L + a0, (uint32_t)(n * sizeof(T)), &st.bar[k]);
-    st.uses[k] += 1;
-    st.ok[k] = 1;
-    st.e0[k] = a0;
-  } else {
-    st.ok[k] = 0;
-  }
-}
-
-// all threads: wait for buffer k (bounded)
-template <typename T>
-__device__ __forceinline__ void stage_wait(Staging<T> &st, int k) {
-  if (!st.ok[k]) return;
-  const uint32_t parity = (st.uses[k] - 1u) & 1u;
-  uint32_t tries = 0;
-  while (!mbar_try_wait(&st.bar[k], parity)) {
-    if (++tries > kWaitTries) {
-      *st.abort = 1;
-      break;
-    }
-  }
-}
-
-// element e of the subdomain's envelope: from the staging buffer when the
-// current block is staged there, else from global memory
-template <typename T>
-__device__ __forceinline__ T env_at(const Staging<T> &st, int k, const T *__restrict__ L, int e) {
-  return st.ok[k] ? st.buf[k][e - st.e0[k]] : L[e];
-}
+// rows of a block handled by one warp (rows w, w+nw, ...); kRowsPerWarp
+// independent accumulators keep several loads in flight per lane
+constexpr int kRowsPerWarp = kRB / (kCtaThreads / 32);
 
 template <typename T>
-__device__ void cta_forward(const CtaMeta &m, const T *__restrict__ L, Staging<T> &st, uint32_t &seq, T *y, T *tri,
-                            T *rect) {
+__device__ void cta_forward(const CtaMeta &m, const T *__restrict__ L, T *y, T *tri, T *rect) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-  const int nblk = (m.nI + kRB - 1) / kRB;
-  if (tid == 0 && nblk > 0) stage_issue(st, m, L, seq & 1, 0, min(kRB, m.nI));
-  __syncthreads();
-  for (int bk = 0; bk < nblk; bk++) {
-    const int r0 = bk * kRB;
+  for (int r0 = 0; r0 < m.nI; r0 += kRB) {
     const int nb = min(kRB, m.nI - r0);
-    const int cur = (seq + bk) & 1;
-    if (tid == 0 && bk + 1 < nblk) stage_issue(st, m, L, (seq + bk + 1) & 1, r0 + kRB, min(r0 + 2 * kRB, m.nI));
-    stage_wait(st, cur);
-    int lo_u[kRowsPerWarp], len_u[kRowsPerWarp], off_u[kRowsPerWarp];
+    int lo_u[kRowsPerWarp], len_u[kRowsPerWarp];
+    const T *row_u[kRowsPerWarp];
     int maxlen = 0;
 #pragma unroll
     for (int u = 0; u < kRowsPerWarp; u++) {
       const int t = warp + u * nw;
+      const int i = r0 + t;
       if (t < nb) {
-        lo_u[u] = m.lo[r0 + t];
-        off_u[u] = m.pr[r0 + t] - lo_u[u];
+        lo_u[u] = m.lo[i];
+        row_u[u] = L + m.pr[i] - lo_u[u];
         len_u[u] = max(0, r0 - lo_u[u]);
       } else {
         lo_u[u] = 0;
-        off_u[u] = 0;
+        row_u[u] = L;
         len_u[u] = 0;
       }
       maxlen = max(maxlen, len_u[u]);
@@ -507,17 +418,17 @@ __device__ void cta_forward(const CtaMeta &m, const T *__restrict__ L, Staging<T
       for (int u = 0; u < kRowsPerWarp; u++) {
         if (k < len_u[u]) {
           const int col = lo_u[u] + k;
-          acc[u] = cadd(acc[u], cmul(env_at(st, cur, L, off_u[u] + col), y[col]));
+          acc[u] = cadd(acc[u], cmul(row_u[u][col], y[col]));
         }
       }
     }
+    // stage the block's triangle: tri[t][j] = L[r0+t][r0+j]
 #pragma unroll
     for (int u = 0; u < kRowsPerWarp; u++) {
       const int t = warp + u * nw;
-      if (t < nb && lane < kRB) {
+      if (t < nb) {
         const int col = r0 + lane;
-        tri[t * kTriStride + lane] =
-            (col < r0 + t && col >= lo_u[u]) ? env_at(st, cur, L, off_u[u] + col) : czero<T>();
+        tri[t * kTriStride + lane] = (col < r0 + t && col >= lo_u[u]) ? row_u[u][col] : czero<T>();
       }
     }
 #pragma unroll
@@ -531,14 +442,12 @@ __device__ void cta_forward(const CtaMeta &m, const T *__restrict__ L, Staging<T
       T val = lane < nb ? csub(y[r0 + lane], rect[lane]) : czero<T>();
       for (int j = 0; j < nb - 1; j++) {
         const T yj = shfl_idx(val, j);
-        if (lane > j && lane < nb) val = csub(val, cmul(tri[lane * kTriStride + j], yj));
+        if (lane > j) val = csub(val, cmul(tri[lane * kTriStride + j], yj));
       }
       if (lane < nb) y[r0 + lane] = val;
     }
     __syncthreads();
-    if (*st.abort) break;
   }
-  seq += nblk;
 }
 
 template <typename T>
@@ -548,30 +457,21 @@ __device__ void cta_diag(const CtaMeta &m, const T *__restrict__ L, T *y) {
 }
 
 template <typename T>
-__device__ void cta_backward(const CtaMeta &m, const T *__restrict__ L, Staging<T> &st, uint32_t &seq, T *y, T *tri) {
+__device__ void cta_backward(const CtaMeta &m, const T *__restrict__ L, T *y, T *tri) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
   const int nblk = (m.nI + kRB - 1) / kRB;
-  if (tid == 0 && nblk > 0) {
-    const int r0 = (nblk - 1) * kRB;
-    stage_issue(st, m, L, seq & 1, r0, m.nI);
-  }
-  __syncthreads();
-  for (int q = 0; q < nblk; q++) {
-    const int bk = nblk - 1 - q;
-    const int r0 = bk * kRB;
+  for (int blk = nblk - 1; blk >= 0; blk--) {
+    const int r0 = blk * kRB;
     const int nb = min(kRB, m.nI - r0);
-    const int cur = (seq + q) & 1;
-    if (tid == 0 && bk > 0) stage_issue(st, m, L, (seq + q + 1) & 1, r0 - kRB, r0);
-    stage_wait(st, cur);
 #pragma unroll
     for (int u = 0; u < kRowsPerWarp; u++) {
       const int t = warp + u * nw;
-      if (t < nb && lane < kRB) {
+      if (t < nb) {
         const int i = r0 + t;
         const int lo_i = m.lo[i];
+        const T *row = L + m.pr[i] - lo_i;
         const int col = r0 + lane;
-        tri[t * kTriStride + lane] =
-            (col < i && col >= lo_i) ? env_at(st, cur, L, m.pr[i] - lo_i + col) : czero<T>();
+        tri[t * kTriStride + lane] = (col < i && col >= lo_i) ? row[col] : czero<T>();
       }
     }
     __syncthreads();
@@ -584,63 +484,54 @@ __device__ void cta_backward(const CtaMeta &m, const T *__restrict__ L, Staging<
       if (lane < nb) y[r0 + lane] = val;
     }
     __syncthreads();
-    // columns left of the block: y_k -= sum_i L_ik x_i
-    const int kmin = m.bmin[bk];
+    // columns left of the block: y_k -= sum_i L_ik x_i, loads issued
+    // unconditionally (clamped index, zero weight outside the row)
+    const int kmin = m.bmin[blk];
     for (int k = kmin + tid; k < r0; k += blockDim.x) {
       T acc = czero<T>();
-#pragma unroll 4
+#pragma unroll 8
       for (int t = 0; t < nb; t++) {
         const int i = r0 + t;
         const int d = k - m.lo[i];
-        if (d >= 0) acc = cadd(acc, cmul(env_at(st, cur, L, m.pr[i] + d), y[i]));
+        const T lv = L[m.pr[i] + max(d, 0)];
+        if (d >= 0) acc = cadd(acc, cmul(lv, y[i]));
       }
       y[k] = csub(y[k], acc);
     }
     __syncthreads();
-    if (*st.abort) break;
   }
-  seq += nblk;
 }
 
 template <typename T>
-__device__ __forceinline__ void cta_solve(const CtaMeta &m, const T *__restrict__ L, Staging<T> &st, uint32_t &seq,
-                                          T *y, T *tri, T *rect) {
-  cta_forward<T>(m, L, st, seq, y, tri, rect);
-  if (*st.abort) return;
+__device__ __forceinline__ void cta_solve(const CtaMeta &m, const T *__restrict__ L, T *y, T *tri, T *rect) {
+  cta_forward<T>(m, L, y, tri, rect);
   cta_diag<T>(m, L, y);
-  cta_backward<T>(m, L, st, seq, y, tri);
-}
-
-// elements per staging buffer
-template <typename T>
-__host__ __device__ constexpr int staging_cap() {
-  return (int)(16384 / sizeof(T));
+  cta_backward<T>(m, L, y, tri);
 }
 
 // Shared-memory bytes of one subdomain CTA.
 __host__ __device__ inline size_t cta_smem_bytes(int nI, int nG, bool fp32) {
-  (void)nG;
   const int nblk = (nI + kRB - 1) / kRB;
   size_t b = 0;
-  b += (size_t)nI * 8 + (size_t)nblk * 4;  // lo, pr, bmin
+  b += (size_t)nI * 8 + (size_t)nblk * 4;        // lo, pr, bmin
   b = (b + 15) & ~(size_t)15;
-  const size_t elem = fp32 ? 8 : 16;
-  if (fp32) b += (size_t)nI * 32;          // x, b (FP64)
-  b += (size_t)nI * elem;                  // y
-  b += (size_t)kRB * kTriStride * elem + kRB * elem;
-  b = (b + 127) & ~(size_t)127;
-  b += 2 * 16384;                          // staging buffers
-  return b + 128;
+  b += (size_t)nG * 16;                           // v
+  if (fp32) {
+    b += (size_t)nI * 32;                         // x, b (FP64)
+    b += (size_t)nI * 8;                          // y (FP32)
+    b += (size_t)kRB * kTriStride * 8 + kRB * 8;  // tri, rect
+  } else {
+    b += (size_t)nI * 16;                         // y
+    b += (size_t)kRB * kTriStride * 16 + kRB * 16;
+  }
+  return b + 64;
 }
 
 template <bool kFp32>
 __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p, int mode) {
   using LT = typename std::conditional<kFp32, float2, double2>::type;
   if (mode == kModeIter && p.sc->status != 0) return;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ uint64_t s_bar[2];
-  __shared__ int32_t s_ok[2], s_e0[2], s_abort;
-  __shared__ uint32_t s_uses[2];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int s = p.sub_order[blockIdx.x];
   const int64_t io = p.int_off[s], go = p.if_off[s];
   const int nI = (int)(p.int_off[s + 1] - io);
@@ -652,6 +543,8 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
   int32_t *pr = lo + nI;
   int32_t *bmin = pr + nI;
   size_t off = ((size_t)nI * 8 + (size_t)nblk * 4 + 15) & ~(size_t)15;
+  double2 *v = (double2 *)(smem_raw + off);
+  off += (size_t)nG * 16;
   double2 *xd = nullptr, *bd = nullptr;
   if (kFp32) {
     xd = (double2 *)(smem_raw + off);
@@ -664,25 +557,6 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
   LT *tri = (LT *)(smem_raw + off);
   off += (size_t)kRB * kTriStride * sizeof(LT);
   LT *rect = (LT *)(smem_raw + off);
-  off += (size_t)kRB * sizeof(LT);
-  off = (off + 127) & ~(size_t)127;
-  Staging<LT> st;
-  st.buf[0] = (LT *)(smem_raw + off);
-  st.buf[1] = (LT *)(smem_raw + off + 16384);
-  st.bar = s_bar;
-  st.ok = s_ok;
-  st.e0 = s_e0;
-  st.uses = s_uses;
-  st.abort = &s_abort;
-  st.cap = staging_cap<LT>();
-  if (tid == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
-    s_uses[0] = s_uses[1] = 0;
-    s_ok[0] = s_ok[1] = 0;
-    s_abort = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
 
   const int64_t base = nI > 0 ? p.env_ptr[io] : 0;
   for (int i = tid; i < nI; i += blockDim.x) {
@@ -691,7 +565,6 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
   }
   const bool with_bc = mode != kModeFirst;
   const bool with_f = mode != kModeIter;
-  double2 *v = p.V + go;
   for (int k = tid; k < nG; k += blockDim.x) v[k] = with_bc ? p.P[p.if_ln[go + k]] : cz();
   __syncthreads();
   for (int b = tid; b < nblk; b += blockDim.x) {
@@ -700,7 +573,6 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
     for (int i = b * kRB; i < e; i++) mn = min(mn, lo[i]);
     bmin[b] = mn;
   }
-  const int nlen = nI > 0 ? pr[nI - 1] + (nI - 1 - lo[nI - 1]) + 1 : 0;
   // Dirichlet elimination: interior right-hand side f_I - A_IG v
   const int32_t *cptr = p.cpl_ptr + io + s;
   const int64_t cbase = p.cpl_off[s];
@@ -711,18 +583,19 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
     y[c] = from_d2<LT>(acc);
   }
   __syncthreads();
-  CtaMeta m{lo, pr, bmin, nI, nlen};
-  uint32_t seq = 0;
-  const LT *L = kFp32 ? (const LT *)p.L32 + base : (const LT *)p.L64 + base;
-  cta_solve<LT>(m, L, st, seq, y, tri, rect);
-  if (kFp32 && !s_abort) {
+  CtaMeta m{lo, pr, bmin, nI};
+  if (!kFp32) {
+    cta_solve<LT>(m, (const LT *)p.L64 + base, y, tri, rect);
+  } else {
+    const LT *L = (const LT *)p.L32 + base;
+    cta_solve<LT>(m, L, y, tri, rect);
     for (int c = tid; c < nI; c += blockDim.x) xd[c] = make_double2((double)y[c].x, (double)y[c].y);
     __syncthreads();
     const int32_t *aptr = p.aii_ptr + io + s;
     const int64_t abase = p.aii_off[s];
     __shared__ double red[kCtaThreads / 32];
     __shared__ int stop;
-    for (int step = 0; step < p.ir_steps && !s_abort; step++) {
+    for (int step = 0; step < p.ir_steps; step++) {
       // FP64 residual of the subdomain system, rounded into the FP32 work vector
       double rn = 0.0;
       for (int c = tid; c < nI; c += blockDim.x) {
@@ -749,24 +622,11 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
         if (stop) break;
       }
       __syncthreads();
-      cta_solve<LT>(m, L, st, seq, y, tri, rect);
+      cta_solve<LT>(m, L, y, tri, rect);
       for (int c = tid; c < nI; c += blockDim.x)
         xd[c] = cadd(xd[c], make_double2((double)y[c].x, (double)y[c].y));
       __syncthreads();
     }
-  }
-  if (s_abort) {
-    // leave no copy in flight into this CTA's shared memory
-    if (tid == 0) {
-      for (int k = 0; k < 2; k++) {
-        if (!s_ok[k]) continue;
-        uint32_t tries = 0;
-        while (!mbar_try_wait(&s_bar[k], (s_uses[k] - 1u) & 1u) && ++tries < kWaitTries) {
-        }
-      }
-      atomicMax(&p.sc->pad, 1);
-    }
-    return;
   }
   // q = A_G. x (- f_G)
   const int32_t *rptr = p.ifr_ptr + go + s;
@@ -793,6 +653,7 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
   if (mode == kModeLast) {
     for (int c = tid; c < nI; c += blockDim.x)
       yout[c] = kFp32 ? xd[c] : make_double2((double)y[c].x, (double)y[c].y);
+    for (int k = tid; k < nG; k += blockDim.x) p.V[go + k] = v[k];
   }
 }
 
@@ -1031,6 +892,7 @@ __global__ void set_status_kernel(CocgScalars *sc, double eps, int32_t max_loop)
   sc->max_loop = max_loop;
   sc->status = 0;
   sc->converged = 0;
+  sc->pad = 0;
 }
 
 // iteration state for kernel timing: never converges, no loop limit

@@ -130,14 +130,17 @@ def algorithmic_bytes(sz: dict, precision: str, ir_steps: int) -> int:
 
 def ncu_traffic(config: str, precision: str):
     """DRAM bytes per launch of the substitution kernel from the committed
-    ncu summary, when it covers this workload."""
-    path = os.path.join(REPO, "profiles", "subsolve_dram_traffic.json")
+    ncu summary (profiles/subsolve_cta_<config>_<precision>.md), when one
+    covers this workload."""
+    path = os.path.join(REPO, "profiles", f"subsolve_cta_{config}_{precision}.md")
     try:
-        with open(path) as f:
-            d = json.load(f)
-        return d.get(f"{config}_{precision}")
-    except Exception:
-        return None
+        for line in open(path):
+            t = line.split()
+            if len(t) == 4 and t[0] == "dram_bytes_per_launch" and t[1] == f"{config}_{precision}":
+                return int(t[3])
+    except OSError:
+        pass
+    return None
 
 
 def make_model(config: str):
