@@ -21,6 +21,7 @@ ERR_NOT_CONVERGED = -4
 ERR_BREAKDOWN = -5
 ERR_NOMEM = -6
 ERR_MESH = -7
+NOALLOC_MAX_ROWS = 262144
 
 PREC_FP64 = 0
 PREC_FP32_IR = 1
@@ -100,6 +101,9 @@ SIGNATURES = {
     "fwgpu_hddm_solve": [ctypes.c_void_p, P(FwSource), P(FwResult)],
     "fwgpu_hddm_resolve": [ctypes.c_void_p, P(FwSource), P(FwResult)],
     "fwgpu_profile_iteration": [ctypes.c_void_p, c_i32, P(FwKernelProfile)],
+    "fwgpu_skyline_solve_noalloc": [c_i32, c_i32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p],
     "fwgpu_get_edge_solution": [ctypes.c_void_p, P(c_dbl)],
     "fwgpu_get_history": [ctypes.c_void_p, P(c_dbl), c_i32, P(c_i32)],
     "fwgpu_get_subdomain_maps": [ctypes.c_void_p, c_i32, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32),

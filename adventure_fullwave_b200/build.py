@@ -19,6 +19,7 @@ SOURCES = [
     ("fw_element.cu", ["-fmad=false"]),
     ("fw_kernels.cu", []),
     ("fw_capi.cu", []),
+    ("fw_noalloc.cu", []),
     ("fw_build.cpp", []),
 ]
 

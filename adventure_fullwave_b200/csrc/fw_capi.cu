@@ -32,6 +32,11 @@ int set_error(int code, const std::string &msg) {
 
 }  // namespace
 
+namespace fw {
+// error text for fwgpu_last_error from entry points outside this file
+void record_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace fw
+
 struct fwgpu_context {
   fw::Model m;
   fw::Plan p;

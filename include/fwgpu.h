@@ -217,6 +217,38 @@ typedef struct {
  * times whole phases with gettimeofday, lib/std/timefunc.c:17-111). */
 int fwgpu_profile_iteration(fwgpu_context *ctx, int32_t reps, fwgpu_kernel_profile *out);
 
+/* -- batched skyline substitution without device allocation -------------- */
+
+/* Rows of the fixed device work array behind fwgpu_skyline_solve_noalloc:
+ * 262,144 complex FP64 values (4 MiB), held by every GPU that loads the
+ * library until the process exits. */
+#define FWGPU_NOALLOC_MAX_ROWS 262144
+
+/* Solves L D L^T x = b for a batch of skyline-factored systems on the
+ * current device without allocating any device memory.  No counterpart in
+ * the reference: it is for callers that cannot call cudaMalloc when they
+ * solve (a host framework that owns the device memory through its own pool,
+ * or a real-time loop that must not enter the allocator), so every buffer
+ * is theirs and the work vectors live in a fixed device array.
+ *
+ * Systems use the reference's skyline layout (advlas_skyline.c:12-128):
+ * system s has rows d_row_off[s]..d_row_off[s+1]-1 of d_idx1/d_idx2 (its
+ * own row numbering), entries d_mat[2*(d_mat_off[s] + idx2[i] + j)] for
+ * j = idx1[i]..i, unit L off the diagonal and 1/d on it (what
+ * fwgpu_get_factor returns).  d_b and d_x hold 2*total_rows doubles
+ * (interleaved complex).  All pointers are device memory; the kernel runs on
+ * `stream` (a cudaStream_t, NULL for the default stream) and the call
+ * returns without synchronising.
+ *
+ * total_rows may not exceed FWGPU_NOALLOC_MAX_ROWS (FWGPU_ERR_ARG
+ * otherwise).  The first call on each device looks up the work array's
+ * device address, so make it before any stream capture.  All calls share
+ * the work array: calls whose kernels overlap on one GPU race and must be
+ * ordered by the caller. */
+int fwgpu_skyline_solve_noalloc(int32_t n_systems, int32_t total_rows, const int32_t *d_row_off,
+                                const int64_t *d_mat_off, const int32_t *d_idx1, const int32_t *d_idx2,
+                                const double *d_mat, const double *d_b, double *d_x, void *stream);
+
 /* -- results -------------------------------------------------------------- */
 
 /* Edge solution per global edge (2*n_edges doubles).  Every subdomain holding
