@@ -101,6 +101,8 @@ SIGNATURES = {
     "fwgpu_hddm_solve": [ctypes.c_void_p, P(FwSource), P(FwResult)],
     "fwgpu_hddm_resolve": [ctypes.c_void_p, P(FwSource), P(FwResult)],
     "fwgpu_profile_iteration": [ctypes.c_void_p, c_i32, P(FwKernelProfile)],
+    "fwgpu_adjoint_gradient": [ctypes.c_void_p, c_i32, P(c_i32), c_i32, P(c_i32), P(c_dbl), P(c_dbl), P(c_dbl),
+                               P(FwResult)],
     "fwgpu_skyline_solve_noalloc": [c_i32, c_i32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p],

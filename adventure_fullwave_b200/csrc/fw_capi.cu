@@ -69,6 +69,8 @@ struct fwgpu_context {
   double2 *d_fI = nullptr, *d_fG = nullptr;
   int64_t *d_edge_src = nullptr;
   double2 *d_xedge = nullptr;
+  double2 *d_xfwd = nullptr;        // forward solution kept during an adjoint solve
+  int32_t *d_te = nullptr;          // tet edges (adjoint gradient)
   fw::DevProblem dp{};
   fw::CocgScalars *d_sc = nullptr;
   fw::CocgScalars *h_sc = nullptr;  // pinned
@@ -747,6 +749,64 @@ int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *
   FW_CUDA(cudaEventRecord(c->ev[3], c->stream));
   FW_CUDA(cudaStreamSynchronize(c->stream));
   return fill_result(c, res);
+}
+
+int fwgpu_adjoint_gradient(fwgpu_context *c, int32_t n_probe, const int32_t *probe_edges, int32_t n_design,
+                           const int32_t *design_tets, double *J, double *grad_eps, double *grad_sigma,
+                           fwgpu_result *adjoint_result) {
+  if (!c || n_probe < 0 || n_design < 0 || (n_probe > 0 && !probe_edges) || (n_design > 0 && !design_tets))
+    return set_error(FWGPU_ERR_ARG, "bad argument");
+  if (c->stage < 4) return set_error(FWGPU_ERR_STATE, "adjoint needs a forward solve");
+  for (int k = 0; k < n_probe; k++)
+    if (probe_edges[k] < 0 || probe_edges[k] >= c->m.ne) return set_error(FWGPU_ERR_ARG, "probe edge out of range");
+  for (int k = 0; k < n_design; k++)
+    if (design_tets[k] < 0 || design_tets[k] >= c->m.nt) return set_error(FWGPU_ERR_ARG, "design element out of range");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  const int64_t ne = c->m.ne;
+  if (!c->d_xfwd) FW_TRY(c->alloc(&c->d_xfwd, ne));
+  if (!c->d_te) FW_TRY(c->upload(&c->d_te, c->m.te));
+  FW_CUDA(cudaMemcpyAsync(c->d_xfwd, c->d_xedge, ne * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+  std::vector<double2> xh(ne);
+  FW_CUDA(cudaMemcpyAsync(xh.data(), c->d_xedge, ne * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  // J and the adjoint source dJ/dx = conj(x_P)
+  double Jv = 0.0;
+  std::vector<int32_t> pe(probe_edges, probe_edges + n_probe);
+  std::vector<double> pv(2 * (size_t)n_probe);
+  for (int k = 0; k < n_probe; k++) {
+    const double2 v = xh[pe[k]];
+    Jv += v.x * v.x + v.y * v.y;
+    pv[2 * k] = v.x;
+    pv[2 * k + 1] = -v.y;
+  }
+  if (J) *J = Jv;
+  fwgpu_source src{n_probe, pe.data(), pv.data()};
+  fwgpu_result res{};
+  const int rc = fwgpu_hddm_resolve(c, &src, &res);
+  if (adjoint_result) *adjoint_result = res;
+  if (rc != FWGPU_OK && rc != FWGPU_ERR_NOT_CONVERGED) return rc;
+  // gradient from the forward solution and the adjoint solution
+  int32_t *d_design = nullptr;
+  double *d_g = nullptr;
+  std::vector<int32_t> dt(design_tets, design_tets + n_design);
+  FW_TRY(c->upload(&d_design, dt));
+  FW_TRY(c->alloc(&d_g, 2 * (size_t)std::max(1, n_design)));
+  fw::launch_adjoint_gradient(n_design, d_design, c->d_tv, c->d_te, c->d_crd, c->m.omega, c->d_xfwd, c->d_xedge, d_g,
+                              d_g + std::max(1, n_design), c->stream);
+  c->launches += 1;
+  FW_CUDA(cudaGetLastError());
+  std::vector<double> gh(2 * (size_t)std::max(1, n_design));
+  FW_CUDA(cudaMemcpyAsync(gh.data(), d_g, gh.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  // the forward solution stays the context's result
+  FW_CUDA(cudaMemcpyAsync(c->d_xedge, c->d_xfwd, ne * sizeof(double2), cudaMemcpyDeviceToDevice, c->stream));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  c->release(d_design);
+  c->release(d_g);
+  for (int k = 0; k < n_design; k++) {
+    if (grad_eps) grad_eps[k] = gh[k];
+    if (grad_sigma) grad_sigma[k] = gh[std::max(1, n_design) + k];
+  }
+  return rc;
 }
 
 int fwgpu_profile_iteration(fwgpu_context *c, int32_t reps, fwgpu_kernel_profile *out) {

@@ -28,29 +28,15 @@ __constant__ int c_tet_n[6][4] = {{0, 1, 2, 3}, {0, 2, 3, 1}, {0, 3, 1, 2}, {1, 
 // 1/mu0 as the reference hard-codes it (make_elem_em.c:37)
 __device__ __forceinline__ double nu_const() { return 7.957747e+05; }
 
-// One thread per element.  el_order[k] is the global element of element slot
-// k; the slot's 6x6 complex matrix is written to out[k*72 .. k*72+71]
-// (row-major, interleaved re/im), rows and columns in the reference's edge
-// table order 01,02,03,12,13,23.  status[0] is raised to 1 when an element
-// has a non-positive volume or an edge with coincident end points (the
-// reference aborts with emessage 2050 there, tetrahedral.c:257-258).
-__global__ void element_matrices_kernel(int64_t n_el, const int32_t *__restrict__ el_order,
-                                        const int32_t *__restrict__ tet_vertices, const double *__restrict__ crd,
-                                        const double *__restrict__ el_eps, const double *__restrict__ el_sigma,
-                                        double omega, double *__restrict__ out, int32_t *__restrict__ status) {
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n_el) return;
-  const int t = el_order[k];
-  double x[4], y[4], z[4];
-  for (int i = 0; i < 4; i++) {
-    const int64_t v = tet_vertices[4 * (int64_t)t + i];
-    x[i] = crd[3 * v + 0];
-    y[i] = crd[3 * v + 1];
-    z[i] = crd[3 * v + 2];
-  }
-  const double eps = el_eps[t];
-  const double sigma = el_sigma[t];
+// Geometry of one tetrahedron as the reference's element routine builds it.
+struct TetGeom {
+  double D, drr, dss;
+  double lsi[6], xi[6], yi[6], zi[6], X[6], Y[6], Z[6], xy[6], yz[6], zx[6], g[3], gxx[6];
+  bool bad;
+};
 
+__device__ __forceinline__ void tet_geometry(const double *x, const double *y, const double *z, TetGeom &G) {
+  G.bad = false;
   // 6 x volume, summed term by term in the reference's order
   double D = -x[0] * y[1] * z[2];
   D = D + x[0] * y[1] * z[3];
@@ -76,56 +62,53 @@ __global__ void element_matrices_kernel(int64_t n_el, const int32_t *__restrict_
   D = D + x[3] * y[1] * z[2];
   D = D + x[3] * y[2] * z[0];
   D = D - x[3] * y[2] * z[1];
-  if (!(D > 0.0)) atomicMax(status, 1);
-
-  double l[6], lsi[6], xi[6], yi[6], zi[6], X[6], Y[6], Z[6], xy[6], yz[6], zx[6];
-  int si[6];
+  if (!(D > 0.0)) G.bad = true;
+  G.D = D;
   for (int i = 0; i < 6; i++) {
     const int a = c_tet_n[i][0], b = c_tet_n[i][1];
     const double dx = x[a] - x[b], dy = y[a] - y[b], dz = z[a] - z[b];
-    l[i] = sqrt(dx * dx + dy * dy + dz * dz);
+    const double l = sqrt(dx * dx + dy * dy + dz * dz);
     // orientation from the first non-zero of (x_b - x_a, y_b - y_a, z_b - z_a)
+    int si;
     double pp = x[b] - x[a];
     if (pp > 0.0) {
-      si[i] = 1;
+      si = 1;
     } else if (pp < 0.0) {
-      si[i] = -1;
+      si = -1;
     } else {
       pp = y[b] - y[a];
       if (pp > 0.0) {
-        si[i] = 1;
+        si = 1;
       } else if (pp < 0.0) {
-        si[i] = -1;
+        si = -1;
       } else {
         pp = z[b] - z[a];
         if (pp > 0.0) {
-          si[i] = 1;
+          si = 1;
         } else if (pp < 0.0) {
-          si[i] = -1;
+          si = -1;
         } else {
-          si[i] = 0;
-          atomicMax(status, 1);
+          si = 0;
+          G.bad = true;
         }
       }
     }
     const int p = c_tet_n[i][2], q = c_tet_n[i][3];
-    xi[i] = x[q] - x[p];
-    yi[i] = y[q] - y[p];
-    zi[i] = z[q] - z[p];
-    const double d = l[i] * (double)si[i];
-    X[i] = d * xi[i];
-    Y[i] = d * yi[i];
-    Z[i] = d * zi[i];
-    xy[i] = x[p] * y[q] - x[q] * y[p];
-    yz[i] = y[p] * z[q] - y[q] * z[p];
-    zx[i] = z[p] * x[q] - z[q] * x[p];
-    lsi[i] = l[i] * (double)si[i];
+    G.xi[i] = x[q] - x[p];
+    G.yi[i] = y[q] - y[p];
+    G.zi[i] = z[q] - z[p];
+    const double d = l * (double)si;
+    G.X[i] = d * G.xi[i];
+    G.Y[i] = d * G.yi[i];
+    G.Z[i] = d * G.zi[i];
+    G.xy[i] = x[p] * y[q] - x[q] * y[p];
+    G.yz[i] = y[p] * z[q] - y[q] * z[p];
+    G.zx[i] = z[p] * x[q] - z[q] * x[p];
+    G.lsi[i] = l * (double)si;
   }
-  double g[3];
-  g[0] = (x[0] + x[1] + x[2] + x[3]) * 0.25;
-  g[1] = (y[0] + y[1] + y[2] + y[3]) * 0.25;
-  g[2] = (z[0] + z[1] + z[2] + z[3]) * 0.25;
-
+  G.g[0] = (x[0] + x[1] + x[2] + x[3]) * 0.25;
+  G.g[1] = (y[0] + y[1] + y[2] + y[3]) * 0.25;
+  G.g[2] = (z[0] + z[1] + z[2] + z[3]) * 0.25;
   // second moments of the vertex coordinates (sideside, tetrahedral.c:377-398)
   double sx = 0.0, sy = 0.0, sz = 0.0;
   for (int i = 0; i < 4; i++) {
@@ -133,41 +116,82 @@ __global__ void element_matrices_kernel(int64_t n_el, const int32_t *__restrict_
     sy += y[i];
     sz += z[i];
   }
-  double gxx[6];
-  gxx[0] = sx * sx;
-  gxx[1] = sy * sy;
-  gxx[2] = sz * sz;
-  gxx[3] = sx * sy;
-  gxx[4] = sy * sz;
-  gxx[5] = sz * sx;
+  G.gxx[0] = sx * sx;
+  G.gxx[1] = sy * sy;
+  G.gxx[2] = sz * sz;
+  G.gxx[3] = sx * sy;
+  G.gxx[4] = sy * sz;
+  G.gxx[5] = sz * sx;
   for (int i = 0; i < 4; i++) {
-    gxx[0] += x[i] * x[i];
-    gxx[1] += y[i] * y[i];
-    gxx[2] += z[i] * z[i];
-    gxx[3] += x[i] * y[i];
-    gxx[4] += y[i] * z[i];
-    gxx[5] += z[i] * x[i];
+    G.gxx[0] += x[i] * x[i];
+    G.gxx[1] += y[i] * y[i];
+    G.gxx[2] += z[i] * z[i];
+    G.gxx[3] += x[i] * y[i];
+    G.gxx[4] += y[i] * z[i];
+    G.gxx[5] += z[i] * x[i];
   }
-  for (int i = 0; i < 6; i++) gxx[i] *= 0.05;
+  for (int i = 0; i < 6; i++) G.gxx[i] *= 0.05;
+  G.drr = 2.0 / (3.0 * D);
+  G.dss = 1.0 / (6.0 * D);
+}
 
-  const double drr = 2.0 / (3.0 * D);
-  const double dss = 1.0 / (6.0 * D);
+// (rot u_i, rot u_j) of the reference (tetNedelec_rotrot)
+__device__ __forceinline__ double tet_rr(const TetGeom &G, int i, int j) {
+  return G.drr * (G.X[i] * G.X[j] + G.Y[i] * G.Y[j] + G.Z[i] * G.Z[j]);
+}
+
+// (u_i, u_j) of the reference (tetNedelec_sideside)
+__device__ __forceinline__ double tet_ss(const TetGeom &G, int i, int j) {
+  const double *zi = G.zi, *yi = G.yi, *xi = G.xi, *yz = G.yz, *zx = G.zx, *xy = G.xy, *gxx = G.gxx, *g = G.g;
+  double e = -zi[i] * (-zi[j] * gxx[1] + yi[j] * gxx[4] + yz[j] * g[1]);
+  e = e + yi[i] * (-zi[j] * gxx[4] + yi[j] * gxx[2] + yz[j] * g[2]);
+  e = e + yz[i] * (-zi[j] * g[1] + yi[j] * g[2] + yz[j]);
+  e = e - xi[i] * (-xi[j] * gxx[2] + zi[j] * gxx[5] + zx[j] * g[2]);
+  e = e + zi[i] * (-xi[j] * gxx[5] + zi[j] * gxx[0] + zx[j] * g[0]);
+  e = e + zx[i] * (-xi[j] * g[2] + zi[j] * g[0] + zx[j]);
+  e = e - yi[i] * (-yi[j] * gxx[0] + xi[j] * gxx[3] + xy[j] * g[0]);
+  e = e + xi[i] * (-yi[j] * gxx[3] + xi[j] * gxx[1] + xy[j] * g[1]);
+  e = e + xy[i] * (-yi[j] * g[0] + xi[j] * g[1] + xy[j]);
+  return G.lsi[i] * G.lsi[j] * G.dss * e;
+}
+
+__device__ __forceinline__ void load_tet(int t, const int32_t *__restrict__ tet_vertices, const double *__restrict__ crd,
+                                         double *x, double *y, double *z) {
+  for (int i = 0; i < 4; i++) {
+    const int64_t v = tet_vertices[4 * (int64_t)t + i];
+    x[i] = crd[3 * v + 0];
+    y[i] = crd[3 * v + 1];
+    z[i] = crd[3 * v + 2];
+  }
+}
+
+// One thread per element.  el_order[k] is the global element of element slot
+// k; the slot's 6x6 complex matrix is written to out[k*72 .. k*72+71]
+// (row-major, interleaved re/im), rows and columns in the reference's edge
+// table order 01,02,03,12,13,23.  status[0] is raised to 1 when an element
+// has a non-positive volume or an edge with coincident end points (the
+// reference aborts with emessage 2050 there, tetrahedral.c:257-258).
+__global__ void element_matrices_kernel(int64_t n_el, const int32_t *__restrict__ el_order,
+                                        const int32_t *__restrict__ tet_vertices, const double *__restrict__ crd,
+                                        const double *__restrict__ el_eps, const double *__restrict__ el_sigma,
+                                        double omega, double *__restrict__ out, int32_t *__restrict__ status) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_el) return;
+  const int t = el_order[k];
+  double x[4], y[4], z[4];
+  load_tet(t, tet_vertices, crd, x, y, z);
+  const double eps = el_eps[t];
+  const double sigma = el_sigma[t];
+  TetGeom G;
+  tet_geometry(x, y, z, G);
+  if (G.bad) atomicMax(status, 1);
   const double nu_omega = nu_const() / omega;
   const double dd = -(eps * omega);
   double *o = out + k * 72;
   for (int i = 0; i < 6; i++) {
     for (int j = 0; j < 6; j++) {
-      const double rr = drr * (X[i] * X[j] + Y[i] * Y[j] + Z[i] * Z[j]);
-      double e = -zi[i] * (-zi[j] * gxx[1] + yi[j] * gxx[4] + yz[j] * g[1]);
-      e = e + yi[i] * (-zi[j] * gxx[4] + yi[j] * gxx[2] + yz[j] * g[2]);
-      e = e + yz[i] * (-zi[j] * g[1] + yi[j] * g[2] + yz[j]);
-      e = e - xi[i] * (-xi[j] * gxx[2] + zi[j] * gxx[5] + zx[j] * g[2]);
-      e = e + zi[i] * (-xi[j] * gxx[5] + zi[j] * gxx[0] + zx[j] * g[0]);
-      e = e + zx[i] * (-xi[j] * g[2] + zi[j] * g[0] + zx[j]);
-      e = e - yi[i] * (-yi[j] * gxx[0] + xi[j] * gxx[3] + xy[j] * g[0]);
-      e = e + xi[i] * (-yi[j] * gxx[3] + xi[j] * gxx[1] + xy[j] * g[1]);
-      e = e + xy[i] * (-yi[j] * g[0] + xi[j] * g[1] + xy[j]);
-      const double ss = lsi[i] * lsi[j] * dss * e;
+      const double rr = tet_rr(G, i, j);
+      const double ss = tet_ss(G, i, j);
       // ae.re = 0 + nu_omega*rr, then += dd*ss; ae.im = 0 + sigma*ss
       double re = 0.0;
       re += nu_omega * rr;
@@ -180,6 +204,48 @@ __global__ void element_matrices_kernel(int64_t n_el, const int32_t *__restrict_
   }
 }
 
+// Adjoint gradient of J(x) with respect to each design element's
+// permittivity eps [F/m] and conductivity sigma [S/m].  With A x = b and
+// A lambda = dJ/dx (A = A^T), dJ/dp = -2 Re(lambda_e^T (dA_e/dp) x_e) and,
+// from A_e = (nu/omega) RR - (eps omega) SS + i sigma SS
+// (make_elem_em.c:227-265), dA_e/deps = -omega SS_e, dA_e/dsigma = i SS_e:
+//   dJ/deps = 2 omega Re(s),  dJ/dsigma = 2 Im(s),  s = lambda_e^T SS_e x_e.
+// SS_e is recomputed from the coordinates, not stored.
+__global__ void adjoint_gradient_kernel(int32_t n_design, const int32_t *__restrict__ design_tets,
+                                        const int32_t *__restrict__ tet_vertices,
+                                        const int32_t *__restrict__ tet_edges, const double *__restrict__ crd,
+                                        double omega, const double2 *__restrict__ x, const double2 *__restrict__ lam,
+                                        double *__restrict__ g_eps, double *__restrict__ g_sigma) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_design) return;
+  const int t = design_tets[k];
+  double vx[4], vy[4], vz[4];
+  load_tet(t, tet_vertices, crd, vx, vy, vz);
+  TetGeom G;
+  tet_geometry(vx, vy, vz, G);
+  // element DOFs in the edge table order: file mid-node slots 0,1,2,3,5,4
+  const int file_slot[6] = {0, 1, 2, 3, 5, 4};
+  double2 xe[6], le[6];
+  for (int i = 0; i < 6; i++) {
+    const int e = tet_edges[6 * (int64_t)t + file_slot[i]];
+    xe[i] = x[e];
+    le[i] = lam[e];
+  }
+  double sr = 0.0, si = 0.0;
+  for (int i = 0; i < 6; i++) {
+    double ar = 0.0, ai = 0.0;
+    for (int j = 0; j < 6; j++) {
+      const double ss = tet_ss(G, i, j);
+      ar += ss * xe[j].x;
+      ai += ss * xe[j].y;
+    }
+    sr += le[i].x * ar - le[i].y * ai;
+    si += le[i].x * ai + le[i].y * ar;
+  }
+  g_eps[k] = 2.0 * omega * sr;
+  g_sigma[k] = 2.0 * si;
+}
+
 void launch_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
                              const double *el_eps, const double *el_sigma, double omega, double *out,
                              int32_t *status, cudaStream_t stream) {
@@ -188,6 +254,14 @@ void launch_element_matrices(int64_t n_el, const int32_t *el_order, const int32_
   const int64_t blocks = (n_el + threads - 1) / threads;
   element_matrices_kernel<<<(unsigned)blocks, threads, 0, stream>>>(n_el, el_order, tet_vertices, crd, el_eps,
                                                                      el_sigma, omega, out, status);
+}
+
+void launch_adjoint_gradient(int32_t n_design, const int32_t *design_tets, const int32_t *tet_vertices,
+                             const int32_t *tet_edges, const double *crd, double omega, const double2 *x,
+                             const double2 *lam, double *g_eps, double *g_sigma, cudaStream_t stream) {
+  if (n_design <= 0) return;
+  adjoint_gradient_kernel<<<(n_design + 127) / 128, 128, 0, stream>>>(n_design, design_tets, tet_vertices, tet_edges,
+                                                                      crd, omega, x, lam, g_eps, g_sigma);
 }
 
 }  // namespace fw

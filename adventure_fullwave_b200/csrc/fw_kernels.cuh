@@ -101,6 +101,9 @@ void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream);
 void launch_edge_solution(int64_t ne, const int64_t *edge_src, const double2 *Y, const double2 *V, double2 *x,
                           cudaStream_t stream);
 void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream);
+void launch_adjoint_gradient(int32_t n_design, const int32_t *design_tets, const int32_t *tet_vertices,
+                             const int32_t *tet_edges, const double *crd, double omega, const double2 *x,
+                             const double2 *lam, double *g_eps, double *g_sigma, cudaStream_t stream);
 void launch_profile_reset(CocgScalars *sc, cudaStream_t stream);
 
 }  // namespace fw

@@ -223,6 +223,25 @@ class HddmSolver:
                           float(r.final_resi_l2), float(r.t_setup_ms), float(r.t_iterate_ms), float(r.t_last_ms),
                           int(r.kernel_launches))
 
+    def adjoint_gradient(self, probe_edges=None, design_tets=None):
+        """Backward of the last ``solve``: J = sum |x_p|^2 over ``probe_edges``
+        and its gradient with respect to the permittivity eps [F/m] and
+        conductivity sigma [S/m] of every element of ``design_tets``, by one
+        adjoint HDDM solve on the same factors.  Returns
+        (J, dJ/deps, dJ/dsigma, adjoint HddmResult)."""
+        pe = np.ascontiguousarray(self.model.probe_edges if probe_edges is None else probe_edges, dtype=np.int32)
+        dt = np.ascontiguousarray(self.model.design_tets if design_tets is None else design_tets, dtype=np.int32)
+        ge = np.zeros(max(1, dt.shape[0]), np.float64)
+        gs = np.zeros(max(1, dt.shape[0]), np.float64)
+        J = ctypes.c_double()
+        res = _lib.FwResult()
+        _lib.check(self._lib.fwgpu_adjoint_gradient(self._h, int(pe.shape[0]), _ptr(pe, ctypes.c_int32),
+                                                    int(dt.shape[0]), _ptr(dt, ctypes.c_int32), ctypes.byref(J),
+                                                    _ptr(ge, ctypes.c_double), _ptr(gs, ctypes.c_double),
+                                                    ctypes.byref(res)), allow=(_lib.ERR_NOT_CONVERGED,))
+        n = dt.shape[0]
+        return J.value, ge[:n], gs[:n], self._result(res)
+
     def profile_iteration(self, reps: int = 50) -> dict:
         """Average device time of the kernels of one interface iteration
         (CUDA events on the solver's stream).  Overwrites the iteration
@@ -283,6 +302,12 @@ class HddmSolver:
         m = np.zeros(2 * nlen, np.float64)
         _lib.check(self._lib.fwgpu_get_factor(self._h, s, _ptr(m, ctypes.c_double)))
         return m[0::2] + 1j * m[1::2]
+
+
+def relative_permittivity_gradient(g_eps: np.ndarray, g_sigma: np.ndarray, omega: float, eps0: float = 8.854e-12):
+    """Gradient with respect to eps_r = eps' - i eps'' of each design element
+    (eps = eps0 eps', sigma = omega eps0 eps''): (dJ/deps', dJ/deps'')."""
+    return eps0 * np.asarray(g_eps), omega * eps0 * np.asarray(g_sigma)
 
 
 def hddm_solver_CS(model, source=0, **opts) -> Tuple[np.ndarray, HddmResult]:

@@ -60,6 +60,9 @@ class Model:
     nsub: int
     # sources: list of right-hand sides; each is (edge ids (k,), values complex (k,))
     sources: List[Tuple[np.ndarray, np.ndarray]]
+    # adjoint design problem: tets with their own flag (complex eps_r), probe edges
+    design_tets: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, np.int32))
+    probe_edges: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, np.int32))
 
     @property
     def n_vertices(self) -> int:
@@ -251,15 +254,25 @@ CONFIGS = {
     "c1": dict(n=16, size=1.0, npml=4, layers=None, nleaves=64, leaf_cap=None, jitter=None),
     "c2": dict(n=48, size=1.5, npml=6, layers=8, nleaves=None, leaf_cap=600, jitter=(0.3, 0.7)),
     "c3": dict(n=96, size=1.5, npml=8, layers=8, nleaves=None, leaf_cap=900, jitter=(0.3, 0.7)),
+    "c4": dict(n=48, size=1.5, npml=6, layers=8, nleaves=None, leaf_cap=600, jitter=(0.3, 0.7), design=12,
+               nprobes=8),
     "c5": dict(n=112, size=1.5, npml=8, layers=8, nleaves=None, leaf_cap=1000, jitter=(0.3, 0.7),
                inclusions=0.05, nsources=16),
 }
 
 
+def design_material(eps_re: np.ndarray, eps_im: np.ndarray, omega: float):
+    """Absolute permittivity and conductivity of a complex relative
+    permittivity eps_r = eps' - i eps'': A_e = (nu/omega) RR - omega eps0 eps_r SS
+    = (nu/omega) RR - (eps omega) SS + i sigma SS with eps = eps0 eps' and
+    sigma = omega eps0 eps'' (the reference's convention, make_elem_em.c:230-265)."""
+    return EPS0 * np.asarray(eps_re), omega * EPS0 * np.asarray(eps_im)
+
+
 def make_model(name: str = "c1", n: Optional[int] = None, size: Optional[float] = None, npml: Optional[int] = None,
                layers: Optional[int] = "default", nleaves: Optional[int] = "default", leaf_cap: Optional[int] = "default",
                jitter="default", freq: float = 300e6, seed: int = 0, inclusions: float = 0.0,
-               nsources: int = 1) -> Model:
+               nsources: int = 1, design: int = 0, nprobes: int = 0) -> Model:
     """Build a named configuration (``c1``, ``c2``, ``c3``, ``c5``) or a
     custom one by overriding its fields.  Unknown names start from ``c1``."""
     base = dict(CONFIGS.get(name, CONFIGS["c1"]))
@@ -279,6 +292,8 @@ def make_model(name: str = "c1", n: Optional[int] = None, size: Optional[float] 
         base["jitter"] = jitter
     inclusions = base.get("inclusions", inclusions) if inclusions == 0.0 else inclusions
     nsources = base.get("nsources", nsources) if nsources == 1 else nsources
+    design = base.get("design", design) if design == 0 else design
+    nprobes = base.get("nprobes", nprobes) if nprobes == 0 else nprobes
     n_, L, npml_ = base["n"], base["size"], base["npml"]
     rng = np.random.default_rng(seed)
     crd, tets, cell_of_tet, cidx = kuhn_mesh(n_, L)
@@ -313,6 +328,25 @@ def make_model(name: str = "c1", n: Optional[int] = None, size: Optional[float] 
             mat_flag.append(base_flag + k)
             mat_eps.append(EPS0 * epsr_inc[k])
             mat_sigma.append(sig_l[layer[t]])
+    design_tets = np.zeros(0, np.int32)
+    omega = 2.0 * math.pi * freq
+    if design > 0:
+        # central design^3 cells, each tet with its own flag and complex eps_r
+        lo_c = (n_ - design) // 2
+        cc = np.stack([c[cell_of_tet] for c in cidx], axis=1)
+        inside = np.all((cc >= lo_c) & (cc < lo_c + design), axis=1)
+        design_tets = np.nonzero(inside)[0].astype(np.int32)
+        drng = np.random.default_rng(seed + 101)
+        er = drng.uniform(2.0, 4.0, size=design_tets.shape[0])
+        ei = drng.uniform(0.0, 0.1, size=design_tets.shape[0])
+        de, ds = design_material(er, ei, omega)
+        base_flag = len(mat_flag)
+        flag = flag.copy()
+        for k, t in enumerate(design_tets):
+            flag[t] = base_flag + k
+            mat_flag.append(base_flag + k)
+            mat_eps.append(de[k])
+            mat_sigma.append(ds[k])
     centroids = crd[tets].mean(axis=1)
     sub = rcb_partition(centroids, leaf_cap=base["leaf_cap"], nleaves=base["nleaves"], jitter=base["jitter"],
                         seed=seed + 1)
@@ -325,11 +359,25 @@ def make_model(name: str = "c1", n: Optional[int] = None, size: Optional[float] 
         hi = L - (npml_ + 2) * h
         for s in range(1, nsources):
             sources.append(dipole_source(edges, crd, rng.uniform(lo, hi, size=3)))
+    probe_edges = np.zeros(0, np.int32)
+    if nprobes > 0:
+        # seeded interior edges outside the PML and outside the design box
+        prng = np.random.default_rng(seed + 202)
+        mid = 0.5 * (crd[edges[:, 0]] + crd[edges[:, 1]])
+        lo_x, hi_x = (npml_ + 0.5) * h, L - (npml_ + 0.5) * h
+        ok = np.all((mid > lo_x) & (mid < hi_x), axis=1)
+        if design > 0:
+            dlo = ((n_ - design) // 2) * h
+            dhi = ((n_ - design) // 2 + design) * h
+            ok &= ~np.all((mid >= dlo) & (mid <= dhi), axis=1)
+        cand = np.nonzero(ok)[0]
+        probe_edges = np.sort(prng.choice(cand, size=min(nprobes, cand.shape[0]), replace=False)).astype(np.int32)
     model = Model(
         name=name, n=n_, size=L, vertex_crd=crd, tets=tets, tet_edges=tet_edges, edges=edges,
         flag=flag.astype(np.int32), mat_flag=np.asarray(mat_flag, dtype=np.int32),
         mat_eps=np.asarray(mat_eps, dtype=np.float64), mat_sigma=np.asarray(mat_sigma, dtype=np.float64),
-        omega=2.0 * math.pi * freq, pec_edge=pec_edges(edges, crd, L), sub_of_tet=sub, nsub=nsub, sources=sources)
+        omega=omega, pec_edge=pec_edges(edges, crd, L), sub_of_tet=sub, nsub=nsub, sources=sources,
+        design_tets=design_tets, probe_edges=probe_edges)
     return model
 
 

@@ -44,6 +44,8 @@ WORKLOADS = {
           "centre z-dipole, jittered RCB (leaf cap 600) 1 part x 1654 subdomains",
     "c3": "C3: [0,1.5]^3 96^3 hexes x 6 tets (5,308,416 tets), 8 random layers, 8-cell PML, PEC wall, 300 MHz, "
           "centre z-dipole, jittered RCB (leaf cap 900)",
+    "c4": "C4: the C2 mesh and medium with a central 12^3-cell design region (10,368 tets, per-tet complex eps_r, "
+          "eps' ~ U[2,4], eps'' ~ U[0,0.1]); J = sum |E|^2 on 8 probe edges; forward solve + adjoint gradient",
 }
 # COCG iterations to 1e-6 of the FP64 GPU solve on each model (B200, this
 # code); the reference's CPU time is extrapolated with them where running the
@@ -246,6 +248,21 @@ def run_ours(args):
     sz = solver.sizes()
     x_check = solver.edge_solution()
 
+    adjoint = None
+    if len(model.design_tets) > 0:
+        # the backward: one adjoint HDDM solve on the forward factors plus the gradient kernel
+        fwd, adj = [], []
+        for _ in range(args.steps):
+            r = solver.solve(0)
+            fwd.append((r.t_setup_ms + r.t_iterate_ms + r.t_last_ms) / 1e3)
+            t0 = time.perf_counter()
+            J, ge, gs, ra = solver.adjoint_gradient()
+            adj.append(time.perf_counter() - t0)
+        adjoint = {"forward_s": float(np.mean(fwd)), "adjoint_s": float(np.mean(adj)),
+                   "adjoint_over_forward": float(np.mean(adj) / np.mean(fwd)), "J": J,
+                   "adjoint_iterations": ra.iterations, "n_design": int(len(model.design_tets)),
+                   "grad_finite": bool(np.all(np.isfinite(ge)) and np.all(np.isfinite(gs)))}
+
     # kernel timing of the dominant kernel for the roofline
     prof = solver.profile_iteration(reps=args.prof_reps)
     solver.resolve(0)
@@ -310,6 +327,8 @@ def run_ours(args):
         "gpu_launches": int(np.sum(launches)),
         "solution_check": {"finite": bool(np.all(np.isfinite(x_check))), "final_resi": results[-1].final_resi},
     }
+    if adjoint is not None:
+        line["adjoint"] = adjoint
     print(json.dumps(line))
     return 0
 
@@ -336,7 +355,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_ir"])
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--max-loop", type=int, default=50000)

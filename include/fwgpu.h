@@ -201,6 +201,23 @@ int fwgpu_hddm_solve(fwgpu_context *ctx, const fwgpu_source *src, fwgpu_result *
  * on the existing factors (multi-source runs). */
 int fwgpu_hddm_resolve(fwgpu_context *ctx, const fwgpu_source *src, fwgpu_result *result);
 
+/* -- adjoint ------------------------------------------------------------- */
+
+/* Backward of fwgpu_hddm_solve (the forward).  No reference counterpart.
+ * For J = sum_p |x_p|^2 over the probe edges of the forward solution x, one
+ * adjoint HDDM solve A lambda = conj(x_P) on the forward factors (A = A^T)
+ * gives, per listed element e with edge values x_e, lambda_e and mass
+ * matrix SS_e (recomputed, lib/fem/tetrahedral.c:362-422),
+ *   grad_eps[k]   = dJ/d eps_e   = 2 omega Re(lambda_e^T SS_e x_e)   [per F/m]
+ *   grad_sigma[k] = dJ/d sigma_e = 2 Im(lambda_e^T SS_e x_e)         [per S/m]
+ * for the element matrix (nu/omega) RR - (eps omega) SS + i sigma SS
+ * (lib/fem/make_elem_em.c:227-265).  J receives the objective, the adjoint
+ * solve's COCG figures go to adjoint_result; fwgpu_get_edge_solution still
+ * returns the forward solution afterwards. */
+int fwgpu_adjoint_gradient(fwgpu_context *ctx, int32_t n_probe, const int32_t *probe_edges, int32_t n_design,
+                           const int32_t *design_tets, double *J, double *grad_eps, double *grad_sigma,
+                           fwgpu_result *adjoint_result);
+
 /* -- measurement ---------------------------------------------------------- */
 
 typedef struct {

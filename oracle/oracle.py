@@ -231,3 +231,45 @@ def factor_sub(model, sub: SubData):
     if n < 0:
         raise RuntimeError("factor buffer too small")
     return idx1, idx2, n, mat[0:2 * n:2] + 1j * mat[1:2 * n:2]
+
+
+def element_ss(model, t: int) -> np.ndarray:
+    """Mass matrix SS_e (tetNedelec_sideside) of element t in the edge-table
+    order, from the restated element routine: with eps = 0 and sigma = 1 its
+    imaginary part is exactly SS_e (make_elem_em.c:254-265)."""
+    lib = load()
+    v = model.tets[t]
+    xyz = np.ascontiguousarray(np.concatenate([model.vertex_crd[v, 0], model.vertex_crd[v, 1],
+                                               model.vertex_crd[v, 2]]), np.float64)
+    ae = np.zeros(72, np.float64)
+    lib.orc_element_matrix.restype = ctypes.c_int
+    lib.orc_element_matrix(_p(xyz, ctypes.c_double), ctypes.c_double(0.0), ctypes.c_double(1.0),
+                           ctypes.c_double(model.omega), _p(ae, ctypes.c_double))
+    return ae[1::2].reshape(6, 6)
+
+
+def adjoint_gradient(model, probe_edges, design_tets, hddm_eps: float = 1e-12, hddm_max_loop: int = 20000):
+    """FP64 reference gradient of J = sum_p |x_p|^2 with respect to eps [F/m]
+    and sigma [S/m] of each design element: forward and adjoint HDDM solves
+    with the restated reference solver, then dJ/deps = 2 omega Re(s),
+    dJ/dsigma = 2 Im(s), s = lambda_e^T SS_e x_e."""
+    part = partition(model, 0)
+    x, _, _, _ = hddm(model, part, hddm_eps, hddm_max_loop)
+    pe = np.asarray(probe_edges)
+    J = float(np.sum(np.abs(x[pe]) ** 2))
+    part_adj = partition(model, (pe, np.conj(x[pe])))
+    lam, _, _, _ = hddm(model, part_adj, hddm_eps, hddm_max_loop)
+    ge = np.zeros(len(design_tets))
+    gs = np.zeros(len(design_tets))
+    for k, t in enumerate(design_tets):
+        edges = model.tet_edges[t][FILE_SLOT]
+        s = lam[edges] @ element_ss(model, int(t)) @ x[edges]
+        ge[k] = 2.0 * model.omega * s.real
+        gs[k] = 2.0 * s.imag
+    return J, ge, gs, x
+
+
+def objective(model, probe_edges, hddm_eps: float = 1e-12, hddm_max_loop: int = 20000) -> float:
+    part = partition(model, 0)
+    x, _, _, _ = hddm(model, part, hddm_eps, hddm_max_loop)
+    return float(np.sum(np.abs(x[np.asarray(probe_edges)]) ** 2))
