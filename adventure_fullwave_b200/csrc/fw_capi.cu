@@ -80,6 +80,8 @@ struct fwgpu_context {
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool factor_bad = false;
   bool factor_fresh = false;       // factor matches the assembled values
+  bool solve_tuned = false;        // the subdomain-solve kernel has been chosen
+  bool warp_ok = false;            // the warp-per-subdomain kernel fits in shared memory
   int64_t launches = 0;            // kernels launched since the last reset
   int64_t *d_env_dst = nullptr;    // lower entry -> envelope position (-1: outside)
 
@@ -274,6 +276,10 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   c->opts = *opts;
   if (c->opts.graph_iterations <= 0) c->opts.graph_iterations = 16;
   if (c->opts.ir_max_steps <= 0) c->opts.ir_max_steps = 1;
+  if (c->opts.solve_kernel < FWGPU_SOLVE_AUTO || c->opts.solve_kernel > FWGPU_SOLVE_GLOBAL) {
+    delete c;
+    return set_error(FWGPU_ERR_ARG, "unknown solve_kernel");
+  }
   fw::Model &m = c->m;
   {
     int rc = model_from_mesh(mesh, m);
@@ -363,6 +369,41 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   dp.gq_ptr = ip;
   FW_TRY(c->upload(&lp, p.gq_slot));
   dp.gq_slot = lp;
+  {
+    // global row pointers and column maps of the grid-wide products of the staged solve
+    const int64_t nI_all = p.sub_int_off[nsub], nG_all = p.sub_if_off[nsub];
+    std::vector<int64_t> crp(nI_all + 1, 0), irp(nG_all + 1, 0), arp(nI_all + 1, 0);
+    std::vector<int32_t> cg(p.cpl_col.size()), ig(p.ifr_col.size()), ag(p.aii_col.size());
+    for (int s = 0; s < nsub; s++) {
+      const int64_t io = p.sub_int_off[s], go = p.sub_if_off[s];
+      const int nI = (int)(p.sub_int_off[s + 1] - io), nG = (int)(p.sub_if_off[s + 1] - go);
+      for (int cI = 0; cI <= nI; cI++) {
+        crp[io + cI] = cpl_off[s] + p.cpl_ptr[io + s + cI];
+        arp[io + cI] = aii_off[s] + p.aii_ptr[io + s + cI];
+      }
+      for (int k = 0; k <= nG; k++) irp[go + k] = ifr_off[s] + p.ifr_ptr[go + s + k];
+      for (int64_t q = cpl_off[s]; q < cpl_off[s + 1]; q++) cg[q] = p.if_ln[go + p.cpl_col[q]];
+      for (int64_t q = ifr_off[s]; q < ifr_off[s + 1]; q++) {
+        const int col = p.ifr_col[q];
+        ig[q] = col >= 0 ? (int32_t)(io + col) : -p.if_ln[go + (-col - 1)] - 1;
+      }
+      for (int64_t q = aii_off[s]; q < aii_off[s + 1]; q++) ag[q] = (int32_t)(io + p.aii_col[q]);
+    }
+    FW_TRY(c->upload(&lp, crp));
+    dp.cpl_rowptr = lp;
+    FW_TRY(c->upload(&ip, cg));
+    dp.cpl_gcol = ip;
+    FW_TRY(c->upload(&lp, irp));
+    dp.ifr_rowptr = lp;
+    FW_TRY(c->upload(&ip, ig));
+    dp.ifr_gcol = ip;
+    FW_TRY(c->upload(&lp, arp));
+    dp.aii_rowptr = lp;
+    FW_TRY(c->upload(&ip, ag));
+    dp.aii_gcol = ip;
+    dp.n_interior = nI_all;
+    dp.n_slots = nG_all;
+  }
   FW_TRY(c->alloc(&c->d_cpl_val, p.cpl_src.size()));
   FW_TRY(c->alloc(&c->d_ifr_val, p.ifr_src.size()));
   FW_TRY(c->alloc(&c->d_pcloc, p.if_diag_src.size()));
@@ -379,6 +420,7 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   if (opts->precision == FWGPU_PREC_FP32_IR) {
     FW_TRY(c->alloc(&dp.B, nI_tot));
     FW_TRY(c->alloc(&dp.Y32, nI_tot));
+    FW_TRY(c->alloc(&dp.Rres, nI_tot));
   }
   const int64_t nf = std::max<int64_t>(1, p.total_free);
   FW_TRY(c->alloc(&dp.P, nf));
@@ -403,6 +445,24 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
     const bool fp32 = opts->precision == FWGPU_PREC_FP32_IR;
     const size_t smem = fw::subsolve_smem_bytes(p.max_interior, p.max_iface, fp32);
     dp.cta_smem = fw::configure_subsolve(smem) == 0 ? (int32_t)smem : 0;
+    dp.max_interior = p.max_interior;
+    dp.max_iface = p.max_iface;
+    // the staged kernel's layout depends on the envelope: it is checked in solve_dom_1st
+    switch (c->opts.solve_kernel) {
+      case FWGPU_SOLVE_WARP:
+        dp.solve_variant = fw::kSolveWarp;
+        break;
+      case FWGPU_SOLVE_CTA:
+        if (dp.cta_smem == 0) return set_error(FWGPU_ERR_ARG, "CTA solve kernel: subdomains too large for shared memory");
+        dp.solve_variant = fw::kSolveCta;
+        break;
+      case FWGPU_SOLVE_GLOBAL:
+        dp.solve_variant = fw::kSolveGlobal;
+        break;
+      default:
+        dp.solve_variant = dp.cta_smem > 0 ? fw::kSolveCta : fw::kSolveGlobal;
+    }
+    c->solve_tuned = c->opts.solve_kernel != FWGPU_SOLVE_AUTO;
   }
   // per-edge solution source: the first subdomain holding each edge
   std::vector<int64_t> esrc(m.ne, -1);
@@ -545,6 +605,89 @@ int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
   return FWGPU_OK;
 }
 
+// Row blocks of the staged solve: at most 32 rows, and stored entries that
+// fit one staging buffer, so that one bulk copy brings a whole block in.
+static int build_stage_blocks(fwgpu_context *c) {
+  const fw::Plan &p = c->p;
+  const int nsub = c->m.nsub;
+  const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
+  int maxrow = 0;
+  for (int s = 0; s < nsub; s++) {
+    const int64_t io = p.sub_int_off[s];
+    const int nI = (int)(p.sub_int_off[s + 1] - io);
+    for (int r = 0; r < nI; r++) maxrow = std::max(maxrow, r - c->h_env_lo[io + r] + 1);
+  }
+  int cap = fp32 ? 2048 : 1024;
+  cap = std::max(cap, (maxrow + 2 + 7) & ~7);
+  std::vector<int32_t> boff(nsub + 1, 0);
+  std::vector<int2> btab;
+  int max_blocks = 0;
+  for (int s = 0; s < nsub; s++) {
+    const int64_t io = p.sub_int_off[s];
+    const int nI = (int)(p.sub_int_off[s + 1] - io);
+    const int64_t base = nI > 0 ? c->h_env_ptr[io] : 0;
+    boff[s] = (int32_t)btab.size();
+    auto row_end = [&](int r) { return (int)(c->h_env_ptr[io + r] - base) + (r - c->h_env_lo[io + r]) + 1; };
+    int r = 0, nb = 0;
+    while (r < nI) {
+      const int r_start = r;
+      const int e0 = (int)(c->h_env_ptr[io + r] - base);
+      int rows = 0;
+      while (r < nI && rows < 32) {
+        if (rows > 0 && row_end(r) - e0 > cap - 2) break;
+        r++;
+        rows++;
+      }
+      btab.push_back(make_int2(r_start, e0));
+      nb++;
+    }
+    btab.push_back(make_int2(nI, nI > 0 ? row_end(nI - 1) : 0));
+    max_blocks = std::max(max_blocks, nb);
+  }
+  boff[nsub] = (int32_t)btab.size();
+  int32_t *d_boff = nullptr;
+  int2 *d_btab = nullptr;
+  FW_TRY(c->upload(&d_boff, boff));
+  FW_TRY(c->upload(&d_btab, btab));
+  c->dp.blk_off = d_boff;
+  c->dp.blk_tab = d_btab;
+  c->dp.max_blocks = max_blocks;
+  c->dp.stage_cap = cap;
+  const size_t smem = fw::subsolve_staged_smem_bytes(p.max_interior, max_blocks, cap, fp32);
+  c->warp_ok = fw::configure_subsolve_staged(smem) == 0;
+  return FWGPU_OK;
+}
+
+// Times the candidate subdomain-solve kernels on the factors just computed
+// (first-solve mode, whose outputs the real first solve then overwrites) and
+// keeps the fastest.
+static int tune_solve_kernel(fwgpu_context *c) {
+  const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
+  const int cand[2] = {fw::kSolveWarp, fw::kSolveCta};
+  float best = -1.f;
+  int pick = c->dp.solve_variant;
+  for (int v : cand) {
+    if (v == fw::kSolveWarp && !c->warp_ok) continue;
+    if (v == fw::kSolveCta && c->dp.cta_smem == 0) continue;
+    c->dp.solve_variant = v;
+    fw::launch_subsolve(c->dp, fw::kModeFirst, fp32, c->stream);
+    FW_CUDA(cudaEventRecord(c->ev[4], c->stream));
+    for (int r = 0; r < 3; r++) fw::launch_subsolve(c->dp, fw::kModeFirst, fp32, c->stream);
+    FW_CUDA(cudaEventRecord(c->ev[5], c->stream));
+    FW_CUDA(cudaEventSynchronize(c->ev[5]));
+    c->launches += 4 * fw::subsolve_launches(c->dp, fp32);
+    float ms = 0.f;
+    FW_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
+    if (best < 0.f || ms < best) {
+      best = ms;
+      pick = v;
+    }
+  }
+  c->dp.solve_variant = pick;
+  c->solve_tuned = true;
+  return FWGPU_OK;
+}
+
 int fwgpu_solve_dom_1st(fwgpu_context *c) {
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (c->stage < 1) return set_error(FWGPU_ERR_STATE, "solve_dom_1st before make_tmp_aij");
@@ -606,6 +749,9 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     c->dp.env_lo = c->d_env_lo;
     c->dp.env_ptr = c->d_env_ptr;
     if (c->opts.precision == FWGPU_PREC_FP32_IR) FW_TRY(c->alloc(&c->d_L32, pos + 64));
+    FW_TRY(build_stage_blocks(c));
+    if (c->opts.solve_kernel == FWGPU_SOLVE_WARP && !c->warp_ok)
+      return set_error(FWGPU_ERR_ARG, "staged solve kernel: subdomains too large for shared memory");
   }
   if (!c->factor_fresh) {
     // envelope values and LDL^T factor (the layout is fixed by the model)
@@ -627,13 +773,19 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     FW_CUDA(cudaStreamSynchronize(c->stream));
     c->factor_bad = fstat != 0;
     c->factor_fresh = true;
+    if (!c->solve_tuned) FW_TRY(tune_solve_kernel(c));
   }
   fw::launch_subsolve(c->dp, fw::kModeFirst, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
-  c->launches += 1;
+  c->launches += fw::subsolve_launches(c->dp, c->opts.precision == FWGPU_PREC_FP32_IR);
   FW_CUDA(cudaGetLastError());
   c->stage = 2;
   if (c->factor_bad) return set_error(FWGPU_ERR_BREAKDOWN, "zero or non-finite pivot in a subdomain factor");
   return FWGPU_OK;
+}
+
+// kernels of one interface iteration: the subdomain solve and 6 COCG kernels
+static int64_t iteration_launches(const fwgpu_context *c) {
+  return 6 + fw::subsolve_launches(c->dp, c->opts.precision == FWGPU_PREC_FP32_IR);
 }
 
 int fwgpu_iteration_s_1st(fwgpu_context *c, int32_t *status) {
@@ -654,7 +806,7 @@ int fwgpu_iteration_s(fwgpu_context *c, int32_t *status) {
   if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "iteration_s outside the interface loop");
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_cocg_iteration(c->dp, c->stream);
-  c->launches += 7;
+  c->launches += iteration_launches(c);
   FW_CUDA(cudaGetLastError());
   FW_TRY(read_status(c, status));
   return FWGPU_OK;
@@ -666,7 +818,7 @@ int fwgpu_solve_dom_last(fwgpu_context *c) {
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_subsolve(c->dp, fw::kModeLast, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
   fw::launch_edge_solution(c->m.ne, c->d_edge_src, c->dp.Y, c->dp.V, c->d_xedge, c->stream);
-  c->launches += 2;
+  c->launches += 1 + fw::subsolve_launches(c->dp, c->opts.precision == FWGPU_PREC_FP32_IR);
   FW_CUDA(cudaGetLastError());
   FW_CUDA(cudaStreamSynchronize(c->stream));
   c->stage = 4;
@@ -687,7 +839,7 @@ static int run_loop(fwgpu_context *c, fwgpu_result *res) {
   int32_t st = c->h_sc->status;
   while (st == 0) {
     FW_CUDA(cudaGraphLaunch(c->graph, c->stream));
-    c->launches += 7 * (int64_t)c->graph_iters;
+    c->launches += iteration_launches(c) * (int64_t)c->graph_iters;
     FW_TRY(read_status(c, &st));
   }
   (void)res;
@@ -711,6 +863,8 @@ static int fill_result(fwgpu_context *c, fwgpu_result *res) {
     cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]);
     res->t_last_ms = ms;
     res->kernel_launches = c->launches;
+    res->solve_kernel = c->dp.solve_variant + 1;
+    res->reserved = 0;
   }
   return sc.converged ? FWGPU_OK : set_error(FWGPU_ERR_NOT_CONVERGED, "hddm_max_loop reached before hddm_eps");
 }
@@ -740,6 +894,7 @@ int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *
   c->launches = 1;
   FW_TRY(build_rhs(c, src));
   fw::launch_subsolve(c->dp, fw::kModeFirst, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
+  c->launches += fw::subsolve_launches(c->dp, c->opts.precision == FWGPU_PREC_FP32_IR);
   int32_t st = 0;
   FW_TRY(fwgpu_iteration_s_1st(c, &st));
   FW_CUDA(cudaEventRecord(c->ev[1], c->stream));

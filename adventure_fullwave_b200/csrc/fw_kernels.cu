@@ -14,6 +14,7 @@
 // One warp works on one subdomain; warps take subdomains largest first.
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cstdint>
 #include <type_traits>
 
@@ -658,6 +659,457 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
 }
 
 // ----------------------------------------------------------------------------
+// Staged subdomain solve: one warp per subdomain, row blocks brought into
+// shared memory by TMA bulk copies.
+//
+// The iteration's subdomain work is split in three launches:
+//   rhs_kernel           f_I - A_IG v for every interior row of every
+//                        subdomain (SetBC, aij_matrix_func.h:60-136),
+//   subsolve_staged_kernel  the envelope substitutions, one warp per subdomain,
+//   iface_product_kernel q = A_G.[x; v] (- f_G) for every interface slot.
+// The two products are grid-wide sparse products: every row of every
+// subdomain in parallel, a few lanes per row, coalesced.  The substitution
+// warp therefore only streams its factor.
+//
+// A subdomain's rows are cut on the host into blocks of at most 32 rows whose
+// stored entries fit one staging buffer (blk_tab).  The block's entries are
+// contiguous in the envelope, so one cp.async.bulk copies the whole block
+// into shared memory, completing on an mbarrier; the copy of block b+1 is in
+// flight while block b is computed (two buffers per warp).  The backward sweep
+// starts on the two blocks the forward sweep left in the buffers.
+//   forward  - entries left of the block: lanes across a row (conflict-free
+//              shared loads of the entry and of y[col]), 8 rows at a time,
+//              one transpose-reduction per 8 rows; then the triangle, one
+//              lane per row, one broadcast shuffle per row; the pivot scaling
+//              z = y/d is written to the z stash for the backward sweep.
+//   backward - the triangle with lanes over columns, then the transposed
+//              update of the columns left of the block (lanes over columns,
+//              rows in the inner loop).
+// With no CTA barrier anywhere, several subdomain warps share an SM and hide
+// each other's dependent chains.  The arithmetic is the reference's
+// row-oriented envelope substitution (advlas_skyline.c:134-167) with the sums
+// regrouped.  Every mbarrier wait is bounded: on a timeout the warp raises
+// the error word and goes on (the host reports the solve as failed).
+constexpr int kSB = 32;        // rows per block at most, one per lane
+constexpr int kSGroup = 8;     // rows whose partial sums are reduced together
+constexpr uint32_t kStageWaitTries = 1u << 22;
+
+__host__ __device__ inline size_t a16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+struct StageLayout {
+  size_t y, buf0, buf1, xb, meta, bar, blk, total;
+};
+
+// Shared-memory slice of one subdomain warp of the staged solve.
+__host__ __device__ inline StageLayout stage_layout(int max_interior, int max_blocks, int cap, bool fp32) {
+  const size_t es = fp32 ? 8 : 16;
+  StageLayout l;
+  size_t o = 0;
+  l.y = o;
+  o += a16((size_t)max_interior * es);
+  l.buf0 = o;
+  o += a16((size_t)cap * es);
+  l.buf1 = o;
+  o += a16((size_t)cap * es);
+  l.xb = o;
+  o += a16(kSB * es);
+  l.meta = o;
+  o += kSB * 8;
+  l.bar = o;
+  o += 16;
+  l.blk = o;
+  o += a16(((size_t)max_blocks + 1) * 8);
+  l.total = o;
+  return l;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// 1D bulk copy global -> shared through the TMA unit (no multicast)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+template <typename T>
+struct Stage {
+  const T *L;          // the subdomain's envelope (global)
+  T *buf0, *buf1;      // shared staging buffers
+  uint64_t *bar;       // [2]
+  const int2 *blk;     // shared: (first row, first element) of each block, then (nI, entries)
+  uint32_t uses0, uses1;  // copies issued into each buffer (warp-uniform)
+  int32_t *err;        // error word raised on a wait timeout
+};
+
+// 16-byte aligned element range of block b
+template <typename T>
+__device__ __forceinline__ int stage_a0(const Stage<T> &st, int b) {
+  constexpr int kA = 16 / (int)sizeof(T);
+  return st.blk[b].y & ~(kA - 1);
+}
+
+// lane 0 starts the copy of block b into buffer b & 1; all lanes count it
+template <typename T>
+__device__ __forceinline__ void stage_issue(Stage<T> &st, int b, int lane) {
+  constexpr int kA = 16 / (int)sizeof(T);
+  const int k = b & 1;
+  if (lane == 0) {
+    const int a0 = stage_a0(st, b);
+    const int n = (st.blk[b + 1].y - a0 + kA - 1) & ~(kA - 1);
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&st.bar[k], (uint32_t)(n * sizeof(T)));
+    bulk_g2s(k ? st.buf1 : st.buf0, st.L + a0, (uint32_t)(n * sizeof(T)), &st.bar[k]);
+  }
+  if (k)
+    st.uses1 += 1;
+  else
+    st.uses0 += 1;
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_wait(Stage<T> &st, int b) {
+  const int k = b & 1;
+  const uint32_t uses = k ? st.uses1 : st.uses0;
+  if (uses == 0) return;
+  const uint32_t parity = (uses - 1u) & 1u;
+  uint32_t tries = 0;
+  while (!mbar_try_wait(&st.bar[k], parity)) {
+    if (++tries > kStageWaitTries) {
+      *st.err = 1;
+      break;
+    }
+  }
+}
+
+// lo and start (relative to the subdomain's envelope) of row r0 + lane
+__device__ __forceinline__ void stage_row_meta(const int32_t *lo_g, const int64_t *ptr_g, int64_t base, int r0,
+                                               int r1, int lane, int &lo, int &pr) {
+  const int i = r0 + lane;
+  if (i < r1) {
+    lo = lo_g[i];
+    pr = (int)(ptr_g[i] - base);
+  } else {
+    lo = INT_MAX / 2;
+    pr = 0;
+  }
+}
+
+// 8 complex partial sums per lane -> lanes 4r..4r+3 hold the warp total of row r
+template <typename T>
+__device__ __forceinline__ T transpose_reduce8(const T (&a)[kSGroup], int lane) {
+  const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+  T b[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) b[i] = cadd(h16 ? a[i + 4] : a[i], shfl_xor(h16 ? a[i] : a[i + 4], 16));
+  T c[2];
+#pragma unroll
+  for (int i = 0; i < 2; i++) c[i] = cadd(h8 ? b[i + 2] : b[i], shfl_xor(h8 ? b[i] : b[i + 2], 8));
+  T d = cadd(h4 ? c[1] : c[0], shfl_xor(h4 ? c[0] : c[1], 4));
+  d = cadd(d, shfl_xor(d, 2));
+  d = cadd(d, shfl_xor(d, 1));
+  return d;
+}
+
+template <typename T>
+__device__ void staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
+                               T *y, int2 *meta, T *zstash, int lane) {
+  int nlo, npr;
+  stage_issue(st, 0, lane);
+  stage_row_meta(lo_g, ptr_g, base, st.blk[0].x, st.blk[1].x, lane, nlo, npr);
+  for (int b = 0; b < nblk; b++) {
+    const int r0 = st.blk[b].x, nb = st.blk[b + 1].x - r0;
+    const int my_lo = nlo, my_pr = npr;
+    meta[lane] = make_int2(nlo, npr);
+    if (b + 1 < nblk) {
+      stage_issue(st, b + 1, lane);
+      stage_row_meta(lo_g, ptr_g, base, st.blk[b + 1].x, st.blk[b + 2].x, lane, nlo, npr);
+    }
+    stage_wait(st, b);
+    __syncwarp();
+    const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);  // S[e]: entry e of the envelope
+    // entries left of the block; the loads of 8 rows are issued together
+    T rect = czero<T>();
+    for (int g = 0; g < nb; g += kSGroup) {
+      int2 mt[kSGroup];
+      int len[kSGroup];
+#pragma unroll
+      for (int u = 0; u < kSGroup; u++) {
+        mt[u] = meta[g + u];
+        len[u] = g + u < nb ? max(0, r0 - mt[u].x) : 0;
+      }
+      T a0[kSGroup], b0[kSGroup], a1[kSGroup], b1[kSGroup];
+#pragma unroll
+      for (int u = 0; u < kSGroup; u++) {
+        const bool c0 = lane < len[u], c1 = lane + 32 < len[u];
+        a0[u] = c0 ? S[mt[u].y + lane] : czero<T>();
+        b0[u] = c0 ? y[mt[u].x + lane] : czero<T>();
+        a1[u] = c1 ? S[mt[u].y + lane + 32] : czero<T>();
+        b1[u] = c1 ? y[mt[u].x + lane + 32] : czero<T>();
+      }
+      T acc[kSGroup];
+      int longest = 0;
+#pragma unroll
+      for (int u = 0; u < kSGroup; u++) {
+        acc[u] = cadd(cmul(a0[u], b0[u]), cmul(a1[u], b1[u]));
+        longest = max(longest, len[u]);
+      }
+      if (longest > 64) {
+#pragma unroll
+        for (int u = 0; u < kSGroup; u++)
+          for (int k = lane + 64; k < len[u]; k += 32) acc[u] = cadd(acc[u], cmul(S[mt[u].y + k], y[mt[u].x + k]));
+      }
+      const T sum = transpose_reduce8(acc, lane);
+      const T pick = shfl_idx(sum, 4 * (lane & 7));
+      if ((lane >> 3) == (g >> 3)) rect = pick;
+    }
+    // the block's triangle: lane t holds row r0 + t; the operands of 4 steps
+    // are loaded ahead of their shuffles
+    T val = lane < nb ? csub(y[r0 + lane], rect) : czero<T>();
+    const T *mine = S + my_pr - my_lo;  // mine[col]: this lane's row at column col
+    for (int j0 = 0; j0 < nb - 1; j0 += 4) {
+      T op[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int j = j0 + u;
+        op[u] = (lane > j && r0 + j >= my_lo) ? mine[r0 + j] : czero<T>();
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const T yj = shfl_idx(val, min(j0 + u, 31));
+        val = csub(val, cmul(op[u], yj));
+      }
+    }
+    if (lane < nb) {
+      y[r0 + lane] = val;
+      zstash[r0 + lane] = cmul(val, mine[r0 + lane]);  // 1/d on the diagonal
+    }
+    __syncwarp();
+  }
+}
+
+template <typename T>
+__device__ void staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
+                                T *y, T *xb, int2 *meta, int lane) {
+  int nlo, npr;
+  stage_row_meta(lo_g, ptr_g, base, st.blk[nblk - 1].x, st.blk[nblk].x, lane, nlo, npr);
+  for (int b = nblk - 1; b >= 0; b--) {
+    const int r0 = st.blk[b].x, nb = st.blk[b + 1].x - r0;
+    const int my_lo = nlo;
+    meta[lane] = make_int2(nlo, npr);
+    // the forward sweep left blocks nblk-1 and nblk-2 in the buffers
+    if (b >= 1) {
+      if (b - 1 < nblk - 2) stage_issue(st, b - 1, lane);
+      stage_row_meta(lo_g, ptr_g, base, st.blk[b - 1].x, st.blk[b].x, lane, nlo, npr);
+    }
+    stage_wait(st, b);
+    __syncwarp();
+    const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);
+    // triangle, lanes over the block's columns; operands of 4 steps loaded ahead
+    T val = lane < nb ? y[r0 + lane] : czero<T>();
+    const int col = r0 + lane;
+    for (int i0 = nb - 1; i0 >= 1; i0 -= 4) {
+      T op[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int i = i0 - u;
+        const int2 mt = meta[max(i, 0)];
+        op[u] = (i >= 1 && lane < i && col >= mt.x) ? S[mt.y + col - mt.x] : czero<T>();
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const T xi = shfl_idx(val, max(i0 - u, 0));
+        val = csub(val, cmul(op[u], xi));
+      }
+    }
+    if (lane < nb) {
+      y[r0 + lane] = val;
+      xb[lane] = val;
+    }
+    int bmin = lane < nb ? my_lo : INT_MAX;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bmin = min(bmin, __shfl_xor_sync(0xffffffffu, bmin, o));
+    __syncwarp();
+    // columns left of the block: y_c -= sum_t L[r0+t][c] x_t, 8 rows' loads in flight
+    for (int cb = bmin; cb < r0; cb += 32) {
+      const int c = cb + lane;
+      const bool act = c < r0;
+      T acc0 = czero<T>(), acc1 = czero<T>();
+      for (int t0 = 0; t0 < nb; t0 += kSGroup) {
+        T v[kSGroup], xv[kSGroup];
+#pragma unroll
+        for (int u = 0; u < kSGroup; u++) {
+          const int t = t0 + u;
+          const int2 mt = meta[t];
+          const int d = c - mt.x;
+          v[u] = (t < nb && act && d >= 0) ? S[mt.y + d] : czero<T>();
+          xv[u] = t < nb ? xb[t] : czero<T>();  // xb past the block may hold anything
+        }
+#pragma unroll
+        for (int u = 0; u < kSGroup; u += 2) {
+          acc0 = cadd(acc0, cmul(v[u], xv[u]));
+          acc1 = cadd(acc1, cmul(v[u + 1], xv[u + 1]));
+        }
+      }
+      if (act) y[c] = csub(y[c], cadd(acc0, acc1));
+    }
+    __syncwarp();
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32) subsolve_staged_kernel(DevProblem p, int mode, const double2 *rhs, double2 *xout,
+                                                             T *zstash, int accumulate, StageLayout lay) {
+  if (mode == kModeIter && p.sc->status != 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x;
+  const int s = p.sub_order[blockIdx.x];
+  const int64_t io = p.int_off[s];
+  const int nI = (int)(p.int_off[s + 1] - io);
+  const int b0 = p.blk_off[s];
+  const int nblk = p.blk_off[s + 1] - b0 - 1;
+  if (nI == 0 || nblk <= 0) return;
+  T *y = (T *)(smem_raw + lay.y);
+  T *xb = (T *)(smem_raw + lay.xb);
+  int2 *meta = (int2 *)(smem_raw + lay.meta);
+  int2 *blk = (int2 *)(smem_raw + lay.blk);
+  Stage<T> st;
+  st.buf0 = (T *)(smem_raw + lay.buf0);
+  st.buf1 = (T *)(smem_raw + lay.buf1);
+  st.bar = (uint64_t *)(smem_raw + lay.bar);
+  st.blk = blk;
+  st.uses0 = st.uses1 = 0;
+  st.err = &p.sc->pad;
+  const int64_t base = p.env_ptr[io];
+  st.L = (sizeof(T) == 8 ? (const T *)(const void *)p.L32 : (const T *)(const void *)p.L64) + base;
+  for (int b = lane; b <= nblk; b += 32) blk[b] = p.blk_tab[b0 + b];
+  if (lane == 0) {
+    mbar_init(&st.bar[0], 1);
+    mbar_init(&st.bar[1], 1);
+    fence_mbar_init();
+  }
+  // right-hand side; a refinement step is skipped when its residual is already small
+  double rn = 0.0, bn = 0.0;
+  for (int c = lane; c < nI; c += 32) {
+    const double2 r = rhs[io + c];
+    y[c] = from_d2<T>(r);
+    if (accumulate) {
+      const double2 bv = p.B[io + c];
+      rn = fmax(rn, fabs(r.x) + fabs(r.y));
+      bn = fmax(bn, fabs(bv.x) + fabs(bv.y));
+    }
+  }
+  if (accumulate && p.ir_tol > 0.0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      rn = fmax(rn, __shfl_xor_sync(0xffffffffu, rn, o));
+      bn = fmax(bn, __shfl_xor_sync(0xffffffffu, bn, o));
+    }
+    if (rn <= p.ir_tol * bn) return;
+  }
+  __syncwarp();
+  const int32_t *lo_g = p.env_lo + io;
+  const int64_t *ptr_g = p.env_ptr + io;
+  T *z = zstash + io;
+  staged_forward<T>(st, nblk, lo_g, ptr_g, base, y, meta, z, lane);
+  for (int c = lane; c < nI; c += 32) y[c] = z[c];
+  __syncwarp();
+  staged_backward<T>(st, nblk, lo_g, ptr_g, base, y, xb, meta, lane);
+  // every copy was waited for above; after a timed-out wait, wait (bounded) again
+  // so that no copy into this warp's shared memory is left in flight
+  stage_wait(st, 0);
+  stage_wait(st, 1);
+  for (int c = lane; c < nI; c += 32) {
+    double2 x = make_double2((double)y[c].x, (double)y[c].y);
+    if (accumulate) x = cadd(xout[io + c], x);
+    xout[io + c] = x;
+  }
+}
+
+// ---- grid-wide products of the staged path, kL lanes per row ------------
+
+template <int kL>
+__device__ __forceinline__ double2 group_sum(double2 v) {
+#pragma unroll
+  for (int o = kL / 2; o > 0; o >>= 1) v = cadd(v, shfl_xor(v, o));
+  return v;
+}
+
+// rhs[g] = f_I[g] (first and last solves) - A_IG v (all but the first)
+template <int kL>
+__global__ void rhs_kernel(DevProblem p, int mode, double2 *__restrict__ out) {
+  if (mode == kModeIter && p.sc->status != 0) return;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = t / kL;
+  const int sub = (int)(t % kL);
+  double2 acc = cz();
+  if (row < p.n_interior && mode != kModeFirst) {
+    const int64_t q1 = p.cpl_rowptr[row + 1];
+    for (int64_t q = p.cpl_rowptr[row] + sub; q < q1; q += kL) acc = cadd(acc, cmul(p.cpl_val[q], p.P[p.cpl_gcol[q]]));
+  }
+  acc = group_sum<kL>(acc);
+  if (row < p.n_interior && sub == 0) out[row] = csub(mode != kModeIter ? p.fI[row] : cz(), acc);
+}
+
+// q[slot] = A_G. [x; v] (- f_G): x from Y, v = P at the slot's interface DOF
+template <int kL>
+__global__ void iface_product_kernel(DevProblem p, int mode) {
+  if (mode == kModeIter && p.sc->status != 0) return;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = t / kL;
+  const int sub = (int)(t % kL);
+  const bool with_bc = mode != kModeFirst;
+  double2 acc = cz();
+  if (row < p.n_slots) {
+    const int64_t q1 = p.ifr_rowptr[row + 1];
+    for (int64_t q = p.ifr_rowptr[row] + sub; q < q1; q += kL) {
+      const int64_t g = p.ifr_gcol[q];
+      const double2 xv = g >= 0 ? p.Y[g] : (with_bc ? p.P[-g - 1] : cz());
+      acc = cadd(acc, cmul(p.ifr_val[q], xv));
+    }
+  }
+  acc = group_sum<kL>(acc);
+  if (row < p.n_slots && sub == 0) {
+    if (mode != kModeIter) acc = csub(acc, p.fG[row]);
+    p.qloc[row] = acc;
+    if (mode == kModeLast) p.V[row] = with_bc ? p.P[p.if_ln[row]] : cz();
+  }
+}
+
+// refinement residual r = b - A_II x of every subdomain, FP64
+template <int kL>
+__global__ void ir_residual_kernel(DevProblem p, int mode) {
+  if (mode == kModeIter && p.sc->status != 0) return;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t row = t / kL;
+  const int sub = (int)(t % kL);
+  double2 acc = cz();
+  if (row < p.n_interior) {
+    const int64_t q1 = p.aii_rowptr[row + 1];
+    for (int64_t q = p.aii_rowptr[row] + sub; q < q1; q += kL) acc = cadd(acc, cmul(p.aii_val[q], p.Y[p.aii_gcol[q]]));
+  }
+  acc = group_sum<kL>(acc);
+  if (row < p.n_interior && sub == 0) p.Rres[row] = csub(p.B[row], acc);
+}
+
+// ----------------------------------------------------------------------------
 // interface COCG (ITERATION_S_1ST / ITERATION_S, hddm_solver_s.h:158-400)
 
 constexpr int kRedThreads = 256;
@@ -904,6 +1356,8 @@ __global__ void profile_reset_kernel(CocgScalars *sc) {
 }
 
 unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+// at least one block: the kernels skip rows past the end
+unsigned blocks_min1(int64_t n, int threads) { return n > 0 ? blocks_for(n, threads) : 1u; }
 
 }  // namespace
 
@@ -952,7 +1406,23 @@ size_t subsolve_smem_bytes(int max_interior, int max_iface, bool fp32) {
 }
 
 void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stream) {
-  if (p.cta_smem > 0) {
+  if (p.solve_variant == kSolveWarp) {
+    const StageLayout lay = stage_layout(p.max_interior, p.max_blocks, p.stage_cap, fp32);
+    double2 *rhs = fp32 ? p.B : p.Y;
+    rhs_kernel<4><<<blocks_min1(p.n_interior * 4, 256), 256, 0, stream>>>(p, mode, rhs);
+    if (fp32) {
+      subsolve_staged_kernel<float2><<<p.nsub, 32, lay.total, stream>>>(p, mode, p.B, p.Y, p.Y32, 0, lay);
+      for (int k = 0; k < p.ir_steps; k++) {
+        ir_residual_kernel<4><<<blocks_min1(p.n_interior * 4, 256), 256, 0, stream>>>(p, mode);
+        subsolve_staged_kernel<float2><<<p.nsub, 32, lay.total, stream>>>(p, mode, p.Rres, p.Y, p.Y32, 1, lay);
+      }
+    } else {
+      subsolve_staged_kernel<double2><<<p.nsub, 32, lay.total, stream>>>(p, mode, p.Y, p.Y, p.Y, 0, lay);
+    }
+    iface_product_kernel<8><<<blocks_min1(p.n_slots * 8, 256), 256, 0, stream>>>(p, mode);
+    return;
+  }
+  if (p.solve_variant == kSolveCta && p.cta_smem > 0) {
     if (fp32)
       subsolve_cta_kernel<true><<<p.nsub, kCtaThreads, p.cta_smem, stream>>>(p, mode);
     else
@@ -965,6 +1435,24 @@ void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stre
     subsolve_kernel<true><<<nb, kThreads, 0, stream>>>(p, mode);
   else
     subsolve_kernel<false><<<nb, kThreads, 0, stream>>>(p, mode);
+}
+
+size_t subsolve_staged_smem_bytes(int max_interior, int max_blocks, int cap, bool fp32) {
+  return stage_layout(max_interior, max_blocks, cap, fp32).total;
+}
+
+int configure_subsolve_staged(size_t smem) {
+  if (smem > 227 * 1024) return -1;
+  cudaError_t e1 =
+      cudaFuncSetAttribute(subsolve_staged_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e2 =
+      cudaFuncSetAttribute(subsolve_staged_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return (e1 == cudaSuccess && e2 == cudaSuccess) ? 0 : -2;
+}
+
+int subsolve_launches(const DevProblem &p, bool fp32) {
+  if (p.solve_variant == kSolveWarp) return 3 + (fp32 ? 2 * p.ir_steps : 0);
+  return 1;
 }
 
 int configure_subsolve(size_t smem) {

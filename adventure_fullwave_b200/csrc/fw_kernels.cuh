@@ -73,9 +73,31 @@ struct DevProblem {
   int32_t n_part_blocks;
   int32_t ir_steps;
   double ir_tol;
-  int32_t cta_smem;              // dynamic shared bytes of the CTA-per-subdomain solve (0: warp path)
+  int32_t cta_smem;              // dynamic shared bytes of the CTA-per-subdomain solve (0: not available)
   int32_t hist_cap;              // entries of hist
+  int32_t solve_variant;         // SolveVariant of the batched subdomain solve
+  int32_t max_interior;          // largest subdomain: interior rows
+  int32_t max_iface;             // largest subdomain: interface DOFs
+  // staged solve (kSolveWarp): row blocks and grid-wide operator products
+  const int32_t *blk_off;        // nsub+1: first block-table entry of each subdomain
+  const int2 *blk_tab;           // per subdomain nblk+1 x (first row, first envelope element)
+  int32_t max_blocks;            // most blocks of one subdomain
+  int32_t stage_cap;             // envelope elements per staging buffer
+  int64_t n_interior;            // interior rows of all subdomains
+  int64_t n_slots;               // interface slots of all subdomains
+  const int64_t *cpl_rowptr;     // n_interior+1 into cpl_val
+  const int32_t *cpl_gcol;       // interface DOF (index into P) of each coupling entry
+  const int64_t *ifr_rowptr;     // n_slots+1 into ifr_val
+  const int32_t *ifr_gcol;       // >=0: global interior row; <0: -(interface DOF)-1
+  const int64_t *aii_rowptr;     // n_interior+1 into aii_val
+  const int32_t *aii_gcol;       // global interior row of each interior entry
+  double2 *Rres;                 // n_interior: refinement residual
 };
+
+// Batched subdomain solve kernels: one warp per subdomain with TMA-staged row
+// blocks and grid-wide operator products, one CTA per subdomain, or one warp
+// per subdomain with the vectors in global memory (any size).
+enum SolveVariant { kSolveWarp = 0, kSolveCta = 1, kSolveGlobal = 2 };
 
 enum SolveMode { kModeFirst = 0, kModeIter = 1, kModeLast = 2 };
 
@@ -96,6 +118,10 @@ void launch_to_fp32(int64_t n, const double2 *src, float2 *dst, cudaStream_t str
 void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stream);
 size_t subsolve_smem_bytes(int max_interior, int max_iface, bool fp32);
 int configure_subsolve(size_t smem);
+size_t subsolve_staged_smem_bytes(int max_interior, int max_blocks, int cap, bool fp32);
+int configure_subsolve_staged(size_t smem);
+// kernels one launch_subsolve call issues
+int subsolve_launches(const DevProblem &p, bool fp32);
 void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream);
 void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream);
 void launch_edge_solution(int64_t ne, const int64_t *edge_src, const double2 *Y, const double2 *V, double2 *x,

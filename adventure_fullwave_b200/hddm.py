@@ -26,6 +26,10 @@ import numpy as np
 from . import _lib
 from ._lib import FwgpuError  # noqa: F401  (re-exported)
 
+# batched subdomain-solve kernels (FWGPU_SOLVE_*); "auto" times the candidates once
+SOLVE_KERNELS = {"auto": 0, "warp": 1, "cta": 2, "global": 3}
+_KERNEL_NAMES = {v: k for k, v in SOLVE_KERNELS.items()}
+
 P = ctypes.POINTER
 
 
@@ -44,6 +48,7 @@ class HddmResult:
     t_iterate_ms: float
     t_last_ms: float
     kernel_launches: int = 0
+    solve_kernel: str = ""
 
 
 def _mesh_struct(model):
@@ -119,7 +124,8 @@ class HddmSolver:
     """
 
     def __init__(self, model, hddm_eps: float = 1e-3, hddm_max_loop: int = 4000, precision: str = "fp64",
-                 ir_max_steps: int = 1, ir_tol: float = 0.0, graph_iterations: int = 16, device: int = 0):
+                 ir_max_steps: int = 1, ir_tol: float = 0.0, graph_iterations: int = 16, device: int = 0,
+                 solve_kernel: str = "auto"):
         lib = _lib.load()
         self._lib = lib
         self.model = model
@@ -144,10 +150,14 @@ class HddmSolver:
                              float(model.omega))
         prec = {"fp64": _lib.PREC_FP64, "fp32_ir": _lib.PREC_FP32_IR}[precision]
         self.precision = precision
+        kern = SOLVE_KERNELS[solve_kernel]
         opts = _lib.FwOptions(self.hddm_eps, self.hddm_max_loop, prec, int(ir_max_steps), float(ir_tol),
-                              int(graph_iterations), int(device))
+                              int(graph_iterations), int(device), kern)
         handle = ctypes.c_void_p()
-        _lib.check(lib.fwgpu_create(ctypes.byref(mesh), ctypes.byref(mt), ctypes.byref(opts), ctypes.byref(handle)))
+        rc = lib.fwgpu_create(ctypes.byref(mesh), ctypes.byref(mt), ctypes.byref(opts), ctypes.byref(handle))
+        if rc != 0 and handle.value:
+            lib.fwgpu_destroy(handle)
+        _lib.check(rc)
         self._h = handle
         self.n_edges = int(model.n_edges)
 
@@ -221,7 +231,7 @@ class HddmSolver:
     def _result(r: _lib.FwResult) -> HddmResult:
         return HddmResult(int(r.iterations), bool(r.converged), float(r.initial_norm), float(r.final_resi),
                           float(r.final_resi_l2), float(r.t_setup_ms), float(r.t_iterate_ms), float(r.t_last_ms),
-                          int(r.kernel_launches))
+                          int(r.kernel_launches), _KERNEL_NAMES.get(int(r.solve_kernel), ""))
 
     def adjoint_gradient(self, probe_edges=None, design_tets=None):
         """Backward of the last ``solve``: J = sum |x_p|^2 over ``probe_edges``

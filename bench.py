@@ -130,11 +130,11 @@ def algorithmic_bytes(sz: dict, precision: str, ir_steps: int) -> int:
     return int(b)
 
 
-def ncu_traffic(config: str, precision: str):
+def ncu_traffic(kernel: str, config: str, precision: str):
     """DRAM bytes per launch of the substitution kernel from the committed
-    ncu summary (profiles/subsolve_cta_<config>_<precision>.md), when one
-    covers this workload."""
-    path = os.path.join(REPO, "profiles", f"subsolve_cta_{config}_{precision}.md")
+    ncu summary (profiles/subsolve_<kernel>_<config>_<precision>.md), when
+    one covers this workload."""
+    path = os.path.join(REPO, "profiles", f"subsolve_{kernel}_{config}_{precision}.md")
     try:
         for line in open(path):
             t = line.split()
@@ -221,7 +221,7 @@ def run_ours(args):
     model = make_model(args.config)
     solver = hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
                              ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, graph_iterations=args.graph_iters,
-                             device=local)
+                             device=local, solve_kernel=args.solve_kernel)
     for _ in range(args.warmup):
         solver.solve(0)
     clocks = ClockSampler(local)
@@ -269,8 +269,10 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     alg = algorithmic_bytes(sz, args.precision, args.ir_steps)
     achieved = alg / (prof["subsolve_ms"] * 1e-3) / 1e9
-    traffic = ncu_traffic(args.config, args.precision)
-    roofline = {"bound": "hbm", "kernel": "subsolve_cta_kernel (one batched subdomain solve)",
+    traffic = ncu_traffic(results[-1].solve_kernel, args.config, args.precision)
+    kname = {"warp": "subsolve_warp_kernel", "cta": "subsolve_cta_kernel", "global": "subsolve_kernel"}.get(
+        results[-1].solve_kernel, results[-1].solve_kernel)
+    roofline = {"bound": "hbm", "kernel": f"{kname} (one batched subdomain solve)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic, "algorithmic_bytes": alg,
                 "kernel_ms": prof["subsolve_ms"], "interface_kernels_ms": prof["interface_ms"],
@@ -286,7 +288,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
                              ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, graph_iterations=args.graph_iters,
-                             device=local) as s2:
+                             device=local, solve_kernel=args.solve_kernel) as s2:
             s2.solve(0)
             xe = s2.edge_solution()
         e2e_times.append(time.perf_counter() - t0)
@@ -340,7 +342,7 @@ def run_ncu_case(args):
 
     model = make_model(args.config)
     with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
-                         ir_max_steps=args.ir_steps, ir_tol=args.ir_tol) as s:
+                         ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, solve_kernel=args.solve_kernel) as s:
         s.make_tmp_aij(0)
         s.solve_dom_1st()
         s.iteration_s_1st()
@@ -362,6 +364,7 @@ def main():
     ap.add_argument("--ir-steps", type=int, default=1)
     ap.add_argument("--ir-tol", type=float, default=0.0)
     ap.add_argument("--graph-iters", type=int, default=32)
+    ap.add_argument("--solve-kernel", default="auto", choices=["auto", "warp", "cta", "global"])
     ap.add_argument("--prof-reps", type=int, default=50)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-iters", type=int, default=10)

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define FWGPU_ABI_VERSION 1
+#define FWGPU_ABI_VERSION 2
 
 enum {
   FWGPU_OK = 0,
@@ -95,7 +95,15 @@ typedef struct {
                             ir_tol * |rhs| (0 = always ir_max_steps) */
   int32_t graph_iterations; /* COCG iterations captured per CUDA graph launch */
   int32_t device;        /* CUDA device ordinal */
+  int32_t solve_kernel;  /* FWGPU_SOLVE_*: batched subdomain-solve kernel (0 = timed choice) */
 } fwgpu_options;
+
+/* Batched subdomain-solve kernels.  AUTO times one launch of each candidate
+ * after the factorisation and keeps the fastest. */
+#define FWGPU_SOLVE_AUTO 0
+#define FWGPU_SOLVE_WARP 1   /* one warp per subdomain, vectors in shared memory */
+#define FWGPU_SOLVE_CTA 2    /* one 256-thread CTA per subdomain */
+#define FWGPU_SOLVE_GLOBAL 3 /* one warp per subdomain, vectors in global memory (any size) */
 
 typedef struct fwgpu_context fwgpu_context;
 
@@ -127,6 +135,8 @@ typedef struct {
   double t_iterate_ms;     /* COCG loop, device time */
   double t_last_ms;        /* final subdomain solves, device time */
   int64_t kernel_launches; /* kernels this library launched for the call */
+  int32_t solve_kernel;    /* FWGPU_SOLVE_* used for the subdomain solves */
+  int32_t reserved;
 } fwgpu_result;
 
 /* -- lifecycle ----------------------------------------------------------- */

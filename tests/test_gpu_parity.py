@@ -84,6 +84,23 @@ def test_fp32_ir_vs_fp64():
     assert rel_l2(x32, x64) <= 1e-6
 
 
+@pytest.mark.parametrize("kernel", ["warp", "cta", "global"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32_ir"])
+def test_solve_kernels_vs_oracle(kernel, precision):
+    """Every batched subdomain-solve kernel against the oracle's FP64 HDDM at
+    a tight tolerance, on subdomains large enough for multi-block sweeps and
+    rows longer than 64 stored entries."""
+    model = meshgen.make_model("x", n=12, size=1.0, npml=2, nleaves=6, seed=5)
+    meshgen.round_trip_material(model)
+    part = oracle.partition(model)
+    xo, _, _, _ = oracle.hddm(model, part, 1e-10, 20000)
+    x, r = hddm.hddm_solver_CS(model, 0, hddm_eps=1e-10, hddm_max_loop=20000, precision=precision,
+                               ir_max_steps=2, solve_kernel=kernel)
+    assert r.converged
+    assert r.solve_kernel == kernel
+    assert rel_l2(x, xo) <= (1e-7 if precision == "fp64" else 1e-6)
+
+
 def test_single_subdomain_is_a_direct_solve():
     model = meshgen.make_model("x", n=4, size=1.0, npml=1, nleaves=1)
     meshgen.round_trip_material(model)
