@@ -57,6 +57,7 @@ class FwOptions(ctypes.Structure):
     _fields_ = [
         ("hddm_eps", c_dbl), ("hddm_max_loop", c_i32), ("precision", c_i32), ("ir_max_steps", c_i32),
         ("ir_tol", c_dbl), ("graph_iterations", c_i32), ("device", c_i32), ("solve_kernel", c_i32),
+        ("stage_cap", c_i32),
     ]
 
 
@@ -73,7 +74,7 @@ class FwResult(ctypes.Structure):
     _fields_ = [
         ("iterations", c_i32), ("converged", c_i32), ("initial_norm", c_dbl), ("final_resi", c_dbl),
         ("final_resi_l2", c_dbl), ("t_setup_ms", c_dbl), ("t_iterate_ms", c_dbl), ("t_last_ms", c_dbl),
-        ("kernel_launches", c_i64), ("solve_kernel", c_i32), ("reserved", c_i32),
+        ("kernel_launches", c_i64), ("solve_kernel", c_i32), ("stage_cap", c_i32),
     ]
 
 

@@ -81,7 +81,10 @@ struct fwgpu_context {
   bool factor_bad = false;
   bool factor_fresh = false;       // factor matches the assembled values
   bool solve_tuned = false;        // the subdomain-solve kernel has been chosen
-  bool warp_ok = false;            // the warp-per-subdomain kernel fits in shared memory
+  bool warp_ok = false;            // the staged warp-per-subdomain kernel fits in shared memory
+  int32_t *d_blk_off = nullptr;    // staged solve block table (current staging capacity)
+  int2 *d_blk_tab = nullptr;
+  std::vector<int> stage_caps;     // staging capacities that fit in shared memory
   int64_t launches = 0;            // kernels launched since the last reset
   int64_t *d_env_dst = nullptr;    // lower entry -> envelope position (-1: outside)
 
@@ -462,7 +465,8 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
       default:
         dp.solve_variant = dp.cta_smem > 0 ? fw::kSolveCta : fw::kSolveGlobal;
     }
-    c->solve_tuned = c->opts.solve_kernel != FWGPU_SOLVE_AUTO;
+    // AUTO times every candidate; WARP times its staging capacities
+    c->solve_tuned = c->opts.solve_kernel != FWGPU_SOLVE_AUTO && c->opts.solve_kernel != FWGPU_SOLVE_WARP;
   }
   // per-edge solution source: the first subdomain holding each edge
   std::vector<int64_t> esrc(m.ne, -1);
@@ -607,18 +611,21 @@ int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
 
 // Row blocks of the staged solve: at most 32 rows, and stored entries that
 // fit one staging buffer, so that one bulk copy brings a whole block in.
-static int build_stage_blocks(fwgpu_context *c) {
+static int stage_max_row(const fwgpu_context *c) {
   const fw::Plan &p = c->p;
-  const int nsub = c->m.nsub;
-  const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
   int maxrow = 0;
-  for (int s = 0; s < nsub; s++) {
+  for (int s = 0; s < c->m.nsub; s++) {
     const int64_t io = p.sub_int_off[s];
     const int nI = (int)(p.sub_int_off[s + 1] - io);
     for (int r = 0; r < nI; r++) maxrow = std::max(maxrow, r - c->h_env_lo[io + r] + 1);
   }
-  int cap = fp32 ? 2048 : 1024;
-  cap = std::max(cap, (maxrow + 2 + 7) & ~7);
+  return maxrow;
+}
+
+// Block table for staging buffers of `cap` envelope elements.
+static int build_stage_blocks(fwgpu_context *c, int cap, int *max_blocks_out) {
+  const fw::Plan &p = c->p;
+  const int nsub = c->m.nsub;
   std::vector<int32_t> boff(nsub + 1, 0);
   std::vector<int2> btab;
   int max_blocks = 0;
@@ -645,16 +652,47 @@ static int build_stage_blocks(fwgpu_context *c) {
     max_blocks = std::max(max_blocks, nb);
   }
   boff[nsub] = (int32_t)btab.size();
-  int32_t *d_boff = nullptr;
-  int2 *d_btab = nullptr;
-  FW_TRY(c->upload(&d_boff, boff));
-  FW_TRY(c->upload(&d_btab, btab));
-  c->dp.blk_off = d_boff;
-  c->dp.blk_tab = d_btab;
+  c->release(c->d_blk_off);
+  c->release(c->d_blk_tab);
+  c->d_blk_off = nullptr;
+  c->d_blk_tab = nullptr;
+  FW_TRY(c->upload(&c->d_blk_off, boff));
+  FW_TRY(c->upload(&c->d_blk_tab, btab));
+  c->dp.blk_off = c->d_blk_off;
+  c->dp.blk_tab = c->d_blk_tab;
   c->dp.max_blocks = max_blocks;
   c->dp.stage_cap = cap;
-  const size_t smem = fw::subsolve_staged_smem_bytes(p.max_interior, max_blocks, cap, fp32);
-  c->warp_ok = fw::configure_subsolve_staged(smem) == 0;
+  if (max_blocks_out) *max_blocks_out = max_blocks;
+  return FWGPU_OK;
+}
+
+// Staging capacities the staged kernel can run with (shared memory of one
+// warp <= 227 KB), the default one's block table, and the kernel's shared
+// memory limit set for the largest of them.
+static int setup_stage(fwgpu_context *c) {
+  const fw::Plan &p = c->p;
+  const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
+  const int min_cap = (stage_max_row(c) + 2 + 7) & ~7;
+  std::vector<int> cand = fp32 ? std::vector<int>{1024, 1536, 2048, 3072} : std::vector<int>{512, 768, 1024, 1536};
+  if (c->opts.stage_cap > 0) cand = {c->opts.stage_cap};
+  c->stage_caps.clear();
+  size_t smem_max = 0;
+  for (int cap : cand) {
+    cap = std::max(cap, min_cap);
+    if (std::find(c->stage_caps.begin(), c->stage_caps.end(), cap) != c->stage_caps.end()) continue;
+    int mb = 0;
+    FW_TRY(build_stage_blocks(c, cap, &mb));
+    const size_t smem = fw::subsolve_staged_smem_bytes(p.max_interior, mb, cap, fp32);
+    if (smem > 227 * 1024) continue;
+    c->stage_caps.push_back(cap);
+    smem_max = std::max(smem_max, smem);
+  }
+  c->warp_ok = !c->stage_caps.empty() && fw::configure_subsolve_staged(smem_max) == 0;
+  if (c->warp_ok) {
+    // the default: the middle capacity
+    FW_TRY(build_stage_blocks(c, c->stage_caps[(c->stage_caps.size() - 1) / 2 + (c->stage_caps.size() > 2 ? 1 : 0)],
+                              nullptr));
+  }
   return FWGPU_OK;
 }
 
@@ -663,13 +701,23 @@ static int build_stage_blocks(fwgpu_context *c) {
 // keeps the fastest.
 static int tune_solve_kernel(fwgpu_context *c) {
   const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
-  const int cand[2] = {fw::kSolveWarp, fw::kSolveCta};
+  struct Cand {
+    int variant, cap;
+  };
+  std::vector<Cand> cand;
+  const bool any = c->opts.solve_kernel == FWGPU_SOLVE_AUTO;
+  if ((any || c->opts.solve_kernel == FWGPU_SOLVE_WARP) && c->warp_ok)
+    for (int cap : c->stage_caps) cand.push_back({fw::kSolveWarp, cap});
+  if (any && c->dp.cta_smem > 0) cand.push_back({fw::kSolveCta, 0});
+  if (cand.empty()) {
+    c->solve_tuned = true;
+    return FWGPU_OK;
+  }
   float best = -1.f;
-  int pick = c->dp.solve_variant;
-  for (int v : cand) {
-    if (v == fw::kSolveWarp && !c->warp_ok) continue;
-    if (v == fw::kSolveCta && c->dp.cta_smem == 0) continue;
-    c->dp.solve_variant = v;
+  Cand pick = cand[0];
+  for (const Cand &k : cand) {
+    c->dp.solve_variant = k.variant;
+    if (k.variant == fw::kSolveWarp) FW_TRY(build_stage_blocks(c, k.cap, nullptr));
     fw::launch_subsolve(c->dp, fw::kModeFirst, fp32, c->stream);
     FW_CUDA(cudaEventRecord(c->ev[4], c->stream));
     for (int r = 0; r < 3; r++) fw::launch_subsolve(c->dp, fw::kModeFirst, fp32, c->stream);
@@ -680,10 +728,11 @@ static int tune_solve_kernel(fwgpu_context *c) {
     FW_CUDA(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
     if (best < 0.f || ms < best) {
       best = ms;
-      pick = v;
+      pick = k;
     }
   }
-  c->dp.solve_variant = pick;
+  c->dp.solve_variant = pick.variant;
+  if (pick.variant == fw::kSolveWarp && c->dp.stage_cap != pick.cap) FW_TRY(build_stage_blocks(c, pick.cap, nullptr));
   c->solve_tuned = true;
   return FWGPU_OK;
 }
@@ -749,7 +798,7 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     c->dp.env_lo = c->d_env_lo;
     c->dp.env_ptr = c->d_env_ptr;
     if (c->opts.precision == FWGPU_PREC_FP32_IR) FW_TRY(c->alloc(&c->d_L32, pos + 64));
-    FW_TRY(build_stage_blocks(c));
+    FW_TRY(setup_stage(c));
     if (c->opts.solve_kernel == FWGPU_SOLVE_WARP && !c->warp_ok)
       return set_error(FWGPU_ERR_ARG, "staged solve kernel: subdomains too large for shared memory");
   }
@@ -864,7 +913,7 @@ static int fill_result(fwgpu_context *c, fwgpu_result *res) {
     res->t_last_ms = ms;
     res->kernel_launches = c->launches;
     res->solve_kernel = c->dp.solve_variant + 1;
-    res->reserved = 0;
+    res->stage_cap = c->dp.solve_variant == fw::kSolveWarp ? c->dp.stage_cap : 0;
   }
   return sc.converged ? FWGPU_OK : set_error(FWGPU_ERR_NOT_CONVERGED, "hddm_max_loop reached before hddm_eps");
 }

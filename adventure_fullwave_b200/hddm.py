@@ -49,6 +49,7 @@ class HddmResult:
     t_last_ms: float
     kernel_launches: int = 0
     solve_kernel: str = ""
+    stage_cap: int = 0
 
 
 def _mesh_struct(model):
@@ -125,7 +126,7 @@ class HddmSolver:
 
     def __init__(self, model, hddm_eps: float = 1e-3, hddm_max_loop: int = 4000, precision: str = "fp64",
                  ir_max_steps: int = 1, ir_tol: float = 0.0, graph_iterations: int = 16, device: int = 0,
-                 solve_kernel: str = "auto"):
+                 solve_kernel: str = "auto", stage_cap: int = 0):
         lib = _lib.load()
         self._lib = lib
         self.model = model
@@ -152,7 +153,7 @@ class HddmSolver:
         self.precision = precision
         kern = SOLVE_KERNELS[solve_kernel]
         opts = _lib.FwOptions(self.hddm_eps, self.hddm_max_loop, prec, int(ir_max_steps), float(ir_tol),
-                              int(graph_iterations), int(device), kern)
+                              int(graph_iterations), int(device), kern, int(stage_cap))
         handle = ctypes.c_void_p()
         rc = lib.fwgpu_create(ctypes.byref(mesh), ctypes.byref(mt), ctypes.byref(opts), ctypes.byref(handle))
         if rc != 0 and handle.value:
@@ -231,7 +232,8 @@ class HddmSolver:
     def _result(r: _lib.FwResult) -> HddmResult:
         return HddmResult(int(r.iterations), bool(r.converged), float(r.initial_norm), float(r.final_resi),
                           float(r.final_resi_l2), float(r.t_setup_ms), float(r.t_iterate_ms), float(r.t_last_ms),
-                          int(r.kernel_launches), _KERNEL_NAMES.get(int(r.solve_kernel), ""))
+                          int(r.kernel_launches), _KERNEL_NAMES.get(int(r.solve_kernel), ""),
+                          int(r.stage_cap))
 
     def adjoint_gradient(self, probe_edges=None, design_tets=None):
         """Backward of the last ``solve``: J = sum |x_p|^2 over ``probe_edges``

@@ -221,7 +221,7 @@ def run_ours(args):
     model = make_model(args.config)
     solver = hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
                              ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, graph_iterations=args.graph_iters,
-                             device=local, solve_kernel=args.solve_kernel)
+                             device=local, solve_kernel=args.solve_kernel, stage_cap=args.stage_cap)
     for _ in range(args.warmup):
         solver.solve(0)
     clocks = ClockSampler(local)
@@ -288,7 +288,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
                              ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, graph_iterations=args.graph_iters,
-                             device=local, solve_kernel=args.solve_kernel) as s2:
+                             device=local, solve_kernel=args.solve_kernel, stage_cap=args.stage_cap) as s2:
             s2.solve(0)
             xe = s2.edge_solution()
         e2e_times.append(time.perf_counter() - t0)
@@ -342,7 +342,8 @@ def run_ncu_case(args):
 
     model = make_model(args.config)
     with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
-                         ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, solve_kernel=args.solve_kernel) as s:
+                         ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, solve_kernel=args.solve_kernel,
+                         stage_cap=args.stage_cap) as s:
         s.make_tmp_aij(0)
         s.solve_dom_1st()
         s.iteration_s_1st()
@@ -365,6 +366,7 @@ def main():
     ap.add_argument("--ir-tol", type=float, default=0.0)
     ap.add_argument("--graph-iters", type=int, default=32)
     ap.add_argument("--solve-kernel", default="auto", choices=["auto", "warp", "cta", "global"])
+    ap.add_argument("--stage-cap", type=int, default=0, help="staging buffer elements (0: timed choice)")
     ap.add_argument("--prof-reps", type=int, default=50)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-iters", type=int, default=10)

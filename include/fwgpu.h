@@ -96,10 +96,13 @@ typedef struct {
   int32_t graph_iterations; /* COCG iterations captured per CUDA graph launch */
   int32_t device;        /* CUDA device ordinal */
   int32_t solve_kernel;  /* FWGPU_SOLVE_*: batched subdomain-solve kernel (0 = timed choice) */
+  int32_t stage_cap;     /* WARP kernel: envelope elements per staging buffer (0 = timed choice) */
 } fwgpu_options;
 
 /* Batched subdomain-solve kernels.  AUTO times one launch of each candidate
- * after the factorisation and keeps the fastest. */
+ * (the WARP kernel with each staging capacity that fits in shared memory)
+ * after the factorisation and keeps the fastest; WARP times only its
+ * staging capacities. */
 #define FWGPU_SOLVE_AUTO 0
 #define FWGPU_SOLVE_WARP 1   /* one warp per subdomain, vectors in shared memory */
 #define FWGPU_SOLVE_CTA 2    /* one 256-thread CTA per subdomain */
@@ -136,7 +139,7 @@ typedef struct {
   double t_last_ms;        /* final subdomain solves, device time */
   int64_t kernel_launches; /* kernels this library launched for the call */
   int32_t solve_kernel;    /* FWGPU_SOLVE_* used for the subdomain solves */
-  int32_t reserved;
+  int32_t stage_cap;       /* WARP kernel: envelope elements per staging buffer, else 0 */
 } fwgpu_result;
 
 /* -- lifecycle ----------------------------------------------------------- */
