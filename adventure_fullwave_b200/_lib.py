@@ -57,7 +57,7 @@ class FwOptions(ctypes.Structure):
     _fields_ = [
         ("hddm_eps", c_dbl), ("hddm_max_loop", c_i32), ("precision", c_i32), ("ir_max_steps", c_i32),
         ("ir_tol", c_dbl), ("graph_iterations", c_i32), ("device", c_i32), ("solve_kernel", c_i32),
-        ("stage_cap", c_i32),
+        ("stage_cap", c_i32), ("ir_relax", c_dbl),
     ]
 
 

@@ -81,6 +81,10 @@ struct fwgpu_context {
   bool factor_bad = false;
   bool factor_fresh = false;       // factor matches the assembled values
   bool solve_tuned = false;        // the subdomain-solve kernel has been chosen
+  // assembly work buffers kept for the context's lifetime (repeated solves)
+  double *d_elmat = nullptr;       // element matrices, 72 doubles per element
+  int64_t *d_cpl_src = nullptr, *d_ifr_src = nullptr, *d_aii_src = nullptr, *d_diag_src = nullptr;
+  std::vector<int32_t> h_src_owner, h_src_local;  // first subdomain holding each edge, and its local DOF
   bool warp_ok = false;            // the staged warp-per-subdomain kernel fits in shared memory
   int32_t *d_blk_off = nullptr;    // staged solve block table (current staging capacity)
   int2 *d_blk_tab = nullptr;
@@ -167,14 +171,18 @@ int build_rhs(fwgpu_context *c, const fwgpu_source *src) {
   if (src && src->n_entries > 0) {
     if (!src->edge || !src->value) return set_error(FWGPU_ERR_ARG, "source without edges or values");
     // owner subdomain and local DOF of every edge: the first subdomain holding it
-    std::vector<int32_t> owner(c->m.ne, -1), local(c->m.ne, -1);
-    for (int s = 0; s < nsub; s++) {
-      const fw::SubHost &h = p.subs[s];
-      for (int r = 0; r < h.nmp; r++) {
-        const int e = h.edge_gid[r];
-        if (owner[e] < 0) {
-          owner[e] = s;
-          local[e] = r;
+    std::vector<int32_t> &owner = c->h_src_owner, &local = c->h_src_local;
+    if (owner.empty()) {
+      owner.assign(c->m.ne, -1);
+      local.assign(c->m.ne, -1);
+      for (int s = 0; s < nsub; s++) {
+        const fw::SubHost &h = p.subs[s];
+        for (int r = 0; r < h.nmp; r++) {
+          const int e = h.edge_gid[r];
+          if (owner[e] < 0) {
+            owner[e] = s;
+            local[e] = r;
+          }
         }
       }
     }
@@ -444,10 +452,11 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   dp.hist_cap = std::max(1, opts->hddm_max_loop) + 2;
   dp.ir_steps = c->opts.ir_max_steps;
   dp.ir_tol = c->opts.ir_tol;
+  dp.ir_relax = c->opts.ir_relax;
   {
     const bool fp32 = opts->precision == FWGPU_PREC_FP32_IR;
     const size_t smem = fw::subsolve_smem_bytes(p.max_interior, p.max_iface, fp32);
-    dp.cta_smem = fw::configure_subsolve(smem) == 0 ? (int32_t)smem : 0;
+    dp.cta_smem = fw::configure_subsolve(smem, fp32) == 0 ? (int32_t)smem : 0;
     dp.max_interior = p.max_interior;
     dp.max_iface = p.max_iface;
     // the staged kernel's layout depends on the envelope: it is checked in solve_dom_1st
@@ -566,43 +575,30 @@ int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
   FW_CUDA(cudaSetDevice(c->opts.device));
   const fw::Plan &p = c->p;
   FW_CUDA(cudaEventRecord(c->ev[0], c->stream));
-  double *d_elmat = nullptr;
-  FW_TRY(c->alloc(&d_elmat, (size_t)c->m.nt * 72));
+  if (!c->d_elmat) {
+    FW_TRY(c->alloc(&c->d_elmat, (size_t)c->m.nt * 72));
+    FW_TRY(c->alloc(&c->d_aval, p.nnz_total));
+    FW_TRY(c->upload(&c->d_cpl_src, p.cpl_src));
+    FW_TRY(c->upload(&c->d_ifr_src, p.ifr_src));
+    if (c->d_aii_val) FW_TRY(c->upload(&c->d_aii_src, p.aii_src));
+    FW_TRY(c->upload(&c->d_diag_src, p.if_diag_src));
+  }
   c->launches += 2;
   fw::launch_element_matrices(c->m.nt, c->d_el_order, c->d_tv, c->d_crd, c->d_el_eps, c->d_el_sigma, c->m.omega,
-                              d_elmat, c->d_mesh_status, c->stream);
-  if (!c->d_aval) FW_TRY(c->alloc(&c->d_aval, p.nnz_total));
-  fw::launch_gather_values(p.nnz_total, c->d_cptr, c->d_contrib, (const double2 *)d_elmat, c->d_aval, c->stream);
+                              c->d_elmat, c->d_mesh_status, c->stream);
+  fw::launch_gather_values(p.nnz_total, c->d_cptr, c->d_contrib, (const double2 *)c->d_elmat, c->d_aval, c->stream);
   FW_CUDA(cudaGetLastError());
   FW_CUDA(cudaStreamSynchronize(c->stream));
-  c->release(d_elmat);
   int32_t mesh_status = 0;
   FW_CUDA(cudaMemcpy(&mesh_status, c->d_mesh_status, sizeof(int32_t), cudaMemcpyDeviceToHost));
   if (mesh_status) return set_error(FWGPU_ERR_MESH, "non-positive element volume or degenerate edge");
   FW_TRY(build_rhs(c, src));
   // operators gathered from the assembled values
-  {
-    int64_t *tmp = nullptr;
-    FW_TRY(c->upload(&tmp, p.cpl_src));
-    c->launches += c->d_aii_val ? 4 : 3;
-    fw::launch_gather_ops((int64_t)p.cpl_src.size(), tmp, c->d_aval, c->d_cpl_val, c->stream);
-    FW_CUDA(cudaStreamSynchronize(c->stream));
-    c->release(tmp);
-    FW_TRY(c->upload(&tmp, p.ifr_src));
-    fw::launch_gather_ops((int64_t)p.ifr_src.size(), tmp, c->d_aval, c->d_ifr_val, c->stream);
-    FW_CUDA(cudaStreamSynchronize(c->stream));
-    c->release(tmp);
-    if (c->d_aii_val) {
-      FW_TRY(c->upload(&tmp, p.aii_src));
-      fw::launch_gather_ops((int64_t)p.aii_src.size(), tmp, c->d_aval, c->d_aii_val, c->stream);
-      FW_CUDA(cudaStreamSynchronize(c->stream));
-      c->release(tmp);
-    }
-    FW_TRY(c->upload(&tmp, p.if_diag_src));
-    fw::launch_diag_pc((int64_t)p.if_diag_src.size(), tmp, c->d_aval, c->d_pcloc, c->stream);
-    FW_CUDA(cudaStreamSynchronize(c->stream));
-    c->release(tmp);
-  }
+  c->launches += c->d_aii_val ? 4 : 3;
+  fw::launch_gather_ops((int64_t)p.cpl_src.size(), c->d_cpl_src, c->d_aval, c->d_cpl_val, c->stream);
+  fw::launch_gather_ops((int64_t)p.ifr_src.size(), c->d_ifr_src, c->d_aval, c->d_ifr_val, c->stream);
+  if (c->d_aii_val) fw::launch_gather_ops((int64_t)p.aii_src.size(), c->d_aii_src, c->d_aval, c->d_aii_val, c->stream);
+  fw::launch_diag_pc((int64_t)p.if_diag_src.size(), c->d_diag_src, c->d_aval, c->d_pcloc, c->stream);
   FW_CUDA(cudaGetLastError());
   c->stage = 1;
   c->factor_fresh = false;
@@ -687,7 +683,7 @@ static int setup_stage(fwgpu_context *c) {
     c->stage_caps.push_back(cap);
     smem_max = std::max(smem_max, smem);
   }
-  c->warp_ok = !c->stage_caps.empty() && fw::configure_subsolve_staged(smem_max) == 0;
+  c->warp_ok = !c->stage_caps.empty() && fw::configure_subsolve_staged(smem_max, fp32) == 0;
   if (c->warp_ok) {
     // the default: the middle capacity
     FW_TRY(build_stage_blocks(c, c->stage_caps[(c->stage_caps.size() - 1) / 2 + (c->stage_caps.size() > 2 ? 1 : 0)],

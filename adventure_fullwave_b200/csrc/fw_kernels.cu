@@ -16,6 +16,7 @@
 
 #include <climits>
 #include <cstdint>
+#include <mutex>
 #include <type_traits>
 
 #include "fw_kernels.cuh"
@@ -87,6 +88,13 @@ __device__ __forceinline__ double2 czero<double2>() {
 template <>
 __device__ __forceinline__ float2 czero<float2>() {
   return make_float2(0.0f, 0.0f);
+}
+
+// An interface iteration's refinement step is skipped once the COCG residual
+// is below ir_relax: the accuracy an inexact Krylov product needs falls as the
+// residual falls.  The first and last solves always refine.
+__device__ __forceinline__ bool refine_skipped(const DevProblem &p, int mode) {
+  return mode == kModeIter && p.ir_relax > 0.0 && p.sc->resi <= p.ir_relax;
 }
 
 __device__ __forceinline__ int warp_id_global() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
@@ -305,7 +313,8 @@ __global__ void __launch_bounds__(kThreads) subsolve_kernel(DevProblem p, int mo
       for (int c = lane; c < nI; c += 32) bnorm = fmax(bnorm, fabs(b[c].x) + fabs(b[c].y));
       for (int o2 = 16; o2 > 0; o2 >>= 1) bnorm = fmax(bnorm, __shfl_xor_sync(0xffffffffu, bnorm, o2));
     }
-    for (int step = 0; step < p.ir_steps; step++) {
+    const int ir_steps = refine_skipped(p, mode) ? 0 : p.ir_steps;
+    for (int step = 0; step < ir_steps; step++) {
       double rnorm = 0.0;
       for (int c = lane; c < nI; c += 32) {
         double2 r = b[c];
@@ -596,7 +605,8 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
     const int64_t abase = p.aii_off[s];
     __shared__ double red[kCtaThreads / 32];
     __shared__ int stop;
-    for (int step = 0; step < p.ir_steps; step++) {
+    const int ir_steps = refine_skipped(p, mode) ? 0 : p.ir_steps;
+    for (int step = 0; step < ir_steps; step++) {
       // FP64 residual of the subdomain system, rounded into the FP32 work vector
       double rn = 0.0;
       for (int c = tid; c < nI; c += blockDim.x) {
@@ -978,6 +988,7 @@ template <typename T>
 __global__ void __launch_bounds__(32) subsolve_staged_kernel(DevProblem p, int mode, const double2 *rhs, double2 *xout,
                                                              T *zstash, int accumulate, StageLayout lay) {
   if (mode == kModeIter && p.sc->status != 0) return;
+  if (accumulate && refine_skipped(p, mode)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x;
   const int s = p.sub_order[blockIdx.x];
@@ -1097,6 +1108,7 @@ __global__ void iface_product_kernel(DevProblem p, int mode) {
 template <int kL>
 __global__ void ir_residual_kernel(DevProblem p, int mode) {
   if (mode == kModeIter && p.sc->status != 0) return;
+  if (refine_skipped(p, mode)) return;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t row = t / kL;
   const int sub = (int)(t % kL);
@@ -1441,13 +1453,26 @@ size_t subsolve_staged_smem_bytes(int max_interior, int max_blocks, int cap, boo
   return stage_layout(max_interior, max_blocks, cap, fp32).total;
 }
 
-int configure_subsolve_staged(size_t smem) {
+// The dynamic shared-memory limit of a kernel is process-wide (per device):
+// it is only ever raised, so that a context configured later with smaller
+// subdomains cannot break the launches of an earlier one.
+int raise_smem_limit(const void *func, int slot, size_t smem) {
+  constexpr int kDevs = 64, kSlots = 4;
+  static std::mutex mu;
+  static size_t current[kDevs][kSlots] = {};
   if (smem > 227 * 1024) return -1;
-  cudaError_t e1 =
-      cudaFuncSetAttribute(subsolve_staged_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaError_t e2 =
-      cudaFuncSetAttribute(subsolve_staged_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  return (e1 == cudaSuccess && e2 == cudaSuccess) ? 0 : -2;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) return -2;
+  std::lock_guard<std::mutex> lock(mu);
+  if (smem <= current[dev][slot]) return 0;
+  if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -2;
+  current[dev][slot] = smem;
+  return 0;
+}
+
+int configure_subsolve_staged(size_t smem, bool fp32) {
+  return fp32 ? raise_smem_limit((const void *)subsolve_staged_kernel<float2>, 0, smem)
+              : raise_smem_limit((const void *)subsolve_staged_kernel<double2>, 1, smem);
 }
 
 int subsolve_launches(const DevProblem &p, bool fp32) {
@@ -1455,11 +1480,9 @@ int subsolve_launches(const DevProblem &p, bool fp32) {
   return 1;
 }
 
-int configure_subsolve(size_t smem) {
-  if (smem > 227 * 1024) return -1;
-  cudaError_t e1 = cudaFuncSetAttribute(subsolve_cta_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaError_t e2 = cudaFuncSetAttribute(subsolve_cta_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  return (e1 == cudaSuccess && e2 == cudaSuccess) ? 0 : -2;
+int configure_subsolve(size_t smem, bool fp32) {
+  return fp32 ? raise_smem_limit((const void *)subsolve_cta_kernel<true>, 2, smem)
+              : raise_smem_limit((const void *)subsolve_cta_kernel<false>, 3, smem);
 }
 
 void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream) {

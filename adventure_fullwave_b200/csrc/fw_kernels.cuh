@@ -73,6 +73,7 @@ struct DevProblem {
   int32_t n_part_blocks;
   int32_t ir_steps;
   double ir_tol;
+  double ir_relax;               // interface iterations refine only while sc->resi > ir_relax
   int32_t cta_smem;              // dynamic shared bytes of the CTA-per-subdomain solve (0: not available)
   int32_t hist_cap;              // entries of hist
   int32_t solve_variant;         // SolveVariant of the batched subdomain solve
@@ -117,9 +118,9 @@ void launch_factor(const DevProblem &p, const int64_t *int_off, const int32_t *e
 void launch_to_fp32(int64_t n, const double2 *src, float2 *dst, cudaStream_t stream);
 void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stream);
 size_t subsolve_smem_bytes(int max_interior, int max_iface, bool fp32);
-int configure_subsolve(size_t smem);
+int configure_subsolve(size_t smem, bool fp32);
 size_t subsolve_staged_smem_bytes(int max_interior, int max_blocks, int cap, bool fp32);
-int configure_subsolve_staged(size_t smem);
+int configure_subsolve_staged(size_t smem, bool fp32);
 // kernels one launch_subsolve call issues
 int subsolve_launches(const DevProblem &p, bool fp32);
 void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream);

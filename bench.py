@@ -12,6 +12,12 @@ solve, download of the edge solution) timed per step.
     python bench.py [--gpus N --steps K --warmup W] [--config c2] [--precision fp64|fp32_ir]
     python bench.py --impl reference ...   # the reference's own CPU solver
 
+``value`` is the FP64 solve (the reference's arithmetic); the line adds
+``mixed_precision`` (the same model solved with FP32 factors and FP64
+refinement to the same tolerance: time, iterations and relative L2 distance
+to the FP64 solution) and ``adjoint`` (the C4 design-region model: one
+forward solve and the backward call on its factors).
+
 Under torchrun (N > 1) every rank solves its own copy of the model (replicas;
 the multi-GPU interface exchange is not in this run), and rank 0 prints the
 line.
@@ -36,7 +42,7 @@ import numpy as np  # noqa: E402
 
 from adventure_fullwave_b200 import meshgen  # noqa: E402
 
-METRIC = "time-to-1e-6 HDDM residual (max-norm relative, interface COCG), 1 B200"
+METRIC = "time-to-1e-6 HDDM residual, batched FP32+IR vs plain FP64, 1 B200; grad time"
 WORKLOADS = {
     "c1": "C1: [0,1]^3 16^3 hexes x 6 Kuhn tets (24,576 tets), vacuum, 4-cell PML, PEC wall, 300 MHz, "
           "centre z-dipole, RCB 1 part x 64 subdomains",
@@ -117,23 +123,26 @@ class ClockSampler:
 
 
 def algorithmic_bytes(sz: dict, precision: str, ir_steps: int) -> int:
-    """Bytes one batched subdomain-solve launch must move at least: one pass
-    over the interior envelope, the interface-row and coupling operators
-    (value + column), row metadata and the interface values in and out."""
+    """Bytes one batched subdomain-solve phase of an interface iteration must
+    move at least: (k+1) passes over the interior envelope (k = refinement
+    steps; FP64 has k = 0, and a second sweep over the same rows counts once),
+    the interface-row and coupling operators once (value + column), the
+    interior operator once per refinement step, c_v = 4 passes over the
+    subdomains' local FP64 vectors and the interface values in and out."""
     elem = 16 if precision == "fp64" else 8
-    b = sz["nlen_interior"] * elem
+    k = 0 if precision == "fp64" else ir_steps
+    b = (k + 1) * sz["nlen_interior"] * elem
     b += (sz["nnz_interface_rows"] + sz["nnz_coupling"]) * 20
-    b += sz["total_interior"] * (4 + 8 + 4) + sz["total_iface_slots"] * (4 + 4)
-    b += sz["total_iface_slots"] * 32
-    if precision != "fp64":
-        b += ir_steps * sz["nnz_interior"] * 20
+    b += k * sz["nnz_interior"] * 20
+    b += sz["total_dofs"] * 16 * 4
+    b += sz["total_iface_slots"] * (4 + 16 + 16)
     return int(b)
 
 
 def ncu_traffic(kernel: str, config: str, precision: str):
-    """DRAM bytes per launch of the substitution kernel from the committed
-    ncu summary (profiles/subsolve_<kernel>_<config>_<precision>.md), when
-    one covers this workload."""
+    """DRAM bytes of one subdomain-solve phase from the committed ncu summary
+    (profiles/subsolve_<kernel>_<config>_<precision>.md), when one covers
+    this workload."""
     path = os.path.join(REPO, "profiles", f"subsolve_{kernel}_{config}_{precision}.md")
     try:
         for line in open(path):
@@ -220,8 +229,9 @@ def run_ours(args):
 
     model = make_model(args.config)
     solver = hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
-                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, graph_iterations=args.graph_iters,
-                             device=local, solve_kernel=args.solve_kernel, stage_cap=args.stage_cap)
+                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
+                             graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
+                             stage_cap=args.stage_cap)
     for _ in range(args.warmup):
         solver.solve(0)
     clocks = ClockSampler(local)
@@ -248,20 +258,57 @@ def run_ours(args):
     sz = solver.sizes()
     x_check = solver.edge_solution()
 
+    mixed = None
+    if args.precision == "fp64" and not args.no_mixed:
+        # the same model with FP32 factors and FP64 refinement, to the same tolerance
+        with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision="fp32_ir",
+                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
+                             graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
+                             stage_cap=args.stage_cap) as s32:
+            s32.solve(0)
+            t32, it32 = [], []
+            for _ in range(args.steps):
+                r32 = s32.solve(0)
+                t32.append((r32.t_setup_ms + r32.t_iterate_ms + r32.t_last_ms) / 1e3)
+                it32.append(r32.iterations)
+            x32 = s32.edge_solution()
+        v32 = float(np.mean(t32))
+        mixed = {"fp32_ir_s": v32, "fp64_s": float(np.mean(times)), "fp64_over_fp32_ir": float(np.mean(times)) / v32,
+                 "fp32_ir_iterations": int(np.mean(it32)), "fp64_iterations": int(np.mean(iters)),
+                 "rel_l2_vs_fp64": float(np.linalg.norm(x32 - x_check) / np.linalg.norm(x_check)),
+                 "ir_steps": args.ir_steps, "ir_relax": args.ir_relax, "converged": bool(r32.converged),
+                 "solve_kernel": r32.solve_kernel, "stage_cap": r32.stage_cap}
+
     adjoint = None
+    adj_model, adj_solver = None, None
     if len(model.design_tets) > 0:
+        adj_model, adj_solver = model, solver
+    elif args.config == "c2" and not args.no_adjoint:
+        # the adjoint is quoted on the C2 mesh with the design region (C4)
+        adj_model = make_model("c4")
+        adj_solver = hddm.HddmSolver(adj_model, hddm_eps=args.eps, hddm_max_loop=args.max_loop,
+                                     precision=args.precision, ir_max_steps=args.ir_steps, ir_tol=args.ir_tol,
+                                     graph_iterations=args.graph_iters, device=local,
+                                     solve_kernel=args.solve_kernel, stage_cap=args.stage_cap)
+        adj_solver.solve(0)
+    if adj_solver is not None:
         # the backward: one adjoint HDDM solve on the forward factors plus the gradient kernel
         fwd, adj = [], []
-        for _ in range(args.steps):
-            r = solver.solve(0)
+        for _ in range(args.adjoint_steps):
+            r = adj_solver.solve(0)
             fwd.append((r.t_setup_ms + r.t_iterate_ms + r.t_last_ms) / 1e3)
             t0 = time.perf_counter()
-            J, ge, gs, ra = solver.adjoint_gradient()
+            J, ge, gs, ra = adj_solver.adjoint_gradient()
             adj.append(time.perf_counter() - t0)
-        adjoint = {"forward_s": float(np.mean(fwd)), "adjoint_s": float(np.mean(adj)),
+        adjoint = {"config": "c4", "forward_s": float(np.mean(fwd)), "adjoint_s": float(np.mean(adj)),
                    "adjoint_over_forward": float(np.mean(adj) / np.mean(fwd)), "J": J,
-                   "adjoint_iterations": ra.iterations, "n_design": int(len(model.design_tets)),
-                   "grad_finite": bool(np.all(np.isfinite(ge)) and np.all(np.isfinite(gs)))}
+                   "forward_iterations": r.iterations, "adjoint_iterations": ra.iterations,
+                   "n_design": int(len(adj_model.design_tets)),
+                   "grad_finite": bool(np.all(np.isfinite(ge)) and np.all(np.isfinite(gs))),
+                   "timing": "forward: device events of one solve; adjoint: host wall time of the backward call "
+                             "(adjoint HDDM solve on the forward factors + gradient kernel)"}
+        if adj_solver is not solver:
+            adj_solver.close()
 
     # kernel timing of the dominant kernel for the roofline
     prof = solver.profile_iteration(reps=args.prof_reps)
@@ -270,9 +317,10 @@ def run_ours(args):
     alg = algorithmic_bytes(sz, args.precision, args.ir_steps)
     achieved = alg / (prof["subsolve_ms"] * 1e-3) / 1e9
     traffic = ncu_traffic(results[-1].solve_kernel, args.config, args.precision)
-    kname = {"warp": "subsolve_warp_kernel", "cta": "subsolve_cta_kernel", "global": "subsolve_kernel"}.get(
-        results[-1].solve_kernel, results[-1].solve_kernel)
-    roofline = {"bound": "hbm", "kernel": f"{kname} (one batched subdomain solve)",
+    kname = {"warp": "rhs_kernel + subsolve_staged_kernel + iface_product_kernel",
+             "cta": "subsolve_cta_kernel", "global": "subsolve_kernel"}.get(results[-1].solve_kernel,
+                                                                           results[-1].solve_kernel)
+    roofline = {"bound": "hbm", "kernel": f"{kname} (one batched subdomain solve of an interface iteration)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic, "algorithmic_bytes": alg,
                 "kernel_ms": prof["subsolve_ms"], "interface_kernels_ms": prof["interface_ms"],
@@ -287,8 +335,9 @@ def run_ours(args):
     for _ in range(args.e2e_steps):
         t0 = time.perf_counter()
         with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
-                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, graph_iterations=args.graph_iters,
-                             device=local, solve_kernel=args.solve_kernel, stage_cap=args.stage_cap) as s2:
+                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
+                             graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
+                             stage_cap=args.stage_cap) as s2:
             s2.solve(0)
             xe = s2.edge_solution()
         e2e_times.append(time.perf_counter() - t0)
@@ -329,6 +378,8 @@ def run_ours(args):
         "gpu_launches": int(np.sum(launches)),
         "solution_check": {"finite": bool(np.all(np.isfinite(x_check))), "final_resi": results[-1].final_resi},
     }
+    if mixed is not None:
+        line["mixed_precision"] = mixed
     if adjoint is not None:
         line["adjoint"] = adjoint
     print(json.dumps(line))
@@ -364,6 +415,10 @@ def main():
     ap.add_argument("--max-loop", type=int, default=50000)
     ap.add_argument("--ir-steps", type=int, default=1)
     ap.add_argument("--ir-tol", type=float, default=0.0)
+    ap.add_argument("--ir-relax", type=float, default=0.0, help="refine only while the COCG residual is above this")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the FP32+IR comparison solve")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the C4 adjoint sample of a C2 run")
+    ap.add_argument("--adjoint-steps", type=int, default=1)
     ap.add_argument("--graph-iters", type=int, default=32)
     ap.add_argument("--solve-kernel", default="auto", choices=["auto", "warp", "cta", "global"])
     ap.add_argument("--stage-cap", type=int, default=0, help="staging buffer elements (0: timed choice)")

@@ -97,6 +97,9 @@ typedef struct {
   int32_t device;        /* CUDA device ordinal */
   int32_t solve_kernel;  /* FWGPU_SOLVE_*: batched subdomain-solve kernel (0 = timed choice) */
   int32_t stage_cap;     /* WARP kernel: envelope elements per staging buffer (0 = timed choice) */
+  double ir_relax;       /* FP32_IR: interface iterations refine only while the COCG relative
+                            residual is above ir_relax (0 = always); the first and last
+                            subdomain solves always refine */
 } fwgpu_options;
 
 /* Batched subdomain-solve kernels.  AUTO times one launch of each candidate

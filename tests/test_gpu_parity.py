@@ -159,3 +159,21 @@ def test_slot_by_slot_equals_driver():
         x = s.edge_solution()
     assert rel_l2(x, z["x"]) <= 1e-8
     assert abs(n - int(z["iterations"][0])) <= 2
+
+
+def test_contexts_with_different_subdomain_sizes_coexist():
+    """Kernel shared-memory limits are process-wide: a context created later
+    with smaller subdomains must not break the launches of an earlier one."""
+    big = meshgen.make_model("x", n=12, size=1.0, npml=2, nleaves=6, seed=5)
+    small = meshgen.make_model("x", n=8, size=1.0, npml=2, nleaves=16, seed=2)
+    for m in (big, small):
+        meshgen.round_trip_material(m)
+    with hddm.HddmSolver(big, hddm_eps=1e-8, hddm_max_loop=20000) as sa:
+        ra = sa.solve(0)
+        xa = sa.edge_solution()
+        for prec in ("fp64", "fp32_ir"):
+            with hddm.HddmSolver(small, hddm_eps=1e-8, hddm_max_loop=20000, precision=prec) as sb:
+                assert sb.solve(0).converged
+        rb = sa.resolve(0)
+        assert ra.converged and rb.converged
+        assert rel_l2(sa.edge_solution(), xa) <= 1e-12
