@@ -828,9 +828,9 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
   return FWGPU_OK;
 }
 
-// kernels of one interface iteration: the subdomain solve and 6 COCG kernels
+// kernels of one interface iteration: the subdomain solve and 3 COCG kernels
 static int64_t iteration_launches(const fwgpu_context *c) {
-  return 6 + fw::subsolve_launches(c->dp, c->opts.precision == FWGPU_PREC_FP32_IR);
+  return 3 + fw::subsolve_launches(c->dp, c->opts.precision == FWGPU_PREC_FP32_IR);
 }
 
 int fwgpu_iteration_s_1st(fwgpu_context *c, int32_t *status) {

@@ -1079,7 +1079,9 @@ __global__ void rhs_kernel(DevProblem p, int mode, double2 *__restrict__ out) {
   if (row < p.n_interior && sub == 0) out[row] = csub(mode != kModeIter ? p.fI[row] : cz(), acc);
 }
 
-// q[slot] = A_G. [x; v] (- f_G): x from Y, v = P at the slot's interface DOF
+// q[slot] = A_G. [x; v] (- f_G): x from Y, v = P at the slot's interface DOF.
+// The first 4 entries of each lane are loaded together (column indices, then
+// values and gathered operands), the rest of a long row in a loop.
 template <int kL>
 __global__ void iface_product_kernel(DevProblem p, int mode) {
   if (mode == kModeIter && p.sc->status != 0) return;
@@ -1089,11 +1091,24 @@ __global__ void iface_product_kernel(DevProblem p, int mode) {
   const bool with_bc = mode != kModeFirst;
   double2 acc = cz();
   if (row < p.n_slots) {
-    const int64_t q1 = p.ifr_rowptr[row + 1];
-    for (int64_t q = p.ifr_rowptr[row] + sub; q < q1; q += kL) {
-      const int64_t g = p.ifr_gcol[q];
-      const double2 xv = g >= 0 ? p.Y[g] : (with_bc ? p.P[-g - 1] : cz());
-      acc = cadd(acc, cmul(p.ifr_val[q], xv));
+    const int64_t q0 = p.ifr_rowptr[row] + sub, q1 = p.ifr_rowptr[row + 1];
+    constexpr int kU = 4;
+    int32_t g[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) g[u] = q0 + u * kL < q1 ? p.ifr_gcol[q0 + u * kL] : 0;
+    double2 a[kU], xv[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      const bool in = q0 + u * kL < q1;
+      a[u] = in ? p.ifr_val[q0 + u * kL] : cz();
+      xv[u] = !in ? cz() : g[u] >= 0 ? p.Y[g[u]] : (with_bc ? p.P[-g[u] - 1] : cz());
+    }
+#pragma unroll
+    for (int u = 0; u < kU; u++) acc = cadd(acc, cmul(a[u], xv[u]));
+    for (int64_t q = q0 + kU * kL; q < q1; q += kL) {
+      const int32_t gq = p.ifr_gcol[q];
+      const double2 x = gq >= 0 ? p.Y[gq] : (with_bc ? p.P[-gq - 1] : cz());
+      acc = cadd(acc, cmul(p.ifr_val[q], x));
     }
   }
   acc = group_sum<kL>(acc);
@@ -1154,7 +1169,7 @@ __device__ __forceinline__ double block_max(double v, double *sh) {
 __device__ double reduce_partials(const double *part, int nb, int f, bool is_max, double *sh) {
   double v = 0.0;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-    const double x = part[f * nb + i];
+    const double x = __ldcg(part + f * nb + i);  // written by other CTAs of this grid
     v = is_max ? fmax(v, x) : v + x;
   }
   double r = is_max ? block_max(v, sh) : block_sum(v, sh);
@@ -1164,6 +1179,18 @@ __device__ double reduce_partials(const double *part, int nb, int f, bool is_max
   r = sh[32];
   __syncthreads();
   return r;
+}
+
+// True in the last CTA of the grid to get here, after every CTA wrote its
+// partials; that CTA then reduces them in block order (deterministic) and
+// resets the ticket for the next launch.
+__device__ __forceinline__ bool last_cta(uint32_t *ticket) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  return last;
 }
 
 __device__ __forceinline__ double2 gather_q(const DevProblem &p, int g) {
@@ -1229,11 +1256,8 @@ __global__ void cocg_first_scalars_kernel(DevProblem p) {
   }
 }
 
-__global__ void cocg_begin_kernel(CocgScalars *sc) {
-  if (sc->status == 1) sc->status = 2;
-}
-
-// Q gathered over subdomains (hddm_solver_s.h:273 with COM_RES_SP) and (p, q)
+// Q gathered over subdomains (hddm_solver_s.h:273 with COM_RES_SP), (p, q),
+// and in the last CTA -alpha = -(r, z) / (p, q)  (hddm_solver_s.h:282-295)
 __global__ void cocg_gather_pq_kernel(DevProblem p) {
   if (p.sc->status != 0) return;
   __shared__ double sh[40];
@@ -1250,13 +1274,7 @@ __global__ void cocg_gather_pq_kernel(DevProblem p) {
   if (threadIdx.x == 0) p.part[kFPqRe * nb + blockIdx.x] = r;
   r = block_sum(im, sh);
   if (threadIdx.x == 0) p.part[kFPqIm * nb + blockIdx.x] = r;
-}
-
-// -alpha = -(r, z) / (p, q)  (hddm_solver_s.h:282-295)
-__global__ void cocg_alpha_kernel(DevProblem p) {
-  if (p.sc->status != 0) return;
-  __shared__ double sh[40];
-  const int nb = p.n_part_blocks;
+  if (!last_cta(&p.sc->ticket[0])) return;
   const double pr = reduce_partials(p.part, nb, kFPqRe, false, sh);
   const double pi = reduce_partials(p.part, nb, kFPqIm, false, sh);
   if (threadIdx.x == 0) {
@@ -1267,6 +1285,7 @@ __global__ void cocg_alpha_kernel(DevProblem p) {
     } else {
       sc->malpha = csub(cz(), cdiv_ref(sc->rz, pq));
     }
+    sc->ticket[0] = 0;
   }
 }
 
@@ -1298,25 +1317,20 @@ __global__ void cocg_update_kernel(DevProblem p) {
   if (threadIdx.x == 0) p.part[kFRzIm * nb + blockIdx.x] = r;
   r = block_sum(l2, sh);
   if (threadIdx.x == 0) p.part[kFL2 * nb + blockIdx.x] = r;
-}
-
-// resi, beta = (r', z') / (r, z), convergence and loop count
-// (hddm_solver_s.h:318-379, hddm_solver.h:125-143)
-__global__ void cocg_beta_kernel(DevProblem p) {
-  if (p.sc->status != 0) return;
-  __shared__ double sh[40];
-  const int nb = p.n_part_blocks;
-  const double mx = reduce_partials(p.part, nb, kFMax, true, sh);
-  const double rzr = reduce_partials(p.part, nb, kFRzRe, false, sh);
-  const double rzi = reduce_partials(p.part, nb, kFRzIm, false, sh);
-  const double l2 = reduce_partials(p.part, nb, kFL2, false, sh);
+  // last CTA: resi, beta = (r', z') / (r, z), convergence and loop count
+  // (hddm_solver_s.h:318-379, hddm_solver.h:125-143)
+  if (!last_cta(&p.sc->ticket[1])) return;
+  const double rmx = reduce_partials(p.part, nb, kFMax, true, sh);
+  const double rzr_t = reduce_partials(p.part, nb, kFRzRe, false, sh);
+  const double rzi_t = reduce_partials(p.part, nb, kFRzIm, false, sh);
+  const double l2_t = reduce_partials(p.part, nb, kFL2, false, sh);
   if (threadIdx.x == 0) {
     CocgScalars *sc = p.sc;
-    const double resi = mx * sc->r0inv;
+    const double resi = rmx * sc->r0inv;
     sc->resi = resi;
-    sc->resi_l2 = sqrt(l2) / sc->l2_0;
+    sc->resi_l2 = sqrt(l2_t) / sc->l2_0;
     if (sc->loop - 1 < p.hist_cap) p.hist[sc->loop - 1] = resi;
-    const double2 rz = make_double2(rzr, rzi);
+    const double2 rz = make_double2(rzr_t, rzi_t);
     if (cabs_ref(rz) < kNearlyZero && cabs_ref(sc->rz) < kNearlyZero) {
       sc->beta = cz();
     } else {
@@ -1330,16 +1344,23 @@ __global__ void cocg_beta_kernel(DevProblem p) {
       sc->status = 1;
     }
     sc->loop += 1;
+    sc->ticket[1] = 0;
   }
 }
 
 // p = z + beta p, or p = u after the last iteration (hddm_solver_s.h:356-376)
+// After the last iteration's p = u the last CTA marks the loop finished
+// (status 2), so that the iterations left in a graph launch do nothing.
 __global__ void cocg_pupdate_kernel(DevProblem p) {
   const int st = p.sc->status;
   if (st == 2) return;
   const double2 be = p.sc->beta;
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
     p.P[g] = st == 1 ? p.U[g] : cadd(p.Z[g], cmul(be, p.P[g]));
+  }
+  if (st == 1 && last_cta(&p.sc->ticket[2]) && threadIdx.x == 0) {
+    p.sc->status = 2;
+    p.sc->ticket[2] = 0;
   }
 }
 
@@ -1352,6 +1373,7 @@ __global__ void edge_solution_kernel(int64_t ne, const int64_t *__restrict__ src
 }
 
 __global__ void set_status_kernel(CocgScalars *sc, double eps, int32_t max_loop) {
+  for (int i = 0; i < 4; i++) sc->ticket[i] = 0;
   sc->eps = eps;
   sc->max_loop = max_loop;
   sc->status = 0;
@@ -1361,6 +1383,7 @@ __global__ void set_status_kernel(CocgScalars *sc, double eps, int32_t max_loop)
 
 // iteration state for kernel timing: never converges, no loop limit
 __global__ void profile_reset_kernel(CocgScalars *sc) {
+  for (int i = 0; i < 4; i++) sc->ticket[i] = 0;
   sc->status = 0;
   sc->eps = -1.0;
   sc->max_loop = 0x7fffffff;
@@ -1431,7 +1454,7 @@ void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stre
     } else {
       subsolve_staged_kernel<double2><<<p.nsub, 32, lay.total, stream>>>(p, mode, p.Y, p.Y, p.Y, 0, lay);
     }
-    iface_product_kernel<8><<<blocks_min1(p.n_slots * 8, 256), 256, 0, stream>>>(p, mode);
+    iface_product_kernel<4><<<blocks_min1(p.n_slots * 4, 256), 256, 0, stream>>>(p, mode);
     return;
   }
   if (p.solve_variant == kSolveCta && p.cta_smem > 0) {
@@ -1491,12 +1514,9 @@ void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t s
 }
 
 void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream) {
-  cocg_begin_kernel<<<1, 1, 0, stream>>>(p.sc);
   launch_subsolve(p, kModeIter, p.L32 != nullptr, stream);
   cocg_gather_pq_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
-  cocg_alpha_kernel<<<1, kRedThreads, 0, stream>>>(p);
   cocg_update_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
-  cocg_beta_kernel<<<1, kRedThreads, 0, stream>>>(p);
   cocg_pupdate_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
 }
 

@@ -26,7 +26,8 @@ struct CocgScalars {
   int32_t max_loop;  // hddm_max_loop
   int32_t converged;
   int32_t factor_status;  // non-zero: a pivot was zero or not finite
-  int32_t pad;
+  int32_t pad;       // non-zero: a subdomain solve gave up waiting for a copy
+  uint32_t ticket[4];  // CTAs of a reduction kernel that wrote their partials (last one reduces)
 };
 
 // Per-problem device pointers used by the iteration kernels.
