@@ -57,7 +57,7 @@ class FwOptions(ctypes.Structure):
     _fields_ = [
         ("hddm_eps", c_dbl), ("hddm_max_loop", c_i32), ("precision", c_i32), ("ir_max_steps", c_i32),
         ("ir_tol", c_dbl), ("graph_iterations", c_i32), ("device", c_i32), ("solve_kernel", c_i32),
-        ("stage_cap", c_i32), ("ir_relax", c_dbl),
+        ("stage_cap", c_i32), ("ir_relax", c_dbl), ("shard_begin", c_i32), ("shard_end", c_i32),
     ]
 
 
@@ -104,6 +104,11 @@ SIGNATURES = {
     "fwgpu_profile_iteration": [ctypes.c_void_p, c_i32, P(FwKernelProfile)],
     "fwgpu_adjoint_gradient": [ctypes.c_void_p, c_i32, P(c_i32), c_i32, P(c_i32), P(c_dbl), P(c_dbl), P(c_dbl),
                                P(FwResult)],
+    "fwgpu_shard_set_exchange": [ctypes.c_void_p, ctypes.c_void_p],
+    "fwgpu_shard_first": [ctypes.c_void_p],
+    "fwgpu_shard_first_finish": [ctypes.c_void_p, P(c_i32)],
+    "fwgpu_shard_iterate": [ctypes.c_void_p],
+    "fwgpu_shard_iterate_finish": [ctypes.c_void_p, P(c_i32)],
     "fwgpu_skyline_solve_noalloc": [c_i32, c_i32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p],

@@ -86,6 +86,8 @@ struct fwgpu_context {
   int64_t *d_cpl_src = nullptr, *d_ifr_src = nullptr, *d_aii_src = nullptr, *d_diag_src = nullptr;
   std::vector<int32_t> h_src_owner, h_src_local;  // first subdomain holding each edge, and its local DOF
   bool warp_ok = false;            // the staged warp-per-subdomain kernel fits in shared memory
+  bool sharded = false;            // solves a range of the subdomains (fwgpu_shard_* calls)
+  double2 *d_exchange = nullptr;   // caller's buffer: partial Q, then partial PC diagonal
   int32_t *d_blk_off = nullptr;    // staged solve block table (current staging capacity)
   int2 *d_blk_tab = nullptr;
   std::vector<int> stage_caps;     // staging capacities that fit in shared memory
@@ -332,15 +334,24 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   FW_TRY(c->alloc(&c->d_mesh_status, 4));
   FW_CUDA(cudaMemsetAsync(c->d_mesh_status, 0, 4 * sizeof(int32_t), c->stream));
 
+  // the subdomains this context solves: all, or a shard's range
+  int s_begin = 0, s_end = nsub;
+  if (opts->shard_begin != 0 || opts->shard_end != 0) {
+    if (opts->shard_begin < 0 || opts->shard_end > nsub || opts->shard_begin >= opts->shard_end)
+      return set_error(FWGPU_ERR_ARG, "shard range outside the subdomains");
+    s_begin = opts->shard_begin;
+    s_end = opts->shard_end;
+    c->sharded = s_begin != 0 || s_end != nsub;
+  }
   // subdomains largest first (by interior DOFs, then local DOFs)
-  std::vector<int32_t> order(nsub);
-  for (int s = 0; s < nsub; s++) order[s] = s;
+  std::vector<int32_t> order(s_end - s_begin);
+  for (int s = s_begin; s < s_end; s++) order[s - s_begin] = s;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     const fw::SubHost &x = p.subs[a], &y = p.subs[b];
     return x.nI != y.nI ? x.nI > y.nI : x.nmp > y.nmp;
   });
   fw::DevProblem &dp = c->dp;
-  dp.nsub = nsub;
+  dp.nsub = s_end - s_begin;
   dp.nfree = p.total_free;
   int32_t *d_order = nullptr;
   int64_t *d_int_off = nullptr, *d_if_off = nullptr;
@@ -412,8 +423,14 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
     dp.aii_rowptr = lp;
     FW_TRY(c->upload(&ip, ag));
     dp.aii_gcol = ip;
-    dp.n_interior = nI_all;
-    dp.n_slots = nG_all;
+    (void)nI_all;
+    (void)nG_all;
+    dp.row0 = p.sub_int_off[s_begin];
+    dp.n_interior = p.sub_int_off[s_end] - p.sub_int_off[s_begin];
+    dp.slot0 = p.sub_if_off[s_begin];
+    dp.n_slots = p.sub_if_off[s_end] - p.sub_if_off[s_begin];
+    dp.xq = nullptr;
+    dp.xpc = nullptr;
   }
   FW_TRY(c->alloc(&c->d_cpl_val, p.cpl_src.size()));
   FW_TRY(c->alloc(&c->d_ifr_val, p.ifr_src.size()));
@@ -835,6 +852,7 @@ static int64_t iteration_launches(const fwgpu_context *c) {
 
 int fwgpu_iteration_s_1st(fwgpu_context *c, int32_t *status) {
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
   if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "iteration_s_1st before solve_dom_1st");
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_set_status(c->d_sc, c->opts.hddm_eps, c->opts.hddm_max_loop, c->stream);
@@ -848,10 +866,73 @@ int fwgpu_iteration_s_1st(fwgpu_context *c, int32_t *status) {
 
 int fwgpu_iteration_s(fwgpu_context *c, int32_t *status) {
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
   if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "iteration_s outside the interface loop");
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_cocg_iteration(c->dp, c->stream);
   c->launches += iteration_launches(c);
+  FW_CUDA(cudaGetLastError());
+  FW_TRY(read_status(c, status));
+  return FWGPU_OK;
+}
+
+int fwgpu_shard_set_exchange(fwgpu_context *c, double *d_exchange) {
+  if (!c || !d_exchange) return set_error(FWGPU_ERR_ARG, "null argument");
+  c->d_exchange = (double2 *)d_exchange;
+  return FWGPU_OK;
+}
+
+int fwgpu_shard_first(fwgpu_context *c) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (!c->d_exchange) return set_error(FWGPU_ERR_STATE, "no exchange buffer (fwgpu_shard_set_exchange)");
+  FW_TRY(fwgpu_solve_dom_1st(c));
+  c->dp.xq = nullptr;
+  c->dp.xpc = nullptr;
+  fw::launch_shard_gather(c->dp, c->d_pcloc, c->d_exchange, c->d_exchange + c->dp.nfree, false, c->stream);
+  c->launches += 1;
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  return FWGPU_OK;
+}
+
+int fwgpu_shard_first_finish(fwgpu_context *c, int32_t *status) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->stage < 2 || !c->d_exchange) return set_error(FWGPU_ERR_STATE, "shard_first_finish before shard_first");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  c->dp.xq = c->d_exchange;
+  c->dp.xpc = c->d_exchange + c->dp.nfree;
+  fw::launch_set_status(c->d_sc, c->opts.hddm_eps, c->opts.hddm_max_loop, c->stream);
+  fw::launch_cocg_first(c->dp, c->d_pcloc, c->stream);
+  c->dp.xq = nullptr;
+  c->dp.xpc = nullptr;
+  c->launches += 3;
+  FW_CUDA(cudaGetLastError());
+  FW_TRY(read_status(c, status));
+  c->stage = 3;
+  return FWGPU_OK;
+}
+
+int fwgpu_shard_iterate(fwgpu_context *c) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "shard_iterate outside the interface loop");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
+  fw::launch_subsolve(c->dp, fw::kModeIter, fp32, c->stream);
+  fw::launch_shard_gather(c->dp, c->d_pcloc, c->d_exchange, nullptr, true, c->stream);
+  c->launches += 1 + fw::subsolve_launches(c->dp, fp32);
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  return FWGPU_OK;
+}
+
+int fwgpu_shard_iterate_finish(fwgpu_context *c, int32_t *status) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "shard_iterate_finish outside the interface loop");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  c->dp.xq = c->d_exchange;
+  fw::launch_cocg_update(c->dp, c->stream);
+  c->dp.xq = nullptr;
+  c->launches += 3;
   FW_CUDA(cudaGetLastError());
   FW_TRY(read_status(c, status));
   return FWGPU_OK;
@@ -862,7 +943,7 @@ int fwgpu_solve_dom_last(fwgpu_context *c) {
   if (c->stage < 3) return set_error(FWGPU_ERR_STATE, "solve_dom_last before the interface loop");
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_subsolve(c->dp, fw::kModeLast, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
-  fw::launch_edge_solution(c->m.ne, c->d_edge_src, c->dp.Y, c->dp.V, c->d_xedge, c->stream);
+  fw::launch_edge_solution(c->dp, c->m.ne, c->d_edge_src, c->dp.Y, c->dp.V, c->d_xedge, c->stream);
   c->launches += 1 + fw::subsolve_launches(c->dp, c->opts.precision == FWGPU_PREC_FP32_IR);
   FW_CUDA(cudaGetLastError());
   FW_CUDA(cudaStreamSynchronize(c->stream));
@@ -916,6 +997,7 @@ static int fill_result(fwgpu_context *c, fwgpu_result *res) {
 
 int fwgpu_hddm_solve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *res) {
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
   if (c->opts.hddm_max_loop == 0) return set_error(FWGPU_ERR_ARG, "hddm_max_loop is 0");
   c->launches = 0;
   FW_TRY(fwgpu_make_tmp_aij(c, src));
@@ -933,6 +1015,7 @@ int fwgpu_hddm_solve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *re
 
 int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *res) {
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
   if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "resolve before the factors exist");
   FW_CUDA(cudaSetDevice(c->opts.device));
   FW_CUDA(cudaEventRecord(c->ev[0], c->stream));

@@ -855,40 +855,67 @@ __device__ void staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, cons
     stage_wait(st, b);
     __syncwarp();
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);  // S[e]: entry e of the envelope
-    // entries left of the block; the loads of 8 rows are issued together
+    // entries left of the block.  FP32: each lane walks its own row (two
+    // accumulators, 4 entries' loads in flight).  FP64: lanes across a row,
+    // 8 rows' loads issued together and one transpose-reduction per 8 rows
+    // (16-byte entries make the per-lane walk's bank conflicts too costly).
     T rect = czero<T>();
-    for (int g = 0; g < nb; g += kSGroup) {
-      int2 mt[kSGroup];
-      int len[kSGroup];
+    if (sizeof(T) == 8) {
+      const int my_len = lane < nb ? max(0, r0 - my_lo) : 0;
+      int longest = my_len;
 #pragma unroll
-      for (int u = 0; u < kSGroup; u++) {
-        mt[u] = meta[g + u];
-        len[u] = g + u < nb ? max(0, r0 - mt[u].x) : 0;
-      }
-      T a0[kSGroup], b0[kSGroup], a1[kSGroup], b1[kSGroup];
+      for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
+      const T *row = S + my_pr;
+      const T *yr = y + (lane < nb ? my_lo : 0);
+      T acc0 = czero<T>(), acc1 = czero<T>();
+      for (int k = 0; k < longest; k += 4) {
+        T a[4], b[4];
 #pragma unroll
-      for (int u = 0; u < kSGroup; u++) {
-        const bool c0 = lane < len[u], c1 = lane + 32 < len[u];
-        a0[u] = c0 ? S[mt[u].y + lane] : czero<T>();
-        b0[u] = c0 ? y[mt[u].x + lane] : czero<T>();
-        a1[u] = c1 ? S[mt[u].y + lane + 32] : czero<T>();
-        b1[u] = c1 ? y[mt[u].x + lane + 32] : czero<T>();
+        for (int u = 0; u < 4; u++) {
+          const bool in = k + u < my_len;
+          a[u] = in ? row[k + u] : czero<T>();
+          b[u] = in ? yr[k + u] : czero<T>();
+        }
+        acc0 = cadd(acc0, cmul(a[0], b[0]));
+        acc1 = cadd(acc1, cmul(a[1], b[1]));
+        acc0 = cadd(acc0, cmul(a[2], b[2]));
+        acc1 = cadd(acc1, cmul(a[3], b[3]));
       }
-      T acc[kSGroup];
-      int longest = 0;
+      rect = cadd(acc0, acc1);
+    } else {
+      for (int g = 0; g < nb; g += kSGroup) {
+        int2 mt[kSGroup];
+        int len[kSGroup];
 #pragma unroll
-      for (int u = 0; u < kSGroup; u++) {
-        acc[u] = cadd(cmul(a0[u], b0[u]), cmul(a1[u], b1[u]));
-        longest = max(longest, len[u]);
-      }
-      if (longest > 64) {
+        for (int u = 0; u < kSGroup; u++) {
+          mt[u] = meta[g + u];
+          len[u] = g + u < nb ? max(0, r0 - mt[u].x) : 0;
+        }
+        T a0[kSGroup], b0[kSGroup], a1[kSGroup], b1[kSGroup];
 #pragma unroll
-        for (int u = 0; u < kSGroup; u++)
-          for (int k = lane + 64; k < len[u]; k += 32) acc[u] = cadd(acc[u], cmul(S[mt[u].y + k], y[mt[u].x + k]));
+        for (int u = 0; u < kSGroup; u++) {
+          const bool c0 = lane < len[u], c1 = lane + 32 < len[u];
+          a0[u] = c0 ? S[mt[u].y + lane] : czero<T>();
+          b0[u] = c0 ? y[mt[u].x + lane] : czero<T>();
+          a1[u] = c1 ? S[mt[u].y + lane + 32] : czero<T>();
+          b1[u] = c1 ? y[mt[u].x + lane + 32] : czero<T>();
+        }
+        T acc[kSGroup];
+        int longest = 0;
+#pragma unroll
+        for (int u = 0; u < kSGroup; u++) {
+          acc[u] = cadd(cmul(a0[u], b0[u]), cmul(a1[u], b1[u]));
+          longest = max(longest, len[u]);
+        }
+        if (longest > 64) {
+#pragma unroll
+          for (int u = 0; u < kSGroup; u++)
+            for (int k = lane + 64; k < len[u]; k += 32) acc[u] = cadd(acc[u], cmul(S[mt[u].y + k], y[mt[u].x + k]));
+        }
+        const T sum = transpose_reduce8(acc, lane);
+        const T pick = shfl_idx(sum, 4 * (lane & 7));
+        if ((lane >> 3) == (g >> 3)) rect = pick;
       }
-      const T sum = transpose_reduce8(acc, lane);
-      const T pick = shfl_idx(sum, 4 * (lane & 7));
-      if ((lane >> 3) == (g >> 3)) rect = pick;
     }
     // the block's triangle: lane t holds row r0 + t; the operands of 4 steps
     // are loaded ahead of their shuffles
@@ -1068,15 +1095,16 @@ template <int kL>
 __global__ void rhs_kernel(DevProblem p, int mode, double2 *__restrict__ out) {
   if (mode == kModeIter && p.sc->status != 0) return;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t row = t / kL;
+  const bool in = t / kL < p.n_interior;
+  const int64_t row = p.row0 + t / kL;
   const int sub = (int)(t % kL);
   double2 acc = cz();
-  if (row < p.n_interior && mode != kModeFirst) {
+  if (in && mode != kModeFirst) {
     const int64_t q1 = p.cpl_rowptr[row + 1];
     for (int64_t q = p.cpl_rowptr[row] + sub; q < q1; q += kL) acc = cadd(acc, cmul(p.cpl_val[q], p.P[p.cpl_gcol[q]]));
   }
   acc = group_sum<kL>(acc);
-  if (row < p.n_interior && sub == 0) out[row] = csub(mode != kModeIter ? p.fI[row] : cz(), acc);
+  if (in && sub == 0) out[row] = csub(mode != kModeIter ? p.fI[row] : cz(), acc);
 }
 
 // q[slot] = A_G. [x; v] (- f_G): x from Y, v = P at the slot's interface DOF.
@@ -1086,11 +1114,12 @@ template <int kL>
 __global__ void iface_product_kernel(DevProblem p, int mode) {
   if (mode == kModeIter && p.sc->status != 0) return;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t row = t / kL;
+  const bool in = t / kL < p.n_slots;
+  const int64_t row = p.slot0 + t / kL;
   const int sub = (int)(t % kL);
   const bool with_bc = mode != kModeFirst;
   double2 acc = cz();
-  if (row < p.n_slots) {
+  if (in) {
     const int64_t q0 = p.ifr_rowptr[row] + sub, q1 = p.ifr_rowptr[row + 1];
     constexpr int kU = 4;
     int32_t g[kU];
@@ -1112,7 +1141,7 @@ __global__ void iface_product_kernel(DevProblem p, int mode) {
     }
   }
   acc = group_sum<kL>(acc);
-  if (row < p.n_slots && sub == 0) {
+  if (in && sub == 0) {
     if (mode != kModeIter) acc = csub(acc, p.fG[row]);
     p.qloc[row] = acc;
     if (mode == kModeLast) p.V[row] = with_bc ? p.P[p.if_ln[row]] : cz();
@@ -1125,15 +1154,16 @@ __global__ void ir_residual_kernel(DevProblem p, int mode) {
   if (mode == kModeIter && p.sc->status != 0) return;
   if (refine_skipped(p, mode)) return;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t row = t / kL;
+  const bool in = t / kL < p.n_interior;
+  const int64_t row = p.row0 + t / kL;
   const int sub = (int)(t % kL);
   double2 acc = cz();
-  if (row < p.n_interior) {
+  if (in) {
     const int64_t q1 = p.aii_rowptr[row + 1];
     for (int64_t q = p.aii_rowptr[row] + sub; q < q1; q += kL) acc = cadd(acc, cmul(p.aii_val[q], p.Y[p.aii_gcol[q]]));
   }
   acc = group_sum<kL>(acc);
-  if (row < p.n_interior && sub == 0) p.Rres[row] = csub(p.B[row], acc);
+  if (in && sub == 0) p.Rres[row] = csub(p.B[row], acc);
 }
 
 // ----------------------------------------------------------------------------
@@ -1193,10 +1223,31 @@ __device__ __forceinline__ bool last_cta(uint32_t *ticket) {
   return last;
 }
 
-__device__ __forceinline__ double2 gather_q(const DevProblem &p, int g) {
+// Sum over the subdomain slots of interface DOF g, in subdomain order; a
+// shard sums its own subdomains' slots only (all slots when not sharded).
+__device__ __forceinline__ double2 gather_slots(const DevProblem &p, const double2 *v, int g) {
   double2 q = cz();
-  for (int t = p.gq_ptr[g]; t < p.gq_ptr[g + 1]; t++) q = cadd(q, p.qloc[p.gq_slot[t]]);
+  for (int t = p.gq_ptr[g]; t < p.gq_ptr[g + 1]; t++) {
+    const int64_t sl = p.gq_slot[t];
+    if (sl >= p.slot0 && sl < p.slot0 + p.n_slots) q = cadd(q, v[sl]);
+  }
   return q;
+}
+__device__ __forceinline__ double2 gather_q(const DevProblem &p, int g) {
+  return p.xq ? p.xq[g] : gather_slots(p, p.qloc, g);
+}
+
+// A shard's partial interface sums, written to the exchange buffer that the
+// caller sums over ranks: Q (and on the first step the diagonal PC sums)
+// over this shard's subdomains (COM_RES_SP / DIAG_GATHER_S over one part's
+// subdomains, hddm_solver_sp.h:8-25, hddm_pc.h:110-124).
+__global__ void shard_gather_kernel(DevProblem p, const double2 *__restrict__ pcloc, double2 *__restrict__ xq,
+                                    double2 *__restrict__ xpc, int status_check) {
+  if (status_check && p.sc->status != 0) return;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
+    xq[g] = gather_slots(p, p.qloc, g);
+    if (xpc) xpc[g] = gather_slots(p, pcloc, g);
+  }
 }
 
 // first step: Q and PC gathered over subdomains (hddm_solver_s.h:174-181),
@@ -1206,8 +1257,7 @@ __global__ void cocg_first_kernel(DevProblem p, const double2 *__restrict__ pclo
   double mx = 0.0, rzr = 0.0, rzi = 0.0, l2 = 0.0;
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
     const double2 q = gather_q(p, g);
-    double2 pc = cz();
-    for (int t = p.gq_ptr[g]; t < p.gq_ptr[g + 1]; t++) pc = cadd(pc, pcloc[p.gq_slot[t]]);
+    double2 pc = p.xpc ? p.xpc[g] : gather_slots(p, pcloc, g);
     pc = ciszero(pc) ? make_double2(1.0, 0.0) : cdiv_ref(make_double2(1.0, 0.0), pc);
     p.PC[g] = pc;
     p.Q[g] = q;
@@ -1364,12 +1414,18 @@ __global__ void cocg_pupdate_kernel(DevProblem p) {
   }
 }
 
+// Edge value from the first subdomain holding the edge; a shard gives the
+// edges whose first holder it owns and zero for the others.
 __global__ void edge_solution_kernel(int64_t ne, const int64_t *__restrict__ src, const double2 *__restrict__ Y,
-                                     const double2 *__restrict__ V, double2 *__restrict__ x) {
+                                     const double2 *__restrict__ V, double2 *__restrict__ x, int64_t row0,
+                                     int64_t nrow, int64_t slot0, int64_t nslot) {
   int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= ne) return;
   const int64_t s = src[e];
-  x[e] = s >= 0 ? Y[s] : (s < -1 ? V[-s - 2] : make_double2(0.0, 0.0));
+  double2 v = make_double2(0.0, 0.0);
+  if (s >= 0 && s >= row0 && s < row0 + nrow) v = Y[s];
+  if (s < -1 && -s - 2 >= slot0 && -s - 2 < slot0 + nslot) v = V[-s - 2];
+  x[e] = v;
 }
 
 __global__ void set_status_kernel(CocgScalars *sc, double eps, int32_t max_loop) {
@@ -1513,17 +1569,27 @@ void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t s
   cocg_first_scalars_kernel<<<1, kRedThreads, 0, stream>>>(p);
 }
 
-void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream) {
-  launch_subsolve(p, kModeIter, p.L32 != nullptr, stream);
+void launch_cocg_update(const DevProblem &p, cudaStream_t stream) {
   cocg_gather_pq_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
   cocg_update_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
   cocg_pupdate_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
 }
 
-void launch_edge_solution(int64_t ne, const int64_t *edge_src, const double2 *Y, const double2 *V, double2 *x,
-                          cudaStream_t stream) {
+void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream) {
+  launch_subsolve(p, kModeIter, p.L32 != nullptr, stream);
+  launch_cocg_update(p, stream);
+}
+
+void launch_edge_solution(const DevProblem &p, int64_t ne, const int64_t *edge_src, const double2 *Y,
+                          const double2 *V, double2 *x, cudaStream_t stream) {
   if (ne <= 0) return;
-  edge_solution_kernel<<<blocks_for(ne, 256), 256, 0, stream>>>(ne, edge_src, Y, V, x);
+  edge_solution_kernel<<<blocks_for(ne, 256), 256, 0, stream>>>(ne, edge_src, Y, V, x, p.row0, p.n_interior, p.slot0,
+                                                                 p.n_slots);
+}
+
+void launch_shard_gather(const DevProblem &p, const double2 *pcloc, double2 *xq, double2 *xpc, bool status_check,
+                         cudaStream_t stream) {
+  shard_gather_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p, pcloc, xq, xpc, status_check ? 1 : 0);
 }
 
 void launch_profile_reset(CocgScalars *sc, cudaStream_t stream) { profile_reset_kernel<<<1, 1, 0, stream>>>(sc); }

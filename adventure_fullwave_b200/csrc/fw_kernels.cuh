@@ -32,9 +32,9 @@ struct CocgScalars {
 
 // Per-problem device pointers used by the iteration kernels.
 struct DevProblem {
-  int32_t nsub;
+  int32_t nsub;                  // subdomains this context solves (all, or a shard's range)
   int32_t nfree;                 // interface DOFs
-  const int32_t *sub_order;      // warps take subdomains in this order
+  const int32_t *sub_order;      // warps take subdomains in this order (nsub entries)
   const int64_t *int_off;        // nsub+1
   const int64_t *if_off;         // nsub+1
   // interior envelope (compressed)
@@ -85,8 +85,12 @@ struct DevProblem {
   const int2 *blk_tab;           // per subdomain nblk+1 x (first row, first envelope element)
   int32_t max_blocks;            // most blocks of one subdomain
   int32_t stage_cap;             // envelope elements per staging buffer
-  int64_t n_interior;            // interior rows of all subdomains
-  int64_t n_slots;               // interface slots of all subdomains
+  int64_t row0, n_interior;      // interior rows of the subdomains this context solves
+  int64_t slot0, n_slots;        // interface slots of the subdomains this context solves
+  // sharded solve: this shard's partial interface sums go to the exchange
+  // buffer (summed over ranks by the caller) and the COCG reads them back
+  const double2 *xq;             // summed Q, or null: gather from this context's slots
+  const double2 *xpc;            // summed PC diagonal (first step), or null
   const int64_t *cpl_rowptr;     // n_interior+1 into cpl_val
   const int32_t *cpl_gcol;       // interface DOF (index into P) of each coupling entry
   const int64_t *ifr_rowptr;     // n_slots+1 into ifr_val
@@ -126,8 +130,12 @@ int configure_subsolve_staged(size_t smem, bool fp32);
 int subsolve_launches(const DevProblem &p, bool fp32);
 void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream);
 void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream);
-void launch_edge_solution(int64_t ne, const int64_t *edge_src, const double2 *Y, const double2 *V, double2 *x,
-                          cudaStream_t stream);
+// the COCG part of an iteration (after the subdomain solves): Q, alpha, updates, beta, p
+void launch_cocg_update(const DevProblem &p, cudaStream_t stream);
+void launch_edge_solution(const DevProblem &p, int64_t ne, const int64_t *edge_src, const double2 *Y,
+                          const double2 *V, double2 *x, cudaStream_t stream);
+void launch_shard_gather(const DevProblem &p, const double2 *pcloc, double2 *xq, double2 *xpc, bool status_check,
+                         cudaStream_t stream);
 void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream);
 void launch_adjoint_gradient(int32_t n_design, const int32_t *design_tets, const int32_t *tet_vertices,
                              const int32_t *tet_edges, const double *crd, double omega, const double2 *x,

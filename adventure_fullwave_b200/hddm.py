@@ -126,7 +126,8 @@ class HddmSolver:
 
     def __init__(self, model, hddm_eps: float = 1e-3, hddm_max_loop: int = 4000, precision: str = "fp64",
                  ir_max_steps: int = 1, ir_tol: float = 0.0, graph_iterations: int = 16, device: int = 0,
-                 solve_kernel: str = "auto", stage_cap: int = 0, ir_relax: float = 0.0):
+                 solve_kernel: str = "auto", stage_cap: int = 0, ir_relax: float = 0.0,
+                 shard: Optional[Tuple[int, int]] = None):
         lib = _lib.load()
         self._lib = lib
         self.model = model
@@ -153,7 +154,8 @@ class HddmSolver:
         self.precision = precision
         kern = SOLVE_KERNELS[solve_kernel]
         opts = _lib.FwOptions(self.hddm_eps, self.hddm_max_loop, prec, int(ir_max_steps), float(ir_tol),
-                              int(graph_iterations), int(device), kern, int(stage_cap), float(ir_relax))
+                              int(graph_iterations), int(device), kern, int(stage_cap), float(ir_relax),
+                              int(shard[0]) if shard else 0, int(shard[1]) if shard else 0)
         handle = ctypes.c_void_p()
         rc = lib.fwgpu_create(ctypes.byref(mesh), ctypes.byref(mt), ctypes.byref(opts), ctypes.byref(handle))
         if rc != 0 and handle.value:
@@ -262,6 +264,27 @@ class HddmSolver:
         _lib.check(self._lib.fwgpu_profile_iteration(self._h, int(reps), ctypes.byref(prof)))
         return dict(subsolve_ms=prof.subsolve_ms, interface_ms=prof.interface_ms, iteration_ms=prof.iteration_ms,
                     reps=prof.reps)
+
+    # -- sharded solve (one context per rank) --------------------------------
+    def shard_set_exchange(self, device_ptr: int) -> None:
+        """Device buffer of 4*total_free doubles for the partial sums."""
+        _lib.check(self._lib.fwgpu_shard_set_exchange(self._h, ctypes.c_void_p(int(device_ptr))))
+
+    def shard_first(self) -> None:
+        _lib.check(self._lib.fwgpu_shard_first(self._h))
+
+    def shard_first_finish(self) -> int:
+        st = ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_shard_first_finish(self._h, ctypes.byref(st)))
+        return st.value
+
+    def shard_iterate(self) -> None:
+        _lib.check(self._lib.fwgpu_shard_iterate(self._h))
+
+    def shard_iterate_finish(self) -> int:
+        st = ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_shard_iterate_finish(self._h, ctypes.byref(st)))
+        return st.value
 
     # -- results -----------------------------------------------------------
     def edge_solution(self) -> np.ndarray:

@@ -18,9 +18,10 @@ refinement to the same tolerance: time, iterations and relative L2 distance
 to the FP64 solution) and ``adjoint`` (the C4 design-region model: one
 forward solve and the backward call on its factors).
 
-Under torchrun (N > 1) every rank solves its own copy of the model (replicas;
-the multi-GPU interface exchange is not in this run), and rank 0 prints the
-line.
+Under torchrun (N > 1) the model is sharded: every rank solves a contiguous
+range of the subdomains and the ranks sum the partial interface vector with
+one NCCL all-reduce per iteration (``adventure_fullwave_b200.shard``); rank 0
+prints the line (``--replicas``: independent copies instead).
 """
 from __future__ import annotations
 
@@ -218,13 +219,19 @@ def run_reference(args):
 def run_ours(args):
     rank, world, local = env_rank()
     dist = None
-    if world > 1:
+    if world > 1 or args.sharded:
         import torch
         import torch.distributed as dist_mod
 
         torch.cuda.set_device(local)
-        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        if not dist_mod.is_initialized():
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29531")
+            dist_mod.init_process_group("nccl", rank=rank, world_size=world,
+                                        timeout=__import__("datetime").timedelta(seconds=600))
         dist = dist_mod
+        if args.sharded or not args.replicas:
+            return run_sharded_bench(args, rank, world, local, dist)
     from adventure_fullwave_b200 import hddm
 
     model = make_model(args.config)
@@ -386,6 +393,74 @@ def run_ours(args):
     return 0
 
 
+def run_sharded_bench(args, rank, world, local, dist):
+    """N > 1: one model sharded over the ranks (contiguous subdomain ranges),
+    the partial interface vector summed over NCCL every iteration.  Total
+    work is fixed as N grows (strong scaling).  Time per solve: CUDA events on
+    each rank around the driver, max over ranks."""
+    import torch
+
+    from adventure_fullwave_b200 import shard
+
+    model = make_model(args.config)
+    lo, hi = shard.shard_ranges(model, world)[rank]
+    opts = dict(hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
+                ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
+                solve_kernel=args.solve_kernel, stage_cap=args.stage_cap)
+    exch = shard.torch_exchange()
+    backend = shard.GpuShard(model, (lo, hi), device=local, **opts)
+    for _ in range(args.warmup):
+        shard.run_sharded(backend, exch, 0)
+    clocks = ClockSampler(local)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    its = []
+    for _ in range(args.steps):
+        x, it = shard.run_sharded(backend, exch, 0)
+        its.append(it)
+    ev1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t = torch.tensor([ev0.elapsed_time(ev1) / 1e3 / args.steps], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    value = float(t.item())
+    backend.close()
+    # end to end: shard setup from host arrays, solve, the summed solution on the host
+    dist.barrier()
+    t0 = time.perf_counter()
+    x, _ = shard.sharded_solve(model, 0, rank=rank, world=world, device=local, **opts)
+    e2e = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(e2e, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    h2d = sum(a.nbytes for a in (model.vertex_crd, model.tets, model.tet_edges, model.flag, model.pec_edge,
+                                 model.sub_of_tet, model.mat_flag, model.mat_eps, model.mat_sigma))
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+        "dtype": "c128" if args.precision == "fp64" else "c64 factor, c128 refinement and COCG",
+        "data": "synthetic (seeded generator; no dataset)",
+        "config": {"workload": WORKLOADS.get(args.config, args.config), "precision": args.precision,
+                   "hddm_eps": args.eps, "n_subdomains": model.nsub,
+                   "l2": "inputs larger than L2",
+                   "parallelism": f"{world} shards (contiguous subdomain ranges), NCCL all-reduce of the "
+                                  f"interface vector per iteration"},
+        "iterations": int(np.mean(its)),
+        "e2e": {"value": float(e2e.item()), "unit": "s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(model.n_edges * 16)},
+        "roofline": None, "cpu_baseline": None, "clocks": clk,
+        "gpu_launches": None,
+        "solution_check": {"finite": bool(np.all(np.isfinite(x)))},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_ncu_case(args):
     """A short run for ncu captures: setup, the first solve and
     ``--ncu-iters`` interface iterations, launched one by one."""
@@ -419,6 +494,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP32+IR comparison solve")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the C4 adjoint sample of a C2 run")
     ap.add_argument("--adjoint-steps", type=int, default=1)
+    ap.add_argument("--replicas", action="store_true", help="N > 1: independent replicas instead of shards")
+    ap.add_argument("--sharded", action="store_true", help="the sharded driver even at N = 1 (one shard)")
     ap.add_argument("--graph-iters", type=int, default=32)
     ap.add_argument("--solve-kernel", default="auto", choices=["auto", "warp", "cta", "global"])
     ap.add_argument("--stage-cap", type=int, default=0, help="staging buffer elements (0: timed choice)")

@@ -100,6 +100,8 @@ typedef struct {
   double ir_relax;       /* FP32_IR: interface iterations refine only while the COCG relative
                             residual is above ir_relax (0 = always); the first and last
                             subdomain solves always refine */
+  int32_t shard_begin;   /* sharded solve: this context solves subdomains [shard_begin, shard_end) */
+  int32_t shard_end;     /* (0, 0 = every subdomain); drive it with the fwgpu_shard_* calls */
 } fwgpu_options;
 
 /* Batched subdomain-solve kernels.  AUTO times one launch of each candidate
@@ -249,6 +251,35 @@ typedef struct {
  * fwgpu_hddm_resolve afterwards.  No reference counterpart (the reference
  * times whole phases with gettimeofday, lib/std/timefunc.c:17-111). */
 int fwgpu_profile_iteration(fwgpu_context *ctx, int32_t reps, fwgpu_kernel_profile *out);
+
+/* -- sharded solve over several GPUs (one context per rank) ---------------- */
+
+/* A context created with shard_begin < shard_end solves the subdomains of
+ * that range only: the reference's "part" (lib/hddm/hddm_solver_ph.h:112-329,
+ * one part per rank).  The interface vectors stay global; every iteration the
+ * ranks sum their partial interface vector Q, and the first step also the
+ * preconditioner diagonal, through a caller-owned device buffer (an NCCL
+ * all-reduce in place); every rank then runs the same COCG update on the same
+ * sums.  Order per solve:
+ *   fwgpu_make_tmp_aij; fwgpu_shard_first; [sum the buffer over ranks];
+ *   fwgpu_shard_first_finish; then until *status != 0:
+ *   fwgpu_shard_iterate; [sum Q over ranks]; fwgpu_shard_iterate_finish;
+ *   fwgpu_solve_dom_last; fwgpu_get_edge_solution gives this shard's edges
+ *   (zero elsewhere): their sum over ranks is the solution.
+ * The whole-solve calls (fwgpu_hddm_solve, fwgpu_iteration_s*) refuse a
+ * sharded context. */
+
+/* d_exchange: 4*total_free doubles on the context's device: the complex
+ * partial Q (2*total_free doubles), then the complex partial diagonal. */
+int fwgpu_shard_set_exchange(fwgpu_context *ctx, double *d_exchange);
+/* solve_dom_1st on this shard; partial Q and diagonal into the buffer */
+int fwgpu_shard_first(fwgpu_context *ctx);
+/* ITERATION_S_1ST from the summed buffer */
+int fwgpu_shard_first_finish(fwgpu_context *ctx, int32_t *status);
+/* the subdomain solves of one iteration; partial Q into the buffer */
+int fwgpu_shard_iterate(fwgpu_context *ctx);
+/* the COCG update of ITERATION_S from the summed Q; *status as fwgpu_iteration_s */
+int fwgpu_shard_iterate_finish(fwgpu_context *ctx, int32_t *status);
 
 /* -- batched skyline substitution without device allocation -------------- */
 
