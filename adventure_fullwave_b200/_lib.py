@@ -25,6 +25,7 @@ NOALLOC_MAX_ROWS = 262144
 
 PREC_FP64 = 0
 PREC_FP32_IR = 1
+MAX_RHS = 16
 
 c_i32 = ctypes.c_int32
 c_i64 = ctypes.c_int64
@@ -104,6 +105,8 @@ SIGNATURES = {
     "fwgpu_profile_iteration": [ctypes.c_void_p, c_i32, P(FwKernelProfile)],
     "fwgpu_adjoint_gradient": [ctypes.c_void_p, c_i32, P(c_i32), c_i32, P(c_i32), P(c_dbl), P(c_dbl), P(c_dbl),
                                P(FwResult)],
+    "fwgpu_hddm_solve_multi": [ctypes.c_void_p, c_i32, P(FwSource), P(FwResult)],
+    "fwgpu_get_edge_solution_multi": [ctypes.c_void_p, c_i32, P(c_dbl)],
     "fwgpu_shard_set_exchange": [ctypes.c_void_p, ctypes.c_void_p],
     "fwgpu_shard_first": [ctypes.c_void_p],
     "fwgpu_shard_first_finish": [ctypes.c_void_p, P(c_i32)],

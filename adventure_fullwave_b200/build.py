@@ -18,6 +18,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = [
     ("fw_element.cu", ["-fmad=false"]),
     ("fw_kernels.cu", []),
+    ("fw_multi.cu", []),
     ("fw_capi.cu", []),
     ("fw_noalloc.cu", []),
     ("fw_build.cpp", []),

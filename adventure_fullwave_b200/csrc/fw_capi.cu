@@ -88,6 +88,11 @@ struct fwgpu_context {
   bool warp_ok = false;            // the staged warp-per-subdomain kernel fits in shared memory
   bool sharded = false;            // solves a range of the subdomains (fwgpu_shard_* calls)
   double2 *d_exchange = nullptr;   // caller's buffer: partial Q, then partial PC diagonal
+  // batched sources (fwgpu_hddm_solve_multi)
+  fw::MultiProblem mp{};
+  fw::MultiScalars *h_ms = nullptr;
+  cudaGraphExec_t multi_graph = nullptr;
+  int multi_n = 0;                 // sources of the last batched solve (0: none)
   int32_t *d_blk_off = nullptr;    // staged solve block table (current staging capacity)
   int2 *d_blk_tab = nullptr;
   std::vector<int> stage_caps;     // staging capacities that fit in shared memory
@@ -557,9 +562,11 @@ int fwgpu_partition_maps(const fwgpu_partition *part, int32_t s, int32_t *nel, i
 int fwgpu_destroy(fwgpu_context *c) {
   if (!c) return FWGPU_OK;
   if (c->graph) cudaGraphExecDestroy(c->graph);
+  if (c->multi_graph) cudaGraphExecDestroy(c->multi_graph);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (void *p : c->allocs) cudaFree(p);
   if (c->h_sc) cudaFreeHost(c->h_sc);
+  if (c->h_ms) cudaFreeHost(c->h_ms);
   for (auto &ev : c->ev)
     if (ev) cudaEventDestroy(ev);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -873,6 +880,148 @@ int fwgpu_iteration_s(fwgpu_context *c, int32_t *status) {
   c->launches += iteration_launches(c);
   FW_CUDA(cudaGetLastError());
   FW_TRY(read_status(c, status));
+  return FWGPU_OK;
+}
+
+// Buffers of the batched-source solve, allocated on first use.
+static int multi_setup(fwgpu_context *c) {
+  if (c->mp.ms) return FWGPU_OK;
+  const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
+  const fw::DevProblem &dp = c->dp;
+  const int64_t R = fw::kMaxRhs;
+  const int64_t nI = c->p.sub_int_off[c->m.nsub], nG = c->p.sub_if_off[c->m.nsub];
+  const int64_t nf = std::max<int64_t>(1, dp.nfree);
+  fw::MultiProblem &m = c->mp;
+  double2 *d = nullptr;
+  FW_TRY(c->alloc(&d, nI * R));
+  m.fI = d;
+  FW_TRY(c->alloc(&d, nG * R));
+  m.fG = d;
+  FW_TRY(c->alloc(&m.Y, nI * R));
+  FW_TRY(c->alloc(&m.V, nG * R));
+  FW_TRY(c->alloc(&m.qloc, nG * R));
+  FW_CUDA(cudaMemsetAsync(m.qloc, 0, nG * R * sizeof(double2), c->stream));
+  if (fp32) {
+    FW_TRY(c->alloc(&m.B, nI * R));
+    FW_TRY(c->alloc(&m.Rres, nI * R));
+    float2 *z = nullptr;
+    FW_TRY(c->alloc(&z, nI * R));
+    m.Zs = z;
+  } else {
+    double2 *z = nullptr;
+    FW_TRY(c->alloc(&z, nI * R));
+    m.Zs = z;
+  }
+  FW_TRY(c->alloc(&m.P, nf * R));
+  FW_TRY(c->alloc(&m.Q, nf * R));
+  FW_TRY(c->alloc(&m.R, nf * R));
+  FW_TRY(c->alloc(&m.Z, nf * R));
+  FW_TRY(c->alloc(&m.U, nf * R));
+  FW_TRY(c->alloc(&m.PC, nf));
+  FW_TRY(c->alloc(&m.part, (size_t)8 * dp.n_part_blocks * R));
+  FW_TRY(c->alloc(&m.ms, 1));
+  FW_CUDA(cudaMallocHost(&c->h_ms, sizeof(fw::MultiScalars)));
+  return FWGPU_OK;
+}
+
+static int read_multi_status(fwgpu_context *c) {
+  FW_CUDA(cudaMemcpyAsync(c->h_ms, c->mp.ms, sizeof(fw::MultiScalars), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->h_ms->err != 0) return set_error(FWGPU_ERR_CUDA, "subdomain solve gave up waiting for a TMA copy");
+  return FWGPU_OK;
+}
+
+int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *srcs, fwgpu_result *res) {
+  if (!c || !srcs || !res) return set_error(FWGPU_ERR_ARG, "null argument");
+  if (n_src < 1 || n_src > fw::kMaxRhs) return set_error(FWGPU_ERR_ARG, "n_src outside 1..FWGPU_MAX_RHS");
+  if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
+  if (c->opts.hddm_max_loop == 0) return set_error(FWGPU_ERR_ARG, "hddm_max_loop is 0");
+  const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
+  c->launches = 0;
+  c->multi_n = 0;
+  FW_TRY(fwgpu_make_tmp_aij(c, &srcs[0]));
+  FW_TRY(fwgpu_solve_dom_1st(c));
+  if (!c->warp_ok) return set_error(FWGPU_ERR_ARG, "batched sources need the staged solve kernel");
+  const size_t smem = fw::multi_smem_bytes(c->dp.max_interior, c->dp.max_blocks, c->dp.stage_cap, fp32);
+  if (fw::configure_multi(smem, fp32) != 0)
+    return set_error(FWGPU_ERR_ARG, "batched sources: subdomains too large for shared memory");
+  FW_TRY(multi_setup(c));
+  fw::MultiProblem &m = c->mp;
+  m.p = c->dp;
+  // right-hand sides: column k of [row][kMaxRhs] is source k (the others zero)
+  const int64_t R = fw::kMaxRhs;
+  const int64_t nI = c->p.sub_int_off[c->m.nsub], nG = c->p.sub_if_off[c->m.nsub];
+  FW_CUDA(cudaMemsetAsync((void *)m.fI, 0, nI * R * sizeof(double2), c->stream));
+  FW_CUDA(cudaMemsetAsync((void *)m.fG, 0, nG * R * sizeof(double2), c->stream));
+  for (int k = 0; k < n_src; k++) {
+    FW_TRY(build_rhs(c, &srcs[k]));
+    if (nI > 0)
+      FW_CUDA(cudaMemcpy2DAsync((double2 *)m.fI + k, R * sizeof(double2), c->d_fI, sizeof(double2), sizeof(double2),
+                                nI, cudaMemcpyDeviceToDevice, c->stream));
+    if (nG > 0)
+      FW_CUDA(cudaMemcpy2DAsync((double2 *)m.fG + k, R * sizeof(double2), c->d_fG, sizeof(double2), sizeof(double2),
+                                nG, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  FW_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  fw::launch_multi_subsolve(m, fw::kModeFirst, fp32, c->stream);
+  fw::launch_multi_set_status(m.ms, c->opts.hddm_eps, c->opts.hddm_max_loop, c->stream);
+  fw::launch_multi_first(m, c->d_pcloc, c->stream);
+  const int per_iter = fw::multi_iteration_launches(fp32, c->dp.ir_steps);
+  c->launches += per_iter - 3 + 2;
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaEventRecord(c->ev[1], c->stream));
+  if (!c->multi_graph) {
+    cudaGraph_t g;
+    FW_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < c->opts.graph_iterations; k++) fw::launch_multi_iteration(m, fp32, c->stream);
+    FW_CUDA(cudaStreamEndCapture(c->stream, &g));
+    FW_CUDA(cudaGraphInstantiate(&c->multi_graph, g, 0));
+    cudaGraphDestroy(g);
+  }
+  FW_TRY(read_multi_status(c));
+  while (c->h_ms->all_status == 0) {
+    FW_CUDA(cudaGraphLaunch(c->multi_graph, c->stream));
+    c->launches += (int64_t)per_iter * c->opts.graph_iterations;
+    FW_TRY(read_multi_status(c));
+  }
+  FW_CUDA(cudaEventRecord(c->ev[2], c->stream));
+  fw::launch_multi_subsolve(m, fw::kModeLast, fp32, c->stream);
+  c->launches += per_iter - 3;
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaEventRecord(c->ev[3], c->stream));
+  FW_TRY(read_multi_status(c));
+  float ms0 = 0.f, ms1 = 0.f, ms2 = 0.f;
+  cudaEventElapsedTime(&ms0, c->ev[0], c->ev[1]);
+  cudaEventElapsedTime(&ms1, c->ev[1], c->ev[2]);
+  cudaEventElapsedTime(&ms2, c->ev[2], c->ev[3]);
+  int all_conv = 1;
+  for (int k = 0; k < n_src; k++) {
+    const fw::CocgScalars &sc = c->h_ms->s[k];
+    res[k].iterations = sc.loop - 1;
+    res[k].converged = sc.converged;
+    res[k].initial_norm = sc.norm0;
+    res[k].final_resi = sc.resi;
+    res[k].final_resi_l2 = sc.resi_l2;
+    res[k].t_setup_ms = ms0;
+    res[k].t_iterate_ms = ms1;
+    res[k].t_last_ms = ms2;
+    res[k].kernel_launches = c->launches;
+    res[k].solve_kernel = fw::kSolveWarp + 1;
+    res[k].stage_cap = c->dp.stage_cap;
+    all_conv &= sc.converged;
+  }
+  c->multi_n = n_src;
+  return all_conv ? FWGPU_OK : set_error(FWGPU_ERR_NOT_CONVERGED, "hddm_max_loop reached before hddm_eps");
+}
+
+int fwgpu_get_edge_solution_multi(fwgpu_context *c, int32_t k, double *x) {
+  if (!c || !x) return set_error(FWGPU_ERR_ARG, "null argument");
+  if (k < 0 || k >= c->multi_n) return set_error(FWGPU_ERR_ARG, "no such source in the last batched solve");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  fw::launch_multi_edge_solution(c->mp, k, c->m.ne, c->d_edge_src, c->d_xedge, c->stream);
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaMemcpyAsync(x, c->d_xedge, c->m.ne * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
   return FWGPU_OK;
 }
 

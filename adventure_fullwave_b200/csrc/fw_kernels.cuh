@@ -107,6 +107,42 @@ enum SolveVariant { kSolveWarp = 0, kSolveCta = 1, kSolveGlobal = 2 };
 
 enum SolveMode { kModeFirst = 0, kModeIter = 1, kModeLast = 2 };
 
+// ---- batched right-hand sides ----------------------------------------------
+// Up to kMaxRhs sources share one set of factors: every vector is stored
+// right-hand-side minor ([row][kMaxRhs]), and each source runs its own COCG
+// (its own scalars and stopping) in lockstep with the others.
+constexpr int kMaxRhs = 16;
+
+struct MultiScalars {
+  CocgScalars s[kMaxRhs];
+  int32_t all_status;  // 0: some right-hand side iterates; 2: every one finished
+  int32_t err;         // non-zero: a subdomain solve gave up waiting for a copy
+  uint32_t ticket[4];
+};
+
+struct MultiProblem {
+  DevProblem p;                 // structure, factors, operators, row ranges
+  const double2 *fI, *fG;       // [n_interior][kMaxRhs], [n_slots][kMaxRhs]
+  double2 *Y;                   // [n_interior][kMaxRhs]: right-hand sides in, interior solutions out
+  double2 *B, *Rres;            // FP32 + refinement: right-hand side copy, residual
+  void *Zs;                     // [n_interior][kMaxRhs] z stash in the factor's precision
+  double2 *V, *qloc;            // [n_slots][kMaxRhs]
+  double2 *P, *Q, *R, *Z, *U;   // [nfree][kMaxRhs]
+  double2 *PC;                  // [nfree]
+  MultiScalars *ms;
+  double *part;                 // [fields][n_part_blocks][kMaxRhs]
+};
+
+size_t multi_smem_bytes(int max_interior, int max_blocks, int cap, bool fp32);
+int configure_multi(size_t smem, bool fp32);
+void launch_multi_subsolve(const MultiProblem &m, int mode, bool fp32, cudaStream_t stream);
+void launch_multi_set_status(MultiScalars *ms, double eps, int32_t max_loop, cudaStream_t stream);
+void launch_multi_first(const MultiProblem &m, const double2 *pcloc, cudaStream_t stream);
+void launch_multi_iteration(const MultiProblem &m, bool fp32, cudaStream_t stream);
+void launch_multi_edge_solution(const MultiProblem &m, int k, int64_t ne, const int64_t *edge_src, double2 *x,
+                                cudaStream_t stream);
+int multi_iteration_launches(bool fp32, int ir_steps);
+
 void launch_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
                              const double *el_eps, const double *el_sigma, double omega, double *out,
                              int32_t *status, cudaStream_t stream);
@@ -126,6 +162,9 @@ size_t subsolve_smem_bytes(int max_interior, int max_iface, bool fp32);
 int configure_subsolve(size_t smem, bool fp32);
 size_t subsolve_staged_smem_bytes(int max_interior, int max_blocks, int cap, bool fp32);
 int configure_subsolve_staged(size_t smem, bool fp32);
+// Raises (never lowers) the dynamic shared-memory limit of kernel `func` on
+// the current device; `slot` names the kernel (0..7).
+int raise_smem_limit(const void *func, int slot, size_t smem);
 // kernels one launch_subsolve call issues
 int subsolve_launches(const DevProblem &p, bool fp32);
 void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream);

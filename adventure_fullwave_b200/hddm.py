@@ -223,6 +223,25 @@ class HddmSolver:
         _lib.check(self._lib.fwgpu_hddm_solve(self._h, ctypes.byref(src), ctypes.byref(res)), allow=allow)
         return self._result(res)
 
+    def solve_multi(self, sources: Sequence, raise_not_converged: bool = False) -> list:
+        """Up to 16 sources solved together on one set of factors (one
+        assembly, one factorisation, the sources' COCGs in lockstep).
+        Returns one result per source; ``edge_solution_multi(k)`` gives
+        source k's solution."""
+        srcs = [self._source(s) for s in sources]
+        if not 1 <= len(srcs) <= _lib.MAX_RHS:
+            raise ValueError(f"1 to {_lib.MAX_RHS} sources")
+        arr = (_lib.FwSource * len(srcs))(*[s for s, _ in srcs])
+        res = (_lib.FwResult * len(srcs))()
+        allow = () if raise_not_converged else (_lib.ERR_NOT_CONVERGED,)
+        _lib.check(self._lib.fwgpu_hddm_solve_multi(self._h, len(srcs), arr, res), allow=allow)
+        return [self._result(r) for r in res]
+
+    def edge_solution_multi(self, k: int) -> np.ndarray:
+        x = np.zeros(2 * self.n_edges, dtype=np.float64)
+        _lib.check(self._lib.fwgpu_get_edge_solution_multi(self._h, int(k), _ptr(x, ctypes.c_double)))
+        return x[0::2] + 1j * x[1::2]
+
     def resolve(self, source, raise_not_converged: bool = False) -> HddmResult:
         src, keep = self._source(source)
         res = _lib.FwResult()

@@ -252,6 +252,22 @@ typedef struct {
  * times whole phases with gettimeofday, lib/std/timefunc.c:17-111). */
 int fwgpu_profile_iteration(fwgpu_context *ctx, int32_t reps, fwgpu_kernel_profile *out);
 
+/* -- several sources on one set of factors --------------------------------- */
+
+/* Right-hand sides one batched solve takes at most. */
+#define FWGPU_MAX_RHS 16
+
+/* Solves n_src (1..FWGPU_MAX_RHS) sources together: one assembly and one
+ * factorisation, then all sources' interface COCGs in lockstep on the same
+ * factors, each with its own scalars and stopping test.  results[k] is
+ * source k's (the times are the batch's).  The reference solves one source
+ * per hddm_solver_CS run (hddm_solver.h:25-183); this is n_src such runs
+ * sharing the factors.  Needs the staged solve kernel (not available when a
+ * subdomain is too large for its shared memory). */
+int fwgpu_hddm_solve_multi(fwgpu_context *ctx, int32_t n_src, const fwgpu_source *sources, fwgpu_result *results);
+/* Edge solution of source k of the last fwgpu_hddm_solve_multi (2*n_edges doubles). */
+int fwgpu_get_edge_solution_multi(fwgpu_context *ctx, int32_t k, double *x);
+
 /* -- sharded solve over several GPUs (one context per rank) ---------------- */
 
 /* A context created with shard_begin < shard_end solves the subdomains of
