@@ -59,6 +59,7 @@ class FwOptions(ctypes.Structure):
         ("hddm_eps", c_dbl), ("hddm_max_loop", c_i32), ("precision", c_i32), ("ir_max_steps", c_i32),
         ("ir_tol", c_dbl), ("graph_iterations", c_i32), ("device", c_i32), ("solve_kernel", c_i32),
         ("stage_cap", c_i32), ("ir_relax", c_dbl), ("shard_begin", c_i32), ("shard_end", c_i32),
+        ("stage_warps", c_i32), ("reserved", c_i32),
     ]
 
 
@@ -76,6 +77,7 @@ class FwResult(ctypes.Structure):
         ("iterations", c_i32), ("converged", c_i32), ("initial_norm", c_dbl), ("final_resi", c_dbl),
         ("final_resi_l2", c_dbl), ("t_setup_ms", c_dbl), ("t_iterate_ms", c_dbl), ("t_last_ms", c_dbl),
         ("kernel_launches", c_i64), ("solve_kernel", c_i32), ("stage_cap", c_i32),
+        ("stage_warps", c_i32), ("reserved", c_i32),
     ]
 
 

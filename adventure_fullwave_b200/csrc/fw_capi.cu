@@ -294,6 +294,10 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   c->opts = *opts;
   if (c->opts.graph_iterations <= 0) c->opts.graph_iterations = 16;
   if (c->opts.ir_max_steps <= 0) c->opts.ir_max_steps = 1;
+  if (c->opts.stage_warps < 0 || c->opts.stage_warps > 2) {
+    delete c;
+    return set_error(FWGPU_ERR_ARG, "stage_warps must be 0, 1 or 2");
+  }
   if (c->opts.solve_kernel < FWGPU_SOLVE_AUTO || c->opts.solve_kernel > FWGPU_SOLVE_GLOBAL) {
     delete c;
     return set_error(FWGPU_ERR_ARG, "unknown solve_kernel");
@@ -682,6 +686,7 @@ static int build_stage_blocks(fwgpu_context *c, int cap, int *max_blocks_out) {
   c->dp.blk_tab = c->d_blk_tab;
   c->dp.max_blocks = max_blocks;
   c->dp.stage_cap = cap;
+  if (c->dp.stage_warps < 1) c->dp.stage_warps = c->opts.stage_warps == 2 ? 2 : 1;
   if (max_blocks_out) *max_blocks_out = max_blocks;
   return FWGPU_OK;
 }
@@ -722,13 +727,15 @@ static int setup_stage(fwgpu_context *c) {
 static int tune_solve_kernel(fwgpu_context *c) {
   const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
   struct Cand {
-    int variant, cap;
+    int variant, cap, warps;
   };
   std::vector<Cand> cand;
   const bool any = c->opts.solve_kernel == FWGPU_SOLVE_AUTO;
   if ((any || c->opts.solve_kernel == FWGPU_SOLVE_WARP) && c->warp_ok)
-    for (int cap : c->stage_caps) cand.push_back({fw::kSolveWarp, cap});
-  if (any && c->dp.cta_smem > 0) cand.push_back({fw::kSolveCta, 0});
+    for (int cap : c->stage_caps)
+      for (int warps = 1; warps <= 2; warps++)
+        if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps) cand.push_back({fw::kSolveWarp, cap, warps});
+  if (any && c->dp.cta_smem > 0) cand.push_back({fw::kSolveCta, 0, 1});
   if (cand.empty()) {
     c->solve_tuned = true;
     return FWGPU_OK;
@@ -737,7 +744,8 @@ static int tune_solve_kernel(fwgpu_context *c) {
   Cand pick = cand[0];
   for (const Cand &k : cand) {
     c->dp.solve_variant = k.variant;
-    if (k.variant == fw::kSolveWarp) FW_TRY(build_stage_blocks(c, k.cap, nullptr));
+    c->dp.stage_warps = k.warps;
+    if (k.variant == fw::kSolveWarp && c->dp.stage_cap != k.cap) FW_TRY(build_stage_blocks(c, k.cap, nullptr));
     fw::launch_subsolve(c->dp, fw::kModeFirst, fp32, c->stream);
     FW_CUDA(cudaEventRecord(c->ev[4], c->stream));
     for (int r = 0; r < 3; r++) fw::launch_subsolve(c->dp, fw::kModeFirst, fp32, c->stream);
@@ -752,6 +760,7 @@ static int tune_solve_kernel(fwgpu_context *c) {
     }
   }
   c->dp.solve_variant = pick.variant;
+  c->dp.stage_warps = pick.warps;
   if (pick.variant == fw::kSolveWarp && c->dp.stage_cap != pick.cap) FW_TRY(build_stage_blocks(c, pick.cap, nullptr));
   c->solve_tuned = true;
   return FWGPU_OK;
@@ -1008,6 +1017,8 @@ int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *
     res[k].kernel_launches = c->launches;
     res[k].solve_kernel = fw::kSolveWarp + 1;
     res[k].stage_cap = c->dp.stage_cap;
+    res[k].stage_warps = c->dp.stage_warps;
+    res[k].reserved = 0;
     all_conv &= sc.converged;
   }
   c->multi_n = n_src;
@@ -1140,6 +1151,8 @@ static int fill_result(fwgpu_context *c, fwgpu_result *res) {
     res->kernel_launches = c->launches;
     res->solve_kernel = c->dp.solve_variant + 1;
     res->stage_cap = c->dp.solve_variant == fw::kSolveWarp ? c->dp.stage_cap : 0;
+    res->stage_warps = c->dp.solve_variant == fw::kSolveWarp ? c->dp.stage_warps : 0;
+    res->reserved = 0;
   }
   return sc.converged ? FWGPU_OK : set_error(FWGPU_ERR_NOT_CONVERGED, "hddm_max_loop reached before hddm_eps");
 }

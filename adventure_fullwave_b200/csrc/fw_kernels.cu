@@ -637,7 +637,7 @@ constexpr int kSB = 32;        // rows per block at most, one per lane
 constexpr int kSGroup = 8;     // rows whose partial sums are reduced together
 
 struct StageLayout {
-  size_t y, buf0, buf1, xb, meta, bar, blk, total;
+  size_t y, buf0, buf1, xb, rb, meta, bar, blk, total;
 };
 
 // Shared-memory slice of one subdomain warp of the staged solve.
@@ -653,6 +653,8 @@ __host__ __device__ inline StageLayout stage_layout(int max_interior, int max_bl
   o += a16((size_t)cap * es);
   l.xb = o;
   o += a16(kSB * es);
+  l.rb = o;
+  o += a16(2 * kSB * es);
   l.meta = o;
   o += kSB * 8;
   l.bar = o;
@@ -681,50 +683,52 @@ __device__ __forceinline__ T transpose_reduce8(const T (&a)[kSGroup], int lane) 
 
 template <typename T>
 __device__ void staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
-                               T *y, int2 *meta, T *zstash, int lane) {
+                               T *y, int2 *meta, T *zstash, T *rectb, int tid, int nw) {
+  const int lane = tid & 31, w = tid >> 5;
   int nlo, npr;
-  stage_issue(st, 0, lane);
+  stage_issue(st, 0, tid);
   stage_row_meta(lo_g, ptr_g, base, st.blk[0].x, st.blk[1].x, lane, nlo, npr);
   for (int b = 0; b < nblk; b++) {
     const int r0 = st.blk[b].x, nb = st.blk[b + 1].x - r0;
     const int my_lo = nlo, my_pr = npr;
-    meta[lane] = make_int2(nlo, npr);
+    if (w == 0) meta[lane] = make_int2(nlo, npr);
     if (b + 1 < nblk) {
-      stage_issue(st, b + 1, lane);
+      stage_issue(st, b + 1, tid);
       stage_row_meta(lo_g, ptr_g, base, st.blk[b + 1].x, st.blk[b + 2].x, lane, nlo, npr);
     }
     stage_wait(st, b);
-    __syncwarp();
+    __syncthreads();
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);  // S[e]: entry e of the envelope
-    // entries left of the block.  FP32: each lane walks its own row (two
-    // accumulators, 4 entries' loads in flight).  FP64: lanes across a row,
-    // 8 rows' loads issued together and one transpose-reduction per 8 rows
-    // (16-byte entries make the per-lane walk's bank conflicts too costly).
-    T rect = czero<T>();
+    // entries left of the block, split over the warps.  FP32: each lane walks
+    // its own row (a share of it per warp; two accumulators, 4 entries' loads
+    // in flight).  FP64: lanes across a row, 8 rows' loads issued together and
+    // one transpose-reduction per 8 rows, groups of 8 rows shared out over the
+    // warps (16-byte entries make the per-lane walk's bank conflicts too costly).
     if (sizeof(T) == 8) {
       const int my_len = lane < nb ? max(0, r0 - my_lo) : 0;
-      int longest = my_len;
+      const int kbeg = (my_len * w) / nw, cnt = (my_len * (w + 1)) / nw - kbeg;
+      int longest = cnt;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
-      const T *row = S + my_pr;
-      const T *yr = y + (lane < nb ? my_lo : 0);
+      const T *row = S + my_pr + kbeg;
+      const T *yr = y + (lane < nb ? my_lo : 0) + kbeg;
       T acc0 = czero<T>(), acc1 = czero<T>();
       for (int k = 0; k < longest; k += 4) {
-        T a[4], b[4];
+        T a[4], bv[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          const bool in = k + u < my_len;
+          const bool in = k + u < cnt;
           a[u] = in ? row[k + u] : czero<T>();
-          b[u] = in ? yr[k + u] : czero<T>();
+          bv[u] = in ? yr[k + u] : czero<T>();
         }
-        acc0 = cadd(acc0, cmul(a[0], b[0]));
-        acc1 = cadd(acc1, cmul(a[1], b[1]));
-        acc0 = cadd(acc0, cmul(a[2], b[2]));
-        acc1 = cadd(acc1, cmul(a[3], b[3]));
+        acc0 = cadd(acc0, cmul(a[0], bv[0]));
+        acc1 = cadd(acc1, cmul(a[1], bv[1]));
+        acc0 = cadd(acc0, cmul(a[2], bv[2]));
+        acc1 = cadd(acc1, cmul(a[3], bv[3]));
       }
-      rect = cadd(acc0, acc1);
+      rectb[w * 32 + lane] = cadd(acc0, acc1);
     } else {
-      for (int g = 0; g < nb; g += kSGroup) {
+      for (int g = w * kSGroup; g < nb; g += kSGroup * nw) {
         int2 mt[kSGroup];
         int len[kSGroup];
 #pragma unroll
@@ -754,79 +758,88 @@ __device__ void staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, cons
             for (int k = lane + 64; k < len[u]; k += 32) acc[u] = cadd(acc[u], cmul(S[mt[u].y + k], y[mt[u].x + k]));
         }
         const T sum = transpose_reduce8(acc, lane);
-        const T pick = shfl_idx(sum, 4 * (lane & 7));
-        if ((lane >> 3) == (g >> 3)) rect = pick;
+        if ((lane & 3) == 0) rectb[g + (lane >> 2)] = sum;  // lanes 4r.. hold row g + r
       }
     }
-    // the block's triangle: lane t holds row r0 + t; the operands of 4 steps
-    // are loaded ahead of their shuffles
-    T val = lane < nb ? csub(y[r0 + lane], rect) : czero<T>();
-    const T *mine = S + my_pr - my_lo;  // mine[col]: this lane's row at column col
-    for (int j0 = 0; j0 < nb - 1; j0 += 4) {
-      T op[4];
+    __syncthreads();
+    if (w == 0) {
+      T rect = rectb[lane];
+      if (sizeof(T) == 8)
+        for (int k = 1; k < nw; k++) rect = cadd(rect, rectb[k * 32 + lane]);
+      // the block's triangle: lane t holds row r0 + t; the operands of 4 steps
+      // are loaded ahead of their shuffles
+      T val = lane < nb ? csub(y[r0 + lane], rect) : czero<T>();
+      const T *mine = S + my_pr - my_lo;  // mine[col]: this lane's row at column col
+      for (int j0 = 0; j0 < nb - 1; j0 += 4) {
+        T op[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int j = j0 + u;
-        op[u] = (lane > j && r0 + j >= my_lo) ? mine[r0 + j] : czero<T>();
-      }
+        for (int u = 0; u < 4; u++) {
+          const int j = j0 + u;
+          op[u] = (lane > j && r0 + j >= my_lo) ? mine[r0 + j] : czero<T>();
+        }
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const T yj = shfl_idx(val, min(j0 + u, 31));
-        val = csub(val, cmul(op[u], yj));
+        for (int u = 0; u < 4; u++) {
+          const T yj = shfl_idx(val, min(j0 + u, 31));
+          val = csub(val, cmul(op[u], yj));
+        }
+      }
+      if (lane < nb) {
+        y[r0 + lane] = val;
+        zstash[r0 + lane] = cmul(val, mine[r0 + lane]);  // 1/d on the diagonal
       }
     }
-    if (lane < nb) {
-      y[r0 + lane] = val;
-      zstash[r0 + lane] = cmul(val, mine[r0 + lane]);  // 1/d on the diagonal
-    }
-    __syncwarp();
+    __syncthreads();
   }
 }
 
 template <typename T>
 __device__ void staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
-                                T *y, T *xb, int2 *meta, int lane) {
+                                T *y, T *xb, int2 *meta, int tid, int nw) {
+  const int lane = tid & 31, w = tid >> 5;
   int nlo, npr;
   stage_row_meta(lo_g, ptr_g, base, st.blk[nblk - 1].x, st.blk[nblk].x, lane, nlo, npr);
   for (int b = nblk - 1; b >= 0; b--) {
     const int r0 = st.blk[b].x, nb = st.blk[b + 1].x - r0;
     const int my_lo = nlo;
-    meta[lane] = make_int2(nlo, npr);
+    if (w == 0) meta[lane] = make_int2(nlo, npr);
     // the forward sweep left blocks nblk-1 and nblk-2 in the buffers
     if (b >= 1) {
-      if (b - 1 < nblk - 2) stage_issue(st, b - 1, lane);
+      if (b - 1 < nblk - 2) stage_issue(st, b - 1, tid);
       stage_row_meta(lo_g, ptr_g, base, st.blk[b - 1].x, st.blk[b].x, lane, nlo, npr);
     }
     stage_wait(st, b);
-    __syncwarp();
+    __syncthreads();
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);
-    // triangle, lanes over the block's columns; operands of 4 steps loaded ahead
-    T val = lane < nb ? y[r0 + lane] : czero<T>();
-    const int col = r0 + lane;
-    for (int i0 = nb - 1; i0 >= 1; i0 -= 4) {
-      T op[4];
+    if (w == 0) {
+      // triangle, lanes over the block's columns; operands of 4 steps loaded ahead
+      T val = lane < nb ? y[r0 + lane] : czero<T>();
+      const int col = r0 + lane;
+      for (int i0 = nb - 1; i0 >= 1; i0 -= 4) {
+        T op[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int i = i0 - u;
-        const int2 mt = meta[max(i, 0)];
-        op[u] = (i >= 1 && lane < i && col >= mt.x) ? S[mt.y + col - mt.x] : czero<T>();
-      }
+        for (int u = 0; u < 4; u++) {
+          const int i = i0 - u;
+          const int2 mt = meta[max(i, 0)];
+          op[u] = (i >= 1 && lane < i && col >= mt.x) ? S[mt.y + col - mt.x] : czero<T>();
+        }
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const T xi = shfl_idx(val, max(i0 - u, 0));
-        val = csub(val, cmul(op[u], xi));
+        for (int u = 0; u < 4; u++) {
+          const T xi = shfl_idx(val, max(i0 - u, 0));
+          val = csub(val, cmul(op[u], xi));
+        }
       }
-    }
-    if (lane < nb) {
-      y[r0 + lane] = val;
-      xb[lane] = val;
+      if (lane < nb) {
+        y[r0 + lane] = val;
+        xb[lane] = val;
+      }
     }
     int bmin = lane < nb ? my_lo : INT_MAX;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) bmin = min(bmin, __shfl_xor_sync(0xffffffffu, bmin, o));
-    __syncwarp();
-    // columns left of the block: y_c -= sum_t L[r0+t][c] x_t, 8 rows' loads in flight
-    for (int cb = bmin; cb < r0; cb += 32) {
+    __syncthreads();
+    // columns left of the block: y_c -= sum_t L[r0+t][c] x_t, 8 rows' loads in
+    // flight, 32-column chunks shared out over the warps
+    for (int cb = bmin + 32 * w; cb < r0; cb += 32 * nw) {
       const int c = cb + lane;
       const bool act = c < r0;
       T acc0 = czero<T>(), acc1 = czero<T>();
@@ -848,17 +861,18 @@ __device__ void staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
       }
       if (act) y[c] = csub(y[c], cadd(acc0, acc1));
     }
-    __syncwarp();
+    __syncthreads();
   }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(32) subsolve_staged_kernel(DevProblem p, int mode, const double2 *rhs, double2 *xout,
+__global__ void __launch_bounds__(64) subsolve_staged_kernel(DevProblem p, int mode, const double2 *rhs, double2 *xout,
                                                              T *zstash, int accumulate, StageLayout lay) {
   if (mode == kModeIter && p.sc->status != 0) return;
   if (accumulate && refine_skipped(p, mode)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x;
+  __shared__ double red[2][2];
+  const int tid = threadIdx.x, nt = blockDim.x, nw = nt >> 5;
   const int s = p.sub_order[blockIdx.x];
   const int64_t io = p.int_off[s];
   const int nI = (int)(p.int_off[s + 1] - io);
@@ -867,6 +881,7 @@ __global__ void __launch_bounds__(32) subsolve_staged_kernel(DevProblem p, int m
   if (nI == 0 || nblk <= 0) return;
   T *y = (T *)(smem_raw + lay.y);
   T *xb = (T *)(smem_raw + lay.xb);
+  T *rectb = (T *)(smem_raw + lay.rb);
   int2 *meta = (int2 *)(smem_raw + lay.meta);
   int2 *blk = (int2 *)(smem_raw + lay.blk);
   Stage<T> st;
@@ -878,15 +893,15 @@ __global__ void __launch_bounds__(32) subsolve_staged_kernel(DevProblem p, int m
   st.err = &p.sc->pad;
   const int64_t base = p.env_ptr[io];
   st.L = (sizeof(T) == 8 ? (const T *)(const void *)p.L32 : (const T *)(const void *)p.L64) + base;
-  for (int b = lane; b <= nblk; b += 32) blk[b] = p.blk_tab[b0 + b];
-  if (lane == 0) {
+  for (int b = tid; b <= nblk; b += nt) blk[b] = p.blk_tab[b0 + b];
+  if (tid == 0) {
     mbar_init(&st.bar[0], 1);
     mbar_init(&st.bar[1], 1);
     fence_mbar_init();
   }
   // right-hand side; a refinement step is skipped when its residual is already small
   double rn = 0.0, bn = 0.0;
-  for (int c = lane; c < nI; c += 32) {
+  for (int c = tid; c < nI; c += nt) {
     const double2 r = rhs[io + c];
     y[c] = from_d2<T>(r);
     if (accumulate) {
@@ -895,27 +910,36 @@ __global__ void __launch_bounds__(32) subsolve_staged_kernel(DevProblem p, int m
       bn = fmax(bn, fabs(bv.x) + fabs(bv.y));
     }
   }
+  __syncthreads();
   if (accumulate && p.ir_tol > 0.0) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       rn = fmax(rn, __shfl_xor_sync(0xffffffffu, rn, o));
       bn = fmax(bn, __shfl_xor_sync(0xffffffffu, bn, o));
     }
-    if (rn <= p.ir_tol * bn) return;
+    if ((tid & 31) == 0) {
+      red[tid >> 5][0] = rn;
+      red[tid >> 5][1] = bn;
+    }
+    __syncthreads();
+    for (int k = 0; k < nw; k++) {
+      rn = fmax(rn, red[k][0]);
+      bn = fmax(bn, red[k][1]);
+    }
+    if (rn <= p.ir_tol * bn) return;  // the same decision in every thread
   }
-  __syncwarp();
   const int32_t *lo_g = p.env_lo + io;
   const int64_t *ptr_g = p.env_ptr + io;
   T *z = zstash + io;
-  staged_forward<T>(st, nblk, lo_g, ptr_g, base, y, meta, z, lane);
-  for (int c = lane; c < nI; c += 32) y[c] = z[c];
-  __syncwarp();
-  staged_backward<T>(st, nblk, lo_g, ptr_g, base, y, xb, meta, lane);
+  staged_forward<T>(st, nblk, lo_g, ptr_g, base, y, meta, z, rectb, tid, nw);
+  for (int c = tid; c < nI; c += nt) y[c] = z[c];
+  __syncthreads();
+  staged_backward<T>(st, nblk, lo_g, ptr_g, base, y, xb, meta, tid, nw);
   // every copy was waited for above; after a timed-out wait, wait (bounded) again
-  // so that no copy into this warp's shared memory is left in flight
+  // so that no copy into this CTA's shared memory is left in flight
   stage_wait(st, 0);
   stage_wait(st, 1);
-  for (int c = lane; c < nI; c += 32) {
+  for (int c = tid; c < nI; c += nt) {
     double2 x = make_double2((double)y[c].x, (double)y[c].y);
     if (accumulate) x = cadd(xout[io + c], x);
     xout[io + c] = x;
@@ -1290,13 +1314,16 @@ void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stre
     double2 *rhs = fp32 ? p.B : p.Y;
     rhs_kernel<4><<<blocks_min1(p.n_interior * 4, 256), 256, 0, stream>>>(p, mode, rhs);
     if (fp32) {
-      subsolve_staged_kernel<float2><<<p.nsub, 32, lay.total, stream>>>(p, mode, p.B, p.Y, p.Y32, 0, lay);
+      subsolve_staged_kernel<float2><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.B, p.Y, p.Y32, 0,
+                                                                                       lay);
       for (int k = 0; k < p.ir_steps; k++) {
         ir_residual_kernel<4><<<blocks_min1(p.n_interior * 4, 256), 256, 0, stream>>>(p, mode);
-        subsolve_staged_kernel<float2><<<p.nsub, 32, lay.total, stream>>>(p, mode, p.Rres, p.Y, p.Y32, 1, lay);
+        subsolve_staged_kernel<float2><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.Rres, p.Y, p.Y32,
+                                                                                         1, lay);
       }
     } else {
-      subsolve_staged_kernel<double2><<<p.nsub, 32, lay.total, stream>>>(p, mode, p.Y, p.Y, p.Y, 0, lay);
+      subsolve_staged_kernel<double2><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.Y, p.Y, p.Y, 0,
+                                                                                          lay);
     }
     iface_product_kernel<4><<<blocks_min1(p.n_slots * 4, 256), 256, 0, stream>>>(p, mode);
     return;

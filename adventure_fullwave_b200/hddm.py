@@ -50,6 +50,7 @@ class HddmResult:
     kernel_launches: int = 0
     solve_kernel: str = ""
     stage_cap: int = 0
+    stage_warps: int = 0
 
 
 def _mesh_struct(model):
@@ -127,7 +128,7 @@ class HddmSolver:
     def __init__(self, model, hddm_eps: float = 1e-3, hddm_max_loop: int = 4000, precision: str = "fp64",
                  ir_max_steps: int = 1, ir_tol: float = 0.0, graph_iterations: int = 16, device: int = 0,
                  solve_kernel: str = "auto", stage_cap: int = 0, ir_relax: float = 0.0,
-                 shard: Optional[Tuple[int, int]] = None):
+                 shard: Optional[Tuple[int, int]] = None, stage_warps: int = 0):
         lib = _lib.load()
         self._lib = lib
         self.model = model
@@ -155,7 +156,7 @@ class HddmSolver:
         kern = SOLVE_KERNELS[solve_kernel]
         opts = _lib.FwOptions(self.hddm_eps, self.hddm_max_loop, prec, int(ir_max_steps), float(ir_tol),
                               int(graph_iterations), int(device), kern, int(stage_cap), float(ir_relax),
-                              int(shard[0]) if shard else 0, int(shard[1]) if shard else 0)
+                              int(shard[0]) if shard else 0, int(shard[1]) if shard else 0, int(stage_warps), 0)
         handle = ctypes.c_void_p()
         rc = lib.fwgpu_create(ctypes.byref(mesh), ctypes.byref(mt), ctypes.byref(opts), ctypes.byref(handle))
         if rc != 0 and handle.value:
@@ -254,7 +255,7 @@ class HddmSolver:
         return HddmResult(int(r.iterations), bool(r.converged), float(r.initial_norm), float(r.final_resi),
                           float(r.final_resi_l2), float(r.t_setup_ms), float(r.t_iterate_ms), float(r.t_last_ms),
                           int(r.kernel_launches), _KERNEL_NAMES.get(int(r.solve_kernel), ""),
-                          int(r.stage_cap))
+                          int(r.stage_cap), int(r.stage_warps))
 
     def adjoint_gradient(self, probe_edges=None, design_tets=None):
         """Backward of the last ``solve``: J = sum |x_p|^2 over ``probe_edges``

@@ -238,7 +238,7 @@ def run_ours(args):
     solver = hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
                              ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
                              graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
-                             stage_cap=args.stage_cap)
+                             stage_cap=args.stage_cap, stage_warps=args.stage_warps)
     for _ in range(args.warmup):
         solver.solve(0)
     clocks = ClockSampler(local)
@@ -271,7 +271,7 @@ def run_ours(args):
         with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision="fp32_ir",
                              ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
                              graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
-                             stage_cap=args.stage_cap) as s32:
+                             stage_cap=args.stage_cap, stage_warps=args.stage_warps) as s32:
             s32.solve(0)
             t32, it32 = [], []
             for _ in range(args.steps):
@@ -296,7 +296,7 @@ def run_ours(args):
         adj_solver = hddm.HddmSolver(adj_model, hddm_eps=args.eps, hddm_max_loop=args.max_loop,
                                      precision=args.precision, ir_max_steps=args.ir_steps, ir_tol=args.ir_tol,
                                      graph_iterations=args.graph_iters, device=local,
-                                     solve_kernel=args.solve_kernel, stage_cap=args.stage_cap)
+                                     solve_kernel=args.solve_kernel, stage_cap=args.stage_cap, stage_warps=args.stage_warps)
         adj_solver.solve(0)
     if adj_solver is not None:
         # the backward: one adjoint HDDM solve on the forward factors plus the gradient kernel
@@ -344,7 +344,7 @@ def run_ours(args):
         with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
                              ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
                              graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
-                             stage_cap=args.stage_cap) as s2:
+                             stage_cap=args.stage_cap, stage_warps=args.stage_warps) as s2:
             s2.solve(0)
             xe = s2.edge_solution()
         e2e_times.append(time.perf_counter() - t0)
@@ -406,7 +406,7 @@ def run_sharded_bench(args, rank, world, local, dist):
     lo, hi = shard.shard_ranges(model, world)[rank]
     opts = dict(hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
                 ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
-                solve_kernel=args.solve_kernel, stage_cap=args.stage_cap)
+                solve_kernel=args.solve_kernel, stage_cap=args.stage_cap, stage_warps=args.stage_warps)
     exch = shard.torch_exchange()
     backend = shard.GpuShard(model, (lo, hi), device=local, **opts)
     for _ in range(args.warmup):
@@ -469,7 +469,7 @@ def run_ncu_case(args):
     model = make_model(args.config)
     with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
                          ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, solve_kernel=args.solve_kernel,
-                         stage_cap=args.stage_cap) as s:
+                         stage_cap=args.stage_cap, stage_warps=args.stage_warps) as s:
         s.make_tmp_aij(0)
         s.solve_dom_1st()
         s.iteration_s_1st()
@@ -499,6 +499,7 @@ def main():
     ap.add_argument("--graph-iters", type=int, default=32)
     ap.add_argument("--solve-kernel", default="auto", choices=["auto", "warp", "cta", "global"])
     ap.add_argument("--stage-cap", type=int, default=0, help="staging buffer elements (0: timed choice)")
+    ap.add_argument("--stage-warps", type=int, default=0, help="warps per subdomain, 1 or 2 (0: timed choice)")
     ap.add_argument("--prof-reps", type=int, default=50)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-iters", type=int, default=10)

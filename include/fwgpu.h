@@ -102,6 +102,8 @@ typedef struct {
                             subdomain solves always refine */
   int32_t shard_begin;   /* sharded solve: this context solves subdomains [shard_begin, shard_end) */
   int32_t shard_end;     /* (0, 0 = every subdomain); drive it with the fwgpu_shard_* calls */
+  int32_t stage_warps;   /* WARP kernel: warps sharing a subdomain's sweeps, 1 or 2 (0 = timed choice) */
+  int32_t reserved;
 } fwgpu_options;
 
 /* Batched subdomain-solve kernels.  AUTO times one launch of each candidate
@@ -145,6 +147,8 @@ typedef struct {
   int64_t kernel_launches; /* kernels this library launched for the call */
   int32_t solve_kernel;    /* FWGPU_SOLVE_* used for the subdomain solves */
   int32_t stage_cap;       /* WARP kernel: envelope elements per staging buffer, else 0 */
+  int32_t stage_warps;     /* WARP kernel: warps per subdomain, else 0 */
+  int32_t reserved;
 } fwgpu_result;
 
 /* -- lifecycle ----------------------------------------------------------- */
