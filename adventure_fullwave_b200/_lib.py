@@ -107,6 +107,8 @@ SIGNATURES = {
     "fwgpu_profile_iteration": [ctypes.c_void_p, c_i32, P(FwKernelProfile)],
     "fwgpu_adjoint_gradient": [ctypes.c_void_p, c_i32, P(c_i32), c_i32, P(c_i32), P(c_dbl), P(c_dbl), P(c_dbl),
                                P(FwResult)],
+    "fwgpu_post_em_E": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    "fwgpu_profile_post": [ctypes.c_void_p, c_i32, P(c_dbl)],
     "fwgpu_hddm_solve_multi": [ctypes.c_void_p, c_i32, P(FwSource), P(FwResult)],
     "fwgpu_get_edge_solution_multi": [ctypes.c_void_p, c_i32, P(c_dbl)],
     "fwgpu_shard_set_exchange": [ctypes.c_void_p, ctypes.c_void_p],

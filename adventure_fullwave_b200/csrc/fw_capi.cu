@@ -98,6 +98,11 @@ struct fwgpu_context {
   std::vector<int> stage_caps;     // staging capacities that fit in shared memory
   int64_t launches = 0;            // kernels launched since the last reset
   int64_t *d_env_dst = nullptr;    // lower entry -> envelope position (-1: outside)
+  // post step (fwgpu_post_em_E)
+  bool xedge_ok = false;           // d_xedge holds a whole edge solution
+  uint8_t *d_el_has_nu = nullptr;
+  double2 *d_post = nullptr;       // 3 x 3 complex per element (B, E, Je), when the caller's buffers are on the host
+  double2 *d_post_x = nullptr;     // the caller's edge solution, when it is on the host
 
   template <typename T>
   int alloc(T **ptr, size_t count) {
@@ -151,6 +156,7 @@ std::vector<int64_t> offsets_from_rel(const std::vector<int32_t> &rel_ptr, const
 int resolve_material(fw::Model &m, const fwgpu_mesh *mesh, const fwgpu_material *mt) {
   m.el_eps.assign(m.nt, 0.0);
   m.el_sigma.assign(m.nt, 0.0);
+  m.el_has_nu.assign(m.nt, 0);
   // the reference searches the tables linearly and takes the first match
   // (lib/fem/make_elem_em.c:98-109); absent flags leave eps = sigma = 0
   for (int t = 0; t < m.nt; t++) {
@@ -158,6 +164,7 @@ int resolve_material(fw::Model &m, const fwgpu_mesh *mesh, const fwgpu_material 
     for (int i = 0; i < mt->n_eps; i++)
       if (mt->eps_flag[i] == f) {
         m.el_eps[t] = mt->eps[i];
+        m.el_has_nu[t] = 1;
         break;
       }
     for (int i = 0; i < mt->n_sigma; i++)
@@ -1031,6 +1038,7 @@ int fwgpu_get_edge_solution_multi(fwgpu_context *c, int32_t k, double *x) {
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_multi_edge_solution(c->mp, k, c->m.ne, c->d_edge_src, c->d_xedge, c->stream);
   FW_CUDA(cudaGetLastError());
+  c->xedge_ok = true;
   FW_CUDA(cudaMemcpyAsync(x, c->d_xedge, c->m.ne * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
   FW_CUDA(cudaStreamSynchronize(c->stream));
   return FWGPU_OK;
@@ -1108,6 +1116,7 @@ int fwgpu_solve_dom_last(fwgpu_context *c) {
   FW_CUDA(cudaGetLastError());
   FW_CUDA(cudaStreamSynchronize(c->stream));
   c->stage = 4;
+  c->xedge_ok = !c->sharded;
   return FWGPU_OK;
 }
 
@@ -1252,6 +1261,111 @@ int fwgpu_adjoint_gradient(fwgpu_context *c, int32_t n_probe, const int32_t *pro
     if (grad_sigma) grad_sigma[k] = gh[std::max(1, n_design) + k];
   }
   return rc;
+}
+
+namespace {
+
+// Device memory of the context's device, 16-byte aligned: a kernel may read
+// or write it in place.  Host memory (pageable or pinned) is not.
+bool usable_on_device(const fwgpu_context *c, const void *p) {
+  if (!p || ((uintptr_t)p & 15u)) return false;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == c->opts.device;
+}
+
+int post_static_data(fwgpu_context *c) {
+  if (!c->d_te) FW_TRY(c->upload(&c->d_te, c->m.te));
+  if (!c->d_el_has_nu) FW_TRY(c->upload(&c->d_el_has_nu, c->m.el_has_nu));
+  return FWGPU_OK;
+}
+
+}  // namespace
+
+int fwgpu_post_em_E(fwgpu_context *c, const double *x, double *el_B, double *el_E, double *el_Je) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (!x && !c->xedge_ok)
+    return set_error(FWGPU_ERR_STATE, c->sharded ? "a sharded context needs the whole edge solution x"
+                                                 : "no edge solution yet: solve first or pass x");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  const int64_t nt = c->m.nt, ne = c->m.ne;
+  FW_TRY(post_static_data(c));
+  const double2 *dx = c->d_xedge;
+  if (x) {
+    if (usable_on_device(c, x)) {
+      dx = reinterpret_cast<const double2 *>(x);
+    } else {
+      if (!c->d_post_x) FW_TRY(c->alloc(&c->d_post_x, ne));
+      FW_CUDA(cudaMemcpyAsync(c->d_post_x, x, ne * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+      dx = c->d_post_x;
+    }
+  }
+  double *user[3] = {el_B, el_E, el_Je};
+  double2 *out[3] = {nullptr, nullptr, nullptr};
+  bool staged[3] = {false, false, false};
+  for (int k = 0; k < 3; k++) {
+    if (!user[k]) continue;
+    if (usable_on_device(c, user[k])) {
+      out[k] = reinterpret_cast<double2 *>(user[k]);
+    } else {
+      if (!c->d_post) FW_TRY(c->alloc(&c->d_post, 9 * (size_t)std::max<int64_t>(1, nt)));
+      out[k] = c->d_post + 3 * nt * k;
+      staged[k] = true;
+    }
+  }
+  FW_CUDA(cudaMemsetAsync(c->d_mesh_status + 2, 0, sizeof(int32_t), c->stream));
+  fw::launch_post_em_E(nt, c->d_tv, c->d_te, c->d_crd, c->d_el_has_nu, c->d_el_sigma, c->m.omega, dx, out[0], out[1],
+                       out[2], c->d_mesh_status + 2, c->stream);
+  c->launches += 1;
+  FW_CUDA(cudaGetLastError());
+  for (int k = 0; k < 3; k++)
+    if (staged[k])
+      FW_CUDA(cudaMemcpyAsync(user[k], out[k], 3 * nt * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  int32_t bad = 0;
+  FW_CUDA(cudaMemcpyAsync(&bad, c->d_mesh_status + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  if (bad) return set_error(FWGPU_ERR_MESH, "degenerate element in the post step");
+  return FWGPU_OK;
+}
+
+int fwgpu_profile_post(fwgpu_context *c, int32_t reps, double *kernel_ms) {
+  if (!c || !kernel_ms || reps <= 0) return set_error(FWGPU_ERR_ARG, "bad argument");
+  if (!c->xedge_ok) return set_error(FWGPU_ERR_STATE, "profile needs an edge solution");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  const int64_t nt = c->m.nt;
+  FW_TRY(post_static_data(c));
+  if (!c->d_post) FW_TRY(c->alloc(&c->d_post, 9 * (size_t)std::max<int64_t>(1, nt)));
+  const size_t flush_bytes = (size_t)256 << 20;
+  uint8_t *flush = nullptr;
+  FW_TRY(c->alloc(&flush, flush_bytes));
+  cudaEvent_t a, b;
+  FW_CUDA(cudaEventCreate(&a));
+  FW_CUDA(cudaEventCreate(&b));
+  double total = 0.0;
+  int rc = FWGPU_OK;
+  for (int r = 0; r <= reps && rc == FWGPU_OK; r++) {  // r = 0 is a warm-up
+    cudaError_t e = cudaMemsetAsync(flush, r & 0xff, flush_bytes, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(a, c->stream);
+    fw::launch_post_em_E(nt, c->d_tv, c->d_te, c->d_crd, c->d_el_has_nu, c->d_el_sigma, c->m.omega, c->d_xedge,
+                         c->d_post, c->d_post + 3 * nt, c->d_post + 6 * nt, nullptr, c->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(b, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    if (e != cudaSuccess) rc = set_error(FWGPU_ERR_CUDA, std::string("profile_post: ") + cudaGetErrorString(e));
+    if (r > 0) total += ms;
+  }
+  c->launches += reps + 1;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  c->release(flush);
+  if (rc) return rc;
+  *kernel_ms = total / reps;
+  return FWGPU_OK;
 }
 
 int fwgpu_profile_iteration(fwgpu_context *c, int32_t reps, fwgpu_kernel_profile *out) {

@@ -246,6 +246,144 @@ __global__ void adjoint_gradient_kernel(int32_t n_design, const int32_t *__restr
   g_sigma[k] = 2.0 * si;
 }
 
+// Element results of the post step, HDDM_post_em_E
+// (main/fullwave/fullwave.c:639-763), one thread per element: the element's
+// six edge values are first scaled by nu/omega (nu = 7.957747e+05 when the
+// element's flag is in the Permittivity list, else 0; fullwave.c:672-677,722)
+// and the scaled values feed all three results:
+//   B  = (2/D)     sum_i i xe_i (X_i, Y_i, Z_i)        (rot E times nu/omega)
+//   E  = (2/D)     sum_i xe_i (Fx_i, Fy_i, Fz_i)       (tetNedelec_Fxyz at the centroid)
+//   Je = (sigma/D) sum_i xe_i (Fx_i, Fy_i, Fz_i)
+// Same operation order as the reference (contraction off), so the results
+// are bit-identical to its own on the same edge values.  Outputs are 3
+// complex per element in global element order; a null output is skipped.
+// status[0] (if given) is raised to 1 for a degenerate element, where the
+// reference stops (tetrahedral.c:257-258).
+__global__ void __launch_bounds__(128) post_em_E_kernel(int64_t nt, const int32_t *__restrict__ tet_vertices,
+                                                        const int32_t *__restrict__ tet_edges,
+                                                        const double *__restrict__ crd,
+                                                        const uint8_t *__restrict__ el_has_nu,
+                                                        const double *__restrict__ el_sigma, double omega,
+                                                        const double2 *__restrict__ xedge, double2 *__restrict__ B,
+                                                        double2 *__restrict__ E, double2 *__restrict__ Je,
+                                                        int32_t *__restrict__ status) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const int4 tv = __ldg(reinterpret_cast<const int4 *>(tet_vertices) + t);
+  const int2 *te2 = reinterpret_cast<const int2 *>(tet_edges + 6 * t);
+  const int2 e01 = __ldg(te2), e23 = __ldg(te2 + 1), e45 = __ldg(te2 + 2);
+  // edge-table order 01,02,03,12,13,23 from file slots 0,1,2,3,5,4
+  const int eid[6] = {e01.x, e01.y, e23.x, e23.y, e45.y, e45.x};
+  double2 xe[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) xe[i] = __ldg(xedge + eid[i]);
+  const int vid[4] = {tv.x, tv.y, tv.z, tv.w};
+  double vx[4], vy[4], vz[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    vx[i] = __ldg(crd + 3 * (int64_t)vid[i]);
+    vy[i] = __ldg(crd + 3 * (int64_t)vid[i] + 1);
+    vz[i] = __ldg(crd + 3 * (int64_t)vid[i] + 2);
+  }
+  const double nu = el_has_nu[t] ? nu_const() : 0.0;
+  const double sigma = el_sigma[t];
+  // one pass over the six edges: the element routine's per-edge quantities
+  // (tet_SideLength, tetNedelec_Direction, _mk, _XYZ, _km_mk, _Fxyz) are
+  // formed and used at once, each sum still taken in edge order
+  constexpr int kN[6][4] = {{0, 1, 2, 3}, {0, 2, 3, 1}, {0, 3, 1, 2}, {1, 2, 0, 3}, {1, 3, 2, 0}, {2, 3, 0, 1}};
+  const double *x = vx, *y = vy, *z = vz;
+  double D = -x[0] * y[1] * z[2];
+  D = D + x[0] * y[1] * z[3];
+  D = D + x[0] * y[2] * z[1];
+  D = D - x[0] * y[2] * z[3];
+  D = D - x[0] * y[3] * z[1];
+  D = D + x[0] * y[3] * z[2];
+  D = D + x[1] * y[0] * z[2];
+  D = D - x[1] * y[0] * z[3];
+  D = D - x[1] * y[2] * z[0];
+  D = D + x[1] * y[2] * z[3];
+  D = D + x[1] * y[3] * z[0];
+  D = D - x[1] * y[3] * z[2];
+  D = D - x[2] * y[0] * z[1];
+  D = D + x[2] * y[0] * z[3];
+  D = D + x[2] * y[1] * z[0];
+  D = D - x[2] * y[1] * z[3];
+  D = D - x[2] * y[3] * z[0];
+  D = D + x[2] * y[3] * z[1];
+  D = D + x[3] * y[0] * z[1];
+  D = D - x[3] * y[0] * z[2];
+  D = D - x[3] * y[1] * z[0];
+  D = D + x[3] * y[1] * z[2];
+  D = D + x[3] * y[2] * z[0];
+  D = D - x[3] * y[2] * z[1];
+  bool bad = !(D > 0.0);
+  double g[3];
+  g[0] = (x[0] + x[1] + x[2] + x[3]) * 0.25;
+  g[1] = (y[0] + y[1] + y[2] + y[3]) * 0.25;
+  g[2] = (z[0] + z[1] + z[2] + z[3]) * 0.25;
+  const double s = nu / omega;
+  double2 rb[3], et[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    rb[k] = make_double2(0.0, 0.0);
+    et[k] = make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    const int a = kN[i][0], b = kN[i][1], p = kN[i][2], q = kN[i][3];
+    const double dx = x[a] - x[b], dy = y[a] - y[b], dz = z[a] - z[b];
+    const double l = sqrt(dx * dx + dy * dy + dz * dz);
+    // orientation from the first non-zero of (x_b - x_a, y_b - y_a, z_b - z_a)
+    int si = 0;
+    const double px = x[b] - x[a], py = y[b] - y[a], pz = z[b] - z[a];
+    if (px > 0.0) si = 1;
+    else if (px < 0.0) si = -1;
+    else if (py > 0.0) si = 1;
+    else if (py < 0.0) si = -1;
+    else if (pz > 0.0) si = 1;
+    else if (pz < 0.0) si = -1;
+    else bad = true;
+    const double xi = x[q] - x[p], yi = y[q] - y[p], zi = z[q] - z[p];
+    const double d = l * (double)si;
+    const double X = d * xi, Y = d * yi, Z = d * zi;
+    const double xy = x[p] * y[q] - x[q] * y[p];
+    const double yz = y[p] * z[q] - y[q] * z[p];
+    const double zx = z[p] * x[q] - z[q] * x[p];
+    const double fx = d * (yz - zi * g[1] + yi * g[2]);
+    const double fy = d * (zx - xi * g[2] + zi * g[0]);
+    const double fz = d * (xy - yi * g[0] + xi * g[1]);
+    const double2 v = make_double2(xe[i].x * s, xe[i].y * s);
+    // v * i, evaluated as the full complex product with (0, 1)
+    const double ccr = v.x * 0.0 - v.y * 1.0;
+    const double cci = v.y * 0.0 + v.x * 1.0;
+    rb[0] = make_double2(rb[0].x + ccr * X, rb[0].y + cci * X);
+    rb[1] = make_double2(rb[1].x + ccr * Y, rb[1].y + cci * Y);
+    rb[2] = make_double2(rb[2].x + ccr * Z, rb[2].y + cci * Z);
+    et[0] = make_double2(et[0].x + v.x * fx, et[0].y + v.y * fx);
+    et[1] = make_double2(et[1].x + v.x * fy, et[1].y + v.y * fy);
+    et[2] = make_double2(et[2].x + v.x * fz, et[2].y + v.y * fz);
+  }
+  if (bad && status) atomicMax(status, 1);
+  const double dd = 2.0 / D;
+  const double ds = sigma / D;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (B) B[3 * t + k] = make_double2(rb[k].x * dd, rb[k].y * dd);
+    if (E) E[3 * t + k] = make_double2(et[k].x * dd, et[k].y * dd);
+    if (Je) Je[3 * t + k] = make_double2(et[k].x * ds, et[k].y * ds);
+  }
+}
+
+void launch_post_em_E(int64_t nt, const int32_t *tet_vertices, const int32_t *tet_edges, const double *crd,
+                      const uint8_t *el_has_nu, const double *el_sigma, double omega, const double2 *x, double2 *B,
+                      double2 *E, double2 *Je, int32_t *status, cudaStream_t stream) {
+  if (nt <= 0) return;
+  const int threads = 128;
+  const int64_t blocks = (nt + threads - 1) / threads;
+  post_em_E_kernel<<<(unsigned)blocks, threads, 0, stream>>>(nt, tet_vertices, tet_edges, crd, el_has_nu, el_sigma,
+                                                              omega, x, B, E, Je, status);
+}
+
 void launch_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
                              const double *el_eps, const double *el_sigma, double omega, double *out,
                              int32_t *status, cudaStream_t stream) {

@@ -47,6 +47,9 @@ struct Model {
   // material resolved per element (the reference's first-match linear search
   // over the flag tables, lib/fem/make_elem_em.c:98-109)
   std::vector<double> el_eps, el_sigma;
+  // 1 when the element's flag is in the Permittivity list: the post step
+  // uses nu = 7.957747e+05 there and 0 elsewhere (main/fullwave/fullwave.c:672-677)
+  std::vector<uint8_t> el_has_nu;
   double omega = 0.0;
 };
 

@@ -177,6 +177,9 @@ void launch_edge_solution(const DevProblem &p, int64_t ne, const int64_t *edge_s
 void launch_shard_gather(const DevProblem &p, const double2 *pcloc, double2 *xq, double2 *xpc, bool status_check,
                          cudaStream_t stream);
 void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream);
+void launch_post_em_E(int64_t nt, const int32_t *tet_vertices, const int32_t *tet_edges, const double *crd,
+                      const uint8_t *el_has_nu, const double *el_sigma, double omega, const double2 *x, double2 *B,
+                      double2 *E, double2 *Je, int32_t *status, cudaStream_t stream);
 void launch_adjoint_gradient(int32_t n_design, const int32_t *design_tets, const int32_t *tet_vertices,
                              const int32_t *tet_edges, const double *crd, double omega, const double2 *x,
                              const double2 *lam, double *g_eps, double *g_sigma, cudaStream_t stream);

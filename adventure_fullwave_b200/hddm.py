@@ -164,6 +164,7 @@ class HddmSolver:
         _lib.check(rc)
         self._h = handle
         self.n_edges = int(model.n_edges)
+        self.n_tets = int(model.n_tets)
 
     # -- lifecycle --------------------------------------------------------
     def close(self) -> None:
@@ -284,6 +285,40 @@ class HddmSolver:
         _lib.check(self._lib.fwgpu_profile_iteration(self._h, int(reps), ctypes.byref(prof)))
         return dict(subsolve_ms=prof.subsolve_ms, interface_ms=prof.interface_ms, iteration_ms=prof.iteration_ms,
                     reps=prof.reps)
+
+    # -- post step -----------------------------------------------------------
+    def post_em_E(self, x=None):
+        """Element results of the post step (``HDDM_post_em_E``,
+        ``main/fullwave/fullwave.c:639-763``) from the edge solution ``x``
+        (complex, n_edges; None: the last solution): (B, E, Je), each
+        (n_tets, 3) complex in global element order, where B is
+        i (nu/omega) rot E, E the field at the centroid and Je = sigma E, all
+        three from the edge values scaled by nu/omega as the reference does."""
+        xin = None
+        if x is not None:
+            x = np.asarray(x)
+            if x.shape != (self.n_edges,):
+                raise ValueError("x needs one value per edge")
+            xin = np.ascontiguousarray(np.stack([x.real, x.imag], 1).ravel(), np.float64)
+        outs = [np.zeros(6 * self.n_tets, np.float64) for _ in range(3)]
+        _lib.check(self._lib.fwgpu_post_em_E(self._h, None if xin is None else _ptr(xin, ctypes.c_double),
+                                             *[_ptr(o, ctypes.c_double) for o in outs]))
+        return tuple((o[0::2] + 1j * o[1::2]).reshape(self.n_tets, 3) for o in outs)
+
+    def post_em_E_into(self, x_ptr: int, b_ptr: int, e_ptr: int, je_ptr: int) -> None:
+        """``post_em_E`` on raw pointers (host memory or 16-byte aligned
+        device memory of the solver's device; 0 for the last solution or to
+        skip a result), e.g. ``tensor.data_ptr()`` of CUDA tensors, so that
+        the results stay on the device."""
+        ptrs = [ctypes.c_void_p(int(p)) if p else None for p in (x_ptr, b_ptr, e_ptr, je_ptr)]
+        _lib.check(self._lib.fwgpu_post_em_E(self._h, *ptrs))
+
+    def profile_post(self, reps: int = 20) -> float:
+        """Average device time [ms] of one post-step kernel launch, L2
+        evicted before each launch."""
+        ms = ctypes.c_double()
+        _lib.check(self._lib.fwgpu_profile_post(self._h, int(reps), ctypes.byref(ms)))
+        return ms.value
 
     # -- sharded solve (one context per rank) --------------------------------
     def shard_set_exchange(self, device_ptr: int) -> None:

@@ -140,6 +140,14 @@ def algorithmic_bytes(sz: dict, precision: str, ir_steps: int) -> int:
     return int(b)
 
 
+def post_algorithmic_bytes(model) -> int:
+    """Bytes the post step must move at least: per element its 4 vertex ids,
+    6 edge ids, Permittivity mark and conductivity (16 + 24 + 1 + 8 B) and
+    its three results (3 x 3 complex, 144 B); each vertex coordinate triple
+    (24 B) and each edge value (16 B) once."""
+    return int(model.n_tets * (16 + 24 + 1 + 8 + 144) + model.n_vertices * 24 + model.n_edges * 16)
+
+
 def ncu_traffic(kernel: str, config: str, precision: str):
     """DRAM bytes of one subdomain-solve phase from the committed ncu summary
     (profiles/subsolve_<kernel>_<config>_<precision>.md), when one covers
@@ -333,6 +341,19 @@ def run_ours(args):
                 "kernel_ms": prof["subsolve_ms"], "interface_kernels_ms": prof["interface_ms"],
                 "iteration_ms_graph": prof["iteration_ms"]}
 
+    # the post step (element B, E, Je from the converged edge values)
+    post = None
+    if not args.no_post:
+        post_ms = solver.profile_post(reps=args.prof_reps)
+        pb = post_algorithmic_bytes(model)
+        B, E, Je = solver.post_em_E()
+        post_gbs = pb / (post_ms * 1e-3) / 1e9
+        post = {"kernel": "post_em_E_kernel (HDDM_post_em_E over every element)", "kernel_ms": post_ms,
+                "algorithmic_bytes": pb, "achieved": post_gbs, "peak": peak, "unit": "GB/s", "frac": post_gbs / peak,
+                "peak_source": f"{peak_kind} hbm_gbs", "n_tets": model.n_tets,
+                "finite": bool(np.isfinite(B).all() and np.isfinite(E).all() and np.isfinite(Je).all()),
+                "timing": "device events per launch, L2 evicted before each"}
+
     # end to end through the public API from host arrays
     solver.close()
     e2e_times = []
@@ -389,6 +410,8 @@ def run_ours(args):
         line["mixed_precision"] = mixed
     if adjoint is not None:
         line["adjoint"] = adjoint
+    if post is not None:
+        line["post"] = post
     print(json.dumps(line))
     return 0
 
@@ -493,6 +516,7 @@ def main():
     ap.add_argument("--ir-relax", type=float, default=0.0, help="refine only while the COCG residual is above this")
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP32+IR comparison solve")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the C4 adjoint sample of a C2 run")
+    ap.add_argument("--no-post", action="store_true", help="skip the post-step measurement")
     ap.add_argument("--adjoint-steps", type=int, default=1)
     ap.add_argument("--replicas", action="store_true", help="N > 1: independent replicas instead of shards")
     ap.add_argument("--sharded", action="store_true", help="the sharded driver even at N = 1 (one shard)")

@@ -240,6 +240,30 @@ int fwgpu_adjoint_gradient(fwgpu_context *ctx, int32_t n_probe, const int32_t *p
                            const int32_t *design_tets, double *J, double *grad_eps, double *grad_sigma,
                            fwgpu_result *adjoint_result);
 
+/* -- post step ------------------------------------------------------------ */
+/* post_sp: HDDM_post_sp_em_E (main/fullwave/fullwave.c:518-529), that is
+ * HDDM_post_dom_em_E (:607-634) over every subdomain with HDDM_post_em_E
+ * (:639-763) per element.  From each element's six edge values it gives the
+ * reference's element results (ResultValue, lib/std/types.h:330-345):
+ *   el_B  = (2/D) sum_i i xe_i (X_i, Y_i, Z_i)     i (nu/omega) rot E
+ *   el_E  = (2/D) sum_i xe_i (Fx_i, Fy_i, Fz_i)    E at the centroid
+ *   el_Je = (sigma/D) sum_i xe_i (Fx_i, Fy_i, Fz_i)
+ * where xe_i is the edge value times nu/omega, nu = 7.957747e+05 for an
+ * element whose flag is in the Permittivity list and 0 otherwise, sigma the
+ * element's Conductor entry (0 if none): the reference scales the edge values
+ * before all three sums.  3 complex (6 doubles) per element, in global
+ * element order (the reference keeps them per subdomain in local element
+ * order; each element lies in one subdomain).
+ *   x      2*n_edges doubles, or NULL for the context's last edge solution
+ *          (fwgpu_solve_dom_last, fwgpu_hddm_solve, fwgpu_hddm_resolve, or the
+ *          source last read with fwgpu_get_edge_solution_multi); a sharded
+ *          context holds only its own edges and needs x.
+ *   el_B, el_E, el_Je   6*n_tets doubles each; NULL skips that result.
+ * Every pointer may be host memory or 16-byte aligned device memory of the
+ * context's device; device results are written in place, without a copy.
+ * Returns FWGPU_ERR_MESH for a degenerate element (the reference stops in
+ * tetNedelec_Direction, lib/fem/tetrahedral.c:257-258). */
+int fwgpu_post_em_E(fwgpu_context *ctx, const double *x, double *el_B, double *el_E, double *el_Je);
 /* -- measurement ---------------------------------------------------------- */
 
 typedef struct {
@@ -255,6 +279,11 @@ typedef struct {
  * fwgpu_hddm_resolve afterwards.  No reference counterpart (the reference
  * times whole phases with gettimeofday, lib/std/timefunc.c:17-111). */
 int fwgpu_profile_iteration(fwgpu_context *ctx, int32_t reps, fwgpu_kernel_profile *out);
+/* Average device time of one post-step kernel launch (fwgpu_post_em_E, all
+ * three results into device memory) over reps launches on the context's last
+ * edge solution, each timed alone with CUDA events after a write of 256 MiB
+ * that evicts the L2.  No reference counterpart. */
+int fwgpu_profile_post(fwgpu_context *ctx, int32_t reps, double *kernel_ms);
 
 /* -- several sources on one set of factors --------------------------------- */
 

@@ -15,6 +15,8 @@
  *   mxv                  __MYMT_AIJ_MAIJMXV_TMP_AIJ__ aij_matrix_func.h:624-658
  *   orc_hddm             s-mode HDDM loop + COCG     lib/hddm/hddm_solver.h:59-183,461-693,
  *                        hddm_solver_s.h:7-424, hddm_solver_sp.h, hddm_pc.h:52-137
+ *   orc_post_em_E        HDDM_post_em_E              main/fullwave/fullwave.c:639-763
+ *                        (tetrahedral.c:27-61,80-86,225-340)
  *
  * Inputs are the per-subdomain arrays make_PartMesh_FW leaves in DomMesh
  * (local nop after the slot-8/9 swap, local vertex coordinates, the
@@ -677,4 +679,126 @@ int orc_hddm(int nsub, const int *nel, const int *nop, const int *nap, const dou
   free(vec);
   free(vbc);
   return rc < 0 ? rc : loop - 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* element results of the post step                                         */
+
+/* HDDM_post_em_E (main/fullwave/fullwave.c:639-763) for every element t of
+ * the mesh: from the six edge values x of the element (global edge ids in
+ * file order 01,02,03,12,23,13, taken in the edge-table order
+ * 01,02,03,12,13,23 that the slot-8/9 swap of make_MESH.c:556-585 gives the
+ * reference's nop), with
+ *   nu    = 7.957747e+05 if the element's flag is in the Permittivity list
+ *           (mtrl.flag_i), else 0          (fullwave.c:672-677)
+ *   sigma = the first Conductor-list match, else 0   (:678-683)
+ * and each edge value first scaled by nu/omega (:722, which the E and Je sums
+ * below then also use):
+ *   B  = (2/D)     sum_i i * xe_i * (X_i, Y_i, Z_i)      (:719-730)
+ *   E  = (2/D)     sum_i xe_i * (Fx_i, Fy_i, Fz_i)       (:735-749)
+ *   Je = (sigma/D) sum_i xe_i * (Fx_i, Fy_i, Fz_i)       (:752-762)
+ * B, E, Je receive 3 complex (6 doubles) per element.  Returns the number of
+ * elements with a zero-length edge (the reference stops there in
+ * tetNedelec_Direction, tetrahedral.c:257-258). */
+int orc_post_em_E(int nt, const int *tet_vertices, const int *tet_edges, const double *crd, const int *flag,
+                  int nflag, const int *flag_i, int nR, const int *R_i, const double *R_sigma, double omega,
+                  const double *xedge, double *B, double *E, double *Je) {
+  static const int file_slot[6] = {0, 1, 2, 3, 5, 4};
+  int bad = 0;
+  for (int t = 0; t < nt; t++) {
+    const int flg = flag[t];
+    double nu = 0.0, sigma = 0.0;
+    for (int i = 0; i < nflag; i++)
+      if (flg == flag_i[i]) {
+        nu = 7.957747e+05;
+        break;
+      }
+    for (int i = 0; i < nR; i++)
+      if (flg == R_i[i]) {
+        sigma = R_sigma[i];
+        break;
+      }
+    cpx xe[6];
+    for (int i = 0; i < 6; i++) {
+      const int e = tet_edges[6 * t + file_slot[i]];
+      xe[i] = (cpx){xedge[2 * e], xedge[2 * e + 1]};
+    }
+    double x[4], y[4], z[4];
+    for (int i = 0; i < 4; i++) {
+      const int v = tet_vertices[4 * t + i];
+      x[i] = crd[3 * v];
+      y[i] = crd[3 * v + 1];
+      z[i] = crd[3 * v + 2];
+    }
+    /* tet_Volume6 */
+    double D = -x[0] * y[1] * z[2] + x[0] * y[1] * z[3] + x[0] * y[2] * z[1] - x[0] * y[2] * z[3] -
+               x[0] * y[3] * z[1] + x[0] * y[3] * z[2] + x[1] * y[0] * z[2] - x[1] * y[0] * z[3] -
+               x[1] * y[2] * z[0] + x[1] * y[2] * z[3] + x[1] * y[3] * z[0] - x[1] * y[3] * z[2] -
+               x[2] * y[0] * z[1] + x[2] * y[0] * z[3] + x[2] * y[1] * z[0] - x[2] * y[1] * z[3] -
+               x[2] * y[3] * z[0] + x[2] * y[3] * z[1] + x[3] * y[0] * z[1] - x[3] * y[0] * z[2] -
+               x[3] * y[1] * z[0] + x[3] * y[1] * z[2] + x[3] * y[2] * z[0] - x[3] * y[2] * z[1];
+    double X[6], Y[6], Z[6], Fx[6], Fy[6], Fz[6], g[3];
+    g[0] = (x[0] + x[1] + x[2] + x[3]) * 0.25; /* tet_Center */
+    g[1] = (y[0] + y[1] + y[2] + y[3]) * 0.25;
+    g[2] = (z[0] + z[1] + z[2] + z[3]) * 0.25;
+    for (int i = 0; i < 6; i++) {
+      const int a = TET_N[i][0], b = TET_N[i][1], p = TET_N[i][2], q = TET_N[i][3];
+      const double l = sqrt(pow(x[a] - x[b], 2) + pow(y[a] - y[b], 2) + pow(z[a] - z[b], 2));
+      int si; /* tetNedelec_Direction */
+      double pp = x[b] - x[a];
+      if (pp > 0.0)
+        si = 1;
+      else if (pp < 0.0)
+        si = -1;
+      else {
+        pp = y[b] - y[a];
+        if (pp > 0.0)
+          si = 1;
+        else if (pp < 0.0)
+          si = -1;
+        else {
+          pp = z[b] - z[a];
+          si = pp > 0.0 ? 1 : (pp < 0.0 ? -1 : 0);
+        }
+      }
+      if (si == 0) bad++;
+      const double xi = x[q] - x[p], yi = y[q] - y[p], zi = z[q] - z[p]; /* tetNedelec_mk */
+      const double d = l * (double)si;
+      X[i] = d * xi; /* tetNedelec_XYZ */
+      Y[i] = d * yi;
+      Z[i] = d * zi;
+      const double xy = x[p] * y[q] - x[q] * y[p]; /* tetNedelec_km_mk */
+      const double yz = y[p] * z[q] - y[q] * z[p];
+      const double zx = z[p] * x[q] - z[q] * x[p];
+      Fx[i] = d * (yz - zi * g[1] + yi * g[2]); /* tetNedelec_Fxyz */
+      Fy[i] = d * (zx - xi * g[2] + zi * g[0]);
+      Fz[i] = d * (xy - yi * g[0] + xi * g[1]);
+    }
+    const cpx ci = {0.0, 1.0};
+    cpx rb[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    for (int i = 0; i < 6; i++) {
+      xe[i] = (cpx){xe[i].re * (nu / omega), xe[i].im * (nu / omega)};
+      const cpx cc = c_mul(xe[i], ci);
+      rb[0] = c_add(rb[0], (cpx){cc.re * X[i], cc.im * X[i]});
+      rb[1] = c_add(rb[1], (cpx){cc.re * Y[i], cc.im * Y[i]});
+      rb[2] = c_add(rb[2], (cpx){cc.re * Z[i], cc.im * Z[i]});
+    }
+    cpx et[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    for (int i = 0; i < 6; i++) {
+      et[0] = c_add(et[0], (cpx){xe[i].re * Fx[i], xe[i].im * Fx[i]});
+      et[1] = c_add(et[1], (cpx){xe[i].re * Fy[i], xe[i].im * Fy[i]});
+      et[2] = c_add(et[2], (cpx){xe[i].re * Fz[i], xe[i].im * Fz[i]});
+    }
+    /* the Je sums repeat the E sums on the same xe and F (:752-762) */
+    const double dd = 2.0 / D, ds = sigma / D;
+    for (int k = 0; k < 3; k++) {
+      B[6 * t + 2 * k] = rb[k].re * dd;
+      B[6 * t + 2 * k + 1] = rb[k].im * dd;
+      E[6 * t + 2 * k] = et[k].re * dd;
+      E[6 * t + 2 * k + 1] = et[k].im * dd;
+      Je[6 * t + 2 * k] = et[k].re * ds;
+      Je[6 * t + 2 * k + 1] = et[k].im * ds;
+    }
+  }
+  return bad;
 }

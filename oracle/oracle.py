@@ -273,3 +273,32 @@ def objective(model, probe_edges, hddm_eps: float = 1e-12, hddm_max_loop: int = 
     part = partition(model, 0)
     x, _, _, _ = hddm(model, part, hddm_eps, hddm_max_loop)
     return float(np.sum(np.abs(x[np.asarray(probe_edges)]) ** 2))
+
+
+def post_em_E(model, xedge, drop_first: bool = False):
+    """Element results of the post step (``HDDM_post_em_E``,
+    ``main/fullwave/fullwave.c:639-763``) from the edge solution ``xedge``:
+    returns (B, E, Je), each (n_tets, 3) complex, in global element order.
+    The Permittivity and Conductor lists are the model's material table;
+    ``drop_first`` leaves out the first entry of each, so that the elements of
+    that flag take the nu = 0 and sigma = 0 branches."""
+    lib = load()
+    flags = np.ascontiguousarray(model.mat_flag, np.int32)
+    sig = np.ascontiguousarray(model.mat_sigma, np.float64)
+    k = 1 if drop_first and flags.shape[0] > 0 else 0
+    flags, sig = np.ascontiguousarray(flags[k:]), np.ascontiguousarray(sig[k:])
+    nt = model.n_tets
+    x = np.ascontiguousarray(np.stack([np.real(xedge), np.imag(xedge)], 1).ravel(), np.float64)
+    out = [np.zeros(6 * nt, np.float64) for _ in range(3)]
+    tv = np.ascontiguousarray(model.tets, np.int32)
+    te = np.ascontiguousarray(model.tet_edges, np.int32)
+    crd = np.ascontiguousarray(model.vertex_crd, np.float64)
+    fl = np.ascontiguousarray(model.flag, np.int32)
+    lib.orc_post_em_E.restype = ctypes.c_int
+    bad = lib.orc_post_em_E(ctypes.c_int(nt), _p(tv, ctypes.c_int), _p(te, ctypes.c_int), _p(crd, ctypes.c_double),
+                            _p(fl, ctypes.c_int), ctypes.c_int(flags.shape[0]), _p(flags, ctypes.c_int),
+                            ctypes.c_int(flags.shape[0]), _p(flags, ctypes.c_int), _p(sig, ctypes.c_double),
+                            ctypes.c_double(model.omega), _p(x, ctypes.c_double), *[_p(o, ctypes.c_double) for o in out])
+    if bad:
+        raise ValueError(f"{bad} elements with a zero-length edge")
+    return tuple((o[0::2] + 1j * o[1::2]).reshape(nt, 3) for o in out)

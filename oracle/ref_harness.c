@@ -21,10 +21,12 @@
  * Usage: fw_ref_harness [reference options] <model_dir>
  * Environment:
  *   FW_HARNESS_OUT   output prefix (default <model_dir>/ref)
- *   FW_HARNESS_DUMP  0: timings + solution, 1: + integer maps,
+ *   FW_HARNESS_DUMP  0: timings + solution, 1: + integer maps and the
+ *                    element results of the post step,
  *                    2: + assembled TMP_AIJ and skyline factors
  * Outputs: <prefix>.json (timings, counts), <prefix>.sol (solution),
- *          <prefix>.ints, <prefix>.aij, <prefix>.fac (dumps), and the
+ *          <prefix>.ints, <prefix>.post, <prefix>.post_drop, <prefix>.aij,
+ *          <prefix>.fac (dumps), and the
  *          reference's own residual log under <model_dir>/calc_log/.
  */
 #include "advfullwave_lib.h"
@@ -249,6 +251,48 @@ static void dump_solution(PartMesh *pm) {
   fclose(f);
 }
 
+/* The reference's element results of HDDM_post_dom_em_E
+   (main/fullwave/fullwave.c:607-634), which hddm_solver_CS runs through the
+   post_sp slot after the last solve: per subdomain its element count, the
+   global element ids (seid2geid) and el_B_c, el_E_c, el_Je_c (3 Complex per
+   element each). */
+static void dump_post(PartMesh *pm, const char *suffix) {
+  char path[FILENAME_MAX];
+  snprintf(path, sizeof(path), "%s.%s", g_prefix, suffix);
+  FILE *f = fopen(path, "wb");
+  if (!f) return;
+  w_i32(f, pm->ndomain);
+  for (int d = 0; d < pm->ndomain; d++) {
+    DomMesh *dm = &pm->dm[d];
+    w_i32(f, dm->nel);
+    fwrite(dm->seid2geid, 4, dm->nel, f);
+    fwrite(dm->rvalue.el_B_c, sizeof(Complex), 3 * dm->nel, f);
+    fwrite(dm->rvalue.el_E_c, sizeof(Complex), 3 * dm->nel, f);
+    fwrite(dm->rvalue.el_Je_c, sizeof(Complex), 3 * dm->nel, f);
+  }
+  fclose(f);
+}
+
+/* HDDM_post_dom_em_E once more on the converged solution with the first
+   entry of the Permittivity list (flag_i) and of the Conductor list (R_i)
+   left out, so that those elements take the nu = 0 and sigma = 0 branches
+   (fullwave.c:672-683).  The MTRL is a shallow copy; the model is unchanged. */
+static void dump_post_dropped(PartMesh *pm) {
+  MTRL m = pm->mtrl;
+  if (m.nflag > 0) {
+    m.nflag -= 1;
+    m.flag_i += 1;
+    m.flag_nu += 1;
+  }
+  if (m.nR > 0) {
+    m.nR -= 1;
+    m.R_i += 1;
+    m.R_sigma += 1;
+  }
+  for (int d = 0; d < pm->ndomain; d++) HDDM_post_dom_em_E(&pm->dm[d], m);
+  dump_post(pm, "post_drop");
+}
+
 int main(int argc, char **argv) {
   OPTIONS options;
   double t0 = t_now();
@@ -320,6 +364,10 @@ int main(int argc, char **argv) {
   if (f_aij) fclose(f_aij);
   if (f_fac) fclose(f_fac);
   dump_solution(&g_pm[0]);
+  if (g_dump >= 1) {
+    dump_post(&g_pm[0], "post");
+    dump_post_dropped(&g_pm[0]);
+  }
 
   char path[FILENAME_MAX];
   snprintf(path, sizeof(path), "%s.json", g_prefix);

@@ -8,7 +8,9 @@ synthetic models.
 Every fixture is one ``.npz`` holding the model parameters it was made from
 and the reference's outputs: the integer maps of make_PartMesh_FW, the
 assembled TMP_AIJ rows, the skyline profile and LDL^T factor of every
-subdomain, the residual history and the converged edge solution.  The C1
+subdomain, the residual history, the converged edge solution and the
+element results B, E, Je of the post step (also once with the first
+Permittivity and Conductor flags left out).  The C1
 fixture keeps the residual history, the iteration count and a strided
 sample of the solution.
 """
@@ -51,6 +53,9 @@ def make_case(name: str) -> str:
     }
     if full:
         arrays["x"] = out["x"]
+        for tag in ("post", "post_drop"):
+            for k, v in zip(("B", "E", "Je"), out[tag]):
+                arrays[f"{tag}_{k}"] = v
         for s, (im, am, fm) in enumerate(zip(out["ints"], out["aij"], out["fac"])):
             for k, v in im.items():
                 arrays[f"s{s}_{k}"] = v

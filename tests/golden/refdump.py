@@ -100,6 +100,28 @@ def read_sol(path: str, nv: int, n_edges: int):
     return xe
 
 
+def read_post(path: str, n_tets: int):
+    """Element results B, E, Je of the reference's post step as the harness
+    dumps them per subdomain, put in global element order: three (n_tets, 3)
+    complex arrays."""
+    b = open(path, "rb").read()
+    nsub = struct.unpack_from("<i", b, 0)[0]
+    o = 4
+    out = [np.zeros((n_tets, 3), np.complex128) for _ in range(3)]
+    seen = np.zeros(n_tets, bool)
+    for _ in range(nsub):
+        n = struct.unpack_from("<i", b, o)[0]
+        o += 4
+        g = np.frombuffer(b, "<i4", n, o)
+        o += 4 * n
+        for a in out:
+            a[g] = np.frombuffer(b, "<c16", 3 * n, o).reshape(n, 3)
+            o += 48 * n
+        seen[g] = True
+    assert o == len(b) and seen.all()
+    return tuple(out)
+
+
 def read_log(path: str):
     """Residual history of the full-wave solve from the reference's calc_log
     (hddm_solver_s.h:203-207, :319-323): returns (norm0, resi per iteration)."""
@@ -133,6 +155,8 @@ def run_harness(model, hddm_eps: float, hddm_max_loop: int, dump: int = 2, workd
     out["norm0"], out["hist"] = read_log(os.path.join(mdir, "calc_log", "log_g_HDDM_Full_Wave"))
     if dump >= 1:
         out["infree"], out["ints"] = read_ints(os.path.join(mdir, "ref.ints"), nv)
+        out["post"] = read_post(os.path.join(mdir, "ref.post"), model.n_tets)
+        out["post_drop"] = read_post(os.path.join(mdir, "ref.post_drop"), model.n_tets)
     if dump >= 2:
         out["aij"] = read_aij(os.path.join(mdir, "ref.aij"))
         out["fac"] = read_fac(os.path.join(mdir, "ref.fac"))

@@ -44,3 +44,19 @@ def test_c1_history_and_solution():
     stride = int(z["x_sample_stride"][0])
     assert np.array_equal(xe[::stride], z["x_sample"])
     assert xe.sum() == z["x_sum"][0]
+
+
+@pytest.mark.parametrize("name", ["tiny", "layered"])
+@pytest.mark.parametrize("tag", ["post", "post_drop"])
+def test_post_em_E_bitwise(name, tag):
+    """HDDM_post_em_E on the reference's converged solution; ``post_drop``
+    leaves the first Permittivity and Conductor flags out, which exercises the
+    nu = 0 and sigma = 0 branches."""
+    z, params, model = golden(name)
+    B, E, Je = oracle.post_em_E(model, z["x"], drop_first=(tag == "post_drop"))
+    assert np.array_equal(B, z[f"{tag}_B"])
+    assert np.array_equal(E, z[f"{tag}_E"])
+    assert np.array_equal(Je, z[f"{tag}_Je"])
+    if tag == "post_drop":
+        dropped = model.flag == model.mat_flag[0]
+        assert dropped.any() and not np.any(B[dropped]) and not np.any(Je[dropped])
