@@ -25,8 +25,9 @@ namespace fw {
 
 __constant__ int c_tet_n[6][4] = {{0, 1, 2, 3}, {0, 2, 3, 1}, {0, 3, 1, 2}, {1, 2, 0, 3}, {1, 3, 2, 0}, {2, 3, 0, 1}};
 
-// 1/mu0 as the reference hard-codes it (make_elem_em.c:37)
-__device__ __forceinline__ double nu_const() { return 7.957747e+05; }
+// 1/mu0 as the reference hard-codes it (make_elem_em.c:37, fullwave.c:674)
+constexpr double nu_const_host = 7.957747e+05;
+__device__ __forceinline__ double nu_const() { return nu_const_host; }
 
 // Geometry of one tetrahedron as the reference's element routine builds it.
 struct TetGeom {
@@ -259,16 +260,13 @@ __global__ void adjoint_gradient_kernel(int32_t n_design, const int32_t *__restr
 // complex per element in global element order; a null output is skipped.
 // status[0] (if given) is raised to 1 for a degenerate element, where the
 // reference stops (tetrahedral.c:257-258).
-__global__ void __launch_bounds__(128) post_em_E_kernel(int64_t nt, const int32_t *__restrict__ tet_vertices,
-                                                        const int32_t *__restrict__ tet_edges,
-                                                        const double *__restrict__ crd,
-                                                        const uint8_t *__restrict__ el_has_nu,
-                                                        const double *__restrict__ el_sigma, double omega,
-                                                        const double2 *__restrict__ xedge, double2 *__restrict__ B,
-                                                        double2 *__restrict__ E, double2 *__restrict__ Je,
-                                                        int32_t *__restrict__ status) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nt) return;
+// One element of the post step: r[0..2] = B, r[3..5] = E, r[6..8] = Je.
+// Returns true for a degenerate element.
+__device__ __forceinline__ bool post_element(int64_t t, const int32_t *__restrict__ tet_vertices,
+                                             const int32_t *__restrict__ tet_edges, const double *__restrict__ crd,
+                                             const uint8_t *__restrict__ el_has_nu,
+                                             const double *__restrict__ el_sigma, double s_nu, double s_zero,
+                                             const double2 *__restrict__ xedge, double2 *r) {
   const int4 tv = __ldg(reinterpret_cast<const int4 *>(tet_vertices) + t);
   const int2 *te2 = reinterpret_cast<const int2 *>(tet_edges + 6 * t);
   const int2 e01 = __ldg(te2), e23 = __ldg(te2 + 1), e45 = __ldg(te2 + 2);
@@ -285,7 +283,8 @@ __global__ void __launch_bounds__(128) post_em_E_kernel(int64_t nt, const int32_
     vy[i] = __ldg(crd + 3 * (int64_t)vid[i] + 1);
     vz[i] = __ldg(crd + 3 * (int64_t)vid[i] + 2);
   }
-  const double nu = el_has_nu[t] ? nu_const() : 0.0;
+  // nu/omega (fullwave.c:722), the same quotient for every element of a kind
+  const double s = el_has_nu[t] ? s_nu : s_zero;
   const double sigma = el_sigma[t];
   // one pass over the six edges: the element routine's per-edge quantities
   // (tet_SideLength, tetNedelec_Direction, _mk, _XYZ, _km_mk, _Fxyz) are
@@ -321,7 +320,6 @@ __global__ void __launch_bounds__(128) post_em_E_kernel(int64_t nt, const int32_
   g[0] = (x[0] + x[1] + x[2] + x[3]) * 0.25;
   g[1] = (y[0] + y[1] + y[2] + y[3]) * 0.25;
   g[2] = (z[0] + z[1] + z[2] + z[3]) * 0.25;
-  const double s = nu / omega;
   double2 rb[3], et[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
@@ -363,14 +361,51 @@ __global__ void __launch_bounds__(128) post_em_E_kernel(int64_t nt, const int32_
     et[1] = make_double2(et[1].x + v.x * fy, et[1].y + v.y * fy);
     et[2] = make_double2(et[2].x + v.x * fz, et[2].y + v.y * fz);
   }
-  if (bad && status) atomicMax(status, 1);
   const double dd = 2.0 / D;
   const double ds = sigma / D;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    if (B) B[3 * t + k] = make_double2(rb[k].x * dd, rb[k].y * dd);
-    if (E) E[3 * t + k] = make_double2(et[k].x * dd, et[k].y * dd);
-    if (Je) Je[3 * t + k] = make_double2(et[k].x * ds, et[k].y * ds);
+    r[k] = make_double2(rb[k].x * dd, rb[k].y * dd);
+    r[3 + k] = make_double2(et[k].x * dd, et[k].y * dd);
+    r[6 + k] = make_double2(et[k].x * ds, et[k].y * ds);
+  }
+  return bad;
+}
+
+constexpr int kPostThreads = 128;
+
+__global__ void __launch_bounds__(kPostThreads, 4) post_em_E_kernel(int64_t nt, const int32_t *__restrict__ tet_vertices,
+                                                                 const int32_t *__restrict__ tet_edges,
+                                                                 const double *__restrict__ crd,
+                                                                 const uint8_t *__restrict__ el_has_nu,
+                                                                 const double *__restrict__ el_sigma, double s_nu,
+                                                                 double s_zero, const double2 *__restrict__ xedge,
+                                                                 double2 *__restrict__ B, double2 *__restrict__ E,
+                                                                 double2 *__restrict__ Je,
+                                                                 int32_t *__restrict__ status) {
+  // results staged per block so that the stores are contiguous
+  __shared__ double2 stage[3][kPostThreads * 3];
+  const int64_t t0 = (int64_t)blockIdx.x * kPostThreads;
+  const int64_t t = t0 + threadIdx.x;
+  const int n_here = nt - t0 < kPostThreads ? (int)(nt - t0) : kPostThreads;
+  if (t < nt) {
+    double2 r[9];
+    if (post_element(t, tet_vertices, tet_edges, crd, el_has_nu, el_sigma, s_nu, s_zero, xedge, r) && status)
+      atomicMax(status, 1);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      stage[0][3 * threadIdx.x + k] = r[k];
+      stage[1][3 * threadIdx.x + k] = r[3 + k];
+      stage[2][3 * threadIdx.x + k] = r[6 + k];
+    }
+  }
+  __syncthreads();
+  double2 *outs[3] = {B, E, Je};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (!outs[k]) continue;
+    double2 *o = outs[k] + 3 * t0;
+    for (int j = threadIdx.x; j < 3 * n_here; j += kPostThreads) o[j] = stage[k][j];
   }
 }
 
@@ -378,10 +413,12 @@ void launch_post_em_E(int64_t nt, const int32_t *tet_vertices, const int32_t *te
                       const uint8_t *el_has_nu, const double *el_sigma, double omega, const double2 *x, double2 *B,
                       double2 *E, double2 *Je, int32_t *status, cudaStream_t stream) {
   if (nt <= 0) return;
-  const int threads = 128;
-  const int64_t blocks = (nt + threads - 1) / threads;
-  post_em_E_kernel<<<(unsigned)blocks, threads, 0, stream>>>(nt, tet_vertices, tet_edges, crd, el_has_nu, el_sigma,
-                                                              omega, x, B, E, Je, status);
+  const int64_t blocks = (nt + kPostThreads - 1) / kPostThreads;
+  // nu/omega divided once here, in double as the reference does per element
+  const double s_nu = nu_const_host / omega;
+  const double s_zero = 0.0 / omega;
+  post_em_E_kernel<<<(unsigned)blocks, kPostThreads, 0, stream>>>(nt, tet_vertices, tet_edges, crd, el_has_nu,
+                                                                   el_sigma, s_nu, s_zero, x, B, E, Je, status);
 }
 
 void launch_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,

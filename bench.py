@@ -485,8 +485,9 @@ def run_sharded_bench(args, rank, world, local, dist):
 
 
 def run_ncu_case(args):
-    """A short run for ncu captures: setup, the first solve and
-    ``--ncu-iters`` interface iterations, launched one by one."""
+    """A short run for ncu captures: setup, the first solve,
+    ``--ncu-iters`` interface iterations launched one by one, the last solve
+    and the post step."""
     from adventure_fullwave_b200 import hddm
 
     model = make_model(args.config)
@@ -498,6 +499,8 @@ def run_ncu_case(args):
         s.iteration_s_1st()
         for _ in range(args.ncu_iters):
             s.iteration_s()
+        s.solve_dom_last()
+        s.post_em_E()
     return 0
 
 
