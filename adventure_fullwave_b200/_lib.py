@@ -54,6 +54,11 @@ class FwSource(ctypes.Structure):
     _fields_ = [("n_entries", c_i32), ("edge", P(c_i32)), ("value", P(c_dbl))]
 
 
+class FwElementSource(ctypes.Structure):
+    _fields_ = [("n_gaps", c_i32), ("gap_box", P(c_dbl)), ("gap_volt", P(c_dbl)), ("n_antennas", c_i32),
+                ("antenna_flag", P(c_i32)), ("antenna_Jo", P(c_dbl)), ("antenna_Jor", P(c_dbl))]
+
+
 class FwOptions(ctypes.Structure):
     _fields_ = [
         ("hddm_eps", c_dbl), ("hddm_max_loop", c_i32), ("precision", c_i32), ("ir_max_steps", c_i32),
@@ -98,6 +103,7 @@ SIGNATURES = {
     "fwgpu_partition_maps": [ctypes.c_void_p, c_i32, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32),
                              P(c_i32), P(c_i32), P(c_i32), P(c_i32)],
     "fwgpu_make_tmp_aij": [ctypes.c_void_p, P(FwSource)],
+    "fwgpu_set_element_source": [ctypes.c_void_p, P(FwElementSource)],
     "fwgpu_solve_dom_1st": [ctypes.c_void_p],
     "fwgpu_iteration_s_1st": [ctypes.c_void_p, P(c_i32)],
     "fwgpu_iteration_s": [ctypes.c_void_p, P(c_i32)],

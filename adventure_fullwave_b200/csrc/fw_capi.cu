@@ -98,6 +98,19 @@ struct fwgpu_context {
   std::vector<int> stage_caps;     // staging capacities that fit in shared memory
   int64_t launches = 0;            // kernels launched since the last reset
   int64_t *d_env_dst = nullptr;    // lower entry -> envelope position (-1: outside)
+  // element right-hand side (fwgpu_set_element_source)
+  bool el_src = false;             // an element source is set
+  bool el_src_off = false;         // the adjoint solve assembles its own source only
+  int32_t n_gaps = 0;
+  double *d_gap = nullptr;         // 7 per gap: box x0 x1 y0 y1 z0 z1, dV
+  int32_t *d_el_ant = nullptr;     // antenna of each element, -1 for none
+  double *d_Jo = nullptr, *d_Jor = nullptr;
+  double2 *d_elrhs = nullptr;      // 6 per element slot
+  int64_t *d_rhs_ptr = nullptr;    // per local DOF (concatenated): its element contributions
+  int32_t *d_rhs_src = nullptr;    // element slot * 6 + edge
+  int64_t *d_int_pos = nullptr, *d_if_pos = nullptr;  // local DOF of each interior / interface entry
+  double2 *d_b_edge = nullptr;     // edge-source TMP_B (host-built)
+  double2 *d_b_local = nullptr;    // TMP_B of every subdomain
   // post step (fwgpu_post_em_E)
   bool xedge_ok = false;           // d_xedge holds a whole edge solution
   uint8_t *d_el_has_nu = nullptr;
@@ -225,9 +238,103 @@ int build_rhs(fwgpu_context *c, const fwgpu_source *src) {
     FW_CUDA(cudaMemcpyAsync(c->d_fI, fI.data(), fI.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
   if (!fG.empty())
     FW_CUDA(cudaMemcpyAsync(c->d_fG, fG.data(), fG.size() * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  if (c->el_src && !c->el_src_off) {
+    // TMP_B = element contributions in element order, then the edge source;
+    // the interior and interface right-hand sides are taken from it
+    const int64_t ndof = p.sub_dof_off[nsub];
+    if (!c->d_b_local) {
+      FW_TRY(c->alloc(&c->d_b_local, ndof));
+      FW_TRY(c->alloc(&c->d_b_edge, ndof));
+    }
+    if (ndof > 0)
+      FW_CUDA(cudaMemcpyAsync(c->d_b_edge, c->h_b_local.data(), ndof * sizeof(double2), cudaMemcpyHostToDevice,
+                              c->stream));
+    fw::launch_rhs_gather(ndof, c->d_rhs_ptr, c->d_rhs_src, c->d_elrhs, c->d_b_edge, c->d_b_local, c->stream);
+    fw::launch_rhs_split((int64_t)fI.size(), c->d_int_pos, c->d_b_local, c->d_fI, c->stream);
+    fw::launch_rhs_split((int64_t)fG.size(), c->d_if_pos, c->d_b_local, c->d_fG, c->stream);
+    c->launches += 3;
+    FW_CUDA(cudaGetLastError());
+  }
   FW_CUDA(cudaStreamSynchronize(c->stream));
   c->dp.fI = c->d_fI;
   c->dp.fG = c->d_fG;
+  return FWGPU_OK;
+}
+
+// Element sources: the per-element right-hand side is computed once (it
+// depends on the geometry, the conductivity and the source only) and the
+// gather lists from local DOFs to element contributions are built.
+int set_element_source(fwgpu_context *c, const fwgpu_element_source *es) {
+  const fw::Plan &p = c->p;
+  const int nsub = c->m.nsub;
+  const int64_t nv = c->m.nv, nt = c->m.nt;
+  if (es->n_gaps < 0 || es->n_antennas < 0) return set_error(FWGPU_ERR_ARG, "negative count");
+  if (es->n_gaps > 0 && (!es->gap_box || !es->gap_volt)) return set_error(FWGPU_ERR_ARG, "gaps without boxes");
+  if (es->n_gaps == 0 && es->n_antennas > 0 && (!es->antenna_flag || !es->antenna_Jo || !es->antenna_Jor))
+    return set_error(FWGPU_ERR_ARG, "antennas without flags or currents");
+  for (void *q : {(void *)c->d_gap, (void *)c->d_el_ant, (void *)c->d_Jo, (void *)c->d_Jor}) c->release(q);
+  c->d_gap = nullptr;
+  c->d_el_ant = nullptr;
+  c->d_Jo = c->d_Jor = nullptr;
+  c->n_gaps = es->n_gaps;
+  std::vector<double> gap(7 * (size_t)std::max(1, es->n_gaps), 0.0);
+  for (int g = 0; g < es->n_gaps; g++) {
+    for (int q = 0; q < 6; q++) gap[7 * g + q] = es->gap_box[6 * g + q];
+    gap[7 * g + 6] = es->gap_volt[g];
+  }
+  FW_TRY(c->upload(&c->d_gap, gap));
+  // first antenna whose flag matches (make_elem_em.c:110-115)
+  const int nant = es->n_gaps > 0 ? 0 : es->n_antennas;
+  std::vector<int32_t> el_ant(nt, -1);
+  for (int64_t t = 0; t < nt; t++)
+    for (int k = 0; k < nant; k++)
+      if (c->m.flag[t] == es->antenna_flag[k]) {
+        el_ant[t] = k;
+        break;
+      }
+  FW_TRY(c->upload(&c->d_el_ant, el_ant));
+  const size_t nj = 3 * (size_t)nv * std::max(1, nant);
+  FW_TRY(c->alloc(&c->d_Jo, nj));
+  FW_TRY(c->alloc(&c->d_Jor, nj));
+  if (nant > 0) {
+    FW_CUDA(cudaMemcpyAsync(c->d_Jo, es->antenna_Jo, nj * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    FW_CUDA(cudaMemcpyAsync(c->d_Jor, es->antenna_Jor, nj * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
+  if (!c->d_rhs_ptr) {
+    // local DOF -> (element slot * 6 + edge), elements in subdomain order
+    const int64_t ndof = p.sub_dof_off[nsub];
+    std::vector<int64_t> ptr(ndof + 1, 0);
+    for (int s = 0; s < nsub; s++) {
+      const fw::SubHost &h = p.subs[s];
+      for (size_t e = 0; e < h.els.size(); e++)
+        for (int i = 0; i < 6; i++) ptr[p.sub_dof_off[s] + h.nop[10 * e + 4 + i] + 1]++;
+    }
+    for (int64_t r = 0; r < ndof; r++) ptr[r + 1] += ptr[r];
+    std::vector<int32_t> src(ptr[ndof]);
+    std::vector<int64_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int s = 0; s < nsub; s++) {
+      const fw::SubHost &h = p.subs[s];
+      for (size_t e = 0; e < h.els.size(); e++)
+        for (int i = 0; i < 6; i++)
+          src[fill[p.sub_dof_off[s] + h.nop[10 * e + 4 + i]]++] = (int32_t)(6 * (p.sub_el_off[s] + (int64_t)e) + i);
+    }
+    std::vector<int64_t> int_pos(p.sub_int_off[nsub]), if_pos(p.sub_if_off[nsub]);
+    for (int s = 0; s < nsub; s++) {
+      for (int64_t k = p.sub_int_off[s]; k < p.sub_int_off[s + 1]; k++) int_pos[k] = p.sub_dof_off[s] + p.int_local[k];
+      for (int64_t k = p.sub_if_off[s]; k < p.sub_if_off[s + 1]; k++) if_pos[k] = p.sub_dof_off[s] + p.if_local[k];
+    }
+    FW_TRY(c->upload(&c->d_rhs_ptr, ptr));
+    FW_TRY(c->upload(&c->d_rhs_src, src));
+    FW_TRY(c->upload(&c->d_int_pos, int_pos));
+    FW_TRY(c->upload(&c->d_if_pos, if_pos));
+    FW_TRY(c->alloc(&c->d_elrhs, 6 * (size_t)std::max<int64_t>(1, nt)));
+  }
+  fw::launch_element_rhs(nt, c->d_el_order, c->d_tv, c->d_crd, c->d_el_sigma, c->m.omega, es->n_gaps, c->d_gap,
+                         c->d_el_ant, c->d_Jo, c->d_Jor, nv, c->d_elrhs, c->stream);
+  c->launches += 1;
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  c->el_src = true;
   return FWGPU_OK;
 }
 
@@ -603,6 +710,16 @@ int fwgpu_get_sizes(const fwgpu_context *c, fwgpu_sizes *sz) {
   sz->max_local_dofs = p.max_local;
   sz->max_interior = p.max_interior;
   return FWGPU_OK;
+}
+
+int fwgpu_set_element_source(fwgpu_context *c, const fwgpu_element_source *es) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (!es) {
+    c->el_src = false;
+    return FWGPU_OK;
+  }
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  return set_element_source(c, es);
 }
 
 int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
@@ -1236,7 +1353,10 @@ int fwgpu_adjoint_gradient(fwgpu_context *c, int32_t n_probe, const int32_t *pro
   if (J) *J = Jv;
   fwgpu_source src{n_probe, pe.data(), pv.data()};
   fwgpu_result res{};
+  // the adjoint right-hand side is dJ/dx alone
+  c->el_src_off = true;
   const int rc = fwgpu_hddm_resolve(c, &src, &res);
+  c->el_src_off = false;
   if (adjoint_result) *adjoint_result = res;
   if (rc != FWGPU_OK && rc != FWGPU_ERR_NOT_CONVERGED) return rc;
   // gradient from the forward solution and the adjoint solution
@@ -1473,10 +1593,12 @@ int fwgpu_get_tmp_aij(fwgpu_context *c, int32_t s, int32_t *nnz, int32_t *row_pt
   }
   *nnz = k;
   if (b) {
+    std::vector<double2> bl(c->h_b_local.begin() + p.sub_dof_off[s], c->h_b_local.begin() + p.sub_dof_off[s + 1]);
+    if (c->el_src && c->d_b_local)
+      FW_CUDA(cudaMemcpy(bl.data(), c->d_b_local + p.sub_dof_off[s], h.nmp * sizeof(double2), cudaMemcpyDeviceToHost));
     for (int r = 0; r < h.nmp; r++) {
-      const double2 bb = c->h_b_local[p.sub_dof_off[s] + r];
-      b[2 * r] = bb.x;
-      b[2 * r + 1] = bb.y;
+      b[2 * r] = bl[r].x;
+      b[2 * r + 1] = bl[r].y;
     }
   }
   return FWGPU_OK;

@@ -421,6 +421,177 @@ void launch_post_em_E(int64_t nt, const int32_t *tet_vertices, const int32_t *te
                                                                    el_sigma, s_nu, s_zero, x, B, E, Je, status);
 }
 
+// Element right-hand side of tet_MakeElement_EM_E (lib/fem/make_elem_em.c:66-330),
+// one thread per element slot, 6 complex per slot in the edge-table order.
+//   n_gaps > 0 (volt.dat dg > 0): DGe_j = (0, dV_k) for the last gap box k
+//     (inclusive) holding vertex j; if any vertex is held,
+//     be_i = (sigma omega) sum_j DGe_j gs_ij, gs = tetNedelec_gradside
+//     (tetrahedral.c:645-661); otherwise be = 0.
+//   n_gaps = 0 (current input): for an element of an antenna flag,
+//     be = 0 + (be_JoA - 0), be_JoA = tetNedelec_JoA_Complex
+//     (tetrahedral.c:794-858) of Joe_j = (-Jo, -Jor) at its vertices; other
+//     elements get be = 0.
+// Contraction is off for this file, so be is bit-identical to the reference's.
+__global__ void __launch_bounds__(128) element_rhs_kernel(int64_t n_el, const int32_t *__restrict__ el_order,
+                                                          const int32_t *__restrict__ tet_vertices,
+                                                          const double *__restrict__ crd,
+                                                          const double *__restrict__ el_sigma, double omega,
+                                                          int32_t n_gaps, const double *__restrict__ gap,
+                                                          const int32_t *__restrict__ el_antenna,
+                                                          const double *__restrict__ Jo,
+                                                          const double *__restrict__ Jor, int64_t n_vertices,
+                                                          double2 *__restrict__ be) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_el) return;
+  const int t = el_order[k];
+  double2 out[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) out[i] = make_double2(0.0, 0.0);
+  const int ant = n_gaps > 0 ? -1 : el_antenna[t];
+  double x[4], y[4], z[4];
+  load_tet(t, tet_vertices, crd, x, y, z);
+  double2 dge[4];
+  bool dvn = false;
+  if (n_gaps > 0) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) dge[j] = make_double2(0.0, 0.0);
+    for (int g = 0; g < n_gaps; g++) {
+      const double *bx = gap + 7 * g;
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if ((bx[0] <= x[j] && x[j] <= bx[1]) && (bx[2] <= y[j] && y[j] <= bx[3]) && (bx[4] <= z[j] && z[j] <= bx[5])) {
+          dge[j] = make_double2(0.0, bx[6]);
+          dvn = true;
+        }
+    }
+  }
+  if (dvn || ant >= 0) {
+    constexpr int kM[4][4] = {{0, 1, 2, 3}, {1, 3, 2, 0}, {2, 3, 0, 1}, {3, 1, 0, 2}};
+    constexpr int kN[6][4] = {{0, 1, 2, 3}, {0, 2, 3, 1}, {0, 3, 1, 2}, {1, 2, 0, 3}, {1, 3, 2, 0}, {2, 3, 0, 1}};
+    double b[4], c[4], d[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {  // tet_simple_b, _c, _d (tetrahedral.c:121-195)
+      const int ii = kM[i][1], jj = kM[i][2], kk = kM[i][3];
+      b[i] = -1.0 * (y[ii] * (z[jj] - z[kk]) + y[jj] * (z[kk] - z[ii]) + y[kk] * (z[ii] - z[jj]));
+      c[i] = -1.0 * (z[ii] * (x[jj] - x[kk]) + z[jj] * (x[kk] - x[ii]) + z[kk] * (x[ii] - x[jj]));
+      d[i] = -1.0 * (x[ii] * (y[jj] - y[kk]) + x[jj] * (y[kk] - y[ii]) + x[kk] * (y[ii] - y[jj]));
+    }
+    if (dvn) {
+      TetGeom G;
+      tet_geometry(x, y, z, G);
+      const double dd = 1.0 / (6.0 * G.D);
+      const double so = el_sigma[t] * omega;
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+        // F at the centroid (tetNedelec_Fxyz, tetrahedral.c:323-340)
+        const double fx = G.lsi[i] * (G.yz[i] - G.zi[i] * G.g[1] + G.yi[i] * G.g[2]);
+        const double fy = G.lsi[i] * (G.zx[i] - G.xi[i] * G.g[2] + G.zi[i] * G.g[0]);
+        const double fz = G.lsi[i] * (G.xy[i] - G.yi[i] * G.g[0] + G.xi[i] * G.g[1]);
+        double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const double gs = dd * (fx * b[j] + fy * c[j] + fz * d[j]);
+          acc = make_double2(acc.x + dge[j].x * gs, acc.y + dge[j].y * gs);
+        }
+        out[i] = make_double2(acc.x * so, acc.y * so);
+      }
+    } else {
+      const double *jo = Jo + (int64_t)ant * 3 * n_vertices;
+      const double *jr = Jor + (int64_t)ant * 3 * n_vertices;
+      double2 joe[4][3];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int64_t v = tet_vertices[4 * (int64_t)t + j];
+#pragma unroll
+        for (int cc = 0; cc < 3; cc++) joe[j][cc] = make_double2(-jo[3 * v + cc], -jr[3 * v + cc]);
+      }
+      constexpr double d0[6][4] = {{2.0, 1.0, 1.0, 1.0}, {2.0, 1.0, 1.0, 1.0}, {2.0, 1.0, 1.0, 1.0},
+                                   {1.0, 2.0, 1.0, 1.0}, {1.0, 2.0, 1.0, 1.0}, {1.0, 1.0, 2.0, 1.0}};
+      constexpr double d1[6][4] = {{-1.0, -2.0, -1.0, -1.0}, {-1.0, -1.0, -2.0, -1.0}, {-1.0, -1.0, -1.0, -2.0},
+                                   {-1.0, -1.0, -2.0, -1.0}, {-1.0, -1.0, -1.0, -2.0}, {-1.0, -1.0, -1.0, -2.0}};
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+        const int a = kN[i][0], bb = kN[i][1];
+        const double dx = x[a] - x[bb], dy = y[a] - y[bb], dz = z[a] - z[bb];
+        const double l = sqrt(dx * dx + dy * dy + dz * dz);
+        int si = 0;
+        const double px = x[bb] - x[a], py = y[bb] - y[a], pz = z[bb] - z[a];
+        if (px > 0.0) si = 1;
+        else if (px < 0.0) si = -1;
+        else if (py > 0.0) si = 1;
+        else if (py < 0.0) si = -1;
+        else if (pz > 0.0) si = 1;
+        else if (pz < 0.0) si = -1;
+        const double dd = (double)si * l / 120.0;
+        double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const double w = dd * (d0[i][j] * b[bb] + d1[i][j] * b[a]);
+          acc = make_double2(acc.x + joe[j][0].x * w, acc.y + joe[j][0].y * w);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const double w = dd * (d0[i][j] * c[bb] + d1[i][j] * c[a]);
+          acc = make_double2(acc.x + joe[j][1].x * w, acc.y + joe[j][1].y * w);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const double w = dd * (d0[i][j] * d[bb] + d1[i][j] * d[a]);
+          acc = make_double2(acc.x + joe[j][2].x * w, acc.y + joe[j][2].y * w);
+        }
+        // be = be + (be_JoA - be_gs); be_gs = sum of 0 * gs = +0 (make_elem_em.c:302-314)
+        out[i] = make_double2(0.0 + (acc.x - 0.0), 0.0 + (acc.y - 0.0));
+      }
+    }
+  }
+  double2 *o = be + 6 * k;
+#pragma unroll
+  for (int i = 0; i < 6; i++) o[i] = out[i];
+}
+
+// TMP_B of every subdomain: for each local DOF the element contributions in
+// element order (SetFe, aij_matrix_func.h:327-338), then the edge source.
+__global__ void rhs_gather_kernel(int64_t n_dof, const int64_t *__restrict__ ptr, const int32_t *__restrict__ src,
+                                  const double2 *__restrict__ be, const double2 *__restrict__ b_edge,
+                                  double2 *__restrict__ b) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_dof) return;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int64_t q = ptr[r]; q < ptr[r + 1]; q++) {
+    const double2 v = be[src[q]];
+    acc = make_double2(acc.x + v.x, acc.y + v.y);
+  }
+  const double2 e = b_edge[r];
+  b[r] = make_double2(acc.x + e.x, acc.y + e.y);
+}
+
+// interior and interface right-hand sides from TMP_B
+__global__ void rhs_split_kernel(int64_t n, const int64_t *__restrict__ pos, const double2 *__restrict__ b,
+                                 double2 *__restrict__ f) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) f[k] = b[pos[k]];
+}
+
+void launch_element_rhs(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
+                        const double *el_sigma, double omega, int32_t n_gaps, const double *gap,
+                        const int32_t *el_antenna, const double *Jo, const double *Jor, int64_t n_vertices,
+                        double2 *be, cudaStream_t stream) {
+  if (n_el <= 0) return;
+  element_rhs_kernel<<<(unsigned)((n_el + 127) / 128), 128, 0, stream>>>(
+      n_el, el_order, tet_vertices, crd, el_sigma, omega, n_gaps, gap, el_antenna, Jo, Jor, n_vertices, be);
+}
+
+void launch_rhs_gather(int64_t n_dof, const int64_t *ptr, const int32_t *src, const double2 *be,
+                       const double2 *b_edge, double2 *b, cudaStream_t stream) {
+  if (n_dof <= 0) return;
+  rhs_gather_kernel<<<(unsigned)((n_dof + 255) / 256), 256, 0, stream>>>(n_dof, ptr, src, be, b_edge, b);
+}
+
+void launch_rhs_split(int64_t n, const int64_t *pos, const double2 *b, double2 *f, cudaStream_t stream) {
+  if (n <= 0) return;
+  rhs_split_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(n, pos, b, f);
+}
+
 void launch_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
                              const double *el_eps, const double *el_sigma, double omega, double *out,
                              int32_t *status, cudaStream_t stream) {

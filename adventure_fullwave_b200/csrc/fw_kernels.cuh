@@ -177,6 +177,13 @@ void launch_edge_solution(const DevProblem &p, int64_t ne, const int64_t *edge_s
 void launch_shard_gather(const DevProblem &p, const double2 *pcloc, double2 *xq, double2 *xpc, bool status_check,
                          cudaStream_t stream);
 void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream);
+void launch_element_rhs(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
+                        const double *el_sigma, double omega, int32_t n_gaps, const double *gap,
+                        const int32_t *el_antenna, const double *Jo, const double *Jor, int64_t n_vertices,
+                        double2 *be, cudaStream_t stream);
+void launch_rhs_gather(int64_t n_dof, const int64_t *ptr, const int32_t *src, const double2 *be,
+                       const double2 *b_edge, double2 *b, cudaStream_t stream);
+void launch_rhs_split(int64_t n, const int64_t *pos, const double2 *b, double2 *f, cudaStream_t stream);
 void launch_post_em_E(int64_t nt, const int32_t *tet_vertices, const int32_t *tet_edges, const double *crd,
                       const uint8_t *el_has_nu, const double *el_sigma, double omega, const double2 *x, double2 *B,
                       double2 *E, double2 *Je, int32_t *status, cudaStream_t stream);

@@ -165,6 +165,8 @@ class HddmSolver:
         self._h = handle
         self.n_edges = int(model.n_edges)
         self.n_tets = int(model.n_tets)
+        if getattr(model, "element_source", None) is not None:
+            self.set_element_source(model.element_source)
 
     # -- lifecycle --------------------------------------------------------
     def close(self) -> None:
@@ -195,6 +197,24 @@ class HddmSolver:
         e = np.ascontiguousarray(edges, dtype=np.int32)
         v = np.ascontiguousarray(np.stack([np.real(vals), np.imag(vals)], axis=1).ravel(), dtype=np.float64)
         return _lib.FwSource(int(e.shape[0]), _ptr(e, ctypes.c_int32), _ptr(v, ctypes.c_double)), (e, v)
+
+    def set_element_source(self, es) -> None:
+        """Delta-gap voltages or antenna currents (``meshgen.ElementSource``)
+        added to every later right-hand side; None clears them."""
+        if es is None:
+            _lib.check(self._lib.fwgpu_set_element_source(self._h, None))
+            return
+        box = np.ascontiguousarray(es.gap_box, np.float64).reshape(-1)
+        volt = np.ascontiguousarray(es.gap_volt, np.float64)
+        flags = np.ascontiguousarray(es.antenna_flag, np.int32)
+        jo = np.ascontiguousarray(es.antenna_Jo, np.float64).reshape(-1)
+        jor = np.ascontiguousarray(es.antenna_Jor, np.float64).reshape(-1)
+        if es.n_antennas and jo.shape[0] != 3 * self.model.n_vertices * es.n_antennas:
+            raise ValueError("antenna currents need 3 values per vertex per antenna")
+        c = _lib.FwElementSource(int(es.n_gaps), _ptr(box, ctypes.c_double), _ptr(volt, ctypes.c_double),
+                                 int(es.n_antennas), _ptr(flags, ctypes.c_int32), _ptr(jo, ctypes.c_double),
+                                 _ptr(jor, ctypes.c_double))
+        _lib.check(self._lib.fwgpu_set_element_source(self._h, ctypes.byref(c)))
 
     # -- the reference's plug-in slots, batched ----------------------------
     def make_tmp_aij(self, source=0) -> None:

@@ -40,6 +40,29 @@ FILE_EDGE_PAIRS = ((0, 1), (0, 2), (0, 3), (1, 2), (2, 3), (1, 3))
 
 
 @dataclasses.dataclass
+class ElementSource:
+    """The element right-hand side inputs of ``tet_MakeElement_EM_E``
+    (``lib/fem/make_elem_em.c:66-330``).  With gaps (``volt.dat`` first line
+    dg > 0) every element with a vertex inside a gap box gets the delta-gap
+    term and the antennas are ignored; without gaps (dg = 0) every element
+    whose flag is an antenna flag gets the antenna current term."""
+
+    gap_box: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 6)))  # x0 x1 y0 y1 z0 z1
+    gap_volt: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
+    antenna_flag: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, np.int32))
+    antenna_Jo: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 0, 3)))   # (k, nv, 3)
+    antenna_Jor: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros((0, 0, 3)))  # (k, nv, 3)
+
+    @property
+    def n_gaps(self) -> int:
+        return int(self.gap_volt.shape[0])
+
+    @property
+    def n_antennas(self) -> int:
+        return int(self.antenna_flag.shape[0])
+
+
+@dataclasses.dataclass
 class Model:
     """A synthetic full-wave model with one part and ``nsub`` subdomains."""
 
@@ -63,6 +86,8 @@ class Model:
     # adjoint design problem: tets with their own flag (complex eps_r), probe edges
     design_tets: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, np.int32))
     probe_edges: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, np.int32))
+    # element right-hand side (delta-gap voltages or antenna currents), or None
+    element_source: Optional[ElementSource] = None
 
     @property
     def n_vertices(self) -> int:
@@ -381,6 +406,48 @@ def make_model(name: str = "c1", n: Optional[int] = None, size: Optional[float] 
     return model
 
 
+def add_region(model: Model, lo: Sequence[float], hi: Sequence[float], eps: float, sigma: float) -> int:
+    """Give the elements whose centroid lies in the box [lo, hi] a new
+    material flag (appended to the table, which stays sorted) and return it."""
+    cen = model.vertex_crd[model.tets].mean(axis=1)
+    inside = np.all((cen >= np.asarray(lo)) & (cen <= np.asarray(hi)), axis=1)
+    if not inside.any():
+        raise ValueError("no element centroid in the box")
+    f = int(model.mat_flag.max()) + 1
+    model.flag = np.where(inside, f, model.flag).astype(np.int32)
+    model.mat_flag = np.append(model.mat_flag, f).astype(np.int32)
+    model.mat_eps = np.append(model.mat_eps, eps)
+    model.mat_sigma = np.append(model.mat_sigma, sigma)
+    return f
+
+
+def delta_gap_source(model: Model, boxes, volts) -> ElementSource:
+    """Delta-gap voltages (``volt.dat`` with dg > 0): gap k drives the
+    vertices inside ``boxes[k]`` = (x0, x1, y0, y1, z0, z1) with ``volts[k]``;
+    it acts through the conductivity of the elements that touch them."""
+    es = ElementSource(gap_box=np.asarray(boxes, np.float64).reshape(-1, 6),
+                       gap_volt=np.asarray(volts, np.float64).ravel())
+    model.element_source = es
+    return es
+
+
+def antenna_source(model: Model, flags, jo, jor) -> ElementSource:
+    """Antenna currents (``volt.dat`` dg = 0): antenna k acts on the
+    elements of flag ``flags[k]`` with the vertex current arrays ``jo[k]``,
+    ``jor[k]`` of shape (n_vertices, 3) (the reference's ``antenna.Jo`` and
+    ``antenna.Jor`` at each vertex)."""
+    nv = model.n_vertices
+    es = ElementSource(antenna_flag=np.asarray(flags, np.int32).ravel(),
+                       antenna_Jo=np.asarray(jo, np.float64).reshape(-1, nv, 3),
+                       antenna_Jor=np.asarray(jor, np.float64).reshape(-1, nv, 3))
+    model.element_source = es
+    return es
+
+
+def _g17(v: float) -> str:
+    return f"{v:.17e}"
+
+
 def canonical_material_text(model: Model) -> str:
     """The reference's ``mtrl.dat`` (``lib/std/fileio.c:3474-3572``), with
     values printed to round-trip exactly."""
@@ -449,9 +516,10 @@ def subdomain_views(model: Model):
 
 def write_hddm_model(model: Model, directory: str, source_index: Optional[int] = None) -> str:
     """Write ``<directory>/model/advhddm_in_0.adv``, ``<directory>/mtrl.dat``,
-    ``<directory>/volt.dat`` (``0``: current source, ``make_elem_em.c:74-96``)
-    and ``<directory>/source.txt`` (the edge right-hand sides, consumed by the
-    oracle harness)."""
+    ``<directory>/volt.dat`` (``0``: current input, or the delta-gap
+    definitions; ``make_elem_em.c:74-96,332-346``), ``<directory>/source.txt``
+    (the edge right-hand sides) and, for antenna currents,
+    ``<directory>/antenna.txt`` (both consumed by the oracle harness)."""
     os.makedirs(os.path.join(directory, "model"), exist_ok=True)
     nv = model.n_vertices
     nnd = nv + model.n_edges
@@ -540,8 +608,25 @@ def write_hddm_model(model: Model, directory: str, source_index: Optional[int] =
             f.write(d)
     with open(os.path.join(directory, "mtrl.dat"), "w") as f:
         f.write(canonical_material_text(model))
+    es = model.element_source
     with open(os.path.join(directory, "volt.dat"), "w") as f:
-        f.write("0\n")
+        # make_elem_em.c:96 reads dg, :332-346 four lines per gap
+        if es is not None and es.n_gaps > 0:
+            f.write(f"{es.n_gaps}\n")
+            for box, dv in zip(es.gap_box, es.gap_volt):
+                f.write(f"{_g17(box[0])} {_g17(box[1])}\n{_g17(box[2])} {_g17(box[3])}\n"
+                        f"{_g17(box[4])} {_g17(box[5])}\n{_g17(dv)}\n")
+        else:
+            f.write("0\n")
+    # antenna currents per vertex, read by the oracle harness
+    if es is not None and es.n_antennas > 0:
+        with open(os.path.join(directory, "antenna.txt"), "w") as f:
+            f.write(f"{es.n_antennas} {nv}\n")
+            for k in range(es.n_antennas):
+                f.write(f"{int(es.antenna_flag[k])}\n")
+                for v in range(nv):
+                    f.write(" ".join(_g17(a) for a in es.antenna_Jo[k, v]) + " " +
+                            " ".join(_g17(a) for a in es.antenna_Jor[k, v]) + "\n")
     srcs = model.sources if source_index is None else [model.sources[source_index]]
     with open(os.path.join(directory, "source.txt"), "w") as f:
         f.write(f"{len(srcs)}\n")

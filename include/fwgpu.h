@@ -79,13 +79,38 @@ typedef struct {
 } fwgpu_material;
 
 /* Right-hand side: edge currents added to the assembled right-hand side of
- * the lowest-numbered subdomain holding each edge. */
+ * the lowest-numbered subdomain holding each edge (after any element source,
+ * fwgpu_set_element_source). */
 typedef struct {
   int32_t n_entries;
   const int32_t *edge;     /* global edge ids */
   const double *value;     /* 2*n_entries (re, im) */
 } fwgpu_source;
 
+/* Element sources of the right-hand side: the two inputs of the element
+ * routine tet_MakeElement_EM_E (lib/fem/make_elem_em.c:66-330), which the
+ * reference selects by the first line dg of ./MODEL/volt.dat.
+ *   n_gaps > 0  delta-gap voltages (dg > 0, :302-329): every element with a
+ *               vertex inside a gap box (bounds inclusive; a later gap wins
+ *               for a vertex in several) gets be_i = (sigma omega) *
+ *               sum_j (0, dV) gs_ij, gs = tetNedelec_gradside
+ *               (lib/fem/tetrahedral.c:645-661); the antennas are ignored.
+ *   n_gaps = 0  antenna currents (dg = 0, :271-300): every element whose flag
+ *               is an antenna's flag (the first match) gets
+ *               be = tetNedelec_JoA_Complex (tetrahedral.c:794-858) of the
+ *               vertex currents Joe = (-Jo, -Jor) of that antenna.
+ * The element vectors are summed into each subdomain's right-hand side in
+ * element order (SetFe, aij_matrix_func.h:327-338); an fwgpu_source passed
+ * to make_tmp_aij / solve / resolve is added after them. */
+typedef struct {
+  int32_t n_gaps;
+  const double *gap_box;        /* 6*n_gaps: x0 x1 y0 y1 z0 z1 per gap (volt.dat) */
+  const double *gap_volt;       /* n_gaps: dV per gap */
+  int32_t n_antennas;           /* mtrl.nantenna */
+  const int32_t *antenna_flag;  /* n_antennas: antenna_def[k].flag */
+  const double *antenna_Jo;     /* 3*n_vertices per antenna (k-major): antenna[k].Jo (x, y, z) per vertex */
+  const double *antenna_Jor;    /* same layout: antenna[k].Jor */
+} fwgpu_element_source;
 typedef struct {
   double hddm_eps;       /* -hddm-eps, max-norm relative residual (default 1e-3) */
   int32_t hddm_max_loop; /* -hddm-max-loop (default 4000) */
@@ -187,6 +212,11 @@ int fwgpu_partition_maps(const fwgpu_partition *part, int32_t s, int32_t *nel, i
  * summed into each subdomain's lower-triangle rows in element order, exact
  * zeros removed (aij_matrix_func.h:260-391), plus the source right-hand side. */
 int fwgpu_make_tmp_aij(fwgpu_context *ctx, const fwgpu_source *src);
+/* Sets (or, with NULL, clears) the element source every later assembly of a
+ * right-hand side adds: make_tmp_aij, hddm_solve, hddm_resolve and each source
+ * of hddm_solve_multi.  The adjoint solve of fwgpu_adjoint_gradient does not
+ * use it.  Arrays are copied. */
+int fwgpu_set_element_source(fwgpu_context *ctx, const fwgpu_element_source *es);
 
 /* solve_dom_1st: hddm_solver_CS_solve_dom_1st_d (lib/hddm/hddm_solver.h:461-555)
  * for every subdomain: Dirichlet elimination, skyline envelope

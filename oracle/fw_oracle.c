@@ -15,6 +15,8 @@
  *   mxv                  __MYMT_AIJ_MAIJMXV_TMP_AIJ__ aij_matrix_func.h:624-658
  *   orc_hddm             s-mode HDDM loop + COCG     lib/hddm/hddm_solver.h:59-183,461-693,
  *                        hddm_solver_s.h:7-424, hddm_solver_sp.h, hddm_pc.h:52-137
+ *   orc_element_rhs      tet_MakeElement_EM_E be     lib/fem/make_elem_em.c:66-330
+ *                        (tetrahedral.c:121-195,645-661,794-858)
  *   orc_post_em_E        HDDM_post_em_E              main/fullwave/fullwave.c:639-763
  *                        (tetrahedral.c:27-61,80-86,225-340)
  *
@@ -801,4 +803,123 @@ int orc_post_em_E(int nt, const int *tet_vertices, const int *tet_edges, const d
     }
   }
   return bad;
+}
+
+/* ------------------------------------------------------------------------ */
+/* element right-hand side                                                  */
+
+static const int TET_M[4][4] = {{0, 1, 2, 3}, {1, 3, 2, 0}, {2, 3, 0, 1}, {3, 1, 0, 2}};
+
+/* The element right-hand side be (6 complex, edge-table order) of
+ * tet_MakeElement_EM_E (lib/fem/make_elem_em.c:66-330) for one element with
+ * vertex coordinates xyz (x0..x3, y0..y3, z0..z3) and conductivity sigma:
+ *   n_gaps > 0 (volt.dat dg > 0, :302-329): DGe_j = (0, dV_k) for the last
+ *     gap box k holding vertex j (boxes inclusive), 0 otherwise; if any
+ *     vertex is in a box, be_i = (sigma omega) sum_j DGe_j gs_ij with
+ *     gs = tetNedelec_gradside (tetrahedral.c:645-661), else be = 0;
+ *   n_gaps = 0 (current input, :271-300): for an antenna element
+ *     (antenna != 0) be = 0 + (be_JoA - 0) with be_JoA =
+ *     tetNedelec_JoA_Complex (tetrahedral.c:794-858) of the vertex currents
+ *     joe (vertex j, component c: re joe[2*(3j+c)], im joe[2*(3j+c)+1], the
+ *     reference's Joe = (-Jo, -Jor)), and be = 0 otherwise.
+ * be receives 12 doubles (re, im per edge). */
+void orc_element_rhs(const double *xyz, double sigma, double omega, int n_gaps, const double *gap_box,
+                     const double *gap_volt, int antenna, const double *joe, double *be) {
+  const double *x = xyz, *y = xyz + 4, *z = xyz + 8;
+  for (int i = 0; i < 12; i++) be[i] = 0.0;
+  double l[6], b[4], c[4], d[4], Fx[6], Fy[6], Fz[6], g[3];
+  int si[6];
+  double D = -x[0] * y[1] * z[2] + x[0] * y[1] * z[3] + x[0] * y[2] * z[1] - x[0] * y[2] * z[3] -
+             x[0] * y[3] * z[1] + x[0] * y[3] * z[2] + x[1] * y[0] * z[2] - x[1] * y[0] * z[3] -
+             x[1] * y[2] * z[0] + x[1] * y[2] * z[3] + x[1] * y[3] * z[0] - x[1] * y[3] * z[2] -
+             x[2] * y[0] * z[1] + x[2] * y[0] * z[3] + x[2] * y[1] * z[0] - x[2] * y[1] * z[3] -
+             x[2] * y[3] * z[0] + x[2] * y[3] * z[1] + x[3] * y[0] * z[1] - x[3] * y[0] * z[2] -
+             x[3] * y[1] * z[0] + x[3] * y[1] * z[2] + x[3] * y[2] * z[0] - x[3] * y[2] * z[1];
+  g[0] = (x[0] + x[1] + x[2] + x[3]) * 0.25;
+  g[1] = (y[0] + y[1] + y[2] + y[3]) * 0.25;
+  g[2] = (z[0] + z[1] + z[2] + z[3]) * 0.25;
+  for (int i = 0; i < 4; i++) { /* tet_simple_b, _c, _d */
+    const int ii = TET_M[i][1], jj = TET_M[i][2], kk = TET_M[i][3];
+    b[i] = -1.0 * (y[ii] * (z[jj] - z[kk]) + y[jj] * (z[kk] - z[ii]) + y[kk] * (z[ii] - z[jj]));
+    c[i] = -1.0 * (z[ii] * (x[jj] - x[kk]) + z[jj] * (x[kk] - x[ii]) + z[kk] * (x[ii] - x[jj]));
+    d[i] = -1.0 * (x[ii] * (y[jj] - y[kk]) + x[jj] * (y[kk] - y[ii]) + x[kk] * (y[ii] - y[jj]));
+  }
+  for (int i = 0; i < 6; i++) {
+    const int a = TET_N[i][0], bb = TET_N[i][1], p = TET_N[i][2], q = TET_N[i][3];
+    l[i] = sqrt(pow(x[a] - x[bb], 2) + pow(y[a] - y[bb], 2) + pow(z[a] - z[bb], 2));
+    double pp = x[bb] - x[a];
+    if (pp > 0.0)
+      si[i] = 1;
+    else if (pp < 0.0)
+      si[i] = -1;
+    else {
+      pp = y[bb] - y[a];
+      if (pp > 0.0)
+        si[i] = 1;
+      else if (pp < 0.0)
+        si[i] = -1;
+      else {
+        pp = z[bb] - z[a];
+        si[i] = pp > 0.0 ? 1 : (pp < 0.0 ? -1 : 0);
+      }
+    }
+    const double xi = x[q] - x[p], yi = y[q] - y[p], zi = z[q] - z[p];
+    const double xy = x[p] * y[q] - x[q] * y[p];
+    const double yz = y[p] * z[q] - y[q] * z[p];
+    const double zx = z[p] * x[q] - z[q] * x[p];
+    const double dl = l[i] * (double)si[i];
+    Fx[i] = dl * (yz - zi * g[1] + yi * g[2]);
+    Fy[i] = dl * (zx - xi * g[2] + zi * g[0]);
+    Fz[i] = dl * (xy - yi * g[0] + xi * g[1]);
+  }
+  if (n_gaps > 0) {
+    cpx dge[4] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    int dvn = 0;
+    for (int k = 0; k < n_gaps; k++) {
+      const double *bx = gap_box + 6 * k;
+      for (int j = 0; j < 4; j++)
+        if ((bx[0] <= x[j] && x[j] <= bx[1]) && (bx[2] <= y[j] && y[j] <= bx[3]) &&
+            (bx[4] <= z[j] && z[j] <= bx[5])) {
+          dge[j] = (cpx){0.0, gap_volt[k]};
+          dvn = 1;
+        }
+    }
+    if (dvn) {
+      const double dd = 1.0 / (6.0 * D);
+      for (int i = 0; i < 6; i++) {
+        cpx s = {0.0, 0.0};
+        for (int j = 0; j < 4; j++) {
+          const double gs = dd * (Fx[i] * b[j] + Fy[i] * c[j] + Fz[i] * d[j]);
+          s = c_add(s, (cpx){dge[j].re * gs, dge[j].im * gs});
+        }
+        be[2 * i] = s.re * (sigma * omega);
+        be[2 * i + 1] = s.im * (sigma * omega);
+      }
+    }
+    return;
+  }
+  if (!antenna) return;
+  static const double d0[6][4] = {{2.0, 1.0, 1.0, 1.0}, {2.0, 1.0, 1.0, 1.0}, {2.0, 1.0, 1.0, 1.0},
+                                  {1.0, 2.0, 1.0, 1.0}, {1.0, 2.0, 1.0, 1.0}, {1.0, 1.0, 2.0, 1.0}};
+  static const double d1[6][4] = {{-1.0, -2.0, -1.0, -1.0}, {-1.0, -1.0, -2.0, -1.0}, {-1.0, -1.0, -1.0, -2.0},
+                                  {-1.0, -1.0, -2.0, -1.0}, {-1.0, -1.0, -1.0, -2.0}, {-1.0, -1.0, -1.0, -2.0}};
+  for (int i = 0; i < 6; i++) {
+    const int p0 = TET_N[i][0], p1 = TET_N[i][1];
+    const double dd = (double)si[i] * l[i] / 120.0;
+    double pn[12];
+    for (int j = 0; j < 4; j++) {
+      pn[j] = dd * (d0[i][j] * b[p1] + d1[i][j] * b[p0]);
+      pn[4 + j] = dd * (d0[i][j] * c[p1] + d1[i][j] * c[p0]);
+      pn[8 + j] = dd * (d0[i][j] * d[p1] + d1[i][j] * d[p0]);
+    }
+    cpx s = {0.0, 0.0};
+    for (int cc = 0; cc < 3; cc++)
+      for (int j = 0; j < 4; j++) {
+        const double w = pn[4 * cc + j];
+        s = c_add(s, (cpx){joe[2 * (3 * j + cc)] * w, joe[2 * (3 * j + cc) + 1] * w});
+      }
+    /* be = be + (be_JoA - be_gs), be_gs = sum of 0 * gs = +0 */
+    be[2 * i] = 0.0 + (s.re - 0.0);
+    be[2 * i + 1] = 0.0 + (s.im - 0.0);
+  }
 }

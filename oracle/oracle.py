@@ -89,6 +89,48 @@ def material_per_element(model) -> tuple:
     return eps, sig
 
 
+def element_rhs(model) -> np.ndarray:
+    """The element right-hand sides of ``model.element_source``
+    (``tet_MakeElement_EM_E``, ``lib/fem/make_elem_em.c:66-330``): (n_tets, 6)
+    complex in the edge-table order, zeros where an element has none."""
+    nt = model.n_tets
+    out = np.zeros((nt, 6), np.complex128)
+    es = getattr(model, "element_source", None)
+    if es is None:
+        return out
+    lib = load()
+    lib.orc_element_rhs.restype = None
+    _, sig = material_per_element(model)
+    ng = es.n_gaps
+    box = np.ascontiguousarray(es.gap_box, np.float64).reshape(-1)
+    volt = np.ascontiguousarray(es.gap_volt, np.float64)
+    if box.size == 0:
+        box = np.zeros(6)
+        volt = np.zeros(1)
+    # first antenna whose flag matches (make_elem_em.c:110-115)
+    ant = np.full(nt, -1, np.int64)
+    if ng == 0:
+        for k in range(es.n_antennas - 1, -1, -1):
+            ant[model.flag == es.antenna_flag[k]] = k
+    be = np.zeros(12, np.float64)
+    joe = np.zeros(24, np.float64)
+    for t in range(nt):
+        if ng == 0 and ant[t] < 0:
+            continue
+        v = model.tets[t]
+        xyz = np.ascontiguousarray(np.concatenate([model.vertex_crd[v, 0], model.vertex_crd[v, 1],
+                                                   model.vertex_crd[v, 2]]), np.float64)
+        if ant[t] >= 0:
+            k = ant[t]
+            joe[0::2] = -es.antenna_Jo[k][v].ravel()
+            joe[1::2] = -es.antenna_Jor[k][v].ravel()
+        lib.orc_element_rhs(_p(xyz, ctypes.c_double), ctypes.c_double(sig[t]), ctypes.c_double(model.omega),
+                            ctypes.c_int(ng), _p(box, ctypes.c_double), _p(volt, ctypes.c_double),
+                            ctypes.c_int(1 if ant[t] >= 0 else 0), _p(joe, ctypes.c_double), _p(be, ctypes.c_double))
+        out[t] = be[0::2] + 1j * be[1::2]
+    return out
+
+
 def partition(model, source=0) -> Partition:
     nv = model.n_vertices
     ne = model.n_edges
@@ -117,6 +159,7 @@ def partition(model, source=0) -> Partition:
         src_e, src_v = model.sources[source]
     else:
         src_e, src_v = source
+    ebe = element_rhs(model) if getattr(model, "element_source", None) is not None else None
     subs = []
     for s in range(nsub):
         els = order[starts[s]:starts[s + 1]]
@@ -132,6 +175,11 @@ def partition(model, source=0) -> Partition:
         pec_l = np.nonzero(model.pec_edge[e])[0]
         if_l = np.nonzero(iface[e])[0]
         b = np.zeros(e.shape[0], dtype=np.complex128)
+        if ebe is not None:
+            # SetFe (aij_matrix_func.h:327-338): element by element, in element order
+            for k in range(els.shape[0]):
+                for i in range(6):
+                    b[nop[k, 4 + i]] += ebe[els[k], i]
         for g, val in zip(np.asarray(src_e).tolist(), np.asarray(src_v).tolist()):
             if owner[g] == s:
                 b[eloc[g]] += val

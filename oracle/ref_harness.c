@@ -12,7 +12,11 @@
  * (main/fullwave/fullwave.c:23-146) gets
  *   - make_TMP_AIJ wrapped to add the edge current source of <dir>/source.txt
  *     to the assembled right-hand side of the subdomain that owns the edge
- *     (the lowest-numbered subdomain holding it), and
+ *     (the lowest-numbered subdomain holding it), and, when <dir>/antenna.txt
+ *     exists, to hand the reference's element routine the antenna flags and
+ *     vertex currents it reads (MTRL.antenna_def[k].flag, DomMesh.antenna[k]
+ *     .enf/.Jo/.Jor; lib/fem/make_elem_em.c:110-115,287-300) in place of the
+ *     correction-Jo pre-solve that fills them in main(), and
  *   - solve_dom_1st / iteration_s / solve_dom_last wrapped to record timings
  *     and, on request, dump the reference's intermediate data.
  * The correction-Jo pre-solve of main.c:92-98 runs only for antennas, which
@@ -70,6 +74,14 @@ typedef struct {
 } SubSource;
 static SubSource *g_src = NULL;
 
+/* antenna currents of <dir>/antenna.txt: per antenna its element flag and the
+   reference's Jo / Jor (3 per global vertex); per subdomain an ANTENNA array
+   whose enf maps local vertex ids to global vertex ids, so that
+   tet_MakeElement_EM_E reads Jo[3 * global vertex + c] */
+static int g_nant = 0;
+static MTRL_ANTENNA_DEFINITION *g_antdef = NULL;
+static ANTENNA **g_dom_ant = NULL;
+
 static double t_now(void) {
   struct timespec ts;
   clock_gettime(CLOCK_MONOTONIC, &ts);
@@ -93,7 +105,18 @@ static void w_i32(FILE *f, int v) { fwrite(&v, 4, 1, f); }
 
 static void harness_make_TMP_AIJ(DomMesh *dm, MTRL mtrl) {
   double t0 = t_now();
-  ref_make_TMP_AIJ(dm, mtrl);
+  if (g_nant > 0) {
+    /* the reference's own element routine with the antennas in place */
+    MTRL m2 = mtrl;
+    ANTENNA *saved = dm->antenna;
+    m2.nantenna = g_nant;
+    m2.antenna_def = g_antdef;
+    dm->antenna = g_dom_ant[dm->domid];
+    ref_make_TMP_AIJ(dm, m2);
+    dm->antenna = saved;
+  } else {
+    ref_make_TMP_AIJ(dm, mtrl);
+  }
   SubSource *s = &g_src[dm->domid];
   for (int k = 0; k < s->n; k++) {
     Complex *b = &dm->tmp_aij.tmp_b_c[s->edge[k]];
@@ -203,6 +226,45 @@ static void load_sources(const char *dir, PartMesh *pm) {
     }
   }
   fclose(f);
+}
+
+static void load_antennas(const char *dir, PartMesh *pm) {
+  char path[FILENAME_MAX];
+  snprintf(path, sizeof(path), "%s/antenna.txt", dir);
+  FILE *f = fopen(path, "r");
+  if (!f) return;
+  int nant = 0, nv = 0;
+  if (fscanf(f, "%d %d", &nant, &nv) != 2 || nant < 1 || nv < 1) {
+    fclose(f);
+    return;
+  }
+  g_antdef = (MTRL_ANTENNA_DEFINITION *)calloc(nant, sizeof(MTRL_ANTENNA_DEFINITION));
+  double **jo = (double **)calloc(nant, sizeof(double *));
+  double **jor = (double **)calloc(nant, sizeof(double *));
+  for (int k = 0; k < nant; k++) {
+    if (fscanf(f, "%d", &g_antdef[k].flag) != 1) break;
+    jo[k] = (double *)calloc(3 * (size_t)nv, sizeof(double));
+    jor[k] = (double *)calloc(3 * (size_t)nv, sizeof(double));
+    for (int v = 0; v < nv; v++)
+      if (fscanf(f, "%lf %lf %lf %lf %lf %lf", &jo[k][3 * v], &jo[k][3 * v + 1], &jo[k][3 * v + 2], &jor[k][3 * v],
+                 &jor[k][3 * v + 1], &jor[k][3 * v + 2]) != 6)
+        break;
+  }
+  fclose(f);
+  g_dom_ant = (ANTENNA **)calloc(pm->ndomain, sizeof(ANTENNA *));
+  for (int d = 0; d < pm->ndomain; d++) {
+    DomMesh *dm = &pm->dm[d];
+    int *enf = (int *)malloc(sizeof(int) * (dm->nap > 0 ? dm->nap : 1));
+    for (int v = 0; v < dm->nap; v++) enf[v] = pm->pnid2gnid[dm->snid2pnid[dm->apid2snid[v]]];
+    g_dom_ant[d] = (ANTENNA *)calloc(nant, sizeof(ANTENNA));
+    for (int k = 0; k < nant; k++) {
+      g_dom_ant[d][k].antenna = k;
+      g_dom_ant[d][k].enf = enf;
+      g_dom_ant[d][k].Jo = jo[k];
+      g_dom_ant[d][k].Jor = jor[k];
+    }
+  }
+  g_nant = nant;
 }
 
 static void dump_ints(PartMesh *pm) {
@@ -347,6 +409,7 @@ int main(int argc, char **argv) {
   }
   double t_init = t_now() - t0;
   load_sources(model_dir, &g_pm[0]);
+  load_antennas(model_dir, &g_pm[0]);
   if (g_dump >= 1) dump_ints(&g_pm[0]);
   if (g_dump >= 2) {
     char path[FILENAME_MAX];

@@ -36,16 +36,53 @@ CASES = {
     "layered": (dict(name="layered", n=6, size=1.5, npml=1, layers=2, nleaves=None, leaf_cap=200,
                      jitter=(0.3, 0.7), seed=3), 1e-10, 4000, True),
     "c1": (dict(name="c1", seed=0), 1e-6, 20000, False),
+    # element sources instead of the edge source: delta-gap voltages in a
+    # conducting block, and an antenna current on a block of its own flag
+    "gap": (dict(name="gap", n=4, size=1.0, npml=1, layers=None, nleaves=4, leaf_cap=None, jitter=None, seed=0),
+            1e-12, 2000, True),
+    "antenna": (dict(name="antenna", n=6, size=1.5, npml=1, layers=2, nleaves=None, leaf_cap=200,
+                     jitter=(0.3, 0.7), seed=3), 1e-10, 4000, True),
 }
+
+EPS0 = 8.8541878128e-12
+
+
+def add_element_source(model, kind: str) -> None:
+    """The element source of the ``gap`` and ``antenna`` cases."""
+    if kind == "gap":
+        meshgen.add_region(model, (0.25, 0.25, 0.25), (0.75, 0.75, 0.75), EPS0, 50.0)
+        # the second box holds one vertex of the first: the later gap wins there
+        meshgen.delta_gap_source(model, [(0.24, 0.76, 0.24, 0.76, 0.49, 0.51), (0.49, 0.51, 0.49, 0.51, 0.49, 0.51)],
+                                 [1.0, 2.0])
+    elif kind == "antenna":
+        f = meshgen.add_region(model, (0.5, 0.5, 0.5), (1.0, 1.0, 1.0), EPS0, 0.0)
+        x, y, z = model.vertex_crd.T
+        jo = np.stack([0.1 * x, -0.2 * y, 1.0 + 0.5 * z], axis=1)
+        jor = np.stack([np.full_like(x, 0.05), 0.3 * x, np.full_like(x, -0.7)], axis=1)
+        meshgen.antenna_source(model, [f], jo[None], jor[None])
+    else:
+        raise ValueError(kind)
+    model.sources = []
+
+
+def build_model(params: dict):
+    """The model a fixture was made from (its parameters as stored)."""
+    model = meshgen.make_model(**params["kw"])
+    if params.get("element_source"):
+        add_element_source(model, params["element_source"])
+    meshgen.round_trip_material(model)
+    return model
 
 
 def make_case(name: str) -> str:
     kw, eps, maxloop, full = CASES[name]
-    model = meshgen.make_model(**kw)
-    meshgen.round_trip_material(model)
+    params = dict(kw=kw, eps=eps, max_loop=maxloop)
+    if name in ("gap", "antenna"):
+        params["element_source"] = name
+    model = build_model(params)
     out = refdump.run_harness(model, eps, maxloop, dump=2 if full else 0)
     arrays = {
-        "params": np.frombuffer(json.dumps(dict(kw=kw, eps=eps, max_loop=maxloop)).encode(), dtype=np.uint8),
+        "params": np.frombuffer(json.dumps(params).encode(), dtype=np.uint8),
         "hist": out["hist"],
         "norm0": np.array([out["norm0"]]),
         "iterations": np.array([out["json"]["iterations"]]),

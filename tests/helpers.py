@@ -13,9 +13,7 @@ def golden(name: str):
 
     z = np.load(os.path.join(GOLDEN, f"ref_{name}.npz"))
     params = make_golden.params_of(z)
-    model = meshgen.make_model(**params["kw"])
-    meshgen.round_trip_material(model)
-    return z, params, model
+    return z, params, make_golden.build_model(params)
 
 
 def rel_l2(a, b) -> float:
