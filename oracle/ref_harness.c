@@ -22,6 +22,11 @@
  * The correction-Jo pre-solve of main.c:92-98 runs only for antennas, which
  * synthetic models do not define.
  *
+ * With FW_HARNESS_MAIN=1 the model is read by the reference's own hddm_Init
+ * and the correction-Jo pre-solve of main.c:92-98 runs first, as in main();
+ * the antenna currents it leaves are dumped to <prefix>.jo.  This runs a
+ * model directory of the reference as its main() would.
+ *
  * Usage: fw_ref_harness [reference options] <model_dir>
  * Environment:
  *   FW_HARNESS_OUT   output prefix (default <model_dir>/ref)
@@ -267,6 +272,42 @@ static void load_antennas(const char *dir, PartMesh *pm) {
   g_nant = nant;
 }
 
+/* The antenna currents Jo, Jor after the correction-Jo pre-solve, per
+   antenna and subdomain: every local vertex with an antenna node
+   (enf >= 0) as (global node id, Jo x y z, Jor x y z). */
+static void dump_jo(PartMesh *pms, int nparts) {
+  char path[FILENAME_MAX];
+  snprintf(path, sizeof(path), "%s.jo", g_prefix);
+  FILE *f = fopen(path, "w");
+  if (!f) return;
+  const int nant = pms[0].mtrl.nantenna;
+  fprintf(f, "%d\n", nant);
+  for (int k = 0; k < nant; k++) {
+    int count = 0;
+    for (int q = 0; q < nparts; q++)
+      for (int d = 0; d < pms[q].ndomain; d++) {
+        ANTENNA *a = &pms[q].dm[d].antenna[k];
+        if (!a->enf) continue;
+        for (int v = 0; v < pms[q].dm[d].nap; v++) count += a->enf[v] > -1;
+      }
+    fprintf(f, "%d %d\n", pms[0].mtrl.antenna_def[k].flag, count);
+    for (int q = 0; q < nparts; q++)
+    for (int d = 0; d < pms[q].ndomain; d++) {
+      PartMesh *pm = &pms[q];
+      DomMesh *dm = &pm->dm[d];
+      ANTENNA *a = &dm->antenna[k];
+      if (!a->enf) continue;
+      for (int v = 0; v < dm->nap; v++) {
+        const int j = a->enf[v];
+        if (j < 0) continue;
+        fprintf(f, "%d %.17e %.17e %.17e %.17e %.17e %.17e\n", pm->pnid2gnid[dm->snid2pnid[dm->apid2snid[v]]],
+                a->Jo[3 * j], a->Jo[3 * j + 1], a->Jo[3 * j + 2], a->Jor[3 * j], a->Jor[3 * j + 1], a->Jor[3 * j + 2]);
+      }
+    }
+  }
+  fclose(f);
+}
+
 static void dump_ints(PartMesh *pm) {
   char path[FILENAME_MAX];
   snprintf(path, sizeof(path), "%s.ints", g_prefix);
@@ -296,19 +337,25 @@ static void dump_ints(PartMesh *pm) {
   fclose(f);
 }
 
-static void dump_solution(PartMesh *pm) {
+/* every part's subdomains, parts in order */
+static void dump_solution(PartMesh *pms, int nparts) {
   char path[FILENAME_MAX];
   snprintf(path, sizeof(path), "%s.sol", g_prefix);
   FILE *f = fopen(path, "wb");
   if (!f) return;
-  w_i32(f, pm->ndomain);
-  for (int d = 0; d < pm->ndomain; d++) {
-    DomMesh *dm = &pm->dm[d];
-    w_i32(f, dm->nmp);
-    int *g = edge_gnid(pm, dm);
-    fwrite(g, 4, dm->nmp, f);
-    free(g);
-    fwrite(dm->x_c, sizeof(Complex), dm->nmp, f);
+  int total = 0;
+  for (int q = 0; q < nparts; q++) total += pms[q].ndomain;
+  w_i32(f, total);
+  for (int q = 0; q < nparts; q++) {
+    PartMesh *pm = &pms[q];
+    for (int d = 0; d < pm->ndomain; d++) {
+      DomMesh *dm = &pm->dm[d];
+      w_i32(f, dm->nmp);
+      int *g = edge_gnid(pm, dm);
+      fwrite(g, 4, dm->nmp, f);
+      free(g);
+      fwrite(dm->x_c, sizeof(Complex), dm->nmp, f);
+    }
   }
   fclose(f);
 }
@@ -386,12 +433,24 @@ int main(int argc, char **argv) {
   if (make_outdata_directory(options.datasw) > 0) return 1;
   if (make_calclog_directory(options.datasw) > 0) return 1;
 
+  const char *main_mode = getenv("FW_HARNESS_MAIN");
+  if (main_mode && atoi(main_mode) == 1) {
+    /* main()'s own flow (main/fullwave/main.c:75-100): hddm_Init, then the
+       correction-Jo pre-solve of every antenna */
+    hddm_Init(&g_pm, options);
+    hddm_sw.t_loop = -2;
+    for (int i = 0; i < g_pm[0].mtrl.nantenna; i++) {
+      hddm_sw.antenna = i;
+      hddm_solver_RS(g_pm, options, set_hddm_func_correct_Jor);
+      hddm_solver_RS(g_pm, options, set_hddm_func_correct_Joi);
+    }
+    dump_jo(g_pm, nrepeat);
+  } else {
   /* hddm_Init (lib/hddm/make_PartMesh.c:58-117) in s-mode, calling
      make_PartMesh_FW directly: make_PartMesh's material check
      (make_MESH_check_flag_2nd, lib/fem/make_MESH.c:78-130) insists on an
      antenna definition, and synthetic models drive the solve through an edge
      current instead. */
-  {
     char fname[FILENAME_MAX];
     nstart = 0;
     nend = COM_GID.nparent;
@@ -426,7 +485,7 @@ int main(int argc, char **argv) {
   double t_solve = t_now() - t1;
   if (f_aij) fclose(f_aij);
   if (f_fac) fclose(f_fac);
-  dump_solution(&g_pm[0]);
+  dump_solution(g_pm, nrepeat);
   if (g_dump >= 1) {
     dump_post(&g_pm[0], "post");
     dump_post_dropped(&g_pm[0]);

@@ -1,0 +1,86 @@
+"""The reader and writer of the reference's model and result files
+(adventure_fullwave_b200.advio): round trips through the part-file writer,
+and the reference's shipped sample model and results where present."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from adventure_fullwave_b200 import advio, meshgen
+from helpers import golden
+
+SAMPLE = "/root/reference/main/fullwave/MODEL"
+
+
+@pytest.mark.parametrize("name", ["layered", "gap"])
+def test_part_file_round_trip(name):
+    z, params, model = golden(name)
+    with tempfile.TemporaryDirectory() as d:
+        meshgen.write_hddm_model(model, d)
+        got = advio.load_model(d).model
+    assert np.array_equal(got.vertex_crd, model.vertex_crd)
+    assert np.array_equal(got.tets, model.tets)
+    assert np.array_equal(got.tet_edges, model.tet_edges)
+    assert np.array_equal(got.edges, model.edges)
+    assert np.array_equal(got.flag, model.flag)
+    assert np.array_equal(got.pec_edge, model.pec_edge)
+    assert np.array_equal(got.sub_of_tet, model.sub_of_tet) and got.nsub == model.nsub
+    assert np.array_equal(got.mat_flag, model.mat_flag)
+    assert np.array_equal(got.mat_eps, model.mat_eps) and np.array_equal(got.mat_sigma, model.mat_sigma)
+    assert got.omega == model.omega
+    if model.element_source is not None:
+        assert np.array_equal(got.element_source.gap_box, model.element_source.gap_box)
+        assert np.array_equal(got.element_source.gap_volt, model.element_source.gap_volt)
+    else:
+        assert got.element_source is None
+
+
+def test_result_round_trip():
+    z, params, model = golden("layered")
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal(model.n_edges) + 1j * rng.standard_normal(model.n_edges)
+    B = rng.standard_normal((model.n_tets, 3)) + 1j * rng.standard_normal((model.n_tets, 3))
+    with tempfile.TemporaryDirectory() as d:
+        meshgen.write_hddm_model(model, d)
+        loaded = advio.load_model(d)
+        path = os.path.join(d, "out.adv")
+        advio.write_result(path, loaded, 0, x, B=B)
+        r = advio.read_result(path)
+    p = loaded.parts[0]
+    eidx = {int(g): k for k, g in enumerate(loaded.edge_gnid.tolist())}
+    for s, rec in enumerate(r["MagneticVectorPotential"]):
+        gn = p.pnid2gnid[p.snid2pnid[s]]
+        assert np.all(np.diff(rec["snid"]) > 0)
+        k = np.array([eidx[int(g)] for g in gn[rec["snid"]]])
+        assert np.array_equal(rec["re"] + 1j * rec["im"], x[k])
+        ge = p.seid2geid[s]
+        assert np.array_equal(r["MagneticFieldReal"][s], B[ge].real)
+        assert np.array_equal(r["MagneticFieldImaginary"][s], B[ge].imag)
+
+
+@pytest.mark.skipif(not os.path.isdir(SAMPLE), reason="the reference's sample model is not on this machine")
+def test_shipped_sample_model_and_results():
+    loaded = advio.load_model(SAMPLE)
+    m = loaded.model
+    assert len(loaded.parts) == 6 and m.nsub == 6 * 73
+    v = m.vertex_crd[m.tets]
+    d6 = np.einsum("ij,ij->i", np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), v[:, 3] - v[:, 0])
+    assert np.all(d6 > 0)
+    # every edge joins two vertices of each element holding it
+    assert np.all(m.edges[:, 0] < m.edges[:, 1])
+    assert loaded.material.antennas == [(1, "md", "antenna.dat")]
+    # the shipped results: one value per edge, the same in every subdomain holding it
+    x = np.full(m.n_edges, np.nan + 0j)
+    eidx = {int(g): k for k, g in enumerate(loaded.edge_gnid.tolist())}
+    for q, p in enumerate(loaded.parts):
+        r = advio.read_result(os.path.join(SAMPLE, "result", f"advhddm_out_{q}.adv"))
+        for s, rec in enumerate(r["MagneticVectorPotential"]):
+            gn = p.pnid2gnid[p.snid2pnid[s]]
+            k = np.array([eidx[int(g)] for g in gn[rec["snid"]]])
+            vals = rec["re"] + 1j * rec["im"]
+            have = ~np.isnan(x[k].real)
+            assert np.array_equal(x[k][have], vals[have])
+            x[k] = vals
+        assert len(r["ElectricFieldReal"]) == len(p.nop)
+    assert not np.isnan(x.real).any()
