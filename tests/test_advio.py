@@ -84,3 +84,18 @@ def test_shipped_sample_model_and_results():
             x[k] = vals
         assert len(r["ElectricFieldReal"]) == len(p.nop)
     assert not np.isnan(x.real).any()
+
+
+def test_sample_fixture_matches_the_reader():
+    """tests/golden/ref_sample.npz holds the shipped sample as this reader
+    gives it; where the reference is present, read it again and compare."""
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_sample.npz"))
+    assert int(z["nsub"][0]) == 438 and z["tets"].shape == (43587, 4)
+    assert int(z["iterations"][0]) > 0 and z["antenna_vertices"].shape[0] > 0
+    if not os.path.isdir(SAMPLE):
+        return
+    m = advio.load_model(SAMPLE).model
+    assert np.array_equal(m.vertex_crd, z["vertex_crd"])
+    assert np.array_equal(m.tets, z["tets"]) and np.array_equal(m.tet_edges, z["tet_edges"])
+    assert np.array_equal(m.flag, z["flag"]) and np.array_equal(m.sub_of_tet, z["sub_of_tet"])
+    assert m.omega == float(z["omega"][0])

@@ -56,3 +56,25 @@ def test_element_source_plus_edge_source_and_clearing():
     assert rel_l2(x_both, xo_both) <= 1e-8
     assert rel_l2(x_edge, xo_edge) <= 1e-8
     assert rel_l2(x_both, x_edge) > 1e-3
+
+
+def test_element_source_in_every_source_of_a_batched_solve():
+    """The element source is added to each source of fwgpu_hddm_solve_multi,
+    as it is to a one-source solve."""
+    z, params, model = golden("antenna")
+    rng = np.random.default_rng(11)
+    srcs = []
+    for _ in range(3):
+        e = np.sort(rng.choice(model.n_edges, 4, replace=False)).astype(np.int32)
+        srcs.append((e, rng.standard_normal(4) + 1j * rng.standard_normal(4)))
+    with hddm.HddmSolver(model, hddm_eps=1e-11, hddm_max_loop=5000) as s:
+        res = s.solve_multi(srcs)
+        xs = [s.edge_solution_multi(k) for k in range(3)]
+        singles = []
+        for k in range(3):
+            s.solve(srcs[k])
+            singles.append(s.edge_solution())
+    for k in range(3):
+        assert res[k].converged
+        assert rel_l2(xs[k], singles[k]) <= 1e-8
+    assert rel_l2(xs[0], xs[1]) > 1e-3
