@@ -219,6 +219,193 @@ def read_volt(path: str) -> Tuple[np.ndarray, np.ndarray]:
     return boxes, volts
 
 
+PI = 3.14159265358979323846  # lib/std/defs.h:218
+
+
+@dataclass
+class AntennaDefinition:
+    """One shape of a ``md`` antenna definition file (``read_Jodefine_file``,
+    ``fileio.c:1170-1470``): a parallelepiped ("pp") with its face
+    equations, or a double sectorial cylinder ("dsc"), each with the real and
+    imaginary current of the Full-Wave analysis."""
+
+    kind: str
+    ap: np.ndarray = None          # pp: 5 corner points (ap[4] opposite ap[0]); dsc: x0 y0 z0 z1
+    abc: np.ndarray = None         # pp: face normals (3, 3)
+    d: np.ndarray = None           # pp: (2, 3) face constants through ap[0] and ap[4]
+    tolerance: float = 0.0
+    jo_re: np.ndarray = None       # pp: (3,), dsc: scalar in [0]
+    jo_im: np.ndarray = None
+    xyz: int = 2                   # dsc axis
+    theta: Tuple[float, float] = (0.0, 0.0)
+    r2: Tuple[float, float] = (0.0, 0.0)
+
+
+def _outer(p, q):
+    n = ((1, 2), (2, 0), (0, 1))
+    return [p[a] * q[b] - p[b] * q[a] for a, b in n]
+
+
+def _face_d(abc, ap):
+    dd = 0.0
+    for i in range(3):
+        dd += abc[i] * ap[i]
+    return -dd
+
+
+def read_jodefine(path: str) -> List[AntennaDefinition]:
+    """The shapes of an antenna definition file, in file order."""
+    toks = open(path).read().split()
+    if not toks or toks[0] != "Full-Wave":
+        raise ValueError(f"{path}: only Full-Wave antenna definitions are read")
+    defs = []
+    i = 1
+    while i < len(toks):
+        t = toks[i]
+        i += 1
+        if t == "Parallelpiped":
+            ap = [[float(toks[i + 3 * k + j]) for j in range(3)] for k in range(4)]
+            i += 12
+            jr = [float(toks[i + j]) for j in range(3)]
+            ji = [float(toks[i + 3 + j]) for j in range(3)]
+            i += 6
+            vec = [[ap[k][j] - ap[0][j] for j in range(3)] for k in range(1, 4)]
+            ap4 = list(ap[0])
+            for k in range(3):
+                for j in range(3):
+                    ap4[j] += vec[k][j]
+            abc = [_outer(vec[0], vec[1]), _outer(vec[0], vec[2]), _outer(vec[1], vec[2])]
+            d = [[_face_d(abc[k], ap[0]) for k in range(3)], [_face_d(abc[k], ap4) for k in range(3)]]
+            tol = 1.0e100
+            for k in range(3):
+                dd = 0.0
+                for j in range(3):
+                    dd += vec[k][j] * vec[k][j]
+                dd = float(np.sqrt(dd))
+                if dd < tol:
+                    tol = dd
+            defs.append(AntennaDefinition("pp", ap=np.array(ap + [ap4]), abc=np.array(abc), d=np.array(d),
+                                          tolerance=tol * 1.0e-05, jo_re=np.array(jr), jo_im=np.array(ji)))
+        elif t == "DoubleSectorialCylinder":
+            ap = [float(toks[i + j]) for j in range(3)]
+            axis = toks[i + 3]
+            height = float(toks[i + 4])
+            i += 5
+            x, y, z = {"x": (1, 2, 0), "y": (2, 0, 1), "z": (0, 1, 2)}[axis]
+            if height == 0.0:
+                raise ValueError(f"{path}: cylinder height 0")
+            if height > 0.0:
+                zr = (ap[z], ap[z] + height)
+            else:
+                zr = (ap[z] + height, ap[z])
+            unit, theta, angle = toks[i], float(toks[i + 1]), float(toks[i + 2])
+            i += 3
+            if unit == "deg":
+                theta = theta * PI / 180.0
+                angle = angle * PI / 180.0
+            elif unit != "rad":
+                raise ValueError(f"{path}: angle unit {unit}")
+            dd = 2.0 * PI
+            if angle == 0.0:
+                raise ValueError(f"{path}: rotation angle 0")
+            elif angle > dd or angle < -dd:
+                th = [0.0, 0.0]
+            elif angle > 0.0:
+                th = [theta, theta + angle]
+            else:
+                th = [theta + angle, theta]
+            while PI < th[0]:
+                th[0] += -dd
+                th[1] += -dd
+            while th[0] < -PI:
+                th[0] += dd
+                th[1] += dd
+            r0, r1 = float(toks[i]), float(toks[i + 1])
+            i += 2
+            if not (0 <= r0 < r1):
+                raise ValueError(f"{path}: cylinder radii")
+            jr, ji = float(toks[i]), float(toks[i + 1])
+            i += 2
+            if height < 0.0:
+                jr, ji = -jr, -ji
+            defs.append(AntennaDefinition("dsc", ap=np.array([ap[x], ap[y], zr[0], zr[1]]),
+                                          jo_re=np.array([jr]), jo_im=np.array([ji]),
+                                          xyz={"x": 0, "y": 1, "z": 2}[axis], theta=(th[0], th[1]),
+                                          r2=(r0 * r0, r1 * r1)))
+        else:
+            raise ValueError(f"{path}: unknown antenna shape {t}")
+    return defs
+
+
+def _pp_side(ap, xyz, tol, abc, d):
+    d0 = d
+    d1 = d
+    for i in range(3):
+        d0 += abc[i] * ap[i]
+        d1 += abc[i] * xyz[i]
+    if abs(d0) < tol:
+        d0 = 0.0
+    if abs(d1) < tol:
+        d1 = 0.0
+    return d0 * d1 >= 0.0
+
+
+def antenna_currents(model: meshgen.Model, flag: int, defs: List[AntennaDefinition]) -> Tuple[np.ndarray, np.ndarray]:
+    """The vertex currents an ``md`` antenna leaves in the reference:
+    ``make_Jo_from_definition`` (``fileio.c:1553-1700``) over the vertices of
+    the antenna's elements (``make_MESH.c:470-495``), shapes applied last to
+    first so the first shape holding a vertex wins.  The reference runs it
+    twice (``make_MESH.c:679,735``): Jor keeps the real-part pass (each shape's
+    first current triple), Jo gets the imaginary part (its second).
+    Returns (Jo, Jor), each (n_vertices, 3)."""
+    nv = model.n_vertices
+    jo = np.zeros((nv, 3))
+    jor = np.zeros((nv, 3))
+    verts = np.unique(model.tets[model.flag == flag])
+    crd = model.vertex_crd
+    for dfn in reversed(defs):
+        for v in verts.tolist():
+            c = crd[v].tolist()
+            if dfn.kind == "pp":
+                ok = True
+                for j in range(3):
+                    ok = _pp_side(c, dfn.ap[0], dfn.tolerance, dfn.abc[j], dfn.d[1][j])
+                    if not ok:
+                        break
+                    ok = _pp_side(c, dfn.ap[4], dfn.tolerance, dfn.abc[j], dfn.d[0][j])
+                    if not ok:
+                        break
+                if ok:
+                    jor[v] = dfn.jo_re
+                    jo[v] = dfn.jo_im
+            else:
+                x, y, z = {0: (1, 2, 0), 1: (2, 0, 1), 2: (0, 1, 2)}[dfn.xyz]
+                a0 = c[x] - dfn.ap[0]
+                a1 = c[y] - dfn.ap[1]
+                a2 = c[z]
+                ll = 0.0
+                ll += a0 * a0
+                ll += a1 * a1
+                if ll < dfn.r2[0] or dfn.r2[1] < ll:
+                    continue
+                if a2 < dfn.ap[2] or dfn.ap[3] < a2:
+                    continue
+                import math
+                theta = math.atan2(a1, a0)
+                if not (dfn.theta[0] == 0.0 and dfn.theta[1] == 0.0):
+                    if dfn.theta[1] < theta:
+                        continue
+                    elif theta < dfn.theta[0]:
+                        theta += 2.0 * PI
+                        if dfn.theta[1] < theta:
+                            continue
+                for arr, cur in ((jor, float(dfn.jo_re[0])), (jo, float(dfn.jo_im[0]))):
+                    arr[v, x] = -cur * math.sin(theta)
+                    arr[v, y] = cur * math.cos(theta)
+                    arr[v, z] = 0.0
+    return jo, jor
+
+
 @dataclass
 class LoadedModel:
     model: meshgen.Model
@@ -240,9 +427,11 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
     Subdomains are numbered part by part.  Vertices and edges are numbered
     in ascending global node id.  An edge is on the PEC wall when its
     mid-node is in a subdomain's DirichletBCs_Axn0 list.  A ``volt.dat``
-    with gaps becomes the model's delta-gap source.  Antenna currents come
-    from the reference's correction-Jo pre-solve and are not in these
-    files, so a model driven by an antenna has no source after loading."""
+    with gaps becomes the model's delta-gap source; otherwise antennas
+    defined by shapes (``md`` in ``mtrl.dat``) become its antenna source,
+    with the vertex currents the reference builds from the definitions
+    (``antenna_currents``).  Antennas given as current data files (``rf``)
+    are not read; such a model has no source after loading."""
     mdir = os.path.join(model_dir, "model")
     files = sorted((f for f in os.listdir(mdir) if f.startswith("advhddm_in_") and f.endswith(".adv")),
                    key=lambda f: int(f[len("advhddm_in_"):-4]))
@@ -314,10 +503,17 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
         mat_sigma=np.array([sig_of.get(f, 0.0) for f in flags.tolist()]), omega=mat.omega, pec_edge=pec,
         sub_of_tet=el_sub, nsub=sub, sources=[])
     vpath = os.path.join(model_dir, "volt.dat")
-    if os.path.exists(vpath):
-        boxes, volts = read_volt(vpath)
-        if volts.shape[0] > 0:
-            meshgen.delta_gap_source(model, boxes, volts)
+    boxes, volts = read_volt(vpath) if os.path.exists(vpath) else (np.zeros((0, 6)), np.zeros(0))
+    if volts.shape[0] > 0:
+        meshgen.delta_gap_source(model, boxes, volts)
+    elif mat.antennas and all(mode == "md" for _, mode, _ in mat.antennas):
+        flags_a, jos, jors = [], [], []
+        for flag, _, fname in mat.antennas:
+            jo, jor = antenna_currents(model, flag, read_jodefine(os.path.join(model_dir, fname)))
+            flags_a.append(flag)
+            jos.append(jo)
+            jors.append(jor)
+        meshgen.antenna_source(model, flags_a, np.array(jos), np.array(jors))
     return LoadedModel(model, parts, mat, vert_g, mid_g, np.asarray(sub_part, np.int32))
 
 

@@ -99,3 +99,42 @@ def test_sample_fixture_matches_the_reader():
     assert np.array_equal(m.tets, z["tets"]) and np.array_equal(m.tet_edges, z["tet_edges"])
     assert np.array_equal(m.flag, z["flag"]) and np.array_equal(m.sub_of_tet, z["sub_of_tet"])
     assert m.omega == float(z["omega"][0])
+    # the antenna currents built from the definition file equal those the
+    # reference's own run left (the fixture's)
+    es = m.element_source
+    assert es is not None and list(es.antenna_flag) == list(z["antenna_flag"])
+    jo = np.zeros((m.n_vertices, 3))
+    jor = np.zeros((m.n_vertices, 3))
+    jo[z["antenna_vertices"]] = z["antenna_Jo"]
+    jor[z["antenna_vertices"]] = z["antenna_Jor"]
+    assert np.array_equal(es.antenna_Jo[0], jo) and np.array_equal(es.antenna_Jor[0], jor)
+
+
+def test_antenna_definition_shapes():
+    """Parallelepiped and double sectorial cylinder definitions on a small
+    model: currents only on vertices of the antenna's elements inside the
+    shape; the cylinder's current is tangential with the given magnitude."""
+    z, params, model = golden("antenna")
+    flag = int(model.element_source.antenna_flag[0])
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "a.dat")
+        with open(path, "w") as f:
+            f.write("Full-Wave\nParallelpiped\n0.5 0.5 0.5\n0.75 0.5 0.5\n0.5 0.75 0.5\n0.5 0.5 0.75\n"
+                    "1.0 2.0 3.0  0.5 0.25 0.125\n")
+        jo, jor = advio.antenna_currents(model, flag, advio.read_jodefine(path))
+        c = model.vertex_crd
+        inside = np.all((c >= 0.5 - 1e-12) & (c <= 0.75 + 1e-12), axis=1)
+        held = np.zeros(model.n_vertices, bool)
+        held[np.unique(model.tets[model.flag == flag])] = True
+        assert np.array_equal(np.any(jor != 0, axis=1), inside & held)
+        assert np.all(jor[inside & held] == [1.0, 2.0, 3.0]) and np.all(jo[inside & held] == [0.5, 0.25, 0.125])
+        with open(path, "w") as f:
+            f.write("Full-Wave\nDoubleSectorialCylinder\n0.75 0.75 0.5 z 0.5\ndeg 0 360\n0.1 0.3\n2.0 -1.0\n")
+        jo, jor = advio.antenna_currents(model, flag, advio.read_jodefine(path))
+    r = np.hypot(c[:, 0] - 0.75, c[:, 1] - 0.75)
+    on = np.any(jor != 0, axis=1)
+    assert on.any() and np.all(held[on])
+    assert np.allclose(np.linalg.norm(jor[on], axis=1), 2.0) and np.allclose(np.linalg.norm(jo[on], axis=1), 1.0)
+    radial = np.stack([c[on, 0] - 0.75, c[on, 1] - 0.75], axis=1)
+    assert np.allclose(np.einsum("ij,ij->i", radial, jor[on, :2]), 0.0) and np.all(jor[on, 2] == 0.0)
+    assert np.all((r[on] ** 2 >= 0.01 - 1e-15) & (r[on] ** 2 <= 0.09 + 1e-15))
