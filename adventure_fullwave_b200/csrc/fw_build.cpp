@@ -18,11 +18,209 @@
 //     DOFs followed by the interface DOFs (change_dbc_Axn0_2nd/3rd,
 //     make_PartMesh.c:1068-1163, sort_inbc :1167-1194).
 #include <algorithm>
+#include <array>
+#include <atomic>
 #include <numeric>
+#include <thread>
 
 #include "fw_internal.h"
 
 namespace fw {
+
+namespace {
+
+// Index lists of one subdomain, with positions local to it: src entries
+// count from the subdomain's first lower-CSR entry, contrib_cnt gives the
+// contributions of each of its entries.  build_plan concatenates them.
+struct SubLists {
+  std::vector<int64_t> contrib;
+  std::vector<int32_t> contrib_cnt;
+  std::vector<int32_t> int_local, cpl_ptr, cpl_col, aii_ptr, aii_col, if_ln, if_local, ifr_ptr, ifr_col;
+  std::vector<int64_t> int_diag_src, cpl_src, aii_src, if_diag_src, ifr_src;
+};
+
+// per-thread scratch: global edge / vertex id -> local id, -1 elsewhere
+struct Scratch {
+  std::vector<int32_t> eloc, vloc;
+  struct Ent {
+    int32_t row, col;
+    int64_t contrib;
+  };
+  std::vector<Ent> ents, tmp;
+  std::vector<int32_t> count;
+};
+
+void build_sub(const Model &m, const Plan &p, const std::vector<int32_t> &iface_of_edge, int s, SubHost &h,
+               SubLists &L, Scratch &w) {
+  const int64_t e0 = p.sub_el_off[s], e1 = p.sub_el_off[s + 1];
+  const int nel = (int)(e1 - e0);
+  h.els.assign(p.el_order.begin() + e0, p.el_order.begin() + e1);
+  std::vector<int32_t> ve, vv;
+  ve.reserve(nel * 2);
+  vv.reserve(nel);
+  for (int k = 0; k < nel; k++) {
+    int t = h.els[k];
+    for (int i = 0; i < 6; i++) ve.push_back(m.te[6 * (int64_t)t + i]);
+    for (int i = 0; i < 4; i++) vv.push_back(m.tv[4 * (int64_t)t + i]);
+  }
+  std::sort(ve.begin(), ve.end());
+  ve.erase(std::unique(ve.begin(), ve.end()), ve.end());
+  std::sort(vv.begin(), vv.end());
+  vv.erase(std::unique(vv.begin(), vv.end()), vv.end());
+  h.nmp = (int32_t)ve.size();
+  h.nap = (int32_t)vv.size();
+  h.edge_gid = ve;
+  for (int i = 0; i < h.nmp; i++) w.eloc[ve[i]] = i;
+  for (int i = 0; i < h.nap; i++) w.vloc[vv[i]] = i;
+  h.nop.resize((size_t)nel * 10);
+  for (int k = 0; k < nel; k++) {
+    int t = h.els[k];
+    for (int i = 0; i < 4; i++) h.nop[10 * k + i] = w.vloc[m.tv[4 * (int64_t)t + i]];
+    for (int i = 0; i < 6; i++) h.nop[10 * k + 4 + i] = w.eloc[m.te[6 * (int64_t)t + kFileSlot[i]]];
+  }
+  for (int i = 0; i < h.nmp; i++) w.eloc[ve[i]] = -1;
+  for (int i = 0; i < h.nap; i++) w.vloc[vv[i]] = -1;
+  // Dirichlet list: PEC then interface (both ascending local id)
+  h.isbc.assign(h.nmp, 0);
+  h.cidx.assign(h.nmp, -1);
+  h.slot.assign(h.nmp, -1);
+  std::vector<int32_t> pecl;
+  for (int i = 0; i < h.nmp; i++) {
+    int e = ve[i];
+    if (m.pec[e]) {
+      pecl.push_back(i);
+      h.isbc[i] = 1;
+    } else if (iface_of_edge[e] >= 0) {
+      h.slot[i] = (int32_t)h.inbc_nfid.size();
+      h.inbc_nfid.push_back(i);
+      h.inbc_ln.push_back(iface_of_edge[e]);
+      h.isbc[i] = 1;
+    }
+  }
+  h.npec = (int32_t)pecl.size();
+  h.ibc = pecl;
+  h.ibc.insert(h.ibc.end(), h.inbc_nfid.begin(), h.inbc_nfid.end());
+  h.nG = (int32_t)h.inbc_nfid.size();
+  int nI = 0;
+  for (int i = 0; i < h.nmp; i++)
+    if (!h.isbc[i]) h.cidx[i] = nI++;
+  h.nI = nI;
+
+  // structural lower rows: entry (row = larger DOF, col = smaller DOF) of
+  // every element, value M[slot(row)][slot(col)] (aij_matrix_func.h:278-322);
+  // contributions stay in element order inside every (row, col): two stable
+  // counting passes, by column and then by row
+  auto &ents = w.ents;
+  ents.clear();
+  for (int k = 0; k < nel; k++) {
+    const int32_t *d = &h.nop[10 * k + 4];
+    int64_t base = (e0 + k) * 36;
+    for (int i = 0; i < 6; i++)
+      for (int j = 0; j < 6; j++)
+        if (d[i] >= d[j]) ents.push_back({d[i], d[j], base + i * 6 + j});
+  }
+  w.tmp.resize(ents.size());
+  for (int pass = 0; pass < 2; pass++) {
+    w.count.assign(h.nmp + 1, 0);
+    for (const auto &x : ents) w.count[(pass ? x.row : x.col) + 1]++;
+    for (int i = 0; i < h.nmp; i++) w.count[i + 1] += w.count[i];
+    for (const auto &x : ents) w.tmp[w.count[pass ? x.row : x.col]++] = x;
+    ents.swap(w.tmp);
+  }
+  h.row_ptr.assign(h.nmp + 1, 0);
+  h.col.clear();
+  L.contrib.resize(ents.size());
+  for (size_t q = 0; q < ents.size(); q++) {
+    bool fresh = q == 0 || ents[q].row != ents[q - 1].row || ents[q].col != ents[q - 1].col;
+    if (fresh) {
+      h.col.push_back(ents[q].col);
+      h.row_ptr[ents[q].row + 1]++;
+      L.contrib_cnt.push_back(0);
+    }
+    L.contrib_cnt.back()++;
+    L.contrib[q] = ents[q].contrib;
+  }
+  for (int i = 0; i < h.nmp; i++) h.row_ptr[i + 1] += h.row_ptr[i];
+
+  // symmetric adjacency with lower-CSR positions.  Rows are filled in
+  // ascending order, a row's own lower entries (ascending columns) first and
+  // the entries above the diagonal as later rows reach them, so every
+  // adjacency row comes out sorted by column.
+  std::vector<int32_t> adj_cnt(h.nmp + 1, 0);
+  for (int r = 0; r < h.nmp; r++)
+    for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++) {
+      adj_cnt[r + 1]++;
+      if (h.col[q] != r) adj_cnt[h.col[q] + 1]++;
+    }
+  for (int i = 0; i < h.nmp; i++) adj_cnt[i + 1] += adj_cnt[i];
+  std::vector<int32_t> adj_col(adj_cnt[h.nmp]);
+  std::vector<int64_t> adj_src(adj_cnt[h.nmp]);
+  {
+    std::vector<int32_t> fill(adj_cnt.begin(), adj_cnt.end() - 1);
+    for (int r = 0; r < h.nmp; r++)
+      for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++) {
+        int c = h.col[q];
+        adj_col[fill[r]] = c;
+        adj_src[fill[r]++] = q;
+        if (c != r) {
+          adj_col[fill[c]] = r;
+          adj_src[fill[c]++] = q;
+        }
+      }
+  }
+  auto diag_pos = [&](int r) -> int64_t {
+    for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++)
+      if (h.col[q] == r) return q;
+    return -1;
+  };
+  // interior rows: coupling to the interface and the interior operator
+  L.cpl_ptr.push_back(0);
+  L.aii_ptr.push_back(0);
+  int32_t cpl_n = 0, aii_n = 0;
+  for (int r = 0; r < h.nmp; r++) {
+    if (h.isbc[r]) continue;
+    L.int_local.push_back(r);
+    L.int_diag_src.push_back(diag_pos(r));
+    for (int q = adj_cnt[r]; q < adj_cnt[r + 1]; q++) {
+      int c = adj_col[q];
+      if (h.slot[c] >= 0) {
+        L.cpl_col.push_back(h.slot[c]);
+        L.cpl_src.push_back(adj_src[q]);
+        cpl_n++;
+      } else if (!h.isbc[c]) {
+        L.aii_col.push_back(h.cidx[c]);
+        L.aii_src.push_back(adj_src[q]);
+        aii_n++;
+      }
+    }
+    L.cpl_ptr.push_back(cpl_n);
+    L.aii_ptr.push_back(aii_n);
+  }
+  // interface rows: q = A(G, :) x with x = (interior solution, interface values)
+  L.ifr_ptr.push_back(0);
+  int32_t ifr_n = 0;
+  for (int k = 0; k < h.nG; k++) {
+    int r = h.inbc_nfid[k];
+    L.if_ln.push_back(h.inbc_ln[k]);
+    L.if_local.push_back(r);
+    L.if_diag_src.push_back(diag_pos(r));
+    for (int q = adj_cnt[r]; q < adj_cnt[r + 1]; q++) {
+      int c = adj_col[q];
+      if (!h.isbc[c]) {
+        L.ifr_col.push_back(h.cidx[c]);
+      } else if (h.slot[c] >= 0) {
+        L.ifr_col.push_back(-(h.slot[c] + 1));
+      } else {
+        continue;  // PEC column: the solution is zero there
+      }
+      L.ifr_src.push_back(adj_src[q]);
+      ifr_n++;
+    }
+    L.ifr_ptr.push_back(ifr_n);
+  }
+}
+
+}  // namespace
 
 std::string build_plan(const Model &m, Plan &p) {
   const int nsub = m.nsub;
@@ -64,6 +262,8 @@ std::string build_plan(const Model &m, Plan &p) {
       }
     }
   }
+  for (int64_t k = 0; k < 4 * (int64_t)m.nt; k++)
+    if (m.tv[k] < 0 || m.tv[k] >= m.nv) return "tet_vertices out of range";
   // part-level interface DOFs in ascending global edge id
   std::vector<int32_t> iface_of_edge(m.ne, -1);
   for (int e = 0; e < m.ne; e++) {
@@ -75,199 +275,114 @@ std::string build_plan(const Model &m, Plan &p) {
   }
   p.total_free = (int32_t)p.iface_gid.size();
 
-  std::vector<int32_t> eloc(m.ne, -1), vloc(m.nv, -1);
+  // the subdomains are independent: built on all host threads
+  std::vector<SubLists> lists(nsub);
+  {
+    const int nthreads = std::max(1, std::min<int>(nsub, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next(0);
+    auto worker = [&]() {
+      Scratch w;
+      w.eloc.assign(m.ne, -1);
+      w.vloc.assign(m.nv, -1);
+      for (int s = next++; s < nsub; s = next++) build_sub(m, p, iface_of_edge, s, p.subs[s], lists[s], w);
+    };
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+  }
+
+  // concatenated in subdomain order: offsets first, then every subdomain's
+  // slice written on all host threads
   p.sub_dof_off.assign(nsub + 1, 0);
   p.sub_nnz_off.assign(nsub + 1, 0);
   p.sub_int_off.assign(nsub + 1, 0);
   p.sub_if_off.assign(nsub + 1, 0);
-
+  enum { kContrib, kNnz, kDof, kRowPtr, kInt, kIntPtr, kCpl, kAii, kIf, kIfPtr, kIfr, kLists };
+  std::vector<std::array<int64_t, kLists>> off(nsub + 1);
+  off[0].fill(0);
   for (int s = 0; s < nsub; s++) {
-    SubHost &h = p.subs[s];
-    const int64_t e0 = p.sub_el_off[s], e1 = p.sub_el_off[s + 1];
-    const int nel = (int)(e1 - e0);
-    h.els.assign(p.el_order.begin() + e0, p.el_order.begin() + e1);
-    std::vector<int32_t> ve, vv;
-    ve.reserve(nel * 2);
-    vv.reserve(nel);
-    for (int k = 0; k < nel; k++) {
-      int t = h.els[k];
-      for (int i = 0; i < 6; i++) ve.push_back(m.te[6 * (int64_t)t + i]);
-      for (int i = 0; i < 4; i++) vv.push_back(m.tv[4 * (int64_t)t + i]);
-    }
-    std::sort(ve.begin(), ve.end());
-    ve.erase(std::unique(ve.begin(), ve.end()), ve.end());
-    std::sort(vv.begin(), vv.end());
-    vv.erase(std::unique(vv.begin(), vv.end()), vv.end());
-    h.nmp = (int32_t)ve.size();
-    h.nap = (int32_t)vv.size();
-    h.edge_gid = ve;
-    for (int i = 0; i < h.nmp; i++) eloc[ve[i]] = i;
-    for (int i = 0; i < h.nap; i++) vloc[vv[i]] = i;
-    h.nop.resize((size_t)nel * 10);
-    for (int k = 0; k < nel; k++) {
-      int t = h.els[k];
-      for (int i = 0; i < 4; i++) h.nop[10 * k + i] = vloc[m.tv[4 * (int64_t)t + i]];
-      for (int i = 0; i < 6; i++) h.nop[10 * k + 4 + i] = eloc[m.te[6 * (int64_t)t + kFileSlot[i]]];
-    }
-    // Dirichlet list: PEC then interface (both ascending local id)
-    h.isbc.assign(h.nmp, 0);
-    h.cidx.assign(h.nmp, -1);
-    h.slot.assign(h.nmp, -1);
-    std::vector<int32_t> pecl;
-    for (int i = 0; i < h.nmp; i++) {
-      int e = ve[i];
-      if (m.pec[e]) {
-        pecl.push_back(i);
-        h.isbc[i] = 1;
-      } else if (iface_of_edge[e] >= 0) {
-        h.slot[i] = (int32_t)h.inbc_nfid.size();
-        h.inbc_nfid.push_back(i);
-        h.inbc_ln.push_back(iface_of_edge[e]);
-        h.isbc[i] = 1;
-      }
-    }
-    h.npec = (int32_t)pecl.size();
-    h.ibc = pecl;
-    h.ibc.insert(h.ibc.end(), h.inbc_nfid.begin(), h.inbc_nfid.end());
-    h.nG = (int32_t)h.inbc_nfid.size();
-    int nI = 0;
-    for (int i = 0; i < h.nmp; i++)
-      if (!h.isbc[i]) h.cidx[i] = nI++;
-    h.nI = nI;
-
-    // structural lower rows: entry (row = larger DOF, col = smaller DOF) of
-    // every element, value M[slot(row)][slot(col)] (aij_matrix_func.h:278-322)
-    struct Ent {
-      int32_t row, col;
-      int64_t contrib;
-    };
-    std::vector<Ent> ents;
-    ents.reserve((size_t)nel * 21);
-    for (int k = 0; k < nel; k++) {
-      const int32_t *d = &h.nop[10 * k + 4];
-      int64_t base = (e0 + k) * 36;
-      for (int i = 0; i < 6; i++)
-        for (int j = 0; j < 6; j++)
-          if (d[i] >= d[j]) ents.push_back({d[i], d[j], base + i * 6 + j});
-    }
-    // stable: keeps element order inside every (row, col)
-    std::stable_sort(ents.begin(), ents.end(), [](const Ent &a, const Ent &b) {
-      return a.row != b.row ? a.row < b.row : a.col < b.col;
-    });
-    h.row_ptr.assign(h.nmp + 1, 0);
-    h.col.clear();
-    const int64_t nnz0 = (int64_t)p.csr_col.size();
-    for (size_t q = 0; q < ents.size(); q++) {
-      bool fresh = q == 0 || ents[q].row != ents[q - 1].row || ents[q].col != ents[q - 1].col;
-      if (fresh) {
-        h.col.push_back(ents[q].col);
-        h.row_ptr[ents[q].row + 1]++;
-        p.contrib_ptr.push_back((int64_t)p.contrib.size());
-      }
-      p.contrib.push_back(ents[q].contrib);
-    }
-    for (int i = 0; i < h.nmp; i++) h.row_ptr[i + 1] += h.row_ptr[i];
-    const int64_t nnz = (int64_t)h.col.size();
-    p.csr_row_ptr.insert(p.csr_row_ptr.end(), h.row_ptr.begin(), h.row_ptr.end());
-    p.csr_col.insert(p.csr_col.end(), h.col.begin(), h.col.end());
-    p.isbc.insert(p.isbc.end(), h.isbc.begin(), h.isbc.end());
-
-    // symmetric adjacency with lower-CSR positions
-    std::vector<int32_t> adj_cnt(h.nmp + 1, 0);
-    for (int r = 0; r < h.nmp; r++)
-      for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++) {
-        adj_cnt[r + 1]++;
-        if (h.col[q] != r) adj_cnt[h.col[q] + 1]++;
-      }
-    for (int i = 0; i < h.nmp; i++) adj_cnt[i + 1] += adj_cnt[i];
-    std::vector<int32_t> adj_col(adj_cnt[h.nmp]);
-    std::vector<int64_t> adj_src(adj_cnt[h.nmp]);
-    {
-      std::vector<int32_t> fill(adj_cnt.begin(), adj_cnt.end() - 1);
-      for (int r = 0; r < h.nmp; r++)
-        for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++) {
-          int c = h.col[q];
-          adj_col[fill[r]] = c;
-          adj_src[fill[r]++] = nnz0 + q;
-          if (c != r) {
-            adj_col[fill[c]] = r;
-            adj_src[fill[c]++] = nnz0 + q;
-          }
-        }
-      // rows of the adjacency sorted by column
-      for (int r = 0; r < h.nmp; r++) {
-        std::vector<std::pair<int32_t, int64_t>> tmp;
-        for (int q = adj_cnt[r]; q < adj_cnt[r + 1]; q++) tmp.push_back({adj_col[q], adj_src[q]});
-        std::sort(tmp.begin(), tmp.end());
-        for (int q = adj_cnt[r], u = 0; q < adj_cnt[r + 1]; q++, u++) {
-          adj_col[q] = tmp[u].first;
-          adj_src[q] = tmp[u].second;
-        }
-      }
-    }
-    auto diag_pos = [&](int r) -> int64_t {
-      for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++)
-        if (h.col[q] == r) return nnz0 + q;
-      return -1;
-    };
-    // interior rows: coupling to the interface and the interior operator
-    p.cpl_ptr.push_back(0);
-    p.aii_ptr.push_back(0);
-    int32_t cpl_n = 0, aii_n = 0;
-    for (int r = 0; r < h.nmp; r++) {
-      if (h.isbc[r]) continue;
-      p.int_local.push_back(r);
-      p.int_diag_src.push_back(diag_pos(r));
-      for (int q = adj_cnt[r]; q < adj_cnt[r + 1]; q++) {
-        int c = adj_col[q];
-        if (h.slot[c] >= 0) {
-          p.cpl_col.push_back(h.slot[c]);
-          p.cpl_src.push_back(adj_src[q]);
-          cpl_n++;
-        } else if (!h.isbc[c]) {
-          p.aii_col.push_back(h.cidx[c]);
-          p.aii_src.push_back(adj_src[q]);
-          aii_n++;
-        }
-      }
-      p.cpl_ptr.push_back(cpl_n);
-      p.aii_ptr.push_back(aii_n);
-    }
-    // interface rows: q = A(G, :) x with x = (interior solution, interface values)
-    p.ifr_ptr.push_back(0);
-    int32_t ifr_n = 0;
-    for (int k = 0; k < h.nG; k++) {
-      int r = h.inbc_nfid[k];
-      p.if_ln.push_back(h.inbc_ln[k]);
-      p.if_local.push_back(r);
-      p.if_diag_src.push_back(diag_pos(r));
-      for (int q = adj_cnt[r]; q < adj_cnt[r + 1]; q++) {
-        int c = adj_col[q];
-        if (!h.isbc[c]) {
-          p.ifr_col.push_back(h.cidx[c]);
-        } else if (h.slot[c] >= 0) {
-          p.ifr_col.push_back(-(h.slot[c] + 1));
-        } else {
-          continue;  // PEC column: the solution is zero there
-        }
-        p.ifr_src.push_back(adj_src[q]);
-        ifr_n++;
-      }
-      p.ifr_ptr.push_back(ifr_n);
-    }
-
+    const SubHost &h = p.subs[s];
+    const SubLists &L = lists[s];
+    const int64_t n[kLists] = {(int64_t)L.contrib.size(), (int64_t)h.col.size(), h.nmp, h.nmp + 1,
+                               (int64_t)L.int_local.size(), (int64_t)L.cpl_ptr.size(), (int64_t)L.cpl_col.size(),
+                               (int64_t)L.aii_col.size(), (int64_t)L.if_ln.size(), (int64_t)L.ifr_ptr.size(),
+                               (int64_t)L.ifr_col.size()};
+    for (int k = 0; k < kLists; k++) off[s + 1][k] = off[s][k] + n[k];
     p.sub_dof_off[s + 1] = p.sub_dof_off[s] + h.nmp;
-    p.sub_nnz_off[s + 1] = p.sub_nnz_off[s] + nnz;
+    p.sub_nnz_off[s + 1] = p.sub_nnz_off[s] + (int64_t)h.col.size();
     p.sub_int_off[s + 1] = p.sub_int_off[s] + h.nI;
     p.sub_if_off[s + 1] = p.sub_if_off[s] + h.nG;
     p.max_local = std::max(p.max_local, h.nmp);
     p.max_interior = std::max(p.max_interior, h.nI);
     p.max_iface = std::max(p.max_iface, h.nG);
-    for (int i = 0; i < h.nmp; i++) eloc[ve[i]] = -1;
-    for (int i = 0; i < h.nap; i++) vloc[vv[i]] = -1;
   }
-  p.nnz_total = (int64_t)p.csr_col.size();
-  p.contrib_ptr.push_back((int64_t)p.contrib.size());
+  const auto &tot = off[nsub];
+  p.contrib.resize(tot[kContrib]);
+  p.contrib_ptr.resize(tot[kNnz] + 1);
+  p.csr_col.resize(tot[kNnz]);
+  p.csr_row_ptr.resize(tot[kRowPtr]);
+  p.isbc.resize(tot[kDof]);
+  p.int_local.resize(tot[kInt]);
+  p.int_diag_src.resize(tot[kInt]);
+  p.cpl_ptr.resize(tot[kIntPtr]);
+  p.aii_ptr.resize(tot[kIntPtr]);
+  p.cpl_col.resize(tot[kCpl]);
+  p.cpl_src.resize(tot[kCpl]);
+  p.aii_col.resize(tot[kAii]);
+  p.aii_src.resize(tot[kAii]);
+  p.if_ln.resize(tot[kIf]);
+  p.if_local.resize(tot[kIf]);
+  p.if_diag_src.resize(tot[kIf]);
+  p.ifr_ptr.resize(tot[kIfPtr]);
+  p.ifr_col.resize(tot[kIfr]);
+  p.ifr_src.resize(tot[kIfr]);
+  {
+    auto copy_to = [](auto &dst, int64_t at, const auto &src) { std::copy(src.begin(), src.end(), dst.begin() + at); };
+    // src positions are local to the subdomain; -1 (no diagonal) stays -1
+    auto copy_src = [](std::vector<int64_t> &dst, int64_t at, const std::vector<int64_t> &src, int64_t nnz0) {
+      for (size_t i = 0; i < src.size(); i++) dst[at + i] = src[i] < 0 ? src[i] : src[i] + nnz0;
+    };
+    std::atomic<int> next(0);
+    auto worker = [&]() {
+      for (int s = next++; s < nsub; s = next++) {
+        const SubHost &h = p.subs[s];
+        const SubLists &L = lists[s];
+        const auto &o = off[s];
+        const int64_t nnz0 = o[kNnz];
+        copy_to(p.contrib, o[kContrib], L.contrib);
+        int64_t c = o[kContrib];
+        for (size_t q = 0; q < L.contrib_cnt.size(); q++) {
+          p.contrib_ptr[nnz0 + q] = c;
+          c += L.contrib_cnt[q];
+        }
+        copy_to(p.csr_col, nnz0, h.col);
+        copy_to(p.csr_row_ptr, o[kRowPtr], h.row_ptr);
+        copy_to(p.isbc, o[kDof], h.isbc);
+        copy_to(p.int_local, o[kInt], L.int_local);
+        copy_src(p.int_diag_src, o[kInt], L.int_diag_src, nnz0);
+        copy_to(p.cpl_ptr, o[kIntPtr], L.cpl_ptr);
+        copy_to(p.aii_ptr, o[kIntPtr], L.aii_ptr);
+        copy_to(p.cpl_col, o[kCpl], L.cpl_col);
+        copy_src(p.cpl_src, o[kCpl], L.cpl_src, nnz0);
+        copy_to(p.aii_col, o[kAii], L.aii_col);
+        copy_src(p.aii_src, o[kAii], L.aii_src, nnz0);
+        copy_to(p.if_ln, o[kIf], L.if_ln);
+        copy_to(p.if_local, o[kIf], L.if_local);
+        copy_src(p.if_diag_src, o[kIf], L.if_diag_src, nnz0);
+        copy_to(p.ifr_ptr, o[kIfPtr], L.ifr_ptr);
+        copy_to(p.ifr_col, o[kIfr], L.ifr_col);
+        copy_src(p.ifr_src, o[kIfr], L.ifr_src, nnz0);
+      }
+    };
+    const int nthreads = std::max(1, std::min<int>(nsub, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+  }
+  p.nnz_total = tot[kNnz];
+  p.contrib_ptr[tot[kNnz]] = tot[kContrib];
 
   // Q[g] = sum over the subdomains holding g, in subdomain order
   // (COM_RES_SP_FUNC, hddm_solver_sp.h:41-54, called per subdomain in order)
