@@ -78,3 +78,22 @@ def test_element_source_in_every_source_of_a_batched_solve():
         assert res[k].converged
         assert rel_l2(xs[k], singles[k]) <= 1e-8
     assert rel_l2(xs[0], xs[1]) > 1e-3
+
+
+def test_element_source_argument_errors():
+    import ctypes
+
+    from adventure_fullwave_b200 import _lib
+
+    z, params, model = golden("gap")
+    with hddm.HddmSolver(model) as s:
+        lib = _lib.load()
+        bad = _lib.FwElementSource(2, None, None, 0, None, None, None)
+        assert lib.fwgpu_set_element_source(s._h, ctypes.byref(bad)) == _lib.ERR_ARG
+        bad = _lib.FwElementSource(0, None, None, 1, None, None, None)
+        assert lib.fwgpu_set_element_source(s._h, ctypes.byref(bad)) == _lib.ERR_ARG
+        bad = _lib.FwElementSource(-1, None, None, 0, None, None, None)
+        assert lib.fwgpu_set_element_source(s._h, ctypes.byref(bad)) == _lib.ERR_ARG
+        # the source set at creation is still in place
+        r = s.solve(None)
+        assert r.converged and r.initial_norm == pytest.approx(float(z["norm0"][0]), rel=1e-6)
