@@ -140,6 +140,33 @@ def algorithmic_bytes(sz: dict, precision: str, ir_steps: int) -> int:
     return int(b)
 
 
+SAMPLE_FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "ref_sample.npz")
+
+
+def sample_model():
+    """The reference's shipped sample model with its antenna currents, from
+    the fixture tests/golden/make_sample.py made by running the reference."""
+    from adventure_fullwave_b200 import advio, meshgen
+
+    z = np.load(SAMPLE_FIXTURE)
+    tets, tet_edges = z["tets"], z["tet_edges"]
+    ne = int(tet_edges.max()) + 1
+    edges = np.zeros((ne, 2), np.int32)
+    for q, (a, b) in enumerate(advio._MID_PAIRS):
+        edges[tet_edges[:, q], 0] = np.minimum(tets[:, a], tets[:, b])
+        edges[tet_edges[:, q], 1] = np.maximum(tets[:, a], tets[:, b])
+    m = meshgen.Model(name="sample", n=0, size=0.0, vertex_crd=z["vertex_crd"], tets=tets, tet_edges=tet_edges,
+                      edges=edges, flag=z["flag"].astype(np.int32), mat_flag=z["mat_flag"], mat_eps=z["mat_eps"],
+                      mat_sigma=z["mat_sigma"], omega=float(z["omega"][0]), pec_edge=np.zeros(ne, bool),
+                      sub_of_tet=z["sub_of_tet"].astype(np.int32), nsub=int(z["nsub"][0]), sources=[])
+    jo = np.zeros((1, m.n_vertices, 3))
+    jor = np.zeros((1, m.n_vertices, 3))
+    jo[0, z["antenna_vertices"]] = z["antenna_Jo"]
+    jor[0, z["antenna_vertices"]] = z["antenna_Jor"]
+    meshgen.antenna_source(m, z["antenna_flag"], jo, jor)
+    return m, z
+
+
 def post_algorithmic_bytes(model) -> int:
     """Bytes the post step must move at least: per element its 4 vertex ids,
     6 edge ids, Permittivity mark and conductivity (16 + 24 + 1 + 8 B) and
@@ -341,6 +368,25 @@ def run_ours(args):
                 "kernel_ms": prof["subsolve_ms"], "interface_kernels_ms": prof["interface_ms"],
                 "iteration_ms_graph": prof["iteration_ms"]}
 
+    # the reference's shipped sample model, to the same tolerance as the
+    # reference's own run kept in tests/golden/ref_sample.npz
+    sample = None
+    if not args.no_sample and os.path.exists(SAMPLE_FIXTURE):
+        sm, z = sample_model()
+        with hddm.HddmSolver(sm, hddm_eps=float(z["eps"][0]), hddm_max_loop=40000, device=local) as ss:
+            ss.solve(None)
+            rs = ss.solve(None)
+            xs = ss.edge_solution()
+        ref = z["x_sample"]
+        got = xs[::int(z["x_sample_stride"][0])]
+        sample = {"model": "the reference's shipped sample (main/fullwave/MODEL): 6 parts x 73 subdomains, "
+                           "one antenna", "n_tets": sm.n_tets, "hddm_eps": float(z["eps"][0]),
+                  "time_s": (rs.t_setup_ms + rs.t_iterate_ms + rs.t_last_ms) / 1e3, "iterations": rs.iterations,
+                  "reference_iterations": int(z["iterations"][0]),
+                  "initial_norm": rs.initial_norm, "reference_initial_norm": float(z["norm0"][0]),
+                  "rel_l2_vs_reference": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
+                  "timing": "device events of one solve (second of two)"}
+
     # the post step (element B, E, Je from the converged edge values)
     post = None
     if not args.no_post:
@@ -412,6 +458,8 @@ def run_ours(args):
         line["adjoint"] = adjoint
     if post is not None:
         line["post"] = post
+    if sample is not None:
+        line["sample"] = sample
     print(json.dumps(line))
     return 0
 
@@ -520,6 +568,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the FP32+IR comparison solve")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the C4 adjoint sample of a C2 run")
     ap.add_argument("--no-post", action="store_true", help="skip the post-step measurement")
+    ap.add_argument("--no-sample", action="store_true", help="skip the reference's shipped sample model")
     ap.add_argument("--adjoint-steps", type=int, default=1)
     ap.add_argument("--replicas", action="store_true", help="N > 1: independent replicas instead of shards")
     ap.add_argument("--sharded", action="store_true", help="the sharded driver even at N = 1 (one shard)")

@@ -4,36 +4,18 @@ antenna) solved through the C ABI with the antenna currents of the
 reference's correction-Jo pre-solve, against the reference's own run to the
 same hddm_eps (fixture tests/golden/ref_sample.npz, made by
 tests/golden/make_sample.py)."""
-import os
-
 import numpy as np
 import pytest
 
-from adventure_fullwave_b200 import advio, hddm, meshgen
-from helpers import GOLDEN
+from adventure_fullwave_b200 import hddm
 
 pytestmark = pytest.mark.gpu
 
 
 def sample_model():
-    z = np.load(os.path.join(GOLDEN, "ref_sample.npz"))
-    tets = z["tets"]
-    tet_edges = z["tet_edges"]
-    ne = int(tet_edges.max()) + 1
-    edges = np.zeros((ne, 2), np.int32)
-    for q, (a, b) in enumerate(advio._MID_PAIRS):
-        edges[tet_edges[:, q], 0] = np.minimum(tets[:, a], tets[:, b])
-        edges[tet_edges[:, q], 1] = np.maximum(tets[:, a], tets[:, b])
-    m = meshgen.Model(name="sample", n=0, size=0.0, vertex_crd=z["vertex_crd"], tets=tets, tet_edges=tet_edges,
-                      edges=edges, flag=z["flag"].astype(np.int32), mat_flag=z["mat_flag"], mat_eps=z["mat_eps"],
-                      mat_sigma=z["mat_sigma"], omega=float(z["omega"][0]), pec_edge=np.zeros(ne, bool),
-                      sub_of_tet=z["sub_of_tet"].astype(np.int32), nsub=int(z["nsub"][0]), sources=[])
-    nv = m.n_vertices
-    jo = np.zeros((1, nv, 3))
-    jor = np.zeros((1, nv, 3))
-    jo[0, z["antenna_vertices"]] = z["antenna_Jo"]
-    jor[0, z["antenna_vertices"]] = z["antenna_Jor"]
-    meshgen.antenna_source(m, z["antenna_flag"], jo, jor)
+    import bench
+
+    m, z = bench.sample_model()
     return z, m
 
 
