@@ -547,13 +547,14 @@ def read_result(path: str) -> Dict[str, List[np.ndarray]]:
 
 
 def write_result(path: str, loaded: LoadedModel, part: int, x: np.ndarray,
-                 B: Optional[np.ndarray] = None, E: Optional[np.ndarray] = None) -> None:
+                 B: Optional[np.ndarray] = None, E: Optional[np.ndarray] = None,
+                 Je: Optional[np.ndarray] = None) -> None:
     """The result file of one part in the reference's layout
     (``write_outdata_file_HDDM_FW``, ``fileio.c:2930-3160``): the edge
     solution per subdomain as (snid, re, im) records keyed by the
     subdomain's own node ids, and, when given, the element fields
-    B = i (nu/omega) rot E and E (from ``HddmSolver.post_em_E``) as real and
-    imaginary (nel, 3) documents in each subdomain's element order."""
+    B = i (nu/omega) rot E, E and Je (from ``HddmSolver.post_em_E``) as real
+    and imaginary (nel, 3) documents in each subdomain's element order."""
     p = loaded.parts[part]
     eidx = {int(g): k for k, g in enumerate(loaded.edge_gnid.tolist())}
     vec = bytearray()
@@ -566,7 +567,7 @@ def write_result(path: str, loaded: LoadedModel, part: int, x: np.ndarray,
             v = x[eidx[int(gn[snid])]]
             vec += struct.pack("<idd", int(snid), float(v.real), float(v.imag))
         ge = p.seid2geid[s]
-        for label, arr in (("MagneticField", B), ("ElectricField", E)):
+        for label, arr in (("MagneticField", B), ("ElectricField", E), ("CurrentDensity", Je)):
             if arr is None:
                 continue
             for suffix, f in (("Real", np.real), ("Imaginary", np.imag)):

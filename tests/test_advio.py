@@ -83,6 +83,19 @@ def test_shipped_sample_model_and_results():
             assert np.array_equal(x[k][have], vals[have])
             x[k] = vals
         assert len(r["ElectricFieldReal"]) == len(p.nop)
+        # the writer gives the same layout: node ids per subdomain, element arrays per subdomain
+        with tempfile.TemporaryDirectory() as d:
+            out = os.path.join(d, "out.adv")
+            z3 = np.zeros((m.n_tets, 3), complex)
+            advio.write_result(out, loaded, q, np.zeros(m.n_edges, complex), B=z3, E=z3, Je=z3)
+            w = advio.read_result(out)
+        assert set(w) == set(r)
+        for label in r:
+            for a, b in zip(w[label], r[label]):
+                if label == "MagneticVectorPotential":
+                    assert np.array_equal(a["snid"], b["snid"])
+                else:
+                    assert a.shape == b.shape
     assert not np.isnan(x.real).any()
 
 
