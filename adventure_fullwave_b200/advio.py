@@ -406,6 +406,42 @@ def antenna_currents(model: meshgen.Model, flag: int, defs: List[AntennaDefiniti
     return jo, jor
 
 
+def read_jodata(path: str) -> Tuple[np.ndarray, np.ndarray]:
+    """A current data file of an ``rf`` antenna (``read_Jodata_file_read``,
+    ``fileio.c:1016-1050``): the count, then per node its global node id and
+    three current components.  Returns (node ids, (n, 3) currents) sorted by
+    node id."""
+    toks = open(path).read().split()
+    n = int(toks[0])
+    ids = np.array([int(toks[1 + 4 * k]) for k in range(n)], np.int64)
+    val = np.array([[float(toks[2 + 4 * k + j]) for j in range(3)] for k in range(n)])
+    order = np.argsort(ids, kind="stable")
+    return ids[order], val[order]
+
+
+def antenna_currents_from_files(model: meshgen.Model, flag: int, vertex_gnid: np.ndarray, real_path: str,
+                                imag_path: str) -> Tuple[np.ndarray, np.ndarray]:
+    """The vertex currents of an ``rf`` antenna: the real-part file
+    (``<name>r``) gives Jor and the imaginary-part file (``<name>i``) gives Jo
+    (``make_MESH.c:674-676,729-733``, ``read_Jodata_file_decompose``,
+    ``fileio.c:1053-1106``), on the vertices of the antenna's elements; a
+    vertex the file does not list gets 0.  Returns (Jo, Jor)."""
+    nv = model.n_vertices
+    held = np.zeros(nv, bool)
+    held[np.unique(model.tets[model.flag == flag])] = True
+    vidx = {int(g): k for k, g in enumerate(np.asarray(vertex_gnid).tolist())}
+    out = []
+    for path in (imag_path, real_path):
+        a = np.zeros((nv, 3))
+        ids, val = read_jodata(path)
+        for g, v in zip(ids.tolist(), val):
+            k = vidx.get(int(g))
+            if k is not None and held[k]:
+                a[k] = v
+        out.append(a)
+    return out[0], out[1]
+
+
 @dataclass
 class LoadedModel:
     model: meshgen.Model
@@ -427,11 +463,10 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
     Subdomains are numbered part by part.  Vertices and edges are numbered
     in ascending global node id.  An edge is on the PEC wall when its
     mid-node is in a subdomain's DirichletBCs_Axn0 list.  A ``volt.dat``
-    with gaps becomes the model's delta-gap source; otherwise antennas
-    defined by shapes (``md`` in ``mtrl.dat``) become its antenna source,
-    with the vertex currents the reference builds from the definitions
-    (``antenna_currents``).  Antennas given as current data files (``rf``)
-    are not read; such a model has no source after loading."""
+    with gaps becomes the model's delta-gap source; otherwise the antennas
+    of ``mtrl.dat`` become its antenna source, with the vertex currents the
+    reference builds: from shape definitions (``md``, ``antenna_currents``)
+    or from current data files (``rf``, ``antenna_currents_from_files``)."""
     mdir = os.path.join(model_dir, "model")
     files = sorted((f for f in os.listdir(mdir) if f.startswith("advhddm_in_") and f.endswith(".adv")),
                    key=lambda f: int(f[len("advhddm_in_"):-4]))
@@ -506,10 +541,16 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
     boxes, volts = read_volt(vpath) if os.path.exists(vpath) else (np.zeros((0, 6)), np.zeros(0))
     if volts.shape[0] > 0:
         meshgen.delta_gap_source(model, boxes, volts)
-    elif mat.antennas and all(mode == "md" for _, mode, _ in mat.antennas):
+    elif mat.antennas:
         flags_a, jos, jors = [], [], []
-        for flag, _, fname in mat.antennas:
-            jo, jor = antenna_currents(model, flag, read_jodefine(os.path.join(model_dir, fname)))
+        for flag, mode, fname in mat.antennas:
+            if mode == "md":
+                jo, jor = antenna_currents(model, flag, read_jodefine(os.path.join(model_dir, fname)))
+            elif mode == "rf":
+                jo, jor = antenna_currents_from_files(model, flag, vert_g, os.path.join(model_dir, fname + "r"),
+                                                      os.path.join(model_dir, fname + "i"))
+            else:
+                raise ValueError(f"antenna mode {mode}")
             flags_a.append(flag)
             jos.append(jo)
             jors.append(jor)
