@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "fw_internal.h"
@@ -171,20 +172,23 @@ int resolve_material(fw::Model &m, const fwgpu_mesh *mesh, const fwgpu_material 
   m.el_sigma.assign(m.nt, 0.0);
   m.el_has_nu.assign(m.nt, 0);
   // the reference searches the tables linearly and takes the first match
-  // (lib/fem/make_elem_em.c:98-109); absent flags leave eps = sigma = 0
+  // (lib/fem/make_elem_em.c:98-109); absent flags leave eps = sigma = 0.
+  // The first entry of each flag, looked up by hash: tables with one flag
+  // per element (per-element materials) stay linear in the element count.
+  std::unordered_map<int32_t, int32_t> eps_at, sigma_at;
+  eps_at.reserve(2 * (size_t)std::max(0, mt->n_eps));
+  sigma_at.reserve(2 * (size_t)std::max(0, mt->n_sigma));
+  for (int i = 0; i < mt->n_eps; i++) eps_at.emplace(mt->eps_flag[i], i);
+  for (int i = 0; i < mt->n_sigma; i++) sigma_at.emplace(mt->sigma_flag[i], i);
   for (int t = 0; t < m.nt; t++) {
     const int f = mesh->tet_flag[t];
-    for (int i = 0; i < mt->n_eps; i++)
-      if (mt->eps_flag[i] == f) {
-        m.el_eps[t] = mt->eps[i];
-        m.el_has_nu[t] = 1;
-        break;
-      }
-    for (int i = 0; i < mt->n_sigma; i++)
-      if (mt->sigma_flag[i] == f) {
-        m.el_sigma[t] = mt->sigma[i];
-        break;
-      }
+    auto e = eps_at.find(f);
+    if (e != eps_at.end()) {
+      m.el_eps[t] = mt->eps[e->second];
+      m.el_has_nu[t] = 1;
+    }
+    auto g = sigma_at.find(f);
+    if (g != sigma_at.end()) m.el_sigma[t] = mt->sigma[g->second];
   }
   return FWGPU_OK;
 }
