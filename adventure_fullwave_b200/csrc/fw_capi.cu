@@ -97,6 +97,8 @@ struct fwgpu_context {
   int32_t *d_blk_off = nullptr;    // staged solve block table (current staging capacity)
   int2 *d_blk_tab = nullptr;
   std::vector<int> stage_caps;     // staging capacities that fit in shared memory
+  std::vector<int32_t> h_order;    // subdomains by interior size, largest first (the device sub_order)
+  std::vector<int32_t> h_nblk;     // staged blocks of each subdomain at the current capacity
   int64_t launches = 0;            // kernels launched since the last reset
   int64_t *d_env_dst = nullptr;    // lower entry -> envelope position (-1: outside)
   // element right-hand side (fwgpu_set_element_source)
@@ -477,6 +479,7 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
     const fw::SubHost &x = p.subs[a], &y = p.subs[b];
     return x.nI != y.nI ? x.nI > y.nI : x.nmp > y.nmp;
   });
+  c->h_order = order;
   fw::DevProblem &dp = c->dp;
   dp.nsub = s_end - s_begin;
   dp.nfree = p.total_free;
@@ -781,6 +784,7 @@ static int build_stage_blocks(fwgpu_context *c, int cap, int *max_blocks_out) {
   std::vector<int32_t> boff(nsub + 1, 0);
   std::vector<int2> btab;
   int max_blocks = 0;
+  c->h_nblk.assign(nsub, 0);
   for (int s = 0; s < nsub; s++) {
     const int64_t io = p.sub_int_off[s];
     const int nI = (int)(p.sub_int_off[s + 1] - io);
@@ -802,6 +806,7 @@ static int build_stage_blocks(fwgpu_context *c, int cap, int *max_blocks_out) {
     }
     btab.push_back(make_int2(nI, nI > 0 ? row_end(nI - 1) : 0));
     max_blocks = std::max(max_blocks, nb);
+    c->h_nblk[s] = nb;
   }
   boff[nsub] = (int32_t)btab.size();
   c->release(c->d_blk_off);
@@ -1061,6 +1066,34 @@ static int multi_setup(fwgpu_context *c) {
   return FWGPU_OK;
 }
 
+// Size buckets of the batched sweep: the subdomains in interior-size order,
+// a new bucket where the size falls below 0.6 of the bucket's largest, so a
+// warp's vectors of many right-hand sides take shared memory for its own size
+// class, not for the largest subdomain of the model.
+static void set_multi_buckets(fwgpu_context *c) {
+  fw::MultiProblem &m = c->mp;
+  const fw::Plan &p = c->p;
+  const int n = (int)c->h_order.size();
+  m.n_buckets = 0;
+  int i = 0;
+  while (i < n) {
+    const int k = m.n_buckets;
+    const int lead = p.subs[c->h_order[i]].nI;
+    int j = i, mb = 0;
+    const bool last = k == fw::kMaxBuckets - 1;
+    while (j < n && (last || p.subs[c->h_order[j]].nI * 10 >= lead * 6 || j == i)) {
+      mb = std::max(mb, c->h_nblk[c->h_order[j]]);
+      j++;
+    }
+    m.bucket_first[k] = i;
+    m.bucket_count[k] = j - i;
+    m.bucket_max_interior[k] = std::max(1, lead);
+    m.bucket_max_blocks[k] = std::max(1, mb);
+    m.n_buckets++;
+    i = j;
+  }
+}
+
 static int read_multi_status(fwgpu_context *c) {
   FW_CUDA(cudaMemcpyAsync(c->h_ms, c->mp.ms, sizeof(fw::MultiScalars), cudaMemcpyDeviceToHost, c->stream));
   FW_CUDA(cudaStreamSynchronize(c->stream));
@@ -1082,6 +1115,7 @@ int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *
   const size_t smem = fw::multi_smem_bytes(c->dp.max_interior, c->dp.max_blocks, c->dp.stage_cap, fp32);
   if (fw::configure_multi(smem, fp32) != 0)
     return set_error(FWGPU_ERR_ARG, "batched sources: subdomains too large for shared memory");
+  set_multi_buckets(c);
   FW_TRY(multi_setup(c));
   fw::MultiProblem &m = c->mp;
   m.p = c->dp;
@@ -1103,7 +1137,7 @@ int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *
   fw::launch_multi_subsolve(m, fw::kModeFirst, fp32, c->stream);
   fw::launch_multi_set_status(m.ms, c->opts.hddm_eps, c->opts.hddm_max_loop, c->stream);
   fw::launch_multi_first(m, c->d_pcloc, c->stream);
-  const int per_iter = fw::multi_iteration_launches(fp32, c->dp.ir_steps);
+  const int per_iter = fw::multi_iteration_launches(fp32, c->dp.ir_steps, c->mp.n_buckets);
   c->launches += per_iter - 3 + 2;
   FW_CUDA(cudaGetLastError());
   FW_CUDA(cudaEventRecord(c->ev[1], c->stream));

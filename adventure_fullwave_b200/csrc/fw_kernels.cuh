@@ -113,6 +113,7 @@ enum SolveMode { kModeFirst = 0, kModeIter = 1, kModeLast = 2 };
 // right-hand-side minor ([row][kMaxRhs]), and each source runs its own COCG
 // (its own scalars and stopping) in lockstep with the others.
 constexpr int kMaxRhs = 16;
+constexpr int kMaxBuckets = 8;
 
 struct MultiScalars {
   CocgScalars s[kMaxRhs];
@@ -132,6 +133,11 @@ struct MultiProblem {
   double2 *PC;                  // [nfree]
   MultiScalars *ms;
   double *part;                 // [fields][n_part_blocks][kMaxRhs]
+  // sweep launches by subdomain size: bucket k covers sub_order[first[k] ..
+  // first[k] + count[k]) with shared memory for its largest subdomain
+  int n_buckets;
+  int bucket_first[kMaxBuckets], bucket_count[kMaxBuckets];
+  int bucket_max_interior[kMaxBuckets], bucket_max_blocks[kMaxBuckets];
 };
 
 size_t multi_smem_bytes(int max_interior, int max_blocks, int cap, bool fp32);
@@ -142,7 +148,7 @@ void launch_multi_first(const MultiProblem &m, const double2 *pcloc, cudaStream_
 void launch_multi_iteration(const MultiProblem &m, bool fp32, cudaStream_t stream);
 void launch_multi_edge_solution(const MultiProblem &m, int k, int64_t ne, const int64_t *edge_src, double2 *x,
                                 cudaStream_t stream);
-int multi_iteration_launches(bool fp32, int ir_steps);
+int multi_iteration_launches(bool fp32, int ir_steps, int n_buckets);
 
 void launch_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
                              const double *el_eps, const double *el_sigma, double omega, double *out,

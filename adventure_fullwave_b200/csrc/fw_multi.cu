@@ -128,7 +128,8 @@ __host__ __device__ inline MultiLayout multi_layout(int max_interior, int max_bl
 // each (c, r) with one writer.  y holds the warp's kRW sources, [row][kRW].
 template <typename T, int kRW>
 __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mode, const double2 *rhs,
-                                                        double2 *xout, T *zstash, int accumulate, MultiLayout lay) {
+                                                        double2 *xout, T *zstash, int accumulate, MultiLayout lay,
+                                                        int first) {
   constexpr int kQ = 32 / kRW;
   constexpr int kWarps = kR / kRW;
   if (multi_stopped(m, mode)) return;
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
   const int r = lane & (kRW - 1);
   const int h = lane / kRW;
   const int part = blockIdx.x % kWarps;  // which kRW sources
-  const int s = p.sub_order[blockIdx.x / kWarps];
+  const int s = p.sub_order[first + blockIdx.x / kWarps];
   const int64_t io = p.int_off[s];
   const int nI = (int)(p.int_off[s + 1] - io);
   const int b0 = p.blk_off[s];
@@ -503,29 +504,47 @@ int configure_multi(size_t smem, bool fp32) {
               : raise_smem_limit((const void *)multi_sweep_kernel<double2, kRwFp64>, 5, smem);
 }
 
+// The sweep, one launch per size bucket, each with the shared memory of its
+// largest subdomain (a single bucket of every subdomain when none are set).
+template <typename T, int kRW>
+static void launch_multi_sweep(const MultiProblem &m, int mode, bool fp32, const double2 *rhs, double2 *xout,
+                               T *zstash, int accumulate, cudaStream_t stream) {
+  const DevProblem &p = m.p;
+  const int nb = m.n_buckets > 0 ? m.n_buckets : 1;
+  for (int k = 0; k < nb; k++) {
+    const int first = m.n_buckets > 0 ? m.bucket_first[k] : 0;
+    const int count = m.n_buckets > 0 ? m.bucket_count[k] : p.nsub;
+    const int mi = m.n_buckets > 0 ? m.bucket_max_interior[k] : p.max_interior;
+    const int mb = m.n_buckets > 0 ? m.bucket_max_blocks[k] : p.max_blocks;
+    if (count <= 0) continue;
+    const MultiLayout lay = multi_layout(mi, mb, p.stage_cap, fp32, kRW);
+    multi_sweep_kernel<T, kRW><<<(unsigned)count * (kR / kRW), 32, lay.total, stream>>>(m, mode, rhs, xout, zstash,
+                                                                                       accumulate, lay, first);
+  }
+}
+
 void launch_multi_subsolve(const MultiProblem &m, int mode, bool fp32, cudaStream_t stream) {
   const DevProblem &p = m.p;
-  const MultiLayout lay =
-      multi_layout(p.max_interior, p.max_blocks, p.stage_cap, fp32, fp32 ? kRwFp32 : kRwFp64);
   const unsigned gi = grid_for(p.n_interior * kR, 256), gs = grid_for(p.n_slots * kR, 256);
   double2 *rhs = fp32 ? m.B : m.Y;
   multi_rhs_kernel<<<gi, 256, 0, stream>>>(m, mode, rhs);
   if (fp32) {
     float2 *zs = (float2 *)m.Zs;
-    const unsigned g = p.nsub * (kR / kRwFp32);
-    multi_sweep_kernel<float2, kRwFp32><<<g, 32, lay.total, stream>>>(m, mode, m.B, m.Y, zs, 0, lay);
+    launch_multi_sweep<float2, kRwFp32>(m, mode, true, m.B, m.Y, zs, 0, stream);
     for (int k = 0; k < p.ir_steps; k++) {
       multi_residual_kernel<<<gi, 256, 0, stream>>>(m, mode);
-      multi_sweep_kernel<float2, kRwFp32><<<g, 32, lay.total, stream>>>(m, mode, m.Rres, m.Y, zs, 1, lay);
+      launch_multi_sweep<float2, kRwFp32>(m, mode, true, m.Rres, m.Y, zs, 1, stream);
     }
   } else {
-    const unsigned g = p.nsub * (kR / kRwFp64);
-    multi_sweep_kernel<double2, kRwFp64><<<g, 32, lay.total, stream>>>(m, mode, m.Y, m.Y, (double2 *)m.Zs, 0, lay);
+    launch_multi_sweep<double2, kRwFp64>(m, mode, false, m.Y, m.Y, (double2 *)m.Zs, 0, stream);
   }
   multi_iface_kernel<<<gs, 256, 0, stream>>>(m, mode);
 }
 
-int multi_iteration_launches(bool fp32, int ir_steps) { return 3 + (fp32 ? 2 * ir_steps : 0) + 3; }
+int multi_iteration_launches(bool fp32, int ir_steps, int n_buckets) {
+  const int nb = n_buckets > 0 ? n_buckets : 1;
+  return 2 + nb * (fp32 ? 1 + ir_steps : 1) + (fp32 ? ir_steps : 0) + 3;
+}
 
 void launch_multi_set_status(MultiScalars *ms, double eps, int32_t max_loop, cudaStream_t stream) {
   multi_set_status_kernel<<<1, 1, 0, stream>>>(ms, eps, max_loop);
