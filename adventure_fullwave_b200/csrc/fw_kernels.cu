@@ -1312,7 +1312,10 @@ void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stre
   if (p.solve_variant == kSolveWarp) {
     const StageLayout lay = stage_layout(p.max_interior, p.max_blocks, p.stage_cap, fp32);
     double2 *rhs = fp32 ? p.B : p.Y;
-    rhs_kernel<4><<<blocks_min1(p.n_interior * 4, 256), 256, 0, stream>>>(p, mode, rhs);
+    // one thread per row for both products: their rows are short (a few to a
+    // few tens of entries) and the loads of several entries in flight per
+    // thread beat lanes sharing a row (timed with 1, 2, 4 and 8 lanes)
+    rhs_kernel<1><<<blocks_min1(p.n_interior, 256), 256, 0, stream>>>(p, mode, rhs);
     if (fp32) {
       subsolve_staged_kernel<float2><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.B, p.Y, p.Y32, 0,
                                                                                        lay);
@@ -1325,7 +1328,7 @@ void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stre
       subsolve_staged_kernel<double2><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.Y, p.Y, p.Y, 0,
                                                                                           lay);
     }
-    iface_product_kernel<4><<<blocks_min1(p.n_slots * 4, 256), 256, 0, stream>>>(p, mode);
+    iface_product_kernel<1><<<blocks_min1(p.n_slots, 256), 256, 0, stream>>>(p, mode);
     return;
   }
   if (p.solve_variant == kSolveCta && p.cta_smem > 0) {
