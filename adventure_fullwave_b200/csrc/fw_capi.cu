@@ -588,7 +588,10 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   FW_TRY(c->alloc(&dp.U, nf));
   FW_TRY(c->alloc(&dp.PC, nf));
   // COCG grid: at most 4 CTAs of 256 threads per SM (timed against 2, 8 and 16)
-  int nb = (int)std::min<int64_t>((p.total_free + 255) / 256, 4 * 148);
+  int n_sm = 148;
+  if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, opts->device) != cudaSuccess || n_sm <= 0)
+    n_sm = 148;
+  int nb = (int)std::min<int64_t>((p.total_free + 255) / 256, 4 * (int64_t)n_sm);
   if (nb < 1) nb = 1;
   dp.n_part_blocks = nb;
   FW_TRY(c->alloc(&dp.part, 8 * (size_t)nb));
