@@ -528,8 +528,12 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
         pec[eidx[g]] = True
     crd = g_crd[vert_g]
     flags = np.union1d(mat.eps_flag, mat.sigma_flag).astype(np.int32)
-    eps_of = dict(zip(mat.eps_flag.tolist(), mat.eps.tolist()))
-    sig_of = dict(zip(mat.sigma_flag.tolist(), mat.sigma.tolist()))
+    # the reference takes the first entry of a flag listed twice (make_elem_em.c:98-109)
+    eps_of, sig_of = {}, {}
+    for f, v in zip(mat.eps_flag.tolist(), mat.eps.tolist()):
+        eps_of.setdefault(f, v)
+    for f, v in zip(mat.sigma_flag.tolist(), mat.sigma.tolist()):
+        sig_of.setdefault(f, v)
     model = meshgen.Model(
         name=name or os.path.basename(os.path.abspath(model_dir)), n=0,
         size=float(np.max(crd.max(axis=0) - crd.min(axis=0))), vertex_crd=np.ascontiguousarray(crd),
