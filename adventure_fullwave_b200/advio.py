@@ -540,7 +540,8 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
         tets=tets, tet_edges=tet_edges, edges=edges, flag=el_flag,
         mat_flag=flags, mat_eps=np.array([eps_of.get(f, 0.0) for f in flags.tolist()]),
         mat_sigma=np.array([sig_of.get(f, 0.0) for f in flags.tolist()]), omega=mat.omega, pec_edge=pec,
-        sub_of_tet=el_sub, nsub=sub, sources=[])
+        sub_of_tet=el_sub, nsub=sub, sources=[],
+        eps_table=(mat.eps_flag.copy(), mat.eps.copy()), sigma_table=(mat.sigma_flag.copy(), mat.sigma.copy()))
     vpath = os.path.join(model_dir, "volt.dat")
     boxes, volts = read_volt(vpath) if os.path.exists(vpath) else (np.zeros((0, 6)), np.zeros(0))
     if volts.shape[0] > 0:

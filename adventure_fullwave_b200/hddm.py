@@ -144,12 +144,19 @@ class HddmSolver:
         a["mf"] = np.ascontiguousarray(model.mat_flag, dtype=np.int32)
         a["me"] = np.ascontiguousarray(model.mat_eps, dtype=np.float64)
         a["ms"] = np.ascontiguousarray(model.mat_sigma, dtype=np.float64)
+        a["ef"], a["sf"] = a["mf"], a["mf"]
+        if getattr(model, "eps_table", None) is not None:
+            a["ef"] = np.ascontiguousarray(model.eps_table[0], dtype=np.int32)
+            a["me"] = np.ascontiguousarray(model.eps_table[1], dtype=np.float64)
+        if getattr(model, "sigma_table", None) is not None:
+            a["sf"] = np.ascontiguousarray(model.sigma_table[0], dtype=np.int32)
+            a["ms"] = np.ascontiguousarray(model.sigma_table[1], dtype=np.float64)
         mesh = _lib.FwMesh(
             int(a["crd"].shape[0]), _ptr(a["crd"], ctypes.c_double), int(a["tv"].shape[0]),
             _ptr(a["tv"], ctypes.c_int32), _ptr(a["te"], ctypes.c_int32), _ptr(a["flag"], ctypes.c_int32),
             int(a["pec"].shape[0]), _ptr(a["pec"], ctypes.c_uint8), int(model.nsub), _ptr(a["sub"], ctypes.c_int32))
-        mt = _lib.FwMaterial(int(a["mf"].shape[0]), _ptr(a["mf"], ctypes.c_int32), _ptr(a["me"], ctypes.c_double),
-                             int(a["mf"].shape[0]), _ptr(a["mf"], ctypes.c_int32), _ptr(a["ms"], ctypes.c_double),
+        mt = _lib.FwMaterial(int(a["ef"].shape[0]), _ptr(a["ef"], ctypes.c_int32), _ptr(a["me"], ctypes.c_double),
+                             int(a["sf"].shape[0]), _ptr(a["sf"], ctypes.c_int32), _ptr(a["ms"], ctypes.c_double),
                              float(model.omega))
         prec = {"fp64": _lib.PREC_FP64, "fp32_ir": _lib.PREC_FP32_IR}[precision]
         self.precision = precision

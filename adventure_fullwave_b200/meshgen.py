@@ -88,6 +88,10 @@ class Model:
     probe_edges: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, np.int32))
     # element right-hand side (delta-gap voltages or antenna currents), or None
     element_source: Optional[ElementSource] = None
+    # the Permittivity and Conductor lists as a model file gives them, when
+    # they differ from the joint table above: (flags, values) each
+    eps_table: Optional[Tuple[np.ndarray, np.ndarray]] = None
+    sigma_table: Optional[Tuple[np.ndarray, np.ndarray]] = None
 
     @property
     def n_vertices(self) -> int:
