@@ -21,6 +21,8 @@ ERR_NOT_CONVERGED = -4
 ERR_BREAKDOWN = -5
 ERR_NOMEM = -6
 ERR_MESH = -7
+ERR_NONFINITE = -8
+ERR_TIMEOUT = -9
 NOALLOC_MAX_ROWS = 262144
 
 PREC_FP64 = 0

@@ -344,12 +344,19 @@ int set_element_source(fwgpu_context *c, const fwgpu_element_source *es) {
   return FWGPU_OK;
 }
 
+// The copy-timeout word is raised by the subdomain solves and cleared only
+// here, at the start of a solve, so that no later launch hides it.
+int clear_copy_timeout(fwgpu_context *c) {
+  FW_CUDA(cudaMemsetAsync(&c->d_sc->copy_timeout, 0, sizeof(int32_t), c->stream));
+  return FWGPU_OK;
+}
+
 int read_status(fwgpu_context *c, int32_t *status) {
   FW_CUDA(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(fw::CocgScalars), cudaMemcpyDeviceToHost, c->stream));
   FW_CUDA(cudaStreamSynchronize(c->stream));
   if (status) *status = c->h_sc->status;
-  if (c->h_sc->pad != 0)
-    return set_error(FWGPU_ERR_CUDA, "subdomain solve gave up waiting for a TMA copy");
+  if (c->h_sc->copy_timeout != 0)
+    return set_error(FWGPU_ERR_TIMEOUT, "subdomain solve gave up waiting for a staged copy");
   return FWGPU_OK;
 }
 
@@ -907,6 +914,7 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (c->stage < 1) return set_error(FWGPU_ERR_STATE, "solve_dom_1st before make_tmp_aij");
   FW_CUDA(cudaSetDevice(c->opts.device));
+  FW_TRY(clear_copy_timeout(c));
   const fw::Plan &p = c->p;
   const int nsub = c->m.nsub;
   const int64_t ndof = p.sub_dof_off[nsub];
@@ -995,6 +1003,8 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
   FW_CUDA(cudaGetLastError());
   c->stage = 2;
   if (c->factor_bad) return set_error(FWGPU_ERR_BREAKDOWN, "zero or non-finite pivot in a subdomain factor");
+  // the timing launches and the first solve above
+  FW_TRY(read_status(c, nullptr));
   return FWGPU_OK;
 }
 
@@ -1101,7 +1111,7 @@ static void set_multi_buckets(fwgpu_context *c) {
 static int read_multi_status(fwgpu_context *c) {
   FW_CUDA(cudaMemcpyAsync(c->h_ms, c->mp.ms, sizeof(fw::MultiScalars), cudaMemcpyDeviceToHost, c->stream));
   FW_CUDA(cudaStreamSynchronize(c->stream));
-  if (c->h_ms->err != 0) return set_error(FWGPU_ERR_CUDA, "subdomain solve gave up waiting for a TMA copy");
+  if (c->h_ms->err != 0) return set_error(FWGPU_ERR_TIMEOUT, "subdomain solve gave up waiting for a staged copy");
   return FWGPU_OK;
 }
 
@@ -1138,6 +1148,7 @@ int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *
                                 nG, cudaMemcpyDeviceToDevice, c->stream));
   }
   FW_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  FW_CUDA(cudaMemsetAsync(&m.ms->err, 0, sizeof(int32_t), c->stream));
   fw::launch_multi_subsolve(m, fw::kModeFirst, fp32, c->stream);
   fw::launch_multi_set_status(m.ms, c->opts.hddm_eps, c->opts.hddm_max_loop, c->stream);
   fw::launch_multi_first(m, c->d_pcloc, c->stream);
@@ -1169,7 +1180,7 @@ int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *
   cudaEventElapsedTime(&ms0, c->ev[0], c->ev[1]);
   cudaEventElapsedTime(&ms1, c->ev[1], c->ev[2]);
   cudaEventElapsedTime(&ms2, c->ev[2], c->ev[3]);
-  int all_conv = 1;
+  int all_conv = 1, any_bad = 0;
   for (int k = 0; k < n_src; k++) {
     const fw::CocgScalars &sc = c->h_ms->s[k];
     res[k].iterations = sc.loop - 1;
@@ -1186,8 +1197,10 @@ int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *
     res[k].stage_warps = c->dp.stage_warps;
     res[k].reserved = 0;
     all_conv &= sc.converged;
+    any_bad |= sc.nonfinite;
   }
   c->multi_n = n_src;
+  if (any_bad) return set_error(FWGPU_ERR_NONFINITE, "an interface residual became NaN or infinite");
   return all_conv ? FWGPU_OK : set_error(FWGPU_ERR_NOT_CONVERGED, "hddm_max_loop reached before hddm_eps");
 }
 
@@ -1273,8 +1286,8 @@ int fwgpu_solve_dom_last(fwgpu_context *c) {
   fw::launch_edge_solution(c->dp, c->m.ne, c->d_edge_src, c->dp.Y, c->dp.V, c->d_xedge, c->stream);
   c->launches += 1 + fw::subsolve_launches(c->dp, c->opts.precision == FWGPU_PREC_FP32_IR);
   FW_CUDA(cudaGetLastError());
-  FW_CUDA(cudaStreamSynchronize(c->stream));
   c->stage = 4;
+  FW_TRY(read_status(c, nullptr));
   c->xedge_ok = !c->sharded;
   return FWGPU_OK;
 }
@@ -1322,6 +1335,7 @@ static int fill_result(fwgpu_context *c, fwgpu_result *res) {
     res->stage_warps = c->dp.solve_variant == fw::kSolveWarp ? c->dp.stage_warps : 0;
     res->reserved = 0;
   }
+  if (sc.nonfinite) return set_error(FWGPU_ERR_NONFINITE, "the interface residual became NaN or infinite");
   return sc.converged ? FWGPU_OK : set_error(FWGPU_ERR_NOT_CONVERGED, "hddm_max_loop reached before hddm_eps");
 }
 
@@ -1349,6 +1363,7 @@ int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *
   if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "resolve before the factors exist");
   FW_CUDA(cudaSetDevice(c->opts.device));
   FW_CUDA(cudaEventRecord(c->ev[0], c->stream));
+  FW_TRY(clear_copy_timeout(c));
   c->launches = 1;
   FW_TRY(build_rhs(c, src));
   fw::launch_subsolve(c->dp, fw::kModeFirst, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);

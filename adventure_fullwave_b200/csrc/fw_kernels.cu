@@ -890,7 +890,7 @@ __global__ void __launch_bounds__(64) subsolve_staged_kernel(DevProblem p, int m
   st.bar = (uint64_t *)(smem_raw + lay.bar);
   st.blk = blk;
   st.uses0 = st.uses1 = 0;
-  st.err = &p.sc->pad;
+  st.err = &p.sc->copy_timeout;
   const int64_t base = p.env_ptr[io];
   st.L = (sizeof(T) == 8 ? (const T *)(const void *)p.L32 : (const T *)(const void *)p.L64) + base;
   for (int b = tid; b <= nblk; b += nt) blk[b] = p.blk_tab[b0 + b];
@@ -1105,16 +1105,18 @@ __global__ void cocg_first_scalars_kernel(DevProblem p) {
   const double l2 = reduce_partials(p.part, nb, kFL2, false, sh);
   if (threadIdx.x == 0) {
     CocgScalars *sc = p.sc;
+    // fmax drops NaN, so a non-finite residual shows in the sums only
+    const bool bad = !isfinite(mx) || !isfinite(l2) || !isfinite(rzr) || !isfinite(rzi);
     sc->norm0 = mx;
     sc->l2_0 = sqrt(l2);
-    sc->status = mx < kNearlyZero ? 1 : 0;
+    sc->status = (bad || mx < kNearlyZero) ? 1 : 0;
     sc->r0inv = 1.0 / mx;
     sc->rz = make_double2(rzr, rzi);
-    sc->pad = 0;
     sc->resi = 1.0;
     sc->resi_l2 = 1.0;
     sc->loop = 1;
-    sc->converged = mx < kNearlyZero ? 1 : 0;
+    sc->converged = (!bad && mx < kNearlyZero) ? 1 : 0;
+    sc->nonfinite = bad ? 1 : 0;
   }
 }
 
@@ -1199,7 +1201,11 @@ __global__ void cocg_update_kernel(DevProblem p) {
       sc->beta = cdiv_ref(rz, sc->rz);
     }
     sc->rz = rz;
-    if (resi < sc->eps) {
+    if (!isfinite(l2_t) || !isfinite(rzr_t) || !isfinite(rzi_t)) {
+      // the reference would run on to hddm_max_loop; stop and report it
+      sc->status = 1;
+      sc->nonfinite = 1;
+    } else if (resi < sc->eps) {
       sc->status = 1;
       sc->converged = 1;
     } else if (sc->loop >= sc->max_loop) {
@@ -1246,7 +1252,7 @@ __global__ void set_status_kernel(CocgScalars *sc, double eps, int32_t max_loop)
   sc->max_loop = max_loop;
   sc->status = 0;
   sc->converged = 0;
-  sc->pad = 0;
+  sc->nonfinite = 0;
 }
 
 // iteration state for kernel timing: never converges, no loop limit

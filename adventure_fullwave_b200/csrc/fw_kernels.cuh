@@ -26,7 +26,9 @@ struct CocgScalars {
   int32_t max_loop;  // hddm_max_loop
   int32_t converged;
   int32_t factor_status;  // non-zero: a pivot was zero or not finite
-  int32_t pad;       // non-zero: a subdomain solve gave up waiting for a copy
+  int32_t copy_timeout;   // non-zero: a subdomain solve gave up waiting for a copy (cleared by the host only)
+  int32_t nonfinite;      // non-zero: the interface residual or (r, z) was not finite; the loop stopped
+  int32_t unused;
   uint32_t ticket[4];  // CTAs of a reduction kernel that wrote their partials (last one reduces)
 };
 

@@ -314,9 +314,9 @@ __global__ void multi_set_status_kernel(MultiScalars *ms, double eps, int32_t ma
     ms->s[r].max_loop = max_loop;
     ms->s[r].status = 0;
     ms->s[r].converged = 0;
+    ms->s[r].nonfinite = 0;
   }
   ms->all_status = 0;
-  ms->err = 0;
   for (int i = 0; i < 4; i++) ms->ticket[i] = 0;
 }
 
@@ -363,8 +363,10 @@ __global__ void multi_first_kernel(MultiProblem m, const double2 *__restrict__ p
     c.resi = 1.0;
     c.resi_l2 = 1.0;
     c.loop = 1;
-    c.status = vmx < kNearlyZero ? 1 : 0;
-    c.converged = vmx < kNearlyZero ? 1 : 0;
+    const bool bad = !isfinite(vmx) || !isfinite(vl2) || !isfinite(vrr) || !isfinite(vri);
+    c.status = (bad || vmx < kNearlyZero) ? 1 : 0;
+    c.converged = (!bad && vmx < kNearlyZero) ? 1 : 0;
+    c.nonfinite = bad ? 1 : 0;
   }
   if (threadIdx.x == 0) m.ms->ticket[0] = 0;
 }
@@ -441,7 +443,10 @@ __global__ void multi_update_kernel(MultiProblem m) {
       const double2 rz = make_double2(vrr, vri);
       c.beta = (cabs_ref(rz) < kNearlyZero && cabs_ref(c.rz) < kNearlyZero) ? cz() : cdiv_ref(rz, c.rz);
       c.rz = rz;
-      if (resi < c.eps) {
+      if (!isfinite(vl2) || !isfinite(vrr) || !isfinite(vri)) {
+        c.status = 1;
+        c.nonfinite = 1;
+      } else if (resi < c.eps) {
         c.status = 1;
         c.converged = 1;
       } else if (c.loop >= c.max_loop) {

@@ -15,13 +15,14 @@
 // host threads) use the same rows of the array and race: the caller must
 // order them on one stream or synchronise between them.
 //
-// The device address of the array is looked up once per device, on the
-// first call made while that device is current; that first call should
-// therefore come before any stream capture the caller starts.
+// The device address of the array is looked up on every call, in the
+// context current on the calling thread: after a cudaDeviceReset, or from a
+// context of the caller's own, the library's module is loaded again and the
+// array has a new address.  The first call in a context loads the module,
+// so it should come before any stream capture the caller starts.
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "../../include/fwgpu.h"
@@ -33,10 +34,6 @@ namespace {
 constexpr int64_t kNoAllocMaxRows = FWGPU_NOALLOC_MAX_ROWS;
 static __device__ __align__(256) double2 g_noalloc_work[kNoAllocMaxRows];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-double2 *g_work_ptr[kMaxDevices] = {nullptr};
-
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -45,11 +42,12 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 // columns idx1[i]..i at mat[idx2[i] + j], unit L off the diagonal and 1/d
 // on it (advlas_skyline.c:12-25,79-128).  Forward row dot products, scaling
 // by 1/d, backward column updates (advlas_skyline_ldl_solve, :134-167).
+// b and x may be the same buffer: a system reads all its rows of b before
+// it writes any row of x, and systems do not share rows.
 __global__ void skyline_solve_noalloc_kernel(int32_t n_systems, int32_t total_rows, const int32_t *__restrict__ row_off,
                                              const int64_t *__restrict__ mat_off, const int32_t *__restrict__ idx1,
                                              const int32_t *__restrict__ idx2, const double2 *__restrict__ mat,
-                                             const double2 *__restrict__ b, double2 *__restrict__ x,
-                                             double2 *__restrict__ work) {
+                                             const double2 *b, double2 *x, double2 *__restrict__ work) {
   const int s = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (s >= n_systems) return;
   const int lane = threadIdx.x & 31;
@@ -63,9 +61,13 @@ __global__ void skyline_solve_noalloc_kernel(int32_t n_systems, int32_t total_ro
   double2 *w = work + r0;
   for (int i = lane; i < n; i += 32) w[i] = b[r0 + i];
   __syncwarp();
+  // a first column outside [0, i] would reach rows of the shared work array
+  // that belong to other systems: it is clamped (the result of such a
+  // malformed system is meaningless, but no other system's rows are touched)
   for (int i = 1; i < n; i++) {
     double re = 0.0, im = 0.0;
-    for (int j = i1[i] + lane; j < i; j += 32) {
+    const int lo = min(max(i1[i], 0), i);
+    for (int j = lo + lane; j < i; j += 32) {
       const double2 t = cmul(m[i2[i] + j], w[j]);
       re += t.x;
       im += t.y;
@@ -81,7 +83,8 @@ __global__ void skyline_solve_noalloc_kernel(int32_t n_systems, int32_t total_ro
   __syncwarp();
   for (int i = n - 1; i >= 1; i--) {
     const double2 xi = w[i];
-    for (int j = i1[i] + lane; j < i; j += 32) {
+    const int lo = min(max(i1[i], 0), i);
+    for (int j = lo + lane; j < i; j += 32) {
       const double2 t = cmul(m[i2[i] + j], xi);
       w[j] = make_double2(w[j].x - t.x, w[j].y - t.y);
     }
@@ -117,20 +120,13 @@ extern "C" int fwgpu_skyline_solve_noalloc(int32_t n_systems, int32_t total_rows
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return noalloc_error(FWGPU_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return noalloc_error(FWGPU_ERR_ARG, "device ordinal beyond the supported range");
-  double2 *work = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_work_ptr[dev]) {
-      // once per device, with that device current
-      void *ptr = nullptr;
-      e = cudaGetSymbolAddress(&ptr, g_noalloc_work);
-      if (e != cudaSuccess)
-        return noalloc_error(FWGPU_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      g_work_ptr[dev] = (double2 *)ptr;
-    }
-    work = g_work_ptr[dev];
-  }
+  // the array's address in the current context (a host-side name of a
+  // __device__ array is not a device address)
+  void *ptr = nullptr;
+  e = cudaGetSymbolAddress(&ptr, g_noalloc_work);
+  if (e != cudaSuccess)
+    return noalloc_error(FWGPU_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  double2 *work = (double2 *)ptr;
   const int threads = 128;
   const unsigned blocks = (unsigned)(((int64_t)n_systems * 32 + threads - 1) / threads);
   skyline_solve_noalloc_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define FWGPU_ABI_VERSION 2
+#define FWGPU_ABI_VERSION 3
 
 enum {
   FWGPU_OK = 0,
@@ -39,7 +39,12 @@ enum {
   FWGPU_ERR_NOT_CONVERGED = -4, /* COCG hit hddm_max_loop before hddm_eps */
   FWGPU_ERR_BREAKDOWN = -5,     /* zero or non-finite pivot in a subdomain factor */
   FWGPU_ERR_NOMEM = -6,         /* device allocation failed */
-  FWGPU_ERR_MESH = -7           /* degenerate or negatively oriented element */
+  FWGPU_ERR_MESH = -7,          /* degenerate or negatively oriented element */
+  FWGPU_ERR_NONFINITE = -8,     /* the interface residual or (r, z) became NaN or infinite (e.g. a
+                                   non-finite right-hand side); the loop stopped at once, where the
+                                   reference would run on to hddm_max_loop */
+  FWGPU_ERR_TIMEOUT = -9        /* a subdomain solve gave up waiting for one of its staged copies
+                                   (every wait on the device is bounded); the solution is invalid */
 };
 
 /* precision of the subdomain factors */
@@ -383,11 +388,19 @@ int fwgpu_shard_iterate_finish(fwgpu_context *ctx, int32_t *status);
  * `stream` (a cudaStream_t, NULL for the default stream) and the call
  * returns without synchronising.
  *
+ * d_row_off must be non-decreasing with d_row_off[0] >= 0 and
+ * d_row_off[n_systems] <= total_rows; a system whose rows fall outside
+ * [0, total_rows) is skipped and its rows of d_x keep what they held.
+ * idx1[i] must lie in [0, i]; a value outside is clamped, which keeps the
+ * other systems' results intact but makes that system's result
+ * meaningless.  d_b may equal d_x (an in-place solve).
+ *
  * total_rows may not exceed FWGPU_NOALLOC_MAX_ROWS (FWGPU_ERR_ARG
- * otherwise).  The first call on each device looks up the work array's
- * device address, so make it before any stream capture.  All calls share
- * the work array: calls whose kernels overlap on one GPU race and must be
- * ordered by the caller. */
+ * otherwise).  Every call looks up the work array's address in the context
+ * current on the calling thread; the first call in a context (also after a
+ * cudaDeviceReset) loads the library's device code into it, so make it
+ * before any stream capture.  All calls share the work array: calls whose
+ * kernels overlap on one GPU race and must be ordered by the caller. */
 int fwgpu_skyline_solve_noalloc(int32_t n_systems, int32_t total_rows, const int32_t *d_row_off,
                                 const int64_t *d_mat_off, const int32_t *d_idx1, const int32_t *d_idx2,
                                 const double *d_mat, const double *d_b, double *d_x, void *stream);

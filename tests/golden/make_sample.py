@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 
 from adventure_fullwave_b200 import advio  # noqa: E402
 
-SAMPLE = "/root/reference/main/fullwave/MODEL"
+SAMPLE = os.path.join(os.environ.get("FW_REFERENCE", "/root/reference"), "main", "fullwave", "MODEL")
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "fw_ref_harness")
 EPS = 1e-6
 STRIDE = 53

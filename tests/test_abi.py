@@ -41,7 +41,7 @@ def test_binding_covers_header():
 def test_abi_version():
     from adventure_fullwave_b200 import _lib
 
-    assert _lib.load().fwgpu_abi_version() == 2
+    assert _lib.load().fwgpu_abi_version() == 3
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")

@@ -10,7 +10,7 @@ import pytest
 from adventure_fullwave_b200 import advio, meshgen
 from helpers import golden
 
-SAMPLE = "/root/reference/main/fullwave/MODEL"
+SAMPLE = os.path.join(os.environ.get("FW_REFERENCE", "/root/reference"), "main", "fullwave", "MODEL")
 
 
 @pytest.mark.parametrize("name", ["layered", "gap"])

@@ -1,0 +1,73 @@
+"""Failure paths of the C ABI on the GPU, each made on the host from bad
+input (no GPU fault is involved): a negatively oriented element, a
+subdomain whose matrix is singular, and a non-finite right-hand side.
+
+The reference has no error handling for any of these: emessage() exits on
+a negative volume (lib/fem/tetrahedral.c tet_Volume6 users), a zero pivot
+gives inf silently (lib/hddm/advlas_skyline.c:122), and a NaN residual
+runs COCG on to hddm_max_loop (lib/hddm/hddm_solver_s.h:318-379).  The
+library returns status codes instead."""
+import numpy as np
+import pytest
+
+from adventure_fullwave_b200 import _lib, hddm, meshgen
+
+pytestmark = pytest.mark.gpu
+
+
+def _model(**kw):
+    m = meshgen.make_model("x", n=6, size=1.0, npml=1, nleaves=6, seed=1, **kw)
+    meshgen.round_trip_material(m)
+    return m
+
+
+def test_inverted_element_is_a_mesh_error():
+    m = _model()
+    # the same tet with vertices 1 and 2 swapped: edges relabelled to match
+    # (01,02,03,12,23,13 -> 02,01,03,12,13,23), orientation negative
+    t = 5
+    m.tets = m.tets.copy()
+    m.tet_edges = m.tet_edges.copy()
+    m.tets[t] = m.tets[t][[0, 2, 1, 3]]
+    m.tet_edges[t] = m.tet_edges[t][[1, 0, 2, 3, 5, 4]]
+    with hddm.HddmSolver(m, hddm_eps=1e-6) as s:
+        with pytest.raises(_lib.FwgpuError) as e:
+            s.make_tmp_aij(0)
+        assert e.value.code == _lib.ERR_MESH
+
+
+def test_singular_subdomain_is_a_breakdown():
+    m = _model()
+    # a flag in neither the Permittivity nor the Conductor table gives zero
+    # element matrices: every interior row of subdomain 0 is zero
+    absent = int(m.mat_flag.max()) + 7
+    m.flag = np.where(m.sub_of_tet == 0, absent, m.flag).astype(np.int32)
+    with hddm.HddmSolver(m, hddm_eps=1e-6) as s:
+        s.make_tmp_aij(0)
+        with pytest.raises(_lib.FwgpuError) as e:
+            s.solve_dom_1st()
+        assert e.value.code == _lib.ERR_BREAKDOWN
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_ir"])
+def test_nan_source_stops_the_loop(precision):
+    m = _model()
+    edges, vals = m.sources[0]
+    bad = (edges, np.where(np.arange(vals.shape[0]) == 0, complex(np.nan, 0.0), vals))
+    with hddm.HddmSolver(m, hddm_eps=1e-10, hddm_max_loop=3000, precision=precision) as s:
+        with pytest.raises(_lib.FwgpuError) as e:
+            s.solve(bad)
+        assert e.value.code == _lib.ERR_NONFINITE
+        # the context stays usable: a finite source solves normally
+        r = s.resolve(0)
+        assert r.converged and np.isfinite(s.edge_solution()).all()
+
+
+def test_nan_source_in_a_batch_stops_that_source_only():
+    m = _model(nsources=2)
+    edges, vals = m.sources[0]
+    bad = (edges, np.full(vals.shape[0], complex(np.inf, 0.0)))
+    with hddm.HddmSolver(m, hddm_eps=1e-8, hddm_max_loop=3000) as s:
+        with pytest.raises(_lib.FwgpuError) as e:
+            s.solve_multi([m.sources[1], bad])
+        assert e.value.code == _lib.ERR_NONFINITE

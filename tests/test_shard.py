@@ -1,4 +1,4 @@
-"""The sharded HDDM solve (one rank per GPU, SURVEY-style p-mode parts):
+"""The sharded HDDM solve (one rank per GPU, the reference's p-mode parts):
 subdomain ranges, and the rank protocol of ``shard.run_sharded`` with two
 gloo ranks on the CPU, against the oracle's single-process solve."""
 import multiprocessing as mp
