@@ -103,6 +103,9 @@ static void (*ref_make_TMP_AIJ)(DomMesh *, MTRL) = NULL;
 static void (*ref_solve_dom_1st)(DomMesh *, HDDM_Opt, SolvOpt, int (*)(AIJ_MAT *, SolvOpt, FILE *),
                                  HDDM_DOM_VEC *, int (*)(TMP_AIJ, HDDM_DOM_VEC *), FILE *) = NULL;
 static void (*ref_iteration_s)(PartMesh *, HDDM_VEC *, HDDM_Opt, int (*)(HDDM_VEC *)) = NULL;
+static void (*ref_iteration_s_1st)(PartMesh *, HDDM_VEC *, HDDM_Opt, int (*)(HDDM_VEC *),
+                                   void (*)(OPinfo **, HDDM_VEC *)) = NULL;
+static FILE *f_hist = NULL;
 static void (*ref_solve_dom_last)(DomMesh *, SolvOpt, int (*)(AIJ_MAT *, SolvOpt, FILE *), HDDM_DOM_VEC *,
                                   FILE *) = NULL;
 
@@ -157,8 +160,36 @@ static void harness_solve_dom_1st(DomMesh *dm, HDDM_Opt hddm_opt, SolvOpt solvop
   }
 }
 
+/* max |r| over the parts' interface residuals, in the loop order and with
+   the ComplexAbs of ITERATION_S (lib/hddm/hddm_solver_s.h:196-200,300-318) */
+static double residual_max(HDDM_VEC *hv) {
+  double m = 0.0;
+  for (int part = 0; part < COM_GID.nparent; part++)
+    for (int i = 0; i < hv[part].infree; i++) {
+      const double t = ComplexAbs(hv[part].r_c[i]);
+      if (t > m) m = t;
+    }
+  return m;
+}
+
+/* the residual history at full precision (the log prints 7 digits): the
+   initial max-norm, then resi = max|r| * r0 after every iteration */
+static void harness_iteration_s_1st(PartMesh *pm, HDDM_VEC *hv, HDDM_Opt hddm_opt, int (*setPC)(HDDM_VEC *),
+                                    void (*gatherPC_s)(OPinfo **, HDDM_VEC *)) {
+  ref_iteration_s_1st(pm, hv, hddm_opt, setPC, gatherPC_s);
+  if (f_hist) {
+    const double n0 = residual_max(hv);
+    fwrite(&n0, sizeof(double), 1, f_hist);
+  }
+}
+
 static void harness_iteration_s(PartMesh *pm, HDDM_VEC *hv, HDDM_Opt hddm_opt, int (*setPC)(HDDM_VEC *)) {
   ref_iteration_s(pm, hv, hddm_opt, setPC);
+  if (f_hist) {
+    double resi = residual_max(hv);
+    resi *= hv[0].r0;
+    fwrite(&resi, sizeof(double), 1, f_hist);
+  }
   double t = t_now();
   if (t_iter_mark >= 0.0) t_iter_total += t - t_iter_mark;
   t_iter_mark = t;
@@ -177,7 +208,9 @@ static void set_hddm_func_harness(HDDM_FUNC *f, OPTIONS options) {
   ref_make_TMP_AIJ = f->make_TMP_AIJ;
   ref_solve_dom_1st = f->solve_dom_1st;
   ref_iteration_s = f->iteration_s;
+  ref_iteration_s_1st = f->iteration_s_1st;
   ref_solve_dom_last = f->solve_dom_last;
+  f->iteration_s_1st = harness_iteration_s_1st;
   f->make_TMP_AIJ = harness_make_TMP_AIJ;
   f->solve_dom_1st = harness_solve_dom_1st;
   f->iteration_s = harness_iteration_s;
@@ -480,9 +513,15 @@ int main(int argc, char **argv) {
 
   hddm_sw.t_loop = -2;
   hddm_sw.antenna = -1;
+  {
+    char path[FILENAME_MAX];
+    snprintf(path, sizeof(path), "%s.hist", g_prefix);
+    f_hist = fopen(path, "wb");
+  }
   double t1 = t_now();
   hddm_solver_CS(g_pm, options, set_hddm_func_harness);
   double t_solve = t_now() - t1;
+  if (f_hist) fclose(f_hist);
   if (f_aij) fclose(f_aij);
   if (f_fac) fclose(f_fac);
   dump_solution(g_pm, nrepeat);

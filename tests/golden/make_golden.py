@@ -10,9 +10,10 @@ and the reference's outputs: the integer maps of make_PartMesh_FW, the
 assembled TMP_AIJ rows, the skyline profile and LDL^T factor of every
 subdomain, the residual history, the converged edge solution and the
 element results B, E, Je of the post step (also once with the first
-Permittivity and Conductor flags left out).  The C1
-fixture keeps the residual history, the iteration count and a strided
-sample of the solution.
+Permittivity and Conductor flags left out).  The C1 fixture (hddm_eps
+1e-10) keeps the residual history, the iteration count and the whole edge
+solution; the C2 fixture keeps the initial norm and the residuals of the
+first 10 interface iterations (hddm_max_loop 10).
 """
 from __future__ import annotations
 
@@ -35,7 +36,8 @@ CASES = {
              1e-12, 2000, True),
     "layered": (dict(name="layered", n=6, size=1.5, npml=1, layers=2, nleaves=None, leaf_cap=200,
                      jitter=(0.3, 0.7), seed=3), 1e-10, 4000, True),
-    "c1": (dict(name="c1", seed=0), 1e-6, 20000, False),
+    "c1": (dict(name="c1", seed=0), 1e-10, 40000, False),
+    "c2_head": (dict(name="c2", seed=0), 1e-6, 10, False),
     # element sources instead of the edge source: delta-gap voltages in a
     # conducting block, and an antenna current on a block of its own flag
     "gap": (dict(name="gap", n=4, size=1.0, npml=1, layers=None, nleaves=4, leaf_cap=None, jitter=None, seed=0),
@@ -85,6 +87,8 @@ def make_case(name: str) -> str:
         "params": np.frombuffer(json.dumps(params).encode(), dtype=np.uint8),
         "hist": out["hist"],
         "norm0": np.array([out["norm0"]]),
+        "hist_full": out["hist_full"],
+        "norm0_full": np.array([out["norm0_full"]]),
         "iterations": np.array([out["json"]["iterations"]]),
         "total_free": np.array([out["json"]["total_free"]]),
     }
@@ -101,12 +105,8 @@ def make_case(name: str) -> str:
             arrays[f"s{s}_idx1"] = fm["idx1"]
             arrays[f"s{s}_idx2"] = fm["idx2"]
             arrays[f"s{s}_fac"] = fm["mat"]
-    else:
-        stride = 97
-        arrays["x_sample_stride"] = np.array([stride])
-        arrays["x_sample"] = out["x"][::stride]
-        arrays["x_sum"] = np.array([out["x"].sum()])
-        arrays["x_abs2"] = np.array([np.sum(np.abs(out["x"]) ** 2)])
+    elif name == "c1":
+        arrays["x"] = out["x"]
     path = os.path.join(HERE, f"ref_{name}.npz")
     np.savez_compressed(path, **arrays)
     return path

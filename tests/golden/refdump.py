@@ -153,6 +153,9 @@ def run_harness(model, hddm_eps: float, hddm_max_loop: int, dump: int = 2, workd
     out = dict(json=json.load(open(os.path.join(mdir, "ref.json"))))
     out["x"] = read_sol(os.path.join(mdir, "ref.sol"), nv, model.n_edges)
     out["norm0"], out["hist"] = read_log(os.path.join(mdir, "calc_log", "log_g_HDDM_Full_Wave"))
+    # the same history at full precision, recorded by the harness
+    h = np.fromfile(os.path.join(mdir, "ref.hist"), dtype="<f8")
+    out["norm0_full"], out["hist_full"] = float(h[0]), h[1:].copy()
     if dump >= 1:
         out["infree"], out["ints"] = read_ints(os.path.join(mdir, "ref.ints"), nv)
         out["post"] = read_post(os.path.join(mdir, "ref.post"), model.n_tets)

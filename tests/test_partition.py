@@ -29,6 +29,7 @@ def test_oracle_partition_matches_reference(name):
 
 @pytest.mark.parametrize("kw", [
     dict(name="c1"),
+    dict(name="c2"),
     dict(name="x", n=8, size=1.5, npml=2, layers=2, nleaves=None, leaf_cap=120, jitter=(0.3, 0.7), seed=1),
     dict(name="x", n=6, size=1.0, npml=1, layers=None, nleaves=1),
     dict(name="x", n=10, size=1.5, npml=2, layers=3, nleaves=None, leaf_cap=50, jitter=(0.3, 0.7), seed=9),
