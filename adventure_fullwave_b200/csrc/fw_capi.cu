@@ -868,6 +868,16 @@ static int setup_stage(fwgpu_context *c) {
 // Times the candidate subdomain-solve kernels on the factors just computed
 // (first-solve mode, whose outputs the real first solve then overwrites) and
 // keeps the fastest.
+//
+// The timed choice never changes the arithmetic, so that a solve gives the
+// same bits on every run: AUTO times only variants that sum in the same
+// order.  The staging capacity sets the row blocks, and with them the
+// order of the sums, so AUTO keeps the default capacity (a rule on the
+// model's envelope, setup_stage) and times one against two warps per
+// subdomain, which in FP64 share out whole row groups and column chunks and
+// so sum alike.  The FP32 sweep splits each row between the warps, so FP32
+// keeps one warp; the CTA kernel sums in another order and runs only when
+// asked for.  An explicit WARP choice times the staging capacities too.
 static int tune_solve_kernel(fwgpu_context *c) {
   const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
   struct Cand {
@@ -875,11 +885,17 @@ static int tune_solve_kernel(fwgpu_context *c) {
   };
   std::vector<Cand> cand;
   const bool any = c->opts.solve_kernel == FWGPU_SOLVE_AUTO;
-  if ((any || c->opts.solve_kernel == FWGPU_SOLVE_WARP) && c->warp_ok)
+  if (any && c->warp_ok) {
+    for (int warps = 1; warps <= (fp32 ? 1 : 2); warps++)
+      if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps)
+        cand.push_back({fw::kSolveWarp, c->dp.stage_cap, warps});
+    if (cand.empty()) cand.push_back({fw::kSolveWarp, c->dp.stage_cap, c->opts.stage_warps});
+  }
+  if (c->opts.solve_kernel == FWGPU_SOLVE_WARP && c->warp_ok)
     for (int cap : c->stage_caps)
       for (int warps = 1; warps <= 2; warps++)
         if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps) cand.push_back({fw::kSolveWarp, cap, warps});
-  if (any && c->dp.cta_smem > 0) cand.push_back({fw::kSolveCta, 0, 1});
+  if (any && !c->warp_ok && c->dp.cta_smem > 0) cand.push_back({fw::kSolveCta, 0, 1});
   if (cand.empty()) {
     c->solve_tuned = true;
     return FWGPU_OK;

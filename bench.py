@@ -1,6 +1,8 @@
 """Benchmark of the B200 HDDM hot path: time to reach a 1e-6 max-norm
 relative interface residual (the reference's COCG criterion,
-lib/hddm/hddm_solver_s.h:311-318,370) on a synthetic layered-PML model.
+lib/hddm/hddm_solver_s.h:311-318,370) on a synthetic layered-PML model,
+by default C3 (96^3 cells x 6 tets, the configuration the FP32+IR target
+is quoted on).
 
 One step = one full HDDM solve with the model resident in HBM: element
 assembly into the subdomain envelopes, LDL^T factors, first solve, COCG to
@@ -9,14 +11,18 @@ assembly into the subdomain envelopes, LDL^T factors, first solve, COCG to
 solve through the public API from host arrays (subdomain setup, uploads,
 solve, download of the edge solution) timed per step.
 
-    python bench.py [--gpus N --steps K --warmup W] [--config c2] [--precision fp64|fp32_ir]
+    python bench.py [--gpus N --steps K --warmup W] [--config c3] [--precision fp64|fp32_ir]
     python bench.py --impl reference ...   # the reference's own CPU solver
 
 ``value`` is the FP64 solve (the reference's arithmetic); the line adds
 ``mixed_precision`` (the same model solved with FP32 factors and FP64
 refinement to the same tolerance: time, iterations and relative L2 distance
-to the FP64 solution) and ``adjoint`` (the C4 design-region model: one
-forward solve and the backward call on its factors).
+to the FP64 solution, ``--mixed-steps`` timed solves), ``adjoint`` (the C4
+design-region model: one forward solve and the backward call on its
+factors), ``c2`` (the C2 model, FP64), ``sample`` (the reference's shipped
+model) and ``accuracy`` (C1 solved in FP64 and FP32+IR, each solution's
+relative L2 error against the FP64 sparse direct solve of the global system
+kept in tests/golden/direct_c1.npz).
 
 Under torchrun (N > 1) the model is sharded: every rank solves a contiguous
 range of the subdomains and the ranks sum the partial interface vector with
@@ -50,14 +56,17 @@ WORKLOADS = {
     "c2": "C2: [0,1.5]^3 48^3 hexes x 6 tets (663,552 tets), 8 random layers, 6-cell PML, PEC wall, 300 MHz, "
           "centre z-dipole, jittered RCB (leaf cap 600) 1 part x 1654 subdomains",
     "c3": "C3: [0,1.5]^3 96^3 hexes x 6 tets (5,308,416 tets), 8 random layers, 8-cell PML, PEC wall, 300 MHz, "
-          "centre z-dipole, jittered RCB (leaf cap 900)",
+          "centre z-dipole, jittered RCB (leaf cap 900) 1 part x 8822 subdomains",
     "c4": "C4: the C2 mesh and medium with a central 12^3-cell design region (10,368 tets, per-tet complex eps_r, "
           "eps' ~ U[2,4], eps'' ~ U[0,0.1]); J = sum |E|^2 on 8 probe edges; forward solve + adjoint gradient",
 }
 # COCG iterations to 1e-6 of the FP64 GPU solve on each model (B200, this
 # code); the reference's CPU time is extrapolated with them where running the
-# reference to convergence would take hours (C2: ~7,800 iterations).
-ITERS_FP64 = {"c1": 450, "c2": 7790}
+# reference to convergence would take hours (C2: ~7,800 iterations at about
+# 1.1 s each, C3: ~9,000 at about 10 s each).
+ITERS_FP64 = {"c1": 450, "c2": 7807, "c3": 8991}
+DIRECT_FIXTURE = os.path.join(REPO, "tests", "golden", "direct_c1.npz")
+TRAFFIC = os.path.join(REPO, "profiles", "dram_traffic.json")
 
 
 def env_rank():
@@ -175,19 +184,16 @@ def post_algorithmic_bytes(model) -> int:
     return int(model.n_tets * (16 + 24 + 1 + 8 + 144) + model.n_vertices * 24 + model.n_edges * 16)
 
 
-def ncu_traffic(kernel: str, config: str, precision: str):
-    """DRAM bytes of one subdomain-solve phase from the committed ncu summary
-    (profiles/subsolve_<kernel>_<config>_<precision>.md), when one covers
-    this workload."""
-    path = os.path.join(REPO, "profiles", f"subsolve_{kernel}_{config}_{precision}.md")
+def ncu_traffic(config: str, precision: str):
+    """DRAM bytes (read + write) of one subdomain-solve phase of an interface
+    iteration, from the ncu capture summarised in profiles/dram_traffic.json
+    (with the command that made it), when one covers this workload."""
     try:
-        for line in open(path):
-            t = line.split()
-            if len(t) == 4 and t[0] == "dram_bytes_per_launch" and t[1] == f"{config}_{precision}":
-                return int(t[3])
-    except OSError:
-        pass
-    return None
+        with open(TRAFFIC) as f:
+            t = json.load(f).get(f"{config}_{precision}")
+        return None if t is None else int(t["bytes_per_phase"])
+    except (OSError, ValueError, KeyError):
+        return None
 
 
 def make_model(config: str):
@@ -196,10 +202,12 @@ def make_model(config: str):
     return model
 
 
-def cpu_baseline_reference(model, config: str, sample_iters: int, n_iters: int):
-    """The reference itself (oracle/_ref/fw_ref_harness, built from its
-    sources, single thread) on a bounded sample of the workload: setup plus
-    ``sample_iters`` COCG iterations, extrapolated to ``n_iters``."""
+def run_reference_sample(model, n_loop: int):
+    """One run of the reference itself (oracle/_ref/fw_ref_harness, built from
+    its sources, single thread) on ``model``: setup, ``n_loop`` COCG
+    iterations, the last solves.  Returns the harness's timings and the
+    seconds of every interface iteration after the first, or None when the
+    harness is not built."""
     sys.path.insert(0, os.path.join(REPO, "tests", "golden"))
     import refdump
 
@@ -208,45 +216,66 @@ def cpu_baseline_reference(model, config: str, sample_iters: int, n_iters: int):
     wd = tempfile.mkdtemp(prefix="fwbench_")
     try:
         t0 = time.time()
-        out = refdump.run_harness(model, 1e-6, sample_iters, dump=0, workdir=wd, timeout=1800)
-        wall = time.time() - t0
-        j = out["json"]
-        per_iter = j["t_iter_total_s"] / max(1, j["t_iter_count"])
-        setup = j["t_init_s"] + j["t_first_s"]
-        total = setup + n_iters * per_iter + j["t_last_s"]
-        return {"value": total, "unit": "s", "cores": 1, "kind": "reference",
-                "sample": f"reference s-mode solver on the {config} model: setup + {sample_iters} COCG iterations "
-                          f"({wall:.1f} s wall), {per_iter:.3f} s/iteration extrapolated to {n_iters} iterations",
-                "setup_s": setup, "per_iteration_s": per_iter, "iterations_assumed": n_iters}
+        out = refdump.run_harness(model, 1e-6, n_loop, dump=0, workdir=wd, timeout=1700)
+        j = dict(out["json"])
+        j["wall_s"] = time.time() - t0
+        j["iteration_s"] = [float(v) for v in out["iteration_s"]]
+        return j
     finally:
         shutil.rmtree(wd, ignore_errors=True)
 
 
+def extrapolate(j, per_iter: float, n_iters: int) -> float:
+    """The reference's time to 1e-6: its setup (reading, integer setup,
+    assembly, factors, first solve) + n_iters interface iterations + the
+    last solves."""
+    return j["t_init_s"] + j["t_first_s"] + n_iters * per_iter + j["t_last_s"]
+
+
+def cpu_baseline_reference(model, config: str, sample_iters: int, n_iters: int):
+    """The reference on a bounded sample of the workload (setup plus
+    ``sample_iters`` + 1 COCG iterations), extrapolated to ``n_iters``."""
+    j = run_reference_sample(model, sample_iters + 1)
+    if j is None:
+        return None
+    per_iter = float(np.mean(j["iteration_s"])) if j["iteration_s"] else 0.0
+    setup = j["t_init_s"] + j["t_first_s"]
+    return {"value": extrapolate(j, per_iter, n_iters), "unit": "s", "cores": 1, "kind": "reference",
+            "sample": f"reference s-mode solver on the {config} model: setup + {sample_iters + 1} COCG iterations "
+                      f"({j['wall_s']:.1f} s wall), {per_iter:.3f} s/iteration (mean of {len(j['iteration_s'])}) "
+                      f"extrapolated to {n_iters} iterations",
+            "setup_s": setup, "per_iteration_s": per_iter, "iterations_assumed": n_iters}
+
+
 def run_reference(args):
+    """The reference arm: one step = one interface iteration of the
+    reference's own solver on the same model (single thread), W warm-up
+    iterations then K timed; the line's value is the reference's setup +
+    the GPU FP64 iteration count x the mean timed iteration + its last
+    solves (a converged reference run of C2 or C3 would take hours)."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
     model = make_model(args.config)
     n_iters = ITERS_FP64.get(args.config, 5000)
-    vals = []
-    last = None
-    for step in range(args.warmup + args.steps):
-        r = cpu_baseline_reference(model, args.config, args.ref_iters, n_iters)
-        if r is None:
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/fw_ref_harness is not built"}))
-            return 0
-        if step >= args.warmup:
-            vals.append(r["value"])
-        last = r
-    value = float(np.mean(vals))
+    j = run_reference_sample(model, args.warmup + args.steps + 1)
+    if j is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/fw_ref_harness is not built"}))
+        return 0
+    timed = j["iteration_s"][args.warmup:args.warmup + args.steps]
+    per_iter = float(np.mean(timed))
+    value = extrapolate(j, per_iter, n_iters)
+    sample = (f"reference s-mode solver on the {args.config} model, single thread: setup "
+              f"{j['t_init_s'] + j['t_first_s']:.1f} s, {args.warmup} warm-up + {len(timed)} timed COCG iterations "
+              f"({per_iter:.3f} s each), extrapolated to {n_iters} iterations (the GPU FP64 count)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_iter * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded generator; no dataset)",
             "config": {"workload": WORKLOADS.get(args.config, args.config), "precision": "fp64",
                        "hddm_eps": args.eps},
-            "cpu_baseline": {k: last[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "step": "one interface iteration of the reference (subdomain solves + COCG step)",
+            "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    line["cpu_baseline"]["value"] = value
     print(json.dumps(line))
     return 0
 
@@ -269,11 +298,19 @@ def run_ours(args):
             return run_sharded_bench(args, rank, world, local, dist)
     from adventure_fullwave_b200 import hddm
 
+    def opts(**kw):
+        o = dict(hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
+                 ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
+                 graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
+                 stage_cap=args.stage_cap, stage_warps=args.stage_warps)
+        o.update(kw)
+        return o
+
+    def solve_s(r):
+        return (r.t_setup_ms + r.t_iterate_ms + r.t_last_ms) / 1e3
+
     model = make_model(args.config)
-    solver = hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
-                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
-                             graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
-                             stage_cap=args.stage_cap, stage_warps=args.stage_warps)
+    solver = hddm.HddmSolver(model, **opts())
     for _ in range(args.warmup):
         solver.solve(0)
     clocks = ClockSampler(local)
@@ -284,7 +321,7 @@ def run_ours(args):
     for _ in range(args.steps):
         r = solver.solve(0)
         results.append(r)
-        times.append((r.t_setup_ms + r.t_iterate_ms + r.t_last_ms) / 1e3)
+        times.append(solve_s(r))
         iters.append(r.iterations)
         launches.append(r.kernel_launches)
     clk = clocks.stop()
@@ -300,65 +337,12 @@ def run_ours(args):
     sz = solver.sizes()
     x_check = solver.edge_solution()
 
-    mixed = None
-    if args.precision == "fp64" and not args.no_mixed:
-        # the same model with FP32 factors and FP64 refinement, to the same tolerance
-        with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision="fp32_ir",
-                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
-                             graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
-                             stage_cap=args.stage_cap, stage_warps=args.stage_warps) as s32:
-            s32.solve(0)
-            t32, it32 = [], []
-            for _ in range(args.steps):
-                r32 = s32.solve(0)
-                t32.append((r32.t_setup_ms + r32.t_iterate_ms + r32.t_last_ms) / 1e3)
-                it32.append(r32.iterations)
-            x32 = s32.edge_solution()
-        v32 = float(np.mean(t32))
-        mixed = {"fp32_ir_s": v32, "fp64_s": float(np.mean(times)), "fp64_over_fp32_ir": float(np.mean(times)) / v32,
-                 "fp32_ir_iterations": int(np.mean(it32)), "fp64_iterations": int(np.mean(iters)),
-                 "rel_l2_vs_fp64": float(np.linalg.norm(x32 - x_check) / np.linalg.norm(x_check)),
-                 "ir_steps": args.ir_steps, "ir_relax": args.ir_relax, "converged": bool(r32.converged),
-                 "solve_kernel": r32.solve_kernel, "stage_cap": r32.stage_cap}
-
-    adjoint = None
-    adj_model, adj_solver = None, None
-    if len(model.design_tets) > 0:
-        adj_model, adj_solver = model, solver
-    elif args.config == "c2" and not args.no_adjoint:
-        # the adjoint is quoted on the C2 mesh with the design region (C4)
-        adj_model = make_model("c4")
-        adj_solver = hddm.HddmSolver(adj_model, hddm_eps=args.eps, hddm_max_loop=args.max_loop,
-                                     precision=args.precision, ir_max_steps=args.ir_steps, ir_tol=args.ir_tol,
-                                     graph_iterations=args.graph_iters, device=local,
-                                     solve_kernel=args.solve_kernel, stage_cap=args.stage_cap, stage_warps=args.stage_warps)
-        adj_solver.solve(0)
-    if adj_solver is not None:
-        # the backward: one adjoint HDDM solve on the forward factors plus the gradient kernel
-        fwd, adj = [], []
-        for _ in range(args.adjoint_steps):
-            r = adj_solver.solve(0)
-            fwd.append((r.t_setup_ms + r.t_iterate_ms + r.t_last_ms) / 1e3)
-            t0 = time.perf_counter()
-            J, ge, gs, ra = adj_solver.adjoint_gradient()
-            adj.append(time.perf_counter() - t0)
-        adjoint = {"config": "c4", "forward_s": float(np.mean(fwd)), "adjoint_s": float(np.mean(adj)),
-                   "adjoint_over_forward": float(np.mean(adj) / np.mean(fwd)), "J": J,
-                   "forward_iterations": r.iterations, "adjoint_iterations": ra.iterations,
-                   "n_design": int(len(adj_model.design_tets)),
-                   "grad_finite": bool(np.all(np.isfinite(ge)) and np.all(np.isfinite(gs))),
-                   "timing": "forward: device events of one solve; adjoint: host wall time of the backward call "
-                             "(adjoint HDDM solve on the forward factors + gradient kernel)"}
-        if adj_solver is not solver:
-            adj_solver.close()
-
-    # kernel timing of the dominant kernel for the roofline
+    # kernel timing of the dominant phase for the roofline
     prof = solver.profile_iteration(reps=args.prof_reps)
-    solver.resolve(0)
     peak, peak_kind = load_peaks()
     alg = algorithmic_bytes(sz, args.precision, args.ir_steps)
     achieved = alg / (prof["subsolve_ms"] * 1e-3) / 1e9
-    traffic = ncu_traffic(results[-1].solve_kernel, args.config, args.precision)
+    traffic = ncu_traffic(args.config, args.precision)
     kname = {"warp": "rhs_kernel + subsolve_staged_kernel + iface_product_kernel",
              "cta": "subsolve_cta_kernel", "global": "subsolve_kernel"}.get(results[-1].solve_kernel,
                                                                            results[-1].solve_kernel)
@@ -366,7 +350,74 @@ def run_ours(args):
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic, "algorithmic_bytes": alg,
                 "kernel_ms": prof["subsolve_ms"], "interface_kernels_ms": prof["interface_ms"],
-                "iteration_ms_graph": prof["iteration_ms"]}
+                "iteration_ms_graph": prof["iteration_ms"],
+                "timing": "CUDA events on the solver's stream over repeated iteration-mode launches"}
+
+    # the post step (element B, E, Je from the converged edge values)
+    post = None
+    if not args.no_post:
+        solver.resolve(0)
+        post_ms = solver.profile_post(reps=args.prof_reps)
+        pb = post_algorithmic_bytes(model)
+        B, E, Je = solver.post_em_E()
+        post_gbs = pb / (post_ms * 1e-3) / 1e9
+        post = {"kernel": "post_em_E_kernel (HDDM_post_em_E over every element)", "kernel_ms": post_ms,
+                "algorithmic_bytes": pb, "achieved": post_gbs, "peak": peak, "unit": "GB/s", "frac": post_gbs / peak,
+                "peak_source": f"{peak_kind} hbm_gbs", "n_tets": model.n_tets,
+                "finite": bool(np.isfinite(B).all() and np.isfinite(E).all() and np.isfinite(Je).all()),
+                "timing": "device events per launch, L2 evicted before each"}
+    solver.close()
+
+    mixed = None
+    if args.precision == "fp64" and not args.no_mixed:
+        # the same model with FP32 factors and FP64 refinement, to the same tolerance
+        with hddm.HddmSolver(model, **opts(precision="fp32_ir")) as s32:
+            s32.solve(0)
+            t32, it32 = [], []
+            for _ in range(args.mixed_steps):
+                r32 = s32.solve(0)
+                t32.append(solve_s(r32))
+                it32.append(r32.iterations)
+            x32 = s32.edge_solution()
+        v32 = float(np.mean(t32))
+        mixed = {"fp32_ir_s": v32, "fp64_s": value, "fp64_over_fp32_ir": value / v32,
+                 "fp32_ir_iterations": int(np.mean(it32)), "fp64_iterations": int(np.mean(iters)),
+                 "rel_l2_vs_fp64": float(np.linalg.norm(x32 - x_check) / np.linalg.norm(x_check)),
+                 "ir_steps": args.ir_steps, "ir_relax": args.ir_relax, "converged": bool(r32.converged),
+                 "solve_kernel": r32.solve_kernel, "stage_cap": r32.stage_cap, "stage_warps": r32.stage_warps,
+                 "timed_solves": args.mixed_steps}
+
+    # the C2 model, FP64 (the configuration of the earlier lines)
+    c2 = None
+    if args.config != "c2" and not args.no_c2:
+        m2 = make_model("c2")
+        with hddm.HddmSolver(m2, **opts()) as s2:
+            s2.solve(0)
+            r2 = s2.solve(0)
+            p2 = s2.profile_iteration(reps=args.prof_reps)
+            a2 = algorithmic_bytes(s2.sizes(), args.precision, args.ir_steps)
+        c2 = {"workload": WORKLOADS["c2"], "time_s": solve_s(r2), "iterations": r2.iterations,
+              "phase_ms": p2["subsolve_ms"], "phase_frac": a2 / (p2["subsolve_ms"] * 1e-3) / 1e9 / peak,
+              "timing": "device events of one solve (second of two)"}
+
+    adjoint = None
+    if not args.no_adjoint:
+        # the adjoint is quoted on the C2 mesh with the design region (C4)
+        adj_model = model if len(model.design_tets) > 0 else make_model("c4")
+        with hddm.HddmSolver(adj_model, **opts()) as adj_solver:
+            adj_solver.solve(0)
+            # the backward: one adjoint HDDM solve on the forward factors plus the gradient kernel
+            r = adj_solver.solve(0)
+            t0 = time.perf_counter()
+            J, ge, gs, ra = adj_solver.adjoint_gradient()
+            t_adj = time.perf_counter() - t0
+        adjoint = {"config": "c4", "forward_s": solve_s(r), "adjoint_s": t_adj,
+                   "adjoint_over_forward": t_adj / solve_s(r), "J": J,
+                   "forward_iterations": r.iterations, "adjoint_iterations": ra.iterations,
+                   "n_design": int(len(adj_model.design_tets)),
+                   "grad_finite": bool(np.all(np.isfinite(ge)) and np.all(np.isfinite(gs))),
+                   "timing": "forward: device events of one solve; adjoint: host wall time of the backward call "
+                             "(adjoint HDDM solve on the forward factors + gradient kernel)"}
 
     # the reference's shipped sample model, to the same tolerance as the
     # reference's own run kept in tests/golden/ref_sample.npz
@@ -381,37 +432,32 @@ def run_ours(args):
         got = xs[::int(z["x_sample_stride"][0])]
         sample = {"model": "the reference's shipped sample (main/fullwave/MODEL): 6 parts x 73 subdomains, "
                            "one antenna", "n_tets": sm.n_tets, "hddm_eps": float(z["eps"][0]),
-                  "time_s": (rs.t_setup_ms + rs.t_iterate_ms + rs.t_last_ms) / 1e3, "iterations": rs.iterations,
+                  "time_s": solve_s(rs), "iterations": rs.iterations,
                   "reference_iterations": int(z["iterations"][0]),
                   "initial_norm": rs.initial_norm, "reference_initial_norm": float(z["norm0"][0]),
                   "rel_l2_vs_reference": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
                   "timing": "device events of one solve (second of two)"}
 
-    # the post step (element B, E, Je from the converged edge values)
-    post = None
-    if not args.no_post:
-        post_ms = solver.profile_post(reps=args.prof_reps)
-        pb = post_algorithmic_bytes(model)
-        B, E, Je = solver.post_em_E()
-        post_gbs = pb / (post_ms * 1e-3) / 1e9
-        post = {"kernel": "post_em_E_kernel (HDDM_post_em_E over every element)", "kernel_ms": post_ms,
-                "algorithmic_bytes": pb, "achieved": post_gbs, "peak": peak, "unit": "GB/s", "frac": post_gbs / peak,
-                "peak_source": f"{peak_kind} hbm_gbs", "n_tets": model.n_tets,
-                "finite": bool(np.isfinite(B).all() and np.isfinite(E).all() and np.isfinite(Je).all()),
-                "timing": "device events per launch, L2 evicted before each"}
+    # C1 against the exact discrete solution (FP64 sparse direct solve)
+    accuracy = None
+    if not args.no_accuracy and os.path.exists(DIRECT_FIXTURE):
+        xd = np.load(DIRECT_FIXTURE)["x"]
+        m1 = make_model("c1")
+        accuracy = {"model": "C1", "reference_solution": "FP64 sparse direct solve of the global system "
+                                                         "(SuperLU, oracle/direct.py)", "hddm_eps": args.eps}
+        for prec in ("fp64", "fp32_ir"):
+            x1, r1 = hddm.hddm_solver_CS(m1, 0, **opts(precision=prec))
+            accuracy[prec] = {"rel_l2_error": float(np.linalg.norm(x1 - xd) / np.linalg.norm(xd)),
+                              "iterations": r1.iterations}
 
     # end to end through the public API from host arrays
-    solver.close()
     e2e_times = []
     h2d = sum(a.nbytes for a in (model.vertex_crd, model.tets, model.tet_edges, model.flag, model.pec_edge,
                                  model.sub_of_tet, model.mat_flag, model.mat_eps, model.mat_sigma))
     d2h = model.n_edges * 16
     for _ in range(args.e2e_steps):
         t0 = time.perf_counter()
-        with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=args.precision,
-                             ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
-                             graph_iterations=args.graph_iters, device=local, solve_kernel=args.solve_kernel,
-                             stage_cap=args.stage_cap, stage_warps=args.stage_warps) as s2:
+        with hddm.HddmSolver(model, **opts()) as s2:
             s2.solve(0)
             xe = s2.edge_solution()
         e2e_times.append(time.perf_counter() - t0)
@@ -445,6 +491,8 @@ def run_ours(args):
                    "parallelism": f"{world} replica(s)"},
         "iterations": int(np.mean(iters)), "setup_ms": float(np.mean([r.t_setup_ms for r in results])),
         "iterate_ms": float(np.mean([r.t_iterate_ms for r in results])),
+        "solve_kernel": {"kernel": results[-1].solve_kernel, "stage_cap": results[-1].stage_cap,
+                         "stage_warps": results[-1].stage_warps},
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": roofline,
         "cpu_baseline": cpu,
@@ -452,14 +500,10 @@ def run_ours(args):
         "gpu_launches": int(np.sum(launches)),
         "solution_check": {"finite": bool(np.all(np.isfinite(x_check))), "final_resi": results[-1].final_resi},
     }
-    if mixed is not None:
-        line["mixed_precision"] = mixed
-    if adjoint is not None:
-        line["adjoint"] = adjoint
-    if post is not None:
-        line["post"] = post
-    if sample is not None:
-        line["sample"] = sample
+    for k, v in (("mixed_precision", mixed), ("adjoint", adjoint), ("c2", c2), ("post", post), ("sample", sample),
+                 ("accuracy", accuracy)):
+        if v is not None:
+            line[k] = v
     print(json.dumps(line))
     return 0
 
@@ -558,7 +602,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_ir"])
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--max-loop", type=int, default=50000)
@@ -569,7 +613,9 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the C4 adjoint sample of a C2 run")
     ap.add_argument("--no-post", action="store_true", help="skip the post-step measurement")
     ap.add_argument("--no-sample", action="store_true", help="skip the reference's shipped sample model")
-    ap.add_argument("--adjoint-steps", type=int, default=1)
+    ap.add_argument("--no-c2", action="store_true", help="skip the C2 solve of a run on another model")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the C1 solves against the direct solution")
+    ap.add_argument("--mixed-steps", type=int, default=1, help="timed FP32+IR solves (after one untimed)")
     ap.add_argument("--replicas", action="store_true", help="N > 1: independent replicas instead of shards")
     ap.add_argument("--sharded", action="store_true", help="the sharded driver even at N = 1 (one shard)")
     ap.add_argument("--graph-iters", type=int, default=32)
@@ -577,8 +623,8 @@ def main():
     ap.add_argument("--stage-cap", type=int, default=0, help="staging buffer elements (0: timed choice)")
     ap.add_argument("--stage-warps", type=int, default=0, help="warps per subdomain, 1 or 2 (0: timed choice)")
     ap.add_argument("--prof-reps", type=int, default=50)
-    ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--ref-iters", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--ref-iters", type=int, default=1, help="timed reference iterations of the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="bench", choices=["bench", "ncu"])
     ap.add_argument("--ncu-iters", type=int, default=20)

@@ -105,7 +105,7 @@ static void (*ref_solve_dom_1st)(DomMesh *, HDDM_Opt, SolvOpt, int (*)(AIJ_MAT *
 static void (*ref_iteration_s)(PartMesh *, HDDM_VEC *, HDDM_Opt, int (*)(HDDM_VEC *)) = NULL;
 static void (*ref_iteration_s_1st)(PartMesh *, HDDM_VEC *, HDDM_Opt, int (*)(HDDM_VEC *),
                                    void (*)(OPinfo **, HDDM_VEC *)) = NULL;
-static FILE *f_hist = NULL;
+static FILE *f_hist = NULL, *f_itimes = NULL;
 static void (*ref_solve_dom_last)(DomMesh *, SolvOpt, int (*)(AIJ_MAT *, SolvOpt, FILE *), HDDM_DOM_VEC *,
                                   FILE *) = NULL;
 
@@ -191,7 +191,12 @@ static void harness_iteration_s(PartMesh *pm, HDDM_VEC *hv, HDDM_Opt hddm_opt, i
     fwrite(&resi, sizeof(double), 1, f_hist);
   }
   double t = t_now();
-  if (t_iter_mark >= 0.0) t_iter_total += t - t_iter_mark;
+  if (t_iter_mark >= 0.0) {
+    /* one whole interface iteration: the subdomain solves and this COCG step */
+    const double dt = t - t_iter_mark;
+    t_iter_total += dt;
+    if (f_itimes) fwrite(&dt, sizeof(double), 1, f_itimes);
+  }
   t_iter_mark = t;
   n_iter++;
 }
@@ -517,11 +522,14 @@ int main(int argc, char **argv) {
     char path[FILENAME_MAX];
     snprintf(path, sizeof(path), "%s.hist", g_prefix);
     f_hist = fopen(path, "wb");
+    snprintf(path, sizeof(path), "%s.itimes", g_prefix);
+    f_itimes = fopen(path, "wb");
   }
   double t1 = t_now();
   hddm_solver_CS(g_pm, options, set_hddm_func_harness);
   double t_solve = t_now() - t1;
   if (f_hist) fclose(f_hist);
+  if (f_itimes) fclose(f_itimes);
   if (f_aij) fclose(f_aij);
   if (f_fac) fclose(f_fac);
   dump_solution(g_pm, nrepeat);

@@ -12,8 +12,8 @@ subdomain, the residual history, the converged edge solution and the
 element results B, E, Je of the post step (also once with the first
 Permittivity and Conductor flags left out).  The C1 fixture (hddm_eps
 1e-10) keeps the residual history, the iteration count and the whole edge
-solution; the C2 fixture keeps the initial norm and the residuals of the
-first 10 interface iterations (hddm_max_loop 10).
+solution; the C2 and C3 fixtures keep the initial norm and the residuals
+of the first 10 and 3 interface iterations (hddm_max_loop 10 and 3).
 """
 from __future__ import annotations
 
@@ -38,6 +38,7 @@ CASES = {
                      jitter=(0.3, 0.7), seed=3), 1e-10, 4000, True),
     "c1": (dict(name="c1", seed=0), 1e-10, 40000, False),
     "c2_head": (dict(name="c2", seed=0), 1e-6, 10, False),
+    "c3_head": (dict(name="c3", seed=0), 1e-6, 3, False),
     # element sources instead of the edge source: delta-gap voltages in a
     # conducting block, and an antenna current on a block of its own flag
     "gap": (dict(name="gap", n=4, size=1.0, npml=1, layers=None, nleaves=4, leaf_cap=None, jitter=None, seed=0),

@@ -156,6 +156,8 @@ def run_harness(model, hddm_eps: float, hddm_max_loop: int, dump: int = 2, workd
     # the same history at full precision, recorded by the harness
     h = np.fromfile(os.path.join(mdir, "ref.hist"), dtype="<f8")
     out["norm0_full"], out["hist_full"] = float(h[0]), h[1:].copy()
+    # seconds of each interface iteration after the first (subdomain solves + COCG step)
+    out["iteration_s"] = np.fromfile(os.path.join(mdir, "ref.itimes"), dtype="<f8")
     if dump >= 1:
         out["infree"], out["ints"] = read_ints(os.path.join(mdir, "ref.ints"), nv)
         out["post"] = read_post(os.path.join(mdir, "ref.post"), model.n_tets)

@@ -1,6 +1,6 @@
 """Failure paths of the C ABI on the GPU, each made on the host from bad
 input (no GPU fault is involved): a negatively oriented element, a
-subdomain whose matrix is singular, and a non-finite right-hand side.
+subdomain whose matrix is not finite, and a non-finite right-hand side.
 
 The reference has no error handling for any of these: emessage() exits on
 a negative volume (lib/fem/tetrahedral.c tet_Volume6 users), a zero pivot
@@ -36,12 +36,19 @@ def test_inverted_element_is_a_mesh_error():
         assert e.value.code == _lib.ERR_MESH
 
 
-def test_singular_subdomain_is_a_breakdown():
+def test_non_finite_subdomain_matrix_is_a_breakdown():
+    """A NaN permittivity on the elements of subdomain 0: its assembled
+    matrix, and with it the first pivot that meets a NaN entry, is not
+    finite.  (No material table gives an exactly singular subdomain: the
+    element matrix always holds the (nu/omega) curl-curl term,
+    make_elem_em.c:227-232, whose null space rounding turns into tiny but
+    finite pivots.)"""
     m = _model()
-    # a flag in neither the Permittivity nor the Conductor table gives zero
-    # element matrices: every interior row of subdomain 0 is zero
-    absent = int(m.mat_flag.max()) + 7
-    m.flag = np.where(m.sub_of_tet == 0, absent, m.flag).astype(np.int32)
+    f = int(m.mat_flag.max()) + 1
+    m.mat_flag = np.append(m.mat_flag, f).astype(np.int32)
+    m.mat_eps = np.append(m.mat_eps, np.nan)
+    m.mat_sigma = np.append(m.mat_sigma, 0.0)
+    m.flag = np.where(m.sub_of_tet == 0, f, m.flag).astype(np.int32)
     with hddm.HddmSolver(m, hddm_eps=1e-6) as s:
         s.make_tmp_aij(0)
         with pytest.raises(_lib.FwgpuError) as e:
