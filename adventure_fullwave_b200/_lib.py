@@ -66,7 +66,7 @@ class FwOptions(ctypes.Structure):
         ("hddm_eps", c_dbl), ("hddm_max_loop", c_i32), ("precision", c_i32), ("ir_max_steps", c_i32),
         ("ir_tol", c_dbl), ("graph_iterations", c_i32), ("device", c_i32), ("solve_kernel", c_i32),
         ("stage_cap", c_i32), ("ir_relax", c_dbl), ("shard_begin", c_i32), ("shard_end", c_i32),
-        ("stage_warps", c_i32), ("reserved", c_i32),
+        ("stage_warps", c_i32), ("stall_copy_test", c_i32),
     ]
 
 

@@ -611,6 +611,7 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   dp.ir_steps = c->opts.ir_max_steps;
   dp.ir_tol = c->opts.ir_tol;
   dp.ir_relax = c->opts.ir_relax;
+  dp.stall_test = c->opts.stall_copy_test ? 1 : 0;
   {
     const bool fp32 = opts->precision == FWGPU_PREC_FP32_IR;
     const size_t smem = fw::subsolve_smem_bytes(p.max_interior, p.max_iface, fp32);

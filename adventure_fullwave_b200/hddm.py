@@ -128,7 +128,7 @@ class HddmSolver:
     def __init__(self, model, hddm_eps: float = 1e-3, hddm_max_loop: int = 4000, precision: str = "fp64",
                  ir_max_steps: int = 1, ir_tol: float = 0.0, graph_iterations: int = 16, device: int = 0,
                  solve_kernel: str = "auto", stage_cap: int = 0, ir_relax: float = 0.0,
-                 shard: Optional[Tuple[int, int]] = None, stage_warps: int = 0):
+                 shard: Optional[Tuple[int, int]] = None, stage_warps: int = 0, stall_copy_test: int = 0):
         lib = _lib.load()
         self._lib = lib
         self.model = model
@@ -163,7 +163,8 @@ class HddmSolver:
         kern = SOLVE_KERNELS[solve_kernel]
         opts = _lib.FwOptions(self.hddm_eps, self.hddm_max_loop, prec, int(ir_max_steps), float(ir_tol),
                               int(graph_iterations), int(device), kern, int(stage_cap), float(ir_relax),
-                              int(shard[0]) if shard else 0, int(shard[1]) if shard else 0, int(stage_warps), 0)
+                              int(shard[0]) if shard else 0, int(shard[1]) if shard else 0, int(stage_warps),
+                              int(stall_copy_test))
         handle = ctypes.c_void_p()
         rc = lib.fwgpu_create(ctypes.byref(mesh), ctypes.byref(mt), ctypes.byref(opts), ctypes.byref(handle))
         if rc != 0 and handle.value:
