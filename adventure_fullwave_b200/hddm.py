@@ -382,6 +382,12 @@ class HddmSolver:
         _lib.check(self._lib.fwgpu_get_history(self._h, _ptr(h, ctypes.c_double), n.value, ctypes.byref(n)))
         return h[: n.value]
 
+    def write_calc_log(self, path: str, result: "HddmResult", mode: str = "a") -> None:
+        """Append (or write, mode "w") the last solve's residual history to
+        ``path`` as the reference's calc_log section (``calc_log_section``)."""
+        with open(path, mode) as f:
+            f.write(calc_log_section(self.sizes()["total_free"], result.initial_norm, self.history()))
+
     def sizes(self) -> dict:
         s = _lib.FwSizes()
         _lib.check(self._lib.fwgpu_get_sizes(self._h, ctypes.byref(s)))
@@ -420,6 +426,20 @@ class HddmSolver:
         m = np.zeros(2 * nlen, np.float64)
         _lib.check(self._lib.fwgpu_get_factor(self._h, s, _ptr(m, ctypes.c_double)))
         return m[0::2] + 1j * m[1::2]
+
+
+def calc_log_section(total_free: int, initial_norm: float, history) -> str:
+    """The full-wave section of the reference's convergence log
+    (calc_log/log_g_HDDM_Full_Wave): two blank lines and the title
+    (HDDM_set_HDDM_Opt_log, lib/hddm/set_hddm_func.c:37-51), the interface
+    DOF count (lib/hddm/hddm_solver.h:88-92), the initial line with the
+    max-norm of r0 (lib/hddm/hddm_solver_s.h:203-207) and one line
+    "iteration resi" per interface iteration (:319-323), in the reference's
+    printf formats."""
+    lines = ["", "", "# Full Wave Analysis", f"# DOF on interface {int(total_free)}",
+             f"0 {1.0:e}  # Norm {float(initial_norm):e}"]
+    lines += [f"{k} {float(r):e}" for k, r in enumerate(history, 1)]
+    return "\n".join(lines) + "\n"
 
 
 def relative_permittivity_gradient(g_eps: np.ndarray, g_sigma: np.ndarray, omega: float, eps0: float = 8.854e-12):
