@@ -78,6 +78,17 @@ typedef struct {
   double *im;
 } SubSource;
 static SubSource *g_src = NULL;
+/* the same sources by global node id of the mid-node */
+static int g_srcn = 0;
+static int *g_srcg = NULL;
+static double *g_srcv = NULL;
+
+#ifdef FW_HARNESS_GPU
+/* adventure_fullwave_b200/dropin/set_hddm_func_gpu.c: the reference's table
+   with the subdomain and interface slots on the GPU library */
+void set_hddm_func_fullwave_gpu(HDDM_FUNC *f, OPTIONS options);
+void hddm_gpu_set_edge_source(int n, const int *mid_gnid, const double *re_im);
+#endif
 
 /* antenna currents of <dir>/antenna.txt: per antenna its element flag and the
    reference's Jo / Jor (3 per global vertex); per subdomain an ANTENNA array
@@ -209,6 +220,18 @@ static void harness_solve_dom_last(DomMesh *dm, SolvOpt solvopt, int (*s)(AIJ_MA
 }
 
 static void set_hddm_func_harness(HDDM_FUNC *f, OPTIONS options) {
+#ifdef FW_HARNESS_GPU
+  /* the GPU table: only the once-per-step slots are timed; the
+     per-subdomain slots of that table do nothing */
+  set_hddm_func_fullwave_gpu(f, options);
+  ref_iteration_s = f->iteration_s;
+  ref_iteration_s_1st = f->iteration_s_1st;
+  ref_solve_dom_last = f->solve_dom_last;
+  f->iteration_s_1st = harness_iteration_s_1st;
+  f->iteration_s = harness_iteration_s;
+  f->solve_dom_last = harness_solve_dom_last;
+  return;
+#endif
   set_hddm_func_fullwave(f, options);
   ref_make_TMP_AIJ = f->make_TMP_AIJ;
   ref_solve_dom_1st = f->solve_dom_1st;
@@ -245,6 +268,12 @@ static void load_sources(const char *dir, PartMesh *pm) {
     int gnid;
     double re, im;
     if (fscanf(f, "%d %lf %lf", &gnid, &re, &im) != 3) break;
+    g_srcg = (int *)realloc(g_srcg, sizeof(int) * (g_srcn + 1));
+    g_srcv = (double *)realloc(g_srcv, sizeof(double) * 2 * (g_srcn + 1));
+    g_srcg[g_srcn] = gnid;
+    g_srcv[2 * g_srcn] = re;
+    g_srcv[2 * g_srcn + 1] = im;
+    g_srcn++;
     for (int d = 0; d < pm->ndomain; d++) {
       DomMesh *dm = &pm->dm[d];
       int *g = edge_gnid(pm, dm);
@@ -518,10 +547,16 @@ int main(int argc, char **argv) {
 
   hddm_sw.t_loop = -2;
   hddm_sw.antenna = -1;
+#ifdef FW_HARNESS_GPU
+  hddm_gpu_set_edge_source(g_srcn, g_srcg, g_srcv);
+#endif
   {
     char path[FILENAME_MAX];
+#ifndef FW_HARNESS_GPU
+    /* the residuals are read from the reference's own interface vectors */
     snprintf(path, sizeof(path), "%s.hist", g_prefix);
     f_hist = fopen(path, "wb");
+#endif
     snprintf(path, sizeof(path), "%s.itimes", g_prefix);
     f_itimes = fopen(path, "wb");
   }
