@@ -41,6 +41,8 @@ class FwMesh(ctypes.Structure):
         ("n_tets", c_i32), ("tet_vertices", P(c_i32)), ("tet_edges", P(c_i32)), ("tet_flag", P(c_i32)),
         ("n_edges", c_i32), ("pec_edge", P(ctypes.c_uint8)),
         ("n_subdomains", c_i32), ("sub_of_tet", P(c_i32)),
+        ("sub_vertex_ptr", P(c_i32)), ("sub_vertex_order", P(c_i32)),
+        ("sub_edge_ptr", P(c_i32)), ("sub_edge_order", P(c_i32)),
     ]
 
 

@@ -31,9 +31,8 @@
  * options) is the reference's own.  Errors of the library are reported the
  * reference's way: a message and exit (lib/std/errormessage.c).
  *
- * The subdomain-local numbering of the library is ascending global node id
- * inside each subdomain, which is the partitioner's order of the models this
- * build writes (adventure_fullwave_b200/meshgen.py write_hddm_model).
+ * Every subdomain keeps the PartMesh's own local numbering (its apid and
+ * mpid order), so the library's skyline profiles are the reference's.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -157,6 +156,20 @@ static void gpu_general_func_2nd(PartMesh *pm, HDDM_VEC *hv, OPTIONS options, HD
   int32_t *flag = (int32_t *)malloc(sizeof(int32_t) * (size_t)(nt > 0 ? nt : 1));
   int32_t *sub = (int32_t *)malloc(sizeof(int32_t) * (size_t)(nt > 0 ? nt : 1));
   uint8_t *pec = (uint8_t *)calloc(ne > 0 ? ne : 1, 1);
+  /* each subdomain's local order: its apid and mpid order */
+  int32_t *vptr = (int32_t *)malloc(sizeof(int32_t) * (nsub + 1));
+  int32_t *eptr = (int32_t *)malloc(sizeof(int32_t) * (nsub + 1));
+  vptr[0] = eptr[0] = 0;
+  {
+    int k = 0;
+    for (int q = 0; q < npart; q++)
+      for (int d = 0; d < pm[q].ndomain; d++, k++) {
+        vptr[k + 1] = vptr[k] + pm[q].dm[d].nap;
+        eptr[k + 1] = eptr[k] + pm[q].dm[d].nmp;
+      }
+  }
+  int32_t *vord = (int32_t *)malloc(sizeof(int32_t) * (vptr[nsub] > 0 ? vptr[nsub] : 1));
+  int32_t *eord = (int32_t *)malloc(sizeof(int32_t) * (eptr[nsub] > 0 ? eptr[nsub] : 1));
   int t = 0, s = 0;
   for (int q = 0; q < npart; q++)
     for (int d = 0; d < pm[q].ndomain; d++, s++) {
@@ -164,7 +177,9 @@ static void gpu_general_func_2nd(PartMesh *pm, HDDM_VEC *hv, OPTIONS options, HD
       for (int a = 0; a < dm->nap; a++) {
         const int v = vtx_of[gnid_of(&pm[q], dm, dm->apid2snid[a])];
         for (int k = 0; k < 3; k++) crd[3 * v + k] = dm->crd[3 * a + k];
+        vord[vptr[s] + a] = v;
       }
+      for (int m = 0; m < dm->nmp; m++) eord[eptr[s] + m] = g_edge_of[gnid_of(&pm[q], dm, dm->mpid2snid[m])];
       for (int el = 0; el < dm->nel; el++, t++) {
         const int *ne_ = &dm->nop[el * dm->nd_elem];
         for (int i = 0; i < 4; i++) tv[4 * t + i] = vtx_of[gnid_of(&pm[q], dm, dm->apid2snid[ne_[i]])];
@@ -183,7 +198,7 @@ static void gpu_general_func_2nd(PartMesh *pm, HDDM_VEC *hv, OPTIONS options, HD
       free(is_if);
     }
   const MTRL *mt = &pm[0].mtrl;
-  fwgpu_mesh mesh = {nv, crd, nt, tv, te, flag, ne, pec, nsub, sub};
+  fwgpu_mesh mesh = {nv, crd, nt, tv, te, flag, ne, pec, nsub, sub, vptr, vord, eptr, eord};
   fwgpu_material mat = {mt->nflag, mt->flag_i, mt->flag_nu, mt->nR, mt->R_i, mt->R_sigma, mt->antenna_omega};
   fwgpu_options o;
   memset(&o, 0, sizeof(o));
@@ -242,6 +257,10 @@ static void gpu_general_func_2nd(PartMesh *pm, HDDM_VEC *hv, OPTIONS options, HD
   free(flag);
   free(sub);
   free(pec);
+  free(vptr);
+  free(vord);
+  free(eptr);
+  free(eord);
   g_x = (double *)calloc(2 * (size_t)(ne > 0 ? ne : 1), sizeof(double));
   g_last_done = 0;
 }

@@ -61,10 +61,17 @@ def _mesh_struct(model):
     a["flag"] = np.ascontiguousarray(model.flag, dtype=np.int32)
     a["pec"] = np.ascontiguousarray(model.pec_edge, dtype=np.uint8)
     a["sub"] = np.ascontiguousarray(model.sub_of_tet, dtype=np.int32)
+    order = [None] * 4
+    so = getattr(model, "sub_order", None)
+    if so is not None:
+        for k, v in enumerate(so):
+            a[f"ord{k}"] = np.ascontiguousarray(v, dtype=np.int32)
+            order[k] = _ptr(a[f"ord{k}"], ctypes.c_int32)
     mesh = _lib.FwMesh(
         int(a["crd"].shape[0]), _ptr(a["crd"], ctypes.c_double), int(a["tv"].shape[0]),
         _ptr(a["tv"], ctypes.c_int32), _ptr(a["te"], ctypes.c_int32), _ptr(a["flag"], ctypes.c_int32),
-        int(a["pec"].shape[0]), _ptr(a["pec"], ctypes.c_uint8), int(model.nsub), _ptr(a["sub"], ctypes.c_int32))
+        int(a["pec"].shape[0]), _ptr(a["pec"], ctypes.c_uint8), int(model.nsub), _ptr(a["sub"], ctypes.c_int32),
+        *order)
     return mesh, a
 
 
@@ -134,13 +141,7 @@ class HddmSolver:
         self.model = model
         self.hddm_eps = float(hddm_eps)
         self.hddm_max_loop = int(hddm_max_loop)
-        a = {}
-        a["crd"] = np.ascontiguousarray(model.vertex_crd, dtype=np.float64)
-        a["tv"] = np.ascontiguousarray(model.tets, dtype=np.int32)
-        a["te"] = np.ascontiguousarray(model.tet_edges, dtype=np.int32)
-        a["flag"] = np.ascontiguousarray(model.flag, dtype=np.int32)
-        a["pec"] = np.ascontiguousarray(model.pec_edge, dtype=np.uint8)
-        a["sub"] = np.ascontiguousarray(model.sub_of_tet, dtype=np.int32)
+        mesh, a = _mesh_struct(model)
         a["mf"] = np.ascontiguousarray(model.mat_flag, dtype=np.int32)
         a["me"] = np.ascontiguousarray(model.mat_eps, dtype=np.float64)
         a["ms"] = np.ascontiguousarray(model.mat_sigma, dtype=np.float64)
@@ -151,10 +152,6 @@ class HddmSolver:
         if getattr(model, "sigma_table", None) is not None:
             a["sf"] = np.ascontiguousarray(model.sigma_table[0], dtype=np.int32)
             a["ms"] = np.ascontiguousarray(model.sigma_table[1], dtype=np.float64)
-        mesh = _lib.FwMesh(
-            int(a["crd"].shape[0]), _ptr(a["crd"], ctypes.c_double), int(a["tv"].shape[0]),
-            _ptr(a["tv"], ctypes.c_int32), _ptr(a["te"], ctypes.c_int32), _ptr(a["flag"], ctypes.c_int32),
-            int(a["pec"].shape[0]), _ptr(a["pec"], ctypes.c_uint8), int(model.nsub), _ptr(a["sub"], ctypes.c_int32))
         mt = _lib.FwMaterial(int(a["ef"].shape[0]), _ptr(a["ef"], ctypes.c_int32), _ptr(a["me"], ctypes.c_double),
                              int(a["sf"].shape[0]), _ptr(a["sf"], ctypes.c_int32), _ptr(a["ms"], ctypes.c_double),
                              float(model.omega))

@@ -69,6 +69,20 @@ typedef struct {
   const uint8_t *pec_edge;     /* n_edges, 1 = edge on the PEC wall (DirichletBCs_Axn0) */
   int32_t n_subdomains;
   const int32_t *sub_of_tet;   /* n_tets, subdomain of each element */
+  /* Optional (all four NULL: ascending global id in every subdomain): each
+   * subdomain's own local order, the node order (snid) of the reference's
+   * part files.  The reference numbers a subdomain's vertices and then its
+   * mid-nodes by their rank in that order (make_MESH_make_ap,
+   * make_MESH_change_ap, lib/fem/make_MESH.c:237-272,539-552), which sets
+   * the skyline profiles and with them the factors' rounding.  Subdomain s
+   * lists its vertices in sub_vertex_order[sub_vertex_ptr[s] ..
+   * sub_vertex_ptr[s+1]) and its edges in sub_edge_order[sub_edge_ptr[s] ..
+   * sub_edge_ptr[s+1]); each list must hold every vertex (edge) of the
+   * subdomain's elements exactly once. */
+  const int32_t *sub_vertex_ptr;   /* n_subdomains+1 */
+  const int32_t *sub_vertex_order; /* global vertex ids */
+  const int32_t *sub_edge_ptr;     /* n_subdomains+1 */
+  const int32_t *sub_edge_order;   /* global edge ids */
 } fwgpu_mesh;
 
 /* Material table: the reference's MTRL (lib/std/types.h:257-279) as read

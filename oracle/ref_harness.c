@@ -375,16 +375,22 @@ static void dump_jo(PartMesh *pms, int nparts) {
   fclose(f);
 }
 
-static void dump_ints(PartMesh *pm) {
+/* every part's subdomains, parts in order; the header counts all of them and
+   gives the first part's interface sizes */
+static void dump_ints(PartMesh *pms, int nparts) {
   char path[FILENAME_MAX];
   snprintf(path, sizeof(path), "%s.ints", g_prefix);
   FILE *f = fopen(path, "wb");
   if (!f) return;
-  w_i32(f, pm->ndomain);
-  w_i32(f, pm->infree);
-  w_i32(f, pm->outfree);
-  w_i32(f, pm->total_free);
-  for (int d = 0; d < pm->ndomain; d++) {
+  int total = 0;
+  for (int q = 0; q < nparts; q++) total += pms[q].ndomain;
+  w_i32(f, total);
+  w_i32(f, pms[0].infree);
+  w_i32(f, pms[0].outfree);
+  w_i32(f, pms[0].total_free);
+  for (int q = 0; q < nparts; q++)
+  for (int d = 0; d < pms[q].ndomain; d++) {
+    PartMesh *pm = &pms[q];
     DomMesh *dm = &pm->dm[d];
     w_i32(f, dm->nmp);
     w_i32(f, dm->nap);
@@ -536,7 +542,7 @@ int main(int argc, char **argv) {
   double t_init = t_now() - t0;
   load_sources(model_dir, &g_pm[0]);
   load_antennas(model_dir, &g_pm[0]);
-  if (g_dump >= 1) dump_ints(&g_pm[0]);
+  if (g_dump >= 1) dump_ints(g_pm, nrepeat);
   if (g_dump >= 2) {
     char path[FILENAME_MAX];
     snprintf(path, sizeof(path), "%s.aij", g_prefix);
