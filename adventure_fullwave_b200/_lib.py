@@ -41,6 +41,8 @@ class FwMesh(ctypes.Structure):
         ("n_tets", c_i32), ("tet_vertices", P(c_i32)), ("tet_edges", P(c_i32)), ("tet_flag", P(c_i32)),
         ("n_edges", c_i32), ("pec_edge", P(ctypes.c_uint8)),
         ("n_subdomains", c_i32), ("sub_of_tet", P(c_i32)),
+        ("sub_vertex_ptr", P(c_i32)), ("sub_vertex_order", P(c_i32)),
+        ("sub_edge_ptr", P(c_i32)), ("sub_edge_order", P(c_i32)),
     ]
 
 
@@ -66,7 +68,7 @@ class FwOptions(ctypes.Structure):
         ("hddm_eps", c_dbl), ("hddm_max_loop", c_i32), ("precision", c_i32), ("ir_max_steps", c_i32),
         ("ir_tol", c_dbl), ("graph_iterations", c_i32), ("device", c_i32), ("solve_kernel", c_i32),
         ("stage_cap", c_i32), ("ir_relax", c_dbl), ("shard_begin", c_i32), ("shard_end", c_i32),
-        ("stage_warps", c_i32), ("reserved", c_i32),
+        ("stage_warps", c_i32), ("stall_copy_test", c_i32),
     ]
 
 

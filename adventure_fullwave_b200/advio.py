@@ -461,7 +461,8 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
     present, ``volt.dat`` into one model with global vertex and edge numbers.
 
     Subdomains are numbered part by part.  Vertices and edges are numbered
-    in ascending global node id.  An edge is on the PEC wall when its
+    in ascending global node id; each subdomain keeps its local order, the
+    part file's node order, in ``model.sub_order``.  An edge is on the PEC wall when its
     mid-node is in a subdomain's DirichletBCs_Axn0 list.  A ``volt.dat``
     with gaps becomes the model's delta-gap source; otherwise the antennas
     of ``mtrl.dat`` become its antenna source, with the vertex currents the
@@ -482,6 +483,7 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
     seen = np.zeros(n_el, bool)
     gcrd: Dict[int, np.ndarray] = {}
     pec_gnid = []
+    sub_nodes = []
     sub_part = []
     sub = 0
     max_g = 0
@@ -503,6 +505,7 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
             el_sub[ge] = sub
             if p.dbc is not None:
                 pec_gnid.append(gn[p.dbc[s]])
+            sub_nodes.append(gn)
             sub_part.append((p.part, s))
             sub += 1
     if not seen.all():
@@ -527,6 +530,18 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
         g = g[eidx[g] >= 0]
         pec[eidx[g]] = True
     crd = g_crd[vert_g]
+    # each subdomain's local order: its vertices, then its mid-nodes, in the
+    # part file's node order (make_MESH_make_ap / make_MESH_change_ap)
+    vptr, vord, eptr, eord = [0], [], [0], []
+    for gn in sub_nodes:
+        v = vidx[gn]
+        e = eidx[gn]
+        vord.append(v[v >= 0])
+        eord.append(e[e >= 0])
+        vptr.append(vptr[-1] + int((v >= 0).sum()))
+        eptr.append(eptr[-1] + int((e >= 0).sum()))
+    sub_order = (np.array(vptr, np.int32), np.concatenate(vord).astype(np.int32), np.array(eptr, np.int32),
+                 np.concatenate(eord).astype(np.int32))
     flags = np.union1d(mat.eps_flag, mat.sigma_flag).astype(np.int32)
     # the reference takes the first entry of a flag listed twice (make_elem_em.c:98-109)
     eps_of, sig_of = {}, {}
@@ -541,7 +556,8 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
         mat_flag=flags, mat_eps=np.array([eps_of.get(f, 0.0) for f in flags.tolist()]),
         mat_sigma=np.array([sig_of.get(f, 0.0) for f in flags.tolist()]), omega=mat.omega, pec_edge=pec,
         sub_of_tet=el_sub, nsub=sub, sources=[],
-        eps_table=(mat.eps_flag.copy(), mat.eps.copy()), sigma_table=(mat.sigma_flag.copy(), mat.sigma.copy()))
+        eps_table=(mat.eps_flag.copy(), mat.eps.copy()), sigma_table=(mat.sigma_flag.copy(), mat.sigma.copy()),
+        sub_order=sub_order)
     vpath = os.path.join(model_dir, "volt.dat")
     boxes, volts = read_volt(vpath) if os.path.exists(vpath) else (np.zeros((0, 6)), np.zeros(0))
     if volts.shape[0] > 0:

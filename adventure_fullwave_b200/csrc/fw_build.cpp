@@ -6,8 +6,9 @@
 //   - local vertex ids ("ap") are ranks of the subdomain's vertex nodes and
 //     local edge DOF ids are ranks of its mid-edge nodes, both in subdomain
 //     node order (make_MESH_make_ap / make_MESH_change_ap,
-//     lib/fem/make_MESH.c:237-272,539-552); subdomain node order is
-//     ascending global node id with vertices before mid-edge nodes;
+//     lib/fem/make_MESH.c:237-272,539-552); subdomain node order is the
+//     caller's (the part file's node order, fwgpu_mesh sub_*_order) or else
+//     ascending global node id;
 //   - nop holds local ids with the mid-node slots 8 and 9 swapped
 //     (make_MESH_change_nop, lib/fem/make_MESH.c:556-585);
 //   - interface DOFs are the mid-edge nodes shared by two or more subdomains
@@ -21,6 +22,7 @@
 #include <array>
 #include <atomic>
 #include <numeric>
+#include <string>
 #include <thread>
 
 #include "fw_internal.h"
@@ -37,6 +39,7 @@ struct SubLists {
   std::vector<int32_t> contrib_cnt;
   std::vector<int32_t> int_local, cpl_ptr, cpl_col, aii_ptr, aii_col, if_ln, if_local, ifr_ptr, ifr_col;
   std::vector<int64_t> int_diag_src, cpl_src, aii_src, if_diag_src, ifr_src;
+  std::string err;  // non-empty: the subdomain's given local order is not a permutation of its nodes
 };
 
 // per-thread scratch: global edge / vertex id -> local id, -1 elsewhere
@@ -67,6 +70,20 @@ void build_sub(const Model &m, const Plan &p, const std::vector<int32_t> &iface_
   ve.erase(std::unique(ve.begin(), ve.end()), ve.end());
   std::sort(vv.begin(), vv.end());
   vv.erase(std::unique(vv.begin(), vv.end()), vv.end());
+  if (!m.sub_eptr.empty()) {
+    // the caller's local order (the part file's node order): the same sets
+    std::vector<int32_t> ge(m.sub_eord.begin() + m.sub_eptr[s], m.sub_eord.begin() + m.sub_eptr[s + 1]);
+    std::vector<int32_t> gv(m.sub_vord.begin() + m.sub_vptr[s], m.sub_vord.begin() + m.sub_vptr[s + 1]);
+    std::vector<int32_t> se(ge), sv(gv);
+    std::sort(se.begin(), se.end());
+    std::sort(sv.begin(), sv.end());
+    if (se != ve || sv != vv) {
+      L.err = "subdomain " + std::to_string(s) + ": the given local order does not list its vertices and edges once each";
+      return;
+    }
+    ve.swap(ge);
+    vv.swap(gv);
+  }
   h.nmp = (int32_t)ve.size();
   h.nap = (int32_t)vv.size();
   h.edge_gid = ve;
@@ -291,6 +308,8 @@ std::string build_plan(const Model &m, Plan &p) {
     worker();
     for (auto &t : pool) t.join();
   }
+  for (int s = 0; s < nsub; s++)
+    if (!lists[s].err.empty()) return lists[s].err;
 
   // concatenated in subdomain order: offsets first, then every subdomain's
   // slice written on all host threads

@@ -401,6 +401,21 @@ static int model_from_mesh(const fwgpu_mesh *mesh, fw::Model &m) {
   m.flag.assign(mesh->tet_flag, mesh->tet_flag + m.nt);
   m.sub_of_tet.assign(mesh->sub_of_tet, mesh->sub_of_tet + m.nt);
   m.pec.assign(mesh->pec_edge, mesh->pec_edge + m.ne);
+  const bool any_order = mesh->sub_vertex_ptr || mesh->sub_vertex_order || mesh->sub_edge_ptr || mesh->sub_edge_order;
+  if (any_order) {
+    if (!mesh->sub_vertex_ptr || !mesh->sub_vertex_order || !mesh->sub_edge_ptr || !mesh->sub_edge_order)
+      return set_error(FWGPU_ERR_ARG, "subdomain orders: give all four arrays or none");
+    const int ns = m.nsub;
+    for (int s = 0; s < ns; s++)
+      if (mesh->sub_vertex_ptr[s + 1] < mesh->sub_vertex_ptr[s] || mesh->sub_edge_ptr[s + 1] < mesh->sub_edge_ptr[s])
+        return set_error(FWGPU_ERR_ARG, "subdomain order offsets decrease");
+    if (mesh->sub_vertex_ptr[0] != 0 || mesh->sub_edge_ptr[0] != 0)
+      return set_error(FWGPU_ERR_ARG, "subdomain order offsets must start at 0");
+    m.sub_vptr.assign(mesh->sub_vertex_ptr, mesh->sub_vertex_ptr + ns + 1);
+    m.sub_eptr.assign(mesh->sub_edge_ptr, mesh->sub_edge_ptr + ns + 1);
+    m.sub_vord.assign(mesh->sub_vertex_order, mesh->sub_vertex_order + m.sub_vptr[ns]);
+    m.sub_eord.assign(mesh->sub_edge_order, mesh->sub_edge_order + m.sub_eptr[ns]);
+  }
   return FWGPU_OK;
 }
 
@@ -611,6 +626,7 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   dp.ir_steps = c->opts.ir_max_steps;
   dp.ir_tol = c->opts.ir_tol;
   dp.ir_relax = c->opts.ir_relax;
+  dp.stall_test = c->opts.stall_copy_test ? 1 : 0;
   {
     const bool fp32 = opts->precision == FWGPU_PREC_FP32_IR;
     const size_t smem = fw::subsolve_smem_bytes(p.max_interior, p.max_iface, fp32);
@@ -632,7 +648,7 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
       default:
         dp.solve_variant = dp.cta_smem > 0 ? fw::kSolveCta : fw::kSolveGlobal;
     }
-    // AUTO times every candidate; WARP times its staging capacities
+    // AUTO times the warps per subdomain; WARP times its staging capacities too
     c->solve_tuned = c->opts.solve_kernel != FWGPU_SOLVE_AUTO && c->opts.solve_kernel != FWGPU_SOLVE_WARP;
   }
   // per-edge solution source: the first subdomain holding each edge

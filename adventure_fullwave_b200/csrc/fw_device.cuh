@@ -25,6 +25,21 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+// acc + a b and acc - a b as four fused multiply-adds into the accumulator
+// (the sweeps' inner products: two FP64 instructions fewer per entry than
+// a product rounded on its own and then added)
+__device__ __forceinline__ double2 cmac(double2 acc, double2 a, double2 b) {
+  return make_double2(fma(-a.y, b.y, fma(a.x, b.x, acc.x)), fma(a.y, b.x, fma(a.x, b.y, acc.y)));
+}
+__device__ __forceinline__ double2 cmsub(double2 acc, double2 a, double2 b) {
+  return make_double2(fma(a.y, b.y, fma(-a.x, b.x, acc.x)), fma(-a.y, b.x, fma(-a.x, b.y, acc.y)));
+}
+__device__ __forceinline__ float2 cmac(float2 acc, float2 a, float2 b) {
+  return make_float2(fmaf(-a.y, b.y, fmaf(a.x, b.x, acc.x)), fmaf(a.y, b.x, fmaf(a.x, b.y, acc.y)));
+}
+__device__ __forceinline__ float2 cmsub(float2 acc, float2 a, float2 b) {
+  return make_float2(fmaf(a.y, b.y, fmaf(-a.x, b.x, acc.x)), fmaf(-a.y, b.x, fmaf(-a.x, b.y, acc.y)));
+}
 __device__ __forceinline__ double cabs_ref(double2 a) { return sqrt(a.x * a.x + a.y * a.y); }  // ComplexAbs
 __device__ __forceinline__ bool ciszero(double2 a) { return a.x == 0.0 && a.y == 0.0; }           // ISZERO
 // ComplexReciprocal / ComplexDivide (lib/std/complex_adv.c:39-52,133-137)
@@ -105,6 +120,25 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
+// the same copy with an L2 eviction policy (createpolicy) for its lines
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                              uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -175,18 +209,36 @@ __device__ __forceinline__ bool last_cta(uint32_t *ticket) {
 // A block's stored entries are contiguous in the envelope: one bulk copy
 // brings the block into a staging buffer, completing on the buffer's
 // mbarrier.  Two buffers alternate; the use counts give the wait parity.
+//
+// Every wait is bounded.  A wait that gives up raises the error word and
+// returns false; the caller then issues no further copy, waits (at the
+// normal bound) for the copies already in flight and returns, so that no
+// copy into its shared memory outlives it.
 
 constexpr uint32_t kStageWaitTries = 1u << 22;
+constexpr uint32_t kStallTestTries = 64;
 
 template <typename T>
 struct Stage {
   const T *L;          // the subdomain's envelope (global)
   T *buf0, *buf1;      // shared staging buffers
-  uint64_t *bar;       // [2]
+  uint64_t *bar;       // [3]: one per buffer, and one no copy ever arrives on (the stall test)
   const int2 *blk;     // shared: (first row, first element) of each block, then (nI, entries)
   uint32_t uses0, uses1;  // copies issued into each buffer (warp-uniform)
   int32_t *err;        // error word raised on a wait timeout
+  uint64_t policy;     // L2 eviction policy of the next copies (hint != 0)
+  int hint;
+  int stall;           // test hook: the next wait polls bar[2], which never completes
 };
+
+template <typename T>
+__device__ __forceinline__ void stage_init(Stage<T> &st, int32_t *err, int stall) {
+  st.uses0 = st.uses1 = 0;
+  st.err = err;
+  st.policy = 0;
+  st.hint = 0;
+  st.stall = stall;
+}
 
 // 16-byte aligned element range of block b
 template <typename T>
@@ -205,7 +257,10 @@ __device__ __forceinline__ void stage_issue(Stage<T> &st, int b, int lane) {
     const int n = (st.blk[b + 1].y - a0 + kA - 1) & ~(kA - 1);
     fence_proxy_async();
     mbar_arrive_expect_tx(&st.bar[k], (uint32_t)(n * sizeof(T)));
-    bulk_g2s(k ? st.buf1 : st.buf0, st.L + a0, (uint32_t)(n * sizeof(T)), &st.bar[k]);
+    if (st.hint)
+      bulk_g2s_hint(k ? st.buf1 : st.buf0, st.L + a0, (uint32_t)(n * sizeof(T)), &st.bar[k], st.policy);
+    else
+      bulk_g2s(k ? st.buf1 : st.buf0, st.L + a0, (uint32_t)(n * sizeof(T)), &st.bar[k]);
   }
   if (k)
     st.uses1 += 1;
@@ -213,19 +268,38 @@ __device__ __forceinline__ void stage_issue(Stage<T> &st, int b, int lane) {
     st.uses0 += 1;
 }
 
+// true once the last copy into block b's buffer has landed; false (error
+// word raised) when the bounded wait gave up
 template <typename T>
-__device__ __forceinline__ void stage_wait(Stage<T> &st, int b) {
+__device__ __forceinline__ bool stage_wait(Stage<T> &st, int b) {
   const int k = b & 1;
   const uint32_t uses = k ? st.uses1 : st.uses0;
-  if (uses == 0) return;
-  const uint32_t parity = (uses - 1u) & 1u;
+  if (uses == 0) return true;
+  uint64_t *bar = &st.bar[k];
+  uint32_t parity = (uses - 1u) & 1u, limit = kStageWaitTries;
+  if (st.stall) {
+    // test hook: a barrier that nothing arrives on, and a short bound
+    st.stall = 0;
+    bar = &st.bar[2];
+    parity = 0;
+    limit = kStallTestTries;
+  }
   uint32_t tries = 0;
-  while (!mbar_try_wait(&st.bar[k], parity)) {
-    if (++tries > kStageWaitTries) {
+  while (!mbar_try_wait(bar, parity)) {
+    if (++tries > limit) {
       *st.err = 1;
-      break;
+      return false;
     }
   }
+  return true;
+}
+
+// the drain: waits at the normal bound for the last copy into each buffer
+template <typename T>
+__device__ __forceinline__ void stage_drain(Stage<T> &st) {
+  st.stall = 0;
+  stage_wait(st, 0);
+  stage_wait(st, 1);
 }
 
 // lo and start (relative to the subdomain's envelope) of row r0 + lane

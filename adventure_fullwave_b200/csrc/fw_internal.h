@@ -44,6 +44,8 @@ struct Model {
   std::vector<double> crd;
   std::vector<int32_t> tv, te, flag, sub_of_tet;
   std::vector<uint8_t> pec;
+  // each subdomain's local vertex and edge order (empty: ascending global id)
+  std::vector<int32_t> sub_vptr, sub_vord, sub_eptr, sub_eord;
   // material resolved per element (the reference's first-match linear search
   // over the flag tables, lib/fem/make_elem_em.c:98-109)
   std::vector<double> el_eps, el_sigma;

@@ -620,24 +620,27 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
 // into shared memory, completing on an mbarrier; the copy of block b+1 is in
 // flight while block b is computed (two buffers per warp).  The backward sweep
 // starts on the two blocks the forward sweep left in the buffers.
-//   forward  - entries left of the block: lanes across a row (conflict-free
-//              shared loads of the entry and of y[col]), 8 rows at a time,
-//              one transpose-reduction per 8 rows; then the triangle, one
-//              lane per row, one broadcast shuffle per row; the pivot scaling
-//              z = y/d is written to the z stash for the backward sweep.
+//   forward  - entries left of the block: eight lanes per row (conflict-free
+//              shared loads of the entry and of y[col]), four rows per step;
+//              then the triangle, one lane per row, one broadcast shuffle per
+//              row; the pivot scaling z = y/d is written to the z stash for
+//              the backward sweep.
 //   backward - the triangle with lanes over columns, then the transposed
 //              update of the columns left of the block (lanes over columns,
-//              rows in the inner loop).
-// With no CTA barrier anywhere, several subdomain warps share an SM and hide
-// each other's dependent chains.  The arithmetic is the reference's
-// row-oriented envelope substitution (advlas_skyline.c:134-167) with the sums
-// regrouped.  Every mbarrier wait is bounded: on a timeout the warp raises
-// the error word and goes on (the host reports the solve as failed).
+//              the block's rows from the last in the inner loop, in place).
+// Several subdomains share an SM and hide each other's dependent chains.  The
+// arithmetic is the reference's row-oriented envelope substitution
+// (advlas_skyline.c:134-167) with the forward sums regrouped; the grouping
+// depends on the rows' entries and the block boundaries only, so one or two
+// warps per subdomain give the same bits.  The copies of the forward sweep
+// keep their lines in L2 (evict_last) for the backward sweep, whose copies
+// are the lines' last use (evict_first).  Every mbarrier wait is bounded: on
+// a timeout the CTA raises the error word, issues no further copy, waits for
+// the copies in flight and returns (the host reports the solve as failed).
 constexpr int kSB = 32;        // rows per block at most, one per lane
-constexpr int kSGroup = 8;     // rows whose partial sums are reduced together
 
 struct StageLayout {
-  size_t y, buf0, buf1, xb, rb, meta, bar, blk, total;
+  size_t y, buf0, buf1, xb, rb, meta, gmin, bar, blk, total;
 };
 
 // Shared-memory slice of one subdomain warp of the staged solve.
@@ -657,34 +660,34 @@ __host__ __device__ inline StageLayout stage_layout(int max_interior, int max_bl
   o += a16(2 * kSB * es);
   l.meta = o;
   o += kSB * 8;
-  l.bar = o;
+  l.gmin = o;
   o += 16;
+  l.bar = o;
+  o += 32;
   l.blk = o;
   o += a16(((size_t)max_blocks + 1) * 8);
   l.total = o;
   return l;
 }
 
-// 8 complex partial sums per lane -> lanes 4r..4r+3 hold the warp total of row r
+// Forward sweep over the row blocks.  Per block of nb <= 32 rows starting at
+// row r0:
+//   - the entries left of the block: eight lanes per row, four rows per
+//     warp step (row groups of four shared out over the warps); lane j of a
+//     row sums the row's entries j, j+8, j+16, ... in order into one
+//     accumulator, and three shuffles add the eight lanes.  The sum of a row
+//     therefore depends on its entries alone, not on the staging capacity or
+//     the number of warps;
+//   - the block's triangle: lane t holds row r0 + t, one broadcast shuffle per
+//     row, the operands of 4 steps loaded ahead;
+//   - the pivot scaling z = y/d goes to the z stash for the backward sweep.
+// Returns false when a staged copy did not arrive (error word raised); the
+// caller drains the copies in flight and stops.
 template <typename T>
-__device__ __forceinline__ T transpose_reduce8(const T (&a)[kSGroup], int lane) {
-  const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
-  T b[4];
-#pragma unroll
-  for (int i = 0; i < 4; i++) b[i] = cadd(h16 ? a[i + 4] : a[i], shfl_xor(h16 ? a[i] : a[i + 4], 16));
-  T c[2];
-#pragma unroll
-  for (int i = 0; i < 2; i++) c[i] = cadd(h8 ? b[i + 2] : b[i], shfl_xor(h8 ? b[i] : b[i + 2], 8));
-  T d = cadd(h4 ? c[1] : c[0], shfl_xor(h4 ? c[0] : c[1], 4));
-  d = cadd(d, shfl_xor(d, 2));
-  d = cadd(d, shfl_xor(d, 1));
-  return d;
-}
-
-template <typename T>
-__device__ void staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
+__device__ bool staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
                                T *y, int2 *meta, T *zstash, T *rectb, int tid, int nw) {
   const int lane = tid & 31, w = tid >> 5;
+  const int q = lane >> 3, j = lane & 7;
   int nlo, npr;
   stage_issue(st, 0, tid);
   stage_row_meta(lo_g, ptr_g, base, st.blk[0].x, st.blk[1].x, lane, nlo, npr);
@@ -696,91 +699,46 @@ __device__ void staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, cons
       stage_issue(st, b + 1, tid);
       stage_row_meta(lo_g, ptr_g, base, st.blk[b + 1].x, st.blk[b + 2].x, lane, nlo, npr);
     }
-    stage_wait(st, b);
-    __syncthreads();
+    const bool late = !stage_wait(st, b);
+    if (__syncthreads_or(late)) return false;
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);  // S[e]: entry e of the envelope
-    // entries left of the block, split over the warps.  FP32: each lane walks
-    // its own row (a share of it per warp; two accumulators, 4 entries' loads
-    // in flight).  FP64: lanes across a row, 8 rows' loads issued together and
-    // one transpose-reduction per 8 rows, groups of 8 rows shared out over the
-    // warps (16-byte entries make the per-lane walk's bank conflicts too costly).
-    if (sizeof(T) == 8) {
-      const int my_len = lane < nb ? max(0, r0 - my_lo) : 0;
-      const int kbeg = (my_len * w) / nw, cnt = (my_len * (w + 1)) / nw - kbeg;
-      int longest = cnt;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, o));
-      const T *row = S + my_pr + kbeg;
-      const T *yr = y + (lane < nb ? my_lo : 0) + kbeg;
-      T acc0 = czero<T>(), acc1 = czero<T>();
-      for (int k = 0; k < longest; k += 4) {
-        T a[4], bv[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const bool in = k + u < cnt;
-          a[u] = in ? row[k + u] : czero<T>();
-          bv[u] = in ? yr[k + u] : czero<T>();
-        }
-        acc0 = cadd(acc0, cmul(a[0], bv[0]));
-        acc1 = cadd(acc1, cmul(a[1], bv[1]));
-        acc0 = cadd(acc0, cmul(a[2], bv[2]));
-        acc1 = cadd(acc1, cmul(a[3], bv[3]));
+    for (int g = w; 4 * g < nb; g += nw) {
+      const int t = 4 * g + q;
+      const int2 mt = t < nb ? meta[t] : make_int2(r0, 0);
+      const int len = t < nb ? max(0, r0 - mt.x) : 0;
+      int longest = max(len, __shfl_xor_sync(0xffffffffu, len, 8));
+      longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, 16));
+      const T *row = S + mt.y;  // the row's entries from its first column
+      const T *yr = y + mt.x;
+      T acc = czero<T>();
+      for (int k = j; k < longest; k += 16) {
+        const bool i0 = k < len, i1 = k + 8 < len;
+        const T a0 = i0 ? row[k] : czero<T>(), b0 = i0 ? yr[k] : czero<T>();
+        const T a1 = i1 ? row[k + 8] : czero<T>(), b1 = i1 ? yr[k + 8] : czero<T>();
+        acc = cmac(acc, a0, b0);
+        acc = cmac(acc, a1, b1);
       }
-      rectb[w * 32 + lane] = cadd(acc0, acc1);
-    } else {
-      for (int g = w * kSGroup; g < nb; g += kSGroup * nw) {
-        int2 mt[kSGroup];
-        int len[kSGroup];
-#pragma unroll
-        for (int u = 0; u < kSGroup; u++) {
-          mt[u] = meta[g + u];
-          len[u] = g + u < nb ? max(0, r0 - mt[u].x) : 0;
-        }
-        T a0[kSGroup], b0[kSGroup], a1[kSGroup], b1[kSGroup];
-#pragma unroll
-        for (int u = 0; u < kSGroup; u++) {
-          const bool c0 = lane < len[u], c1 = lane + 32 < len[u];
-          a0[u] = c0 ? S[mt[u].y + lane] : czero<T>();
-          b0[u] = c0 ? y[mt[u].x + lane] : czero<T>();
-          a1[u] = c1 ? S[mt[u].y + lane + 32] : czero<T>();
-          b1[u] = c1 ? y[mt[u].x + lane + 32] : czero<T>();
-        }
-        T acc[kSGroup];
-        int longest = 0;
-#pragma unroll
-        for (int u = 0; u < kSGroup; u++) {
-          acc[u] = cadd(cmul(a0[u], b0[u]), cmul(a1[u], b1[u]));
-          longest = max(longest, len[u]);
-        }
-        if (longest > 64) {
-#pragma unroll
-          for (int u = 0; u < kSGroup; u++)
-            for (int k = lane + 64; k < len[u]; k += 32) acc[u] = cadd(acc[u], cmul(S[mt[u].y + k], y[mt[u].x + k]));
-        }
-        const T sum = transpose_reduce8(acc, lane);
-        if ((lane & 3) == 0) rectb[g + (lane >> 2)] = sum;  // lanes 4r.. hold row g + r
-      }
+      acc = cadd(acc, shfl_xor(acc, 4));
+      acc = cadd(acc, shfl_xor(acc, 2));
+      acc = cadd(acc, shfl_xor(acc, 1));
+      if (j == 0 && t < nb) rectb[t] = acc;
     }
     __syncthreads();
     if (w == 0) {
-      T rect = rectb[lane];
-      if (sizeof(T) == 8)
-        for (int k = 1; k < nw; k++) rect = cadd(rect, rectb[k * 32 + lane]);
-      // the block's triangle: lane t holds row r0 + t; the operands of 4 steps
-      // are loaded ahead of their shuffles
+      const T rect = rectb[lane];
       T val = lane < nb ? csub(y[r0 + lane], rect) : czero<T>();
       const T *mine = S + my_pr - my_lo;  // mine[col]: this lane's row at column col
       for (int j0 = 0; j0 < nb - 1; j0 += 4) {
         T op[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-          const int j = j0 + u;
-          op[u] = (lane > j && r0 + j >= my_lo) ? mine[r0 + j] : czero<T>();
+          const int jj = j0 + u;
+          op[u] = (lane > jj && r0 + jj >= my_lo) ? mine[r0 + jj] : czero<T>();
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           const T yj = shfl_idx(val, min(j0 + u, 31));
-          val = csub(val, cmul(op[u], yj));
+          val = cmsub(val, op[u], yj);
         }
       }
       if (lane < nb) {
@@ -790,25 +748,39 @@ __device__ void staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, cons
     }
     __syncthreads();
   }
+  return true;
 }
 
+// Backward sweep, blocks from the last.  Per block: the triangle with lanes
+// over the block's columns (warp 0), then the columns left of the block in
+// 32-column chunks shared out over the warps: the lane of column c applies
+// y_c -= L_tc x_t for the block's rows t from the last to the first, in
+// place, as the reference does (advlas_skyline.c:157-165); a group of eight
+// rows none of which reaches the chunk is skipped.
 template <typename T>
-__device__ void staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
-                                T *y, T *xb, int2 *meta, int tid, int nw) {
+__device__ bool staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
+                                T *y, T *xb, int2 *meta, int *gmin, int tid, int nw) {
   const int lane = tid & 31, w = tid >> 5;
   int nlo, npr;
   stage_row_meta(lo_g, ptr_g, base, st.blk[nblk - 1].x, st.blk[nblk].x, lane, nlo, npr);
   for (int b = nblk - 1; b >= 0; b--) {
     const int r0 = st.blk[b].x, nb = st.blk[b + 1].x - r0;
     const int my_lo = nlo;
-    if (w == 0) meta[lane] = make_int2(nlo, npr);
+    if (w == 0) {
+      meta[lane] = make_int2(nlo, npr);
+      int m = lane < nb ? nlo : INT_MAX;
+      m = min(m, __shfl_xor_sync(0xffffffffu, m, 1));
+      m = min(m, __shfl_xor_sync(0xffffffffu, m, 2));
+      m = min(m, __shfl_xor_sync(0xffffffffu, m, 4));
+      if ((lane & 7) == 0) gmin[lane >> 3] = m;
+    }
     // the forward sweep left blocks nblk-1 and nblk-2 in the buffers
     if (b >= 1) {
       if (b - 1 < nblk - 2) stage_issue(st, b - 1, tid);
       stage_row_meta(lo_g, ptr_g, base, st.blk[b - 1].x, st.blk[b].x, lane, nlo, npr);
     }
-    stage_wait(st, b);
-    __syncthreads();
+    const bool late = !stage_wait(st, b);
+    if (__syncthreads_or(late)) return false;
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);
     if (w == 0) {
       // triangle, lanes over the block's columns; operands of 4 steps loaded ahead
@@ -825,7 +797,7 @@ __device__ void staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
 #pragma unroll
         for (int u = 0; u < 4; u++) {
           const T xi = shfl_idx(val, max(i0 - u, 0));
-          val = csub(val, cmul(op[u], xi));
+          val = cmsub(val, op[u], xi);
         }
       }
       if (lane < nb) {
@@ -837,32 +809,29 @@ __device__ void staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) bmin = min(bmin, __shfl_xor_sync(0xffffffffu, bmin, o));
     __syncthreads();
-    // columns left of the block: y_c -= sum_t L[r0+t][c] x_t, 8 rows' loads in
-    // flight, 32-column chunks shared out over the warps
     for (int cb = bmin + 32 * w; cb < r0; cb += 32 * nw) {
       const int c = cb + lane;
       const bool act = c < r0;
-      T acc0 = czero<T>(), acc1 = czero<T>();
-      for (int t0 = 0; t0 < nb; t0 += kSGroup) {
-        T v[kSGroup], xv[kSGroup];
+      T yc = act ? y[c] : czero<T>();
+      for (int t0 = (nb - 1) & ~7; t0 >= 0; t0 -= 8) {
+        if (gmin[t0 >> 3] >= cb + 32) continue;  // no row of the group reaches this chunk
+        T v[8], xv[8];
 #pragma unroll
-        for (int u = 0; u < kSGroup; u++) {
-          const int t = t0 + u;
+        for (int u = 0; u < 8; u++) {
+          const int t = t0 + 7 - u;
           const int2 mt = meta[t];
           const int d = c - mt.x;
           v[u] = (t < nb && act && d >= 0) ? S[mt.y + d] : czero<T>();
           xv[u] = t < nb ? xb[t] : czero<T>();  // xb past the block may hold anything
         }
 #pragma unroll
-        for (int u = 0; u < kSGroup; u += 2) {
-          acc0 = cadd(acc0, cmul(v[u], xv[u]));
-          acc1 = cadd(acc1, cmul(v[u + 1], xv[u + 1]));
-        }
+        for (int u = 0; u < 8; u++) yc = cmsub(yc, v[u], xv[u]);
       }
-      if (act) y[c] = csub(y[c], cadd(acc0, acc1));
+      if (act) y[c] = yc;
     }
     __syncthreads();
   }
+  return true;
 }
 
 template <typename T>
@@ -883,20 +852,21 @@ __global__ void __launch_bounds__(64) subsolve_staged_kernel(DevProblem p, int m
   T *xb = (T *)(smem_raw + lay.xb);
   T *rectb = (T *)(smem_raw + lay.rb);
   int2 *meta = (int2 *)(smem_raw + lay.meta);
+  int *gmin = (int *)(smem_raw + lay.gmin);
   int2 *blk = (int2 *)(smem_raw + lay.blk);
   Stage<T> st;
   st.buf0 = (T *)(smem_raw + lay.buf0);
   st.buf1 = (T *)(smem_raw + lay.buf1);
   st.bar = (uint64_t *)(smem_raw + lay.bar);
   st.blk = blk;
-  st.uses0 = st.uses1 = 0;
-  st.err = &p.sc->copy_timeout;
+  stage_init(st, &p.sc->copy_timeout, p.stall_test);
   const int64_t base = p.env_ptr[io];
   st.L = (sizeof(T) == 8 ? (const T *)(const void *)p.L32 : (const T *)(const void *)p.L64) + base;
   for (int b = tid; b <= nblk; b += nt) blk[b] = p.blk_tab[b0 + b];
   if (tid == 0) {
     mbar_init(&st.bar[0], 1);
     mbar_init(&st.bar[1], 1);
+    mbar_init(&st.bar[2], 1);
     fence_mbar_init();
   }
   // right-hand side; a refinement step is skipped when its residual is already small
@@ -931,14 +901,20 @@ __global__ void __launch_bounds__(64) subsolve_staged_kernel(DevProblem p, int m
   const int32_t *lo_g = p.env_lo + io;
   const int64_t *ptr_g = p.env_ptr + io;
   T *z = zstash + io;
-  staged_forward<T>(st, nblk, lo_g, ptr_g, base, y, meta, z, rectb, tid, nw);
-  for (int c = tid; c < nI; c += nt) y[c] = z[c];
-  __syncthreads();
-  staged_backward<T>(st, nblk, lo_g, ptr_g, base, y, xb, meta, tid, nw);
-  // every copy was waited for above; after a timed-out wait, wait (bounded) again
-  // so that no copy into this CTA's shared memory is left in flight
-  stage_wait(st, 0);
-  stage_wait(st, 1);
+  // L2: the forward sweep's blocks are read again by the backward sweep, the
+  // backward sweep's reads are the last use
+  st.hint = 1;
+  st.policy = l2_evict_last();
+  bool ok = staged_forward<T>(st, nblk, lo_g, ptr_g, base, y, meta, z, rectb, tid, nw);
+  if (ok) {
+    for (int c = tid; c < nI; c += nt) y[c] = z[c];
+    __syncthreads();
+    st.policy = l2_evict_first();
+    ok = staged_backward<T>(st, nblk, lo_g, ptr_g, base, y, xb, meta, gmin, tid, nw);
+  }
+  // every copy issued into this CTA's shared memory has landed before it exits
+  stage_drain(st);
+  if (!ok) return;
   for (int c = tid; c < nI; c += nt) {
     double2 x = make_double2((double)y[c].x, (double)y[c].y);
     if (accumulate) x = cadd(xout[io + c], x);

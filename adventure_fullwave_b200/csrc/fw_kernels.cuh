@@ -80,6 +80,7 @@ struct DevProblem {
   int32_t cta_smem;              // dynamic shared bytes of the CTA-per-subdomain solve (0: not available)
   int32_t hist_cap;              // entries of hist
   int32_t solve_variant;         // SolveVariant of the batched subdomain solve
+  int32_t stall_test;            // test hook: the staged solves' first copy wait gives up (bounded)
   int32_t max_interior;          // largest subdomain: interior rows
   int32_t max_iface;             // largest subdomain: interface DOFs
   // staged solve (kSolveWarp): row blocks and grid-wide operator products

@@ -153,8 +153,7 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
   st.buf1 = (T *)(smem_raw + lay.buf1);
   st.bar = (uint64_t *)(smem_raw + lay.bar);
   st.blk = blk;
-  st.uses0 = st.uses1 = 0;
-  st.err = &m.ms->err;
+  stage_init(st, &m.ms->err, 0);
   const int64_t base = p.env_ptr[io];
   st.L = (sizeof(T) == 8 ? (const T *)(const void *)p.L32 : (const T *)(const void *)p.L64) + base;
   for (int b = lane; b <= nblk; b += 32) blk[b] = p.blk_tab[b0 + b];
@@ -172,6 +171,7 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
   T *z = zstash + g0;
 
   // forward
+  bool ok = true;
   int nlo, npr;
   stage_issue(st, 0, lane);
   stage_row_meta(lo_g, ptr_g, base, blk[0].x, blk[1].x, lane, nlo, npr);
@@ -182,7 +182,10 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
       stage_issue(st, b + 1, lane);
       stage_row_meta(lo_g, ptr_g, base, blk[b + 1].x, blk[b + 2].x, lane, nlo, npr);
     }
-    stage_wait(st, b);
+    if (!__all_sync(0xffffffffu, stage_wait(st, b))) {
+      ok = false;
+      break;
+    }
     __syncwarp();
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);
     for (int t = 0; t < nb; t++) {
@@ -220,14 +223,17 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
 
   // backward
   stage_row_meta(lo_g, ptr_g, base, blk[nblk - 1].x, blk[nblk].x, lane, nlo, npr);
-  for (int b = nblk - 1; b >= 0; b--) {
+  for (int b = nblk - 1; b >= 0 && ok; b--) {
     const int r0 = blk[b].x, nb = blk[b + 1].x - r0;
     meta[lane] = make_int2(nlo, npr);
     if (b >= 1) {
       if (b - 1 < nblk - 2) stage_issue(st, b - 1, lane);
       stage_row_meta(lo_g, ptr_g, base, blk[b - 1].x, blk[b].x, lane, nlo, npr);
     }
-    stage_wait(st, b);
+    if (!__all_sync(0xffffffffu, stage_wait(st, b))) {
+      ok = false;
+      break;
+    }
     __syncwarp();
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);
     for (int t = nb - 1; t >= 0; t--) {
@@ -250,8 +256,9 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
       __syncwarp();
     }
   }
-  stage_wait(st, 0);
-  stage_wait(st, 1);
+  // every copy issued into this CTA's shared memory has landed before it exits
+  stage_drain(st);
+  if (!ok) return;
   for (int e = lane; e < nI * kRW; e += 32) {
     const int64_t ge = g0 + (int64_t)(e / kRW) * kR + (e % kRW);
     double2 x = make_double2((double)y[e].x, (double)y[e].y);

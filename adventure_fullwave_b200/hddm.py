@@ -61,10 +61,17 @@ def _mesh_struct(model):
     a["flag"] = np.ascontiguousarray(model.flag, dtype=np.int32)
     a["pec"] = np.ascontiguousarray(model.pec_edge, dtype=np.uint8)
     a["sub"] = np.ascontiguousarray(model.sub_of_tet, dtype=np.int32)
+    order = [None] * 4
+    so = getattr(model, "sub_order", None)
+    if so is not None:
+        for k, v in enumerate(so):
+            a[f"ord{k}"] = np.ascontiguousarray(v, dtype=np.int32)
+            order[k] = _ptr(a[f"ord{k}"], ctypes.c_int32)
     mesh = _lib.FwMesh(
         int(a["crd"].shape[0]), _ptr(a["crd"], ctypes.c_double), int(a["tv"].shape[0]),
         _ptr(a["tv"], ctypes.c_int32), _ptr(a["te"], ctypes.c_int32), _ptr(a["flag"], ctypes.c_int32),
-        int(a["pec"].shape[0]), _ptr(a["pec"], ctypes.c_uint8), int(model.nsub), _ptr(a["sub"], ctypes.c_int32))
+        int(a["pec"].shape[0]), _ptr(a["pec"], ctypes.c_uint8), int(model.nsub), _ptr(a["sub"], ctypes.c_int32),
+        *order)
     return mesh, a
 
 
@@ -128,19 +135,13 @@ class HddmSolver:
     def __init__(self, model, hddm_eps: float = 1e-3, hddm_max_loop: int = 4000, precision: str = "fp64",
                  ir_max_steps: int = 1, ir_tol: float = 0.0, graph_iterations: int = 16, device: int = 0,
                  solve_kernel: str = "auto", stage_cap: int = 0, ir_relax: float = 0.0,
-                 shard: Optional[Tuple[int, int]] = None, stage_warps: int = 0):
+                 shard: Optional[Tuple[int, int]] = None, stage_warps: int = 0, stall_copy_test: int = 0):
         lib = _lib.load()
         self._lib = lib
         self.model = model
         self.hddm_eps = float(hddm_eps)
         self.hddm_max_loop = int(hddm_max_loop)
-        a = {}
-        a["crd"] = np.ascontiguousarray(model.vertex_crd, dtype=np.float64)
-        a["tv"] = np.ascontiguousarray(model.tets, dtype=np.int32)
-        a["te"] = np.ascontiguousarray(model.tet_edges, dtype=np.int32)
-        a["flag"] = np.ascontiguousarray(model.flag, dtype=np.int32)
-        a["pec"] = np.ascontiguousarray(model.pec_edge, dtype=np.uint8)
-        a["sub"] = np.ascontiguousarray(model.sub_of_tet, dtype=np.int32)
+        mesh, a = _mesh_struct(model)
         a["mf"] = np.ascontiguousarray(model.mat_flag, dtype=np.int32)
         a["me"] = np.ascontiguousarray(model.mat_eps, dtype=np.float64)
         a["ms"] = np.ascontiguousarray(model.mat_sigma, dtype=np.float64)
@@ -151,10 +152,6 @@ class HddmSolver:
         if getattr(model, "sigma_table", None) is not None:
             a["sf"] = np.ascontiguousarray(model.sigma_table[0], dtype=np.int32)
             a["ms"] = np.ascontiguousarray(model.sigma_table[1], dtype=np.float64)
-        mesh = _lib.FwMesh(
-            int(a["crd"].shape[0]), _ptr(a["crd"], ctypes.c_double), int(a["tv"].shape[0]),
-            _ptr(a["tv"], ctypes.c_int32), _ptr(a["te"], ctypes.c_int32), _ptr(a["flag"], ctypes.c_int32),
-            int(a["pec"].shape[0]), _ptr(a["pec"], ctypes.c_uint8), int(model.nsub), _ptr(a["sub"], ctypes.c_int32))
         mt = _lib.FwMaterial(int(a["ef"].shape[0]), _ptr(a["ef"], ctypes.c_int32), _ptr(a["me"], ctypes.c_double),
                              int(a["sf"].shape[0]), _ptr(a["sf"], ctypes.c_int32), _ptr(a["ms"], ctypes.c_double),
                              float(model.omega))
@@ -163,7 +160,8 @@ class HddmSolver:
         kern = SOLVE_KERNELS[solve_kernel]
         opts = _lib.FwOptions(self.hddm_eps, self.hddm_max_loop, prec, int(ir_max_steps), float(ir_tol),
                               int(graph_iterations), int(device), kern, int(stage_cap), float(ir_relax),
-                              int(shard[0]) if shard else 0, int(shard[1]) if shard else 0, int(stage_warps), 0)
+                              int(shard[0]) if shard else 0, int(shard[1]) if shard else 0, int(stage_warps),
+                              int(stall_copy_test))
         handle = ctypes.c_void_p()
         rc = lib.fwgpu_create(ctypes.byref(mesh), ctypes.byref(mt), ctypes.byref(opts), ctypes.byref(handle))
         if rc != 0 and handle.value:
@@ -381,6 +379,12 @@ class HddmSolver:
         _lib.check(self._lib.fwgpu_get_history(self._h, _ptr(h, ctypes.c_double), n.value, ctypes.byref(n)))
         return h[: n.value]
 
+    def write_calc_log(self, path: str, result: "HddmResult", mode: str = "a") -> None:
+        """Append (or write, mode "w") the last solve's residual history to
+        ``path`` as the reference's calc_log section (``calc_log_section``)."""
+        with open(path, mode) as f:
+            f.write(calc_log_section(self.sizes()["total_free"], result.initial_norm, self.history()))
+
     def sizes(self) -> dict:
         s = _lib.FwSizes()
         _lib.check(self._lib.fwgpu_get_sizes(self._h, ctypes.byref(s)))
@@ -419,6 +423,20 @@ class HddmSolver:
         m = np.zeros(2 * nlen, np.float64)
         _lib.check(self._lib.fwgpu_get_factor(self._h, s, _ptr(m, ctypes.c_double)))
         return m[0::2] + 1j * m[1::2]
+
+
+def calc_log_section(total_free: int, initial_norm: float, history) -> str:
+    """The full-wave section of the reference's convergence log
+    (calc_log/log_g_HDDM_Full_Wave): two blank lines and the title
+    (HDDM_set_HDDM_Opt_log, lib/hddm/set_hddm_func.c:37-51), the interface
+    DOF count (lib/hddm/hddm_solver.h:88-92), the initial line with the
+    max-norm of r0 (lib/hddm/hddm_solver_s.h:203-207) and one line
+    "iteration resi" per interface iteration (:319-323), in the reference's
+    printf formats."""
+    lines = ["", "", "# Full Wave Analysis", f"# DOF on interface {int(total_free)}",
+             f"0 {1.0:e}  # Norm {float(initial_norm):e}"]
+    lines += [f"{k} {float(r):e}" for k, r in enumerate(history, 1)]
+    return "\n".join(lines) + "\n"
 
 
 def relative_permittivity_gradient(g_eps: np.ndarray, g_sigma: np.ndarray, omega: float, eps0: float = 8.854e-12):

@@ -92,6 +92,10 @@ class Model:
     # they differ from the joint table above: (flags, values) each
     eps_table: Optional[Tuple[np.ndarray, np.ndarray]] = None
     sigma_table: Optional[Tuple[np.ndarray, np.ndarray]] = None
+    # each subdomain's local vertex and edge order, as a model file gives it
+    # (its node order): (vertex ptr, vertex ids, edge ptr, edge ids), or None
+    # for ascending global id
+    sub_order: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]] = None
 
     @property
     def n_vertices(self) -> int:

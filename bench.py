@@ -167,7 +167,8 @@ def sample_model():
     m = meshgen.Model(name="sample", n=0, size=0.0, vertex_crd=z["vertex_crd"], tets=tets, tet_edges=tet_edges,
                       edges=edges, flag=z["flag"].astype(np.int32), mat_flag=z["mat_flag"], mat_eps=z["mat_eps"],
                       mat_sigma=z["mat_sigma"], omega=float(z["omega"][0]), pec_edge=np.zeros(ne, bool),
-                      sub_of_tet=z["sub_of_tet"].astype(np.int32), nsub=int(z["nsub"][0]), sources=[])
+                      sub_of_tet=z["sub_of_tet"].astype(np.int32), nsub=int(z["nsub"][0]), sources=[],
+                      sub_order=(z["sub_vertex_ptr"], z["sub_vertex_order"], z["sub_edge_ptr"], z["sub_edge_order"]))
     jo = np.zeros((1, m.n_vertices, 3))
     jor = np.zeros((1, m.n_vertices, 3))
     jo[0, z["antenna_vertices"]] = z["antenna_Jo"]

@@ -69,6 +69,20 @@ typedef struct {
   const uint8_t *pec_edge;     /* n_edges, 1 = edge on the PEC wall (DirichletBCs_Axn0) */
   int32_t n_subdomains;
   const int32_t *sub_of_tet;   /* n_tets, subdomain of each element */
+  /* Optional (all four NULL: ascending global id in every subdomain): each
+   * subdomain's own local order, the node order (snid) of the reference's
+   * part files.  The reference numbers a subdomain's vertices and then its
+   * mid-nodes by their rank in that order (make_MESH_make_ap,
+   * make_MESH_change_ap, lib/fem/make_MESH.c:237-272,539-552), which sets
+   * the skyline profiles and with them the factors' rounding.  Subdomain s
+   * lists its vertices in sub_vertex_order[sub_vertex_ptr[s] ..
+   * sub_vertex_ptr[s+1]) and its edges in sub_edge_order[sub_edge_ptr[s] ..
+   * sub_edge_ptr[s+1]); each list must hold every vertex (edge) of the
+   * subdomain's elements exactly once. */
+  const int32_t *sub_vertex_ptr;   /* n_subdomains+1 */
+  const int32_t *sub_vertex_order; /* global vertex ids */
+  const int32_t *sub_edge_ptr;     /* n_subdomains+1 */
+  const int32_t *sub_edge_order;   /* global edge ids */
 } fwgpu_mesh;
 
 /* Material table: the reference's MTRL (lib/std/types.h:257-279) as read
@@ -133,7 +147,10 @@ typedef struct {
   int32_t shard_begin;   /* sharded solve: this context solves subdomains [shard_begin, shard_end) */
   int32_t shard_end;     /* (0, 0 = every subdomain); drive it with the fwgpu_shard_* calls */
   int32_t stage_warps;   /* WARP kernel: warps sharing a subdomain's sweeps, 1 or 2 (0 = timed choice) */
-  int32_t reserved;
+  int32_t stall_copy_test; /* test hook, 0 in normal use: 1 makes the staged subdomain solves' first wait
+                              for a copy poll a barrier that nothing completes, give up after a few polls
+                              and raise FWGPU_ERR_TIMEOUT (each CTA still waits for its copies in flight
+                              before it exits) */
 } fwgpu_options;
 
 /* Batched subdomain-solve kernels.  AUTO times one launch of each candidate

@@ -78,6 +78,17 @@ typedef struct {
   double *im;
 } SubSource;
 static SubSource *g_src = NULL;
+/* the same sources by global node id of the mid-node */
+static int g_srcn = 0;
+static int *g_srcg = NULL;
+static double *g_srcv = NULL;
+
+#ifdef FW_HARNESS_GPU
+/* adventure_fullwave_b200/dropin/set_hddm_func_gpu.c: the reference's table
+   with the subdomain and interface slots on the GPU library */
+void set_hddm_func_fullwave_gpu(HDDM_FUNC *f, OPTIONS options);
+void hddm_gpu_set_edge_source(int n, const int *mid_gnid, const double *re_im);
+#endif
 
 /* antenna currents of <dir>/antenna.txt: per antenna its element flag and the
    reference's Jo / Jor (3 per global vertex); per subdomain an ANTENNA array
@@ -209,6 +220,18 @@ static void harness_solve_dom_last(DomMesh *dm, SolvOpt solvopt, int (*s)(AIJ_MA
 }
 
 static void set_hddm_func_harness(HDDM_FUNC *f, OPTIONS options) {
+#ifdef FW_HARNESS_GPU
+  /* the GPU table: only the once-per-step slots are timed; the
+     per-subdomain slots of that table do nothing */
+  set_hddm_func_fullwave_gpu(f, options);
+  ref_iteration_s = f->iteration_s;
+  ref_iteration_s_1st = f->iteration_s_1st;
+  ref_solve_dom_last = f->solve_dom_last;
+  f->iteration_s_1st = harness_iteration_s_1st;
+  f->iteration_s = harness_iteration_s;
+  f->solve_dom_last = harness_solve_dom_last;
+  return;
+#endif
   set_hddm_func_fullwave(f, options);
   ref_make_TMP_AIJ = f->make_TMP_AIJ;
   ref_solve_dom_1st = f->solve_dom_1st;
@@ -245,6 +268,12 @@ static void load_sources(const char *dir, PartMesh *pm) {
     int gnid;
     double re, im;
     if (fscanf(f, "%d %lf %lf", &gnid, &re, &im) != 3) break;
+    g_srcg = (int *)realloc(g_srcg, sizeof(int) * (g_srcn + 1));
+    g_srcv = (double *)realloc(g_srcv, sizeof(double) * 2 * (g_srcn + 1));
+    g_srcg[g_srcn] = gnid;
+    g_srcv[2 * g_srcn] = re;
+    g_srcv[2 * g_srcn + 1] = im;
+    g_srcn++;
     for (int d = 0; d < pm->ndomain; d++) {
       DomMesh *dm = &pm->dm[d];
       int *g = edge_gnid(pm, dm);
@@ -346,16 +375,22 @@ static void dump_jo(PartMesh *pms, int nparts) {
   fclose(f);
 }
 
-static void dump_ints(PartMesh *pm) {
+/* every part's subdomains, parts in order; the header counts all of them and
+   gives the first part's interface sizes */
+static void dump_ints(PartMesh *pms, int nparts) {
   char path[FILENAME_MAX];
   snprintf(path, sizeof(path), "%s.ints", g_prefix);
   FILE *f = fopen(path, "wb");
   if (!f) return;
-  w_i32(f, pm->ndomain);
-  w_i32(f, pm->infree);
-  w_i32(f, pm->outfree);
-  w_i32(f, pm->total_free);
-  for (int d = 0; d < pm->ndomain; d++) {
+  int total = 0;
+  for (int q = 0; q < nparts; q++) total += pms[q].ndomain;
+  w_i32(f, total);
+  w_i32(f, pms[0].infree);
+  w_i32(f, pms[0].outfree);
+  w_i32(f, pms[0].total_free);
+  for (int q = 0; q < nparts; q++)
+  for (int d = 0; d < pms[q].ndomain; d++) {
+    PartMesh *pm = &pms[q];
     DomMesh *dm = &pm->dm[d];
     w_i32(f, dm->nmp);
     w_i32(f, dm->nap);
@@ -507,7 +542,7 @@ int main(int argc, char **argv) {
   double t_init = t_now() - t0;
   load_sources(model_dir, &g_pm[0]);
   load_antennas(model_dir, &g_pm[0]);
-  if (g_dump >= 1) dump_ints(&g_pm[0]);
+  if (g_dump >= 1) dump_ints(g_pm, nrepeat);
   if (g_dump >= 2) {
     char path[FILENAME_MAX];
     snprintf(path, sizeof(path), "%s.aij", g_prefix);
@@ -518,10 +553,16 @@ int main(int argc, char **argv) {
 
   hddm_sw.t_loop = -2;
   hddm_sw.antenna = -1;
+#ifdef FW_HARNESS_GPU
+  hddm_gpu_set_edge_source(g_srcn, g_srcg, g_srcv);
+#endif
   {
     char path[FILENAME_MAX];
+#ifndef FW_HARNESS_GPU
+    /* the residuals are read from the reference's own interface vectors */
     snprintf(path, sizeof(path), "%s.hist", g_prefix);
     f_hist = fopen(path, "wb");
+#endif
     snprintf(path, sizeof(path), "%s.itimes", g_prefix);
     f_itimes = fopen(path, "wb");
   }

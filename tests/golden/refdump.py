@@ -14,6 +14,8 @@ import numpy as np
 
 REPO = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
 HARNESS = os.path.join(REPO, "oracle", "_ref", "fw_ref_harness")
+# the same driver with the reference's table replaced by the GPU drop-in
+HARNESS_GPU = os.path.join(REPO, "oracle", "_ref", "fw_ref_gpu")
 
 
 def read_ints(path: str, nv: int):
@@ -136,7 +138,8 @@ def read_log(path: str):
     return norm0, np.array(hist)
 
 
-def run_harness(model, hddm_eps: float, hddm_max_loop: int, dump: int = 2, workdir: str = None, timeout=3600):
+def run_harness(model, hddm_eps: float, hddm_max_loop: int, dump: int = 2, workdir: str = None, timeout=3600,
+                binary: str = HARNESS):
     """Write ``model`` in the reference's part-file layout and run the
     reference on it.  Returns a dict of the parsed outputs."""
     from adventure_fullwave_b200 import meshgen
@@ -146,16 +149,19 @@ def run_harness(model, hddm_eps: float, hddm_max_loop: int, dump: int = 2, workd
     mdir = os.path.join(wd, "MODEL")
     meshgen.write_hddm_model(model, mdir)
     env = dict(os.environ, FW_HARNESS_DUMP=str(dump), FW_HARNESS_OUT=os.path.join(mdir, "ref"))
-    cmd = [HARNESS, "-memlimit", "60000", "-hddm-eps", repr(hddm_eps), "-hddm-max-loop", str(hddm_max_loop), "MODEL"]
+    cmd = [binary, "-memlimit", "60000", "-hddm-eps", repr(hddm_eps), "-hddm-max-loop", str(hddm_max_loop), "MODEL"]
     subprocess.run(cmd, cwd=wd, env=env, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
                    timeout=timeout)
     nv = model.n_vertices
     out = dict(json=json.load(open(os.path.join(mdir, "ref.json"))))
     out["x"] = read_sol(os.path.join(mdir, "ref.sol"), nv, model.n_edges)
     out["norm0"], out["hist"] = read_log(os.path.join(mdir, "calc_log", "log_g_HDDM_Full_Wave"))
-    # the same history at full precision, recorded by the harness
-    h = np.fromfile(os.path.join(mdir, "ref.hist"), dtype="<f8")
-    out["norm0_full"], out["hist_full"] = float(h[0]), h[1:].copy()
+    # the same history at full precision, recorded by the harness (not by the
+    # GPU table, whose interface vectors stay on the device)
+    hp = os.path.join(mdir, "ref.hist")
+    if os.path.exists(hp):
+        h = np.fromfile(hp, dtype="<f8")
+        out["norm0_full"], out["hist_full"] = float(h[0]), h[1:].copy()
     # seconds of each interface iteration after the first (subdomain solves + COCG step)
     out["iteration_s"] = np.fromfile(os.path.join(mdir, "ref.itimes"), dtype="<f8")
     if dump >= 1:

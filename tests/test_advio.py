@@ -123,6 +123,26 @@ def test_sample_fixture_matches_the_reader():
     assert np.array_equal(es.antenna_Jo[0], jo) and np.array_equal(es.antenna_Jor[0], jor)
 
 
+def test_sample_maps_match_the_reference():
+    """The shipped sample's integer setup with every subdomain in the part
+    file's node order: nop, Dirichlet list, interface DOFs and the edge of
+    every local DOF equal the reference's own (make_PartMesh_FW on the six
+    parts, dumped by oracle/ref_harness.c), for all 438 subdomains."""
+    import bench
+    from adventure_fullwave_b200 import hddm
+
+    m, z = bench.sample_model()
+    part = hddm.Partition(m)
+    assert part.n_subdomains == 438
+    for k in range(m.nsub):
+        got = part.maps(k)
+        for key, name in (("nop", "nop"), ("ibc", "ibc"), ("inbc_nfid", "inbc_nfid")):
+            p = z[f"ref_{key}_ptr"]
+            assert np.array_equal(np.asarray(got[name]).ravel(), z[f"ref_{key}"][p[k]:p[k + 1]]), (k, key)
+        d = z["ref_dof_ptr"]
+        assert np.array_equal(got["edge_gid"], z["ref_edge"][d[k]:d[k + 1]]), k
+
+
 def test_antenna_definition_shapes():
     """Parallelepiped and double sectorial cylinder definitions on a small
     model: currents only on vertices of the antenna's elements inside the

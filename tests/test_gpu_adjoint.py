@@ -3,15 +3,15 @@ the oracle and against central finite differences of GPU forward solves."""
 import numpy as np
 import pytest
 
-from adventure_fullwave_b200 import hddm
+from adventure_fullwave_b200 import hddm, meshgen
 from test_oracle_adjoint import perturbed, small_design_model
 from oracle import oracle
 
 pytestmark = pytest.mark.gpu
 
 
-def gpu_objective(model):
-    with hddm.HddmSolver(model, hddm_eps=1e-12, hddm_max_loop=20000) as s:
+def gpu_objective(model, hddm_eps=1e-12, hddm_max_loop=20000):
+    with hddm.HddmSolver(model, hddm_eps=hddm_eps, hddm_max_loop=hddm_max_loop) as s:
         s.solve(0)
         x = s.edge_solution()
     return float(np.sum(np.abs(x[model.probe_edges]) ** 2))
@@ -46,3 +46,39 @@ def test_adjoint_requires_a_forward_solve():
         with pytest.raises(_lib.FwgpuError) as e:
             s.adjoint_gradient()
         assert e.value.code == _lib.ERR_STATE
+
+
+def test_c4_gradient_vs_central_differences():
+    """C4 (the C2 mesh, 663,552 tets, with 10,368 design tets of their own
+    complex eps_r): the adjoint gradient against central differences of
+    forward solves at 16 seeded design tets, for the real and the imaginary
+    part of eps_r.  Step: 1e-6 |eps_r| in each part; eps = eps0 eps' and
+    sigma = omega eps0 eps'' (the reference's convention)."""
+    eps0 = meshgen.EPS0
+    m = meshgen.make_model("c4")
+    meshgen.round_trip_material(m)
+    assert m.design_tets.shape[0] == 10368
+    tol = dict(hddm_eps=1e-10, hddm_max_loop=60000)
+    with hddm.HddmSolver(m, **tol) as s:
+        s.solve(0)
+        J, ge, gs, ra = s.adjoint_gradient()
+    assert ra.converged
+    d_re, d_im = hddm.relative_permittivity_gradient(ge, gs, m.omega, eps0)
+    picks = np.random.default_rng(2024).choice(m.design_tets.shape[0], 16, replace=False)
+    dev_re, dev_im = [], []
+    for k in picks:
+        t = int(m.design_tets[k])
+        i = int(np.searchsorted(m.mat_flag, m.flag[t]))
+        er = complex(m.mat_eps[i] / eps0, m.mat_sigma[i] / (m.omega * eps0))
+        h = 1e-6 * abs(er)
+        he, hs = eps0 * h, m.omega * eps0 * h
+        fd_re = (gpu_objective(perturbed(m, t, d_eps=he), **tol) - gpu_objective(perturbed(m, t, d_eps=-he), **tol)) / (2 * h)
+        fd_im = (gpu_objective(perturbed(m, t, d_sigma=hs), **tol)
+                 - gpu_objective(perturbed(m, t, d_sigma=-hs), **tol)) / (2 * h)
+        dev_re.append(abs(fd_re - d_re[k]))
+        dev_im.append(abs(fd_im - d_im[k]))
+    scale_re, scale_im = np.max(np.abs(d_re[picks])), np.max(np.abs(d_im[picks]))
+    print(f"C4 FD vs adjoint, 16 tets: max |dev| / max |g|: eps' {max(dev_re) / scale_re:.1e}, "
+          f"eps'' {max(dev_im) / scale_im:.1e}")
+    assert max(dev_re) <= 1e-3 * scale_re
+    assert max(dev_im) <= 1e-3 * scale_im

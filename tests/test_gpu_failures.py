@@ -78,3 +78,19 @@ def test_nan_source_in_a_batch_stops_that_source_only():
         with pytest.raises(_lib.FwgpuError) as e:
             s.solve_multi([m.sources[1], bad])
         assert e.value.code == _lib.ERR_NONFINITE
+
+
+def test_copy_wait_timeout_is_reported():
+    """The staged solves' bounded wait for a copy: with the test hook the
+    first wait polls an mbarrier that nothing completes, gives up after a
+    few polls, raises the error word, and the kernel still waits for its
+    copies in flight before it exits.  The host reports FWGPU_ERR_TIMEOUT;
+    the device stays usable (a context without the hook solves normally)."""
+    m = _model()
+    with hddm.HddmSolver(m, hddm_eps=1e-8, hddm_max_loop=3000, solve_kernel="warp", stall_copy_test=1) as s:
+        s.make_tmp_aij(0)
+        with pytest.raises(_lib.FwgpuError) as e:
+            s.solve_dom_1st()
+        assert e.value.code == _lib.ERR_TIMEOUT
+    x, r = hddm.hddm_solver_CS(m, 0, hddm_eps=1e-8, hddm_max_loop=3000, solve_kernel="warp")
+    assert r.converged and np.isfinite(x).all()
