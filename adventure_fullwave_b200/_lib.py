@@ -121,6 +121,8 @@ SIGNATURES = {
     "fwgpu_profile_post": [ctypes.c_void_p, c_i32, P(c_dbl)],
     "fwgpu_hddm_solve_multi": [ctypes.c_void_p, c_i32, P(FwSource), P(FwResult)],
     "fwgpu_get_edge_solution_multi": [ctypes.c_void_p, c_i32, P(c_dbl)],
+    "fwgpu_adjoint_gradient_multi": [ctypes.c_void_p, c_i32, P(c_i32), c_i32, P(c_i32), P(c_dbl), P(c_dbl), P(c_dbl),
+                                     P(FwResult)],
     "fwgpu_shard_set_exchange": [ctypes.c_void_p, ctypes.c_void_p],
     "fwgpu_shard_first": [ctypes.c_void_p],
     "fwgpu_shard_first_finish": [ctypes.c_void_p, P(c_i32)],

@@ -1147,16 +1147,12 @@ static int read_multi_status(fwgpu_context *c) {
   return FWGPU_OK;
 }
 
-int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *srcs, fwgpu_result *res) {
-  if (!c || !srcs || !res) return set_error(FWGPU_ERR_ARG, "null argument");
-  if (n_src < 1 || n_src > fw::kMaxRhs) return set_error(FWGPU_ERR_ARG, "n_src outside 1..FWGPU_MAX_RHS");
-  if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
-  if (c->opts.hddm_max_loop == 0) return set_error(FWGPU_ERR_ARG, "hddm_max_loop is 0");
+// The batched solve of n_src sources on the context's factors (assembled and
+// factored already): right-hand sides, first solves, the COCGs in lockstep,
+// last solves.
+static int multi_run(fwgpu_context *c, int32_t n_src, const fwgpu_source *srcs, fwgpu_result *res) {
   const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
-  c->launches = 0;
   c->multi_n = 0;
-  FW_TRY(fwgpu_make_tmp_aij(c, &srcs[0]));
-  FW_TRY(fwgpu_solve_dom_1st(c));
   if (!c->warp_ok) return set_error(FWGPU_ERR_ARG, "batched sources need the staged solve kernel");
   const size_t smem = fw::multi_smem_bytes(c->dp.max_interior, c->dp.max_blocks, c->dp.stage_cap, fp32);
   if (fw::configure_multi(smem, fp32) != 0)
@@ -1234,6 +1230,99 @@ int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *
   c->multi_n = n_src;
   if (any_bad) return set_error(FWGPU_ERR_NONFINITE, "an interface residual became NaN or infinite");
   return all_conv ? FWGPU_OK : set_error(FWGPU_ERR_NOT_CONVERGED, "hddm_max_loop reached before hddm_eps");
+}
+
+int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *srcs, fwgpu_result *res) {
+  if (!c || !srcs || !res) return set_error(FWGPU_ERR_ARG, "null argument");
+  if (n_src < 1 || n_src > fw::kMaxRhs) return set_error(FWGPU_ERR_ARG, "n_src outside 1..FWGPU_MAX_RHS");
+  if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
+  if (c->opts.hddm_max_loop == 0) return set_error(FWGPU_ERR_ARG, "hddm_max_loop is 0");
+  c->launches = 0;
+  c->multi_n = 0;
+  FW_TRY(fwgpu_make_tmp_aij(c, &srcs[0]));
+  FW_TRY(fwgpu_solve_dom_1st(c));
+  return multi_run(c, n_src, srcs, res);
+}
+
+int fwgpu_adjoint_gradient_multi(fwgpu_context *c, int32_t n_probe, const int32_t *probe_edges, int32_t n_design,
+                                 const int32_t *design_tets, double *J, double *grad_eps, double *grad_sigma,
+                                 fwgpu_result *adjoint_results) {
+  if (!c || n_probe < 0 || n_design < 0 || (n_probe > 0 && !probe_edges) || (n_design > 0 && !design_tets))
+    return set_error(FWGPU_ERR_ARG, "bad argument");
+  const int n_src = c->multi_n;
+  if (n_src < 1) return set_error(FWGPU_ERR_STATE, "the batched adjoint needs a batched forward solve");
+  for (int k = 0; k < n_probe; k++)
+    if (probe_edges[k] < 0 || probe_edges[k] >= c->m.ne) return set_error(FWGPU_ERR_ARG, "probe edge out of range");
+  for (int k = 0; k < n_design; k++)
+    if (design_tets[k] < 0 || design_tets[k] >= c->m.nt) return set_error(FWGPU_ERR_ARG, "design element out of range");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  const int64_t ne = c->m.ne;
+  if (!c->d_te) FW_TRY(c->upload(&c->d_te, c->m.te));
+  // every source's forward solution, and its probe values on the host
+  double2 *d_xf = nullptr;
+  FW_TRY(c->alloc(&d_xf, (size_t)ne * n_src));
+  std::vector<double2> probe_x((size_t)n_src * std::max(1, n_probe));
+  for (int k = 0; k < n_src; k++) {
+    fw::launch_multi_edge_solution(c->mp, k, ne, c->d_edge_src, d_xf + (size_t)k * ne, c->stream);
+    for (int q = 0; q < n_probe; q++)
+      FW_CUDA(cudaMemcpyAsync(&probe_x[(size_t)k * n_probe + q], d_xf + (size_t)k * ne + probe_edges[q],
+                              sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  }
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  c->launches += n_src;
+  // J_k and the adjoint sources dJ_k/dx = conj(x_k at the probes)
+  std::vector<int32_t> pe(probe_edges, probe_edges + n_probe);
+  std::vector<double> pv(2 * (size_t)n_src * std::max(1, n_probe));
+  std::vector<fwgpu_source> srcs(n_src);
+  for (int k = 0; k < n_src; k++) {
+    double Jv = 0.0;
+    for (int q = 0; q < n_probe; q++) {
+      const double2 v = probe_x[(size_t)k * n_probe + q];
+      Jv += v.x * v.x + v.y * v.y;
+      pv[2 * ((size_t)k * n_probe + q)] = v.x;
+      pv[2 * ((size_t)k * n_probe + q) + 1] = -v.y;
+    }
+    if (J) J[k] = Jv;
+    srcs[k] = fwgpu_source{n_probe, pe.data(), pv.data() + 2 * (size_t)k * n_probe};
+  }
+  std::vector<fwgpu_result> ares(n_src);
+  // the adjoint right-hand sides are dJ_k/dx alone, on the forward factors
+  c->el_src_off = true;
+  const int rc = multi_run(c, n_src, srcs.data(), ares.data());
+  c->el_src_off = false;
+  if (adjoint_results)
+    for (int k = 0; k < n_src; k++) adjoint_results[k] = ares[k];
+  if (rc != FWGPU_OK && rc != FWGPU_ERR_NOT_CONVERGED) {
+    c->release(d_xf);
+    return rc;
+  }
+  int32_t *d_design = nullptr;
+  double *d_g = nullptr;
+  std::vector<int32_t> dt(design_tets, design_tets + n_design);
+  const int nd1 = std::max(1, n_design);
+  FW_TRY(c->upload(&d_design, dt));
+  FW_TRY(c->alloc(&d_g, 2 * (size_t)nd1));
+  if (!c->d_xedge) FW_TRY(c->alloc(&c->d_xedge, ne));
+  std::vector<double> gh(2 * (size_t)nd1);
+  for (int k = 0; k < n_src; k++) {
+    fw::launch_multi_edge_solution(c->mp, k, ne, c->d_edge_src, c->d_xedge, c->stream);
+    fw::launch_adjoint_gradient(n_design, d_design, c->d_tv, c->d_te, c->d_crd, c->m.omega, d_xf + (size_t)k * ne,
+                                c->d_xedge, d_g, d_g + nd1, c->stream);
+    FW_CUDA(cudaGetLastError());
+    FW_CUDA(cudaMemcpyAsync(gh.data(), d_g, gh.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FW_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < n_design; i++) {
+      if (grad_eps) grad_eps[(size_t)k * n_design + i] = gh[i];
+      if (grad_sigma) grad_sigma[(size_t)k * n_design + i] = gh[nd1 + i];
+    }
+  }
+  c->launches += 2 * n_src;
+  c->xedge_ok = false;
+  c->release(d_design);
+  c->release(d_g);
+  c->release(d_xf);
+  return rc;
 }
 
 int fwgpu_get_edge_solution_multi(fwgpu_context *c, int32_t k, double *x) {

@@ -168,6 +168,7 @@ class HddmSolver:
             lib.fwgpu_destroy(handle)
         _lib.check(rc)
         self._h = handle
+        self._multi_n = 0
         self.n_edges = int(model.n_edges)
         self.n_tets = int(model.n_tets)
         if getattr(model, "element_source", None) is not None:
@@ -261,7 +262,9 @@ class HddmSolver:
         arr = (_lib.FwSource * len(srcs))(*[s for s, _ in srcs])
         res = (_lib.FwResult * len(srcs))()
         allow = () if raise_not_converged else (_lib.ERR_NOT_CONVERGED,)
+        self._multi_n = 0
         _lib.check(self._lib.fwgpu_hddm_solve_multi(self._h, len(srcs), arr, res), allow=allow)
+        self._multi_n = len(srcs)
         return [self._result(r) for r in res]
 
     def edge_solution_multi(self, k: int) -> np.ndarray:
@@ -301,6 +304,27 @@ class HddmSolver:
                                                     ctypes.byref(res)), allow=(_lib.ERR_NOT_CONVERGED,))
         n = dt.shape[0]
         return J.value, ge[:n], gs[:n], self._result(res)
+
+    def adjoint_gradient_multi(self, probe_edges=None, design_tets=None):
+        """Backward of the last ``solve_multi`` for every source at once: the
+        adjoint right-hand sides of all sources in one batched solve on the
+        same factors.  Returns (J (n_src,), dJ/deps (n_src, n_design),
+        dJ/dsigma (n_src, n_design), adjoint HddmResults)."""
+        pe = np.ascontiguousarray(self.model.probe_edges if probe_edges is None else probe_edges, dtype=np.int32)
+        dt = np.ascontiguousarray(self.model.design_tets if design_tets is None else design_tets, dtype=np.int32)
+        ns = _lib.MAX_RHS
+        J = np.zeros(ns, np.float64)
+        ge = np.zeros(ns * max(1, dt.shape[0]), np.float64)
+        gs = np.zeros(ns * max(1, dt.shape[0]), np.float64)
+        res = (_lib.FwResult * ns)()
+        _lib.check(self._lib.fwgpu_adjoint_gradient_multi(self._h, int(pe.shape[0]), _ptr(pe, ctypes.c_int32),
+                                                          int(dt.shape[0]), _ptr(dt, ctypes.c_int32),
+                                                          _ptr(J, ctypes.c_double), _ptr(ge, ctypes.c_double),
+                                                          _ptr(gs, ctypes.c_double), res),
+                   allow=(_lib.ERR_NOT_CONVERGED,))
+        n = self._multi_n
+        nd = dt.shape[0]
+        return (J[:n], ge[:n * nd].reshape(n, nd), gs[:n * nd].reshape(n, nd), [self._result(r) for r in res[:n]])
 
     def profile_iteration(self, reps: int = 50) -> dict:
         """Average device time of the kernels of one interface iteration

@@ -352,6 +352,20 @@ int fwgpu_profile_post(fwgpu_context *ctx, int32_t reps, double *kernel_ms);
 int fwgpu_hddm_solve_multi(fwgpu_context *ctx, int32_t n_src, const fwgpu_source *sources, fwgpu_result *results);
 /* Edge solution of source k of the last fwgpu_hddm_solve_multi (2*n_edges doubles). */
 int fwgpu_get_edge_solution_multi(fwgpu_context *ctx, int32_t k, double *x);
+/* The adjoint of every source of the last fwgpu_hddm_solve_multi at once: for
+ * source k, J[k] = sum over the probes of |x_k|^2, and its gradient with
+ * respect to the permittivity and conductivity of each design element, as
+ * fwgpu_adjoint_gradient gives it for one source.  The n_src adjoint
+ * right-hand sides conj(x_k at the probes) are solved together, as one
+ * batched solve on the forward factors (A = A^T); then one gradient launch
+ * per source.  grad_eps and grad_sigma hold n_src * n_design values, source
+ * by source (NULL to skip); adjoint_results (NULL to skip) gets n_src
+ * results.  Afterwards fwgpu_get_edge_solution_multi(k) returns source k's
+ * adjoint solution.  No counterpart in the reference (as
+ * fwgpu_adjoint_gradient). */
+int fwgpu_adjoint_gradient_multi(fwgpu_context *ctx, int32_t n_probe, const int32_t *probe_edges, int32_t n_design,
+                                 const int32_t *design_tets, double *J, double *grad_eps, double *grad_sigma,
+                                 fwgpu_result *adjoint_results);
 
 /* -- sharded solve over several GPUs (one context per rank) ---------------- */
 
