@@ -59,6 +59,10 @@ WORKLOADS = {
           "centre z-dipole, jittered RCB (leaf cap 900) 1 part x 8822 subdomains",
     "c4": "C4: the C2 mesh and medium with a central 12^3-cell design region (10,368 tets, per-tet complex eps_r, "
           "eps' ~ U[2,4], eps'' ~ U[0,0.1]); J = sum |E|^2 on 8 probe edges; forward solve + adjoint gradient",
+    "c5": "C5: [0,1.5]^3 112^3 hexes x 6 tets (8,429,568 tets), 8 random layers + 5% inclusions eps_r ~ U[10,20], "
+          "8-cell PML, PEC wall, 300 MHz, jittered RCB (leaf cap 1000); 16 seeded z-dipoles solved together on "
+          "one set of FP32 factors with FP64 refinement, then the adjoint gradient of J = sum |E|^2 on 8 probe edges "
+          "over a central 12^3-cell design region for every source (one batched adjoint solve)",
 }
 # COCG iterations to 1e-6 of the FP64 GPU solve on each model (B200, this
 # code); the reference's CPU time is extrapolated with them where running the
@@ -509,6 +513,59 @@ def run_ours(args):
     return 0
 
 
+def run_c5(args):
+    """C5: one step = the 16 sources solved together to ``--eps`` on one set
+    of factors (``fwgpu_hddm_solve_multi``, FP32 factors with FP64
+    refinement unless --precision fp64), then the batched adjoint of every
+    source (``fwgpu_adjoint_gradient_multi``).  The value is the device time
+    of the batched forward solve; a 16-source solve to 1e-6 takes minutes at
+    this size, so run it with small --steps / --warmup by hand."""
+    from adventure_fullwave_b200 import hddm
+
+    precision = "fp32_ir" if args.precision == "fp64" and not args.c5_fp64 else args.precision
+    model = meshgen.make_model("c5", design=12, nprobes=8)
+    meshgen.round_trip_material(model)
+    clocks = ClockSampler(0)
+    with hddm.HddmSolver(model, hddm_eps=args.eps, hddm_max_loop=args.max_loop, precision=precision,
+                         ir_max_steps=args.ir_steps, ir_relax=args.ir_relax, graph_iterations=args.graph_iters) as s:
+        srcs = list(range(len(model.sources)))
+        for _ in range(args.warmup):
+            s.solve_multi(srcs)
+        clocks.start()
+        times, iters, adj = [], [], []
+        for _ in range(args.steps):
+            res = s.solve_multi(srcs)
+            times.append((res[0].t_setup_ms + res[0].t_iterate_ms + res[0].t_last_ms) / 1e3)
+            iters.append([r.iterations for r in res])
+            if not args.no_adjoint:
+                t0 = time.perf_counter()
+                J, ge, gs, ares = s.adjoint_gradient_multi()
+                adj.append(time.perf_counter() - t0)
+        clk = clocks.stop()
+        conv = [bool(r.converged) for r in res]
+        sz = s.sizes()
+    value = float(np.mean(times))
+    line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 factor, c128 refinement and COCG" if precision == "fp32_ir" else "c128",
+            "data": "synthetic (seeded generator; no dataset)",
+            "config": {"workload": WORKLOADS["c5"], "precision": precision, "hddm_eps": args.eps,
+                       "n_tets": model.n_tets, "n_subdomains": model.nsub, "interface_dofs": sz["total_free"],
+                       "sources": len(model.sources), "parallelism": "1 GPU"},
+            "iterations_per_source": iters[-1], "converged": conv,
+            "per_source_iteration_ms": value * 1e3 / max(1, max(iters[-1])),
+            "clocks": clk}
+    if adj:
+        line["adjoint"] = {"batched_adjoint_s": float(np.mean(adj)), "adjoint_over_forward": float(np.mean(adj)) / value,
+                           "adjoint_iterations_per_source": [r.iterations for r in ares],
+                           "adjoint_converged": [bool(r.converged) for r in ares],
+                           "n_design": int(model.design_tets.shape[0]), "J": [float(v) for v in J],
+                           "grad_finite": bool(np.isfinite(ge).all() and np.isfinite(gs).all()),
+                           "timing": "host wall time of the batched backward call"}
+    print(json.dumps(line))
+    return 0
+
+
 def run_sharded_bench(args, rank, world, local, dist):
     """N > 1: one model sharded over the ranks (contiguous subdomain ranges),
     the partial interface vector summed over NCCL every iteration.  Total
@@ -603,7 +660,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--c5-fp64", action="store_true", help="C5 in FP64 (default: FP32 factors + FP64 refinement)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_ir"])
     ap.add_argument("--eps", type=float, default=1e-6)
     ap.add_argument("--max-loop", type=int, default=50000)
@@ -634,6 +692,8 @@ def main():
         return run_ncu_case(args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "c5":
+        return run_c5(args)
     return run_ours(args)
 
 
