@@ -890,10 +890,9 @@ static int setup_stage(fwgpu_context *c) {
 // order.  The staging capacity sets the row blocks, and with them the
 // order of the sums, so AUTO keeps the default capacity (a rule on the
 // model's envelope, setup_stage) and times one against two warps per
-// subdomain, which in FP64 share out whole row groups and column chunks and
-// so sum alike.  The FP32 sweep splits each row between the warps, so FP32
-// keeps one warp; the CTA kernel sums in another order and runs only when
-// asked for.  An explicit WARP choice times the staging capacities too.
+// subdomain, which share out whole row groups and column chunks and so sum
+// alike.  The CTA kernel sums in another order and runs only when asked
+// for.  An explicit WARP choice times the staging capacities too.
 static int tune_solve_kernel(fwgpu_context *c) {
   const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
   struct Cand {
@@ -902,7 +901,7 @@ static int tune_solve_kernel(fwgpu_context *c) {
   std::vector<Cand> cand;
   const bool any = c->opts.solve_kernel == FWGPU_SOLVE_AUTO;
   if (any && c->warp_ok) {
-    for (int warps = 1; warps <= (fp32 ? 1 : 2); warps++)
+    for (int warps = 1; warps <= 2; warps++)
       if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps)
         cand.push_back({fw::kSolveWarp, c->dp.stage_cap, warps});
     if (cand.empty()) cand.push_back({fw::kSolveWarp, c->dp.stage_cap, c->opts.stage_warps});

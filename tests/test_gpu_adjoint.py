@@ -52,33 +52,42 @@ def test_c4_gradient_vs_central_differences():
     """C4 (the C2 mesh, 663,552 tets, with 10,368 design tets of their own
     complex eps_r): the adjoint gradient against central differences of
     forward solves at 16 seeded design tets, for the real and the imaginary
-    part of eps_r.  Step: 1e-6 |eps_r| in each part; eps = eps0 eps' and
-    sigma = omega eps0 eps'' (the reference's convention)."""
+    part of eps_r (eps = eps0 eps', sigma = omega eps0 eps'', the
+    reference's convention).
+
+    One tet moves J very little: with a step of 1e-6 |eps_r| the change of J
+    is about 1e-10 of J, the size of the solves' own error.  The 16 tets are
+    therefore drawn (seeded) from the 5 % of the design region with the
+    largest gradient, the step is 1e-4 |eps_r| (the central difference's
+    truncation error is then about 1e-8 relative) and every solve runs to
+    hddm_eps 1e-12; each tet's difference quotient must agree with its
+    gradient to 1e-3."""
     eps0 = meshgen.EPS0
     m = meshgen.make_model("c4")
     meshgen.round_trip_material(m)
     assert m.design_tets.shape[0] == 10368
-    tol = dict(hddm_eps=1e-10, hddm_max_loop=60000)
+    tol = dict(hddm_eps=1e-12, hddm_max_loop=100000)
     with hddm.HddmSolver(m, **tol) as s:
         s.solve(0)
         J, ge, gs, ra = s.adjoint_gradient()
     assert ra.converged
     d_re, d_im = hddm.relative_permittivity_gradient(ge, gs, m.omega, eps0)
-    picks = np.random.default_rng(2024).choice(m.design_tets.shape[0], 16, replace=False)
-    dev_re, dev_im = [], []
-    for k in picks:
-        t = int(m.design_tets[k])
-        i = int(np.searchsorted(m.mat_flag, m.flag[t]))
-        er = complex(m.mat_eps[i] / eps0, m.mat_sigma[i] / (m.omega * eps0))
-        h = 1e-6 * abs(er)
-        he, hs = eps0 * h, m.omega * eps0 * h
-        fd_re = (gpu_objective(perturbed(m, t, d_eps=he), **tol) - gpu_objective(perturbed(m, t, d_eps=-he), **tol)) / (2 * h)
-        fd_im = (gpu_objective(perturbed(m, t, d_sigma=hs), **tol)
-                 - gpu_objective(perturbed(m, t, d_sigma=-hs), **tol)) / (2 * h)
-        dev_re.append(abs(fd_re - d_re[k]))
-        dev_im.append(abs(fd_im - d_im[k]))
-    scale_re, scale_im = np.max(np.abs(d_re[picks])), np.max(np.abs(d_im[picks]))
-    print(f"C4 FD vs adjoint, 16 tets: max |dev| / max |g|: eps' {max(dev_re) / scale_re:.1e}, "
-          f"eps'' {max(dev_im) / scale_im:.1e}")
-    assert max(dev_re) <= 1e-3 * scale_re
-    assert max(dev_im) <= 1e-3 * scale_im
+    rng = np.random.default_rng(2024)
+    worst = 0.0
+    for part, d in (("re", d_re), ("im", d_im)):
+        top = np.argsort(-np.abs(d))[: d.shape[0] // 20]
+        for k in rng.choice(top, 8, replace=False):
+            t = int(m.design_tets[k])
+            i = int(np.searchsorted(m.mat_flag, m.flag[t]))
+            er = complex(m.mat_eps[i] / eps0, m.mat_sigma[i] / (m.omega * eps0))
+            h = 1e-4 * abs(er)
+            if part == "re":
+                plus, minus = perturbed(m, t, d_eps=eps0 * h), perturbed(m, t, d_eps=-eps0 * h)
+            else:
+                plus, minus = perturbed(m, t, d_sigma=m.omega * eps0 * h), perturbed(m, t, d_sigma=-m.omega * eps0 * h)
+            fd = (gpu_objective(plus, **tol) - gpu_objective(minus, **tol)) / (2 * h)
+            dev = abs(fd - d[k]) / abs(d[k])
+            worst = max(worst, dev)
+            print(f"C4 tet {t} eps_r {part}: adjoint {d[k]:+.6e}, central difference {fd:+.6e}, rel dev {dev:.1e}")
+            assert dev <= 1e-3
+    print(f"C4 FD vs adjoint, 16 tets (8 eps', 8 eps''): worst rel dev {worst:.1e}")
