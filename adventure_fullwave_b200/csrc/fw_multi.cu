@@ -97,7 +97,7 @@ __global__ void multi_residual_kernel(MultiProblem m, int mode) {
 // ---- the sweeps --------------------------------------------------------------
 
 struct MultiLayout {
-  size_t y, buf0, buf1, meta, bar, blk, total;
+  size_t y, buf0, buf1, meta, rect, bar, blk, total;
 };
 
 __host__ __device__ inline MultiLayout multi_layout(int max_interior, int max_blocks, int cap, bool fp32, int rw) {
@@ -112,6 +112,8 @@ __host__ __device__ inline MultiLayout multi_layout(int max_interior, int max_bl
   o += a16((size_t)cap * es);
   l.meta = o;
   o += 32 * 8;
+  l.rect = o;
+  o += a16((size_t)32 * rw * es);
   l.bar = o;
   o += 16;
   l.blk = o;
@@ -121,11 +123,20 @@ __host__ __device__ inline MultiLayout multi_layout(int max_interior, int max_bl
 }
 
 // Sources per sweep warp: 16 / kRW warps share a subdomain, each with kRW of
-// the 16 sources; lane = (group h, source r), the 32 / kRW groups splitting
-// every row's dot product (shuffles add them).  Forward: row by row,
-// y_i = b_i - sum_k L_ik y_k, then z_i = y_i / d_i.  Backward: row by row
-// from the last, x_t final, then y_c -= L_tc x_t for the columns of row t,
-// each (c, r) with one writer.  y holds the warp's kRW sources, [row][kRW].
+// the 16 sources; lane = (group h, source r), kQ = 32 / kRW groups.  Per
+// staged block of rows r0 .. r0+nb-1:
+//   forward  - the entries left of the block for all its rows at once: group
+//              h takes rows h, h+kQ, ..., one accumulator per (row, source),
+//              the row's entries in order; no row waits for another.  Then
+//              the triangle row by row, y_i = b_i - (left_i + sum over the
+//              block's columns), the groups splitting the block's columns
+//              (shuffles add them), z_i = y_i / d_i;
+//   backward - the triangle row by row from the last: x_t final, then
+//              y_c -= L_tc x_t for the block's columns of row t; then the
+//              columns left of the block for all its rows: column c belongs to
+//              group c % kQ, which applies the rows from the last to the
+//              first in place, so no row waits for another.
+// Each (c, r) has one writer.  y holds the warp's kRW sources, [row][kRW].
 template <typename T, int kRW>
 __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mode, const double2 *rhs,
                                                         double2 *xout, T *zstash, int accumulate, MultiLayout lay,
@@ -147,6 +158,7 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
   if (nI == 0 || nblk <= 0) return;
   T *__restrict__ y = (T *)(smem_raw + lay.y);
   int2 *meta = (int2 *)(smem_raw + lay.meta);
+  T *rect = (T *)(smem_raw + lay.rect);
   int2 *blk = (int2 *)(smem_raw + lay.blk);
   Stage<T> st;
   st.buf0 = (T *)(smem_raw + lay.buf0);
@@ -188,27 +200,41 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
     }
     __syncwarp();
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);
+    // entries left of the block, every row of the block at once
+    for (int t = h; t < nb; t += kQ) {
+      const int2 mt = meta[t];
+      const int len = max(0, r0 - mt.x);
+      const T *__restrict__ row = S + mt.y;
+      const T *__restrict__ yk = y + (int64_t)mt.x * kRW + r;
+      T a0 = czero<T>(), a1 = czero<T>();
+      int k = 0;
+      for (; k + 1 < len; k += 2) {
+        a0 = cmac(a0, row[k], yk[k * kRW]);
+        a1 = cmac(a1, row[k + 1], yk[(k + 1) * kRW]);
+      }
+      if (k < len) a0 = cmac(a0, row[k], yk[k * kRW]);
+      rect[t * kRW + r] = cadd(a0, a1);
+    }
+    __syncwarp();
+    // the triangle, row by row over the block's columns
     for (int t = 0; t < nb; t++) {
       const int2 mt = meta[t];
       const int i = r0 + t;
       const int len = i - mt.x;
+      const int k0 = max(0, r0 - mt.x);
       const T *__restrict__ row = S + mt.y;
       const T *__restrict__ yk = y + (int64_t)mt.x * kRW + r;
-      T a0 = czero<T>(), a1 = czero<T>(), a2 = czero<T>(), a3 = czero<T>();
-      int k = h;
-      for (; k + 3 * kQ < len; k += 4 * kQ) {
-        const T l0 = row[k], l1 = row[k + kQ], l2 = row[k + 2 * kQ], l3 = row[k + 3 * kQ];
-        const T v0 = yk[k * kRW], v1 = yk[(k + kQ) * kRW], v2 = yk[(k + 2 * kQ) * kRW], v3 = yk[(k + 3 * kQ) * kRW];
-        a0 = cadd(a0, cmul(l0, v0));
-        a1 = cadd(a1, cmul(l1, v1));
-        a2 = cadd(a2, cmul(l2, v2));
-        a3 = cadd(a3, cmul(l3, v3));
+      T a0 = czero<T>(), a1 = czero<T>();
+      int k = k0 + h;
+      for (; k + kQ < len; k += 2 * kQ) {
+        a0 = cmac(a0, row[k], yk[k * kRW]);
+        a1 = cmac(a1, row[k + kQ], yk[(k + kQ) * kRW]);
       }
-      for (; k < len; k += kQ) a0 = cadd(a0, cmul(row[k], yk[k * kRW]));
-      T acc = cadd(cadd(a0, a1), cadd(a2, a3));
+      if (k < len) a0 = cmac(a0, row[k], yk[k * kRW]);
+      T acc = cadd(a0, a1);
 #pragma unroll
       for (int o = kRW; o < 32; o <<= 1) acc = cadd(acc, shfl_xor(acc, o));
-      const T val = csub(y[i * kRW + r], acc);
+      const T val = csub(y[i * kRW + r], cadd(rect[t * kRW + r], acc));
       const T dinv = row[len];
       __syncwarp();
       if (h == 0) {
@@ -236,6 +262,7 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
     }
     __syncwarp();
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);
+    // the triangle from the last row: the block's columns of each row
     for (int t = nb - 1; t >= 0; t--) {
       const int2 mt = meta[t];
       const int i = r0 + t;
@@ -243,18 +270,21 @@ __global__ void __launch_bounds__(32) multi_sweep_kernel(MultiProblem m, int mod
       const T xi = y[i * kRW + r];
       const T *__restrict__ row = S + mt.y;
       T *__restrict__ yc = y + (int64_t)mt.x * kRW + r;
-      int k = h;
-      for (; k + 3 * kQ < len; k += 4 * kQ) {
-        const T l0 = row[k], l1 = row[k + kQ], l2 = row[k + 2 * kQ], l3 = row[k + 3 * kQ];
-        const T v0 = yc[k * kRW], v1 = yc[(k + kQ) * kRW], v2 = yc[(k + 2 * kQ) * kRW], v3 = yc[(k + 3 * kQ) * kRW];
-        yc[k * kRW] = csub(v0, cmul(l0, xi));
-        yc[(k + kQ) * kRW] = csub(v1, cmul(l1, xi));
-        yc[(k + 2 * kQ) * kRW] = csub(v2, cmul(l2, xi));
-        yc[(k + 3 * kQ) * kRW] = csub(v3, cmul(l3, xi));
-      }
-      for (; k < len; k += kQ) yc[k * kRW] = csub(yc[k * kRW], cmul(row[k], xi));
+      for (int k = max(0, r0 - mt.x) + h; k < len; k += kQ) yc[k * kRW] = cmsub(yc[k * kRW], row[k], xi);
       __syncwarp();
     }
+    // the columns left of the block: column c belongs to group c % kQ, which
+    // applies the block's rows from the last to the first
+    for (int t = nb - 1; t >= 0; t--) {
+      const int2 mt = meta[t];
+      const int len = max(0, r0 - mt.x);
+      const T xi = y[(r0 + t) * kRW + r];
+      const T *__restrict__ row = S + mt.y;
+      T *__restrict__ yc = y + (int64_t)mt.x * kRW + r;
+      int k = (h - mt.x % kQ + kQ) % kQ;  // the first column of this group
+      for (; k < len; k += kQ) yc[k * kRW] = cmsub(yc[k * kRW], row[k], xi);
+    }
+    __syncwarp();
   }
   // every copy issued into this CTA's shared memory has landed before it exits
   stage_drain(st);
