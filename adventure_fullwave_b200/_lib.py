@@ -123,10 +123,14 @@ SIGNATURES = {
     "fwgpu_get_edge_solution_multi": [ctypes.c_void_p, c_i32, P(c_dbl)],
     "fwgpu_adjoint_gradient_multi": [ctypes.c_void_p, c_i32, P(c_i32), c_i32, P(c_i32), P(c_dbl), P(c_dbl), P(c_dbl),
                                      P(FwResult)],
-    "fwgpu_shard_set_exchange": [ctypes.c_void_p, ctypes.c_void_p],
+    "fwgpu_shard_set_layout": [ctypes.c_void_p, c_i32, P(c_i32), P(c_i32)],
+    "fwgpu_shard_set_exchange": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "fwgpu_shard_first": [ctypes.c_void_p],
+    "fwgpu_shard_first_sums": [ctypes.c_void_p],
     "fwgpu_shard_first_finish": [ctypes.c_void_p, P(c_i32)],
     "fwgpu_shard_iterate": [ctypes.c_void_p],
+    "fwgpu_shard_iterate_pq": [ctypes.c_void_p],
+    "fwgpu_shard_iterate_update": [ctypes.c_void_p],
     "fwgpu_shard_iterate_finish": [ctypes.c_void_p, P(c_i32)],
     "fwgpu_skyline_solve_noalloc": [c_i32, c_i32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

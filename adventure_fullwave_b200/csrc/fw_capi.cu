@@ -88,7 +88,12 @@ struct fwgpu_context {
   std::vector<int32_t> h_src_owner, h_src_local;  // first subdomain holding each edge, and its local DOF
   bool warp_ok = false;            // the staged warp-per-subdomain kernel fits in shared memory
   bool sharded = false;            // solves a range of the subdomains (fwgpu_shard_* calls)
-  double2 *d_exchange = nullptr;   // caller's buffer: partial Q, then partial PC diagonal
+  // sharded solve: the caller's packed exchange and scalar buffers, and the
+  // shard layout (held interface DOFs, owned, packed positions)
+  double2 *d_pack = nullptr;
+  double *d_scal = nullptr;
+  int32_t shard_lo = 0, shard_hi = 0;
+  int32_t n_shared = -1;           // -1: no layout yet
   // batched sources (fwgpu_hddm_solve_multi)
   fw::MultiProblem mp{};
   fw::MultiScalars *h_ms = nullptr;
@@ -581,8 +586,8 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
     dp.n_interior = p.sub_int_off[s_end] - p.sub_int_off[s_begin];
     dp.slot0 = p.sub_if_off[s_begin];
     dp.n_slots = p.sub_if_off[s_end] - p.sub_if_off[s_begin];
-    dp.xq = nullptr;
-    dp.xpc = nullptr;
+    c->shard_lo = s_begin;
+    c->shard_hi = s_end;
   }
   FW_TRY(c->alloc(&c->d_cpl_val, p.cpl_src.size()));
   FW_TRY(c->alloc(&c->d_ifr_val, p.ifr_src.size()));
@@ -1336,36 +1341,111 @@ int fwgpu_get_edge_solution_multi(fwgpu_context *c, int32_t k, double *x) {
   return FWGPU_OK;
 }
 
-int fwgpu_shard_set_exchange(fwgpu_context *c, double *d_exchange) {
-  if (!c || !d_exchange) return set_error(FWGPU_ERR_ARG, "null argument");
-  c->d_exchange = (double2 *)d_exchange;
+int fwgpu_shard_set_layout(fwgpu_context *c, int32_t n_shards, const int32_t *shard_first, int32_t *n_shared) {
+  if (!c || !shard_first || n_shards < 1) return set_error(FWGPU_ERR_ARG, "bad argument");
+  if (!c->sharded) return set_error(FWGPU_ERR_STATE, "not a sharded context");
+  const fw::Plan &p = c->p;
+  const int nsub = c->m.nsub;
+  if (shard_first[0] != 0 || shard_first[n_shards] != nsub) return set_error(FWGPU_ERR_ARG, "shard ranges must cover the subdomains");
+  int me = -1;
+  for (int k = 0; k < n_shards; k++) {
+    if (shard_first[k + 1] <= shard_first[k]) return set_error(FWGPU_ERR_ARG, "empty or decreasing shard range");
+    if (shard_first[k] == c->shard_lo && shard_first[k + 1] == c->shard_hi) me = k;
+  }
+  if (me < 0) return set_error(FWGPU_ERR_ARG, "this context's range is not one of the shards");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  std::vector<int32_t> shard_of(nsub), slot_shard(p.sub_if_off[nsub]);
+  for (int k = 0; k < n_shards; k++)
+    for (int s = shard_first[k]; s < shard_first[k + 1]; s++) shard_of[s] = k;
+  for (int s = 0; s < nsub; s++)
+    for (int64_t q = p.sub_if_off[s]; q < p.sub_if_off[s + 1]; q++) slot_shard[q] = shard_of[s];
+  // the slots of a DOF are in subdomain order, so its shards come in
+  // ascending order: the first is its owner
+  std::vector<int32_t> dof, pos;
+  std::vector<uint8_t> own;
+  int32_t shared = 0;
+  for (int g = 0; g < p.total_free; g++) {
+    int first = -1, last = -1, distinct = 0;
+    bool mine = false;
+    for (int t = p.gq_ptr[g]; t < p.gq_ptr[g + 1]; t++) {
+      const int k = slot_shard[p.gq_slot[t]];
+      if (k != last) distinct++;
+      if (first < 0) first = k;
+      last = k;
+      mine |= k == me;
+    }
+    const int ps = distinct >= 2 ? shared++ : -1;
+    if (mine) {
+      dof.push_back(g);
+      own.push_back(first == me ? 1 : 0);
+      pos.push_back(ps);
+    }
+  }
+  int32_t *d_dof = nullptr, *d_pos = nullptr;
+  uint8_t *d_own = nullptr;
+  FW_TRY(c->upload(&d_dof, dof));
+  FW_TRY(c->upload(&d_pos, pos));
+  FW_TRY(c->upload(&d_own, own));
+  c->dp.dist_dof = d_dof;
+  c->dp.dist_pos = d_pos;
+  c->dp.dist_own = d_own;
+  c->dp.dist_n = (int32_t)dof.size();
+  c->dp.n_shared = shared;
+  c->n_shared = shared;
+  if (n_shared) *n_shared = shared;
+  return FWGPU_OK;
+}
+
+int fwgpu_shard_set_exchange(fwgpu_context *c, double *d_pack, double *d_scal) {
+  if (!c || !d_pack || !d_scal) return set_error(FWGPU_ERR_ARG, "null argument");
+  c->d_pack = (double2 *)d_pack;
+  c->d_scal = d_scal;
+  c->dp.dist_pack = c->d_pack;
+  c->dp.dist_scal = d_scal;
+  return FWGPU_OK;
+}
+
+static int shard_ready(fwgpu_context *c) {
+  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  if (c->n_shared < 0) return set_error(FWGPU_ERR_STATE, "no shard layout (fwgpu_shard_set_layout)");
+  if (!c->d_pack) return set_error(FWGPU_ERR_STATE, "no exchange buffers (fwgpu_shard_set_exchange)");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  return FWGPU_OK;
+}
+
+static int zero_pack(fwgpu_context *c, int vectors) {
+  if (c->n_shared > 0)
+    FW_CUDA(cudaMemsetAsync(c->d_pack, 0, (size_t)vectors * c->n_shared * sizeof(double2), c->stream));
   return FWGPU_OK;
 }
 
 int fwgpu_shard_first(fwgpu_context *c) {
-  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
-  if (!c->d_exchange) return set_error(FWGPU_ERR_STATE, "no exchange buffer (fwgpu_shard_set_exchange)");
+  FW_TRY(shard_ready(c));
   FW_TRY(fwgpu_solve_dom_1st(c));
-  c->dp.xq = nullptr;
-  c->dp.xpc = nullptr;
-  fw::launch_shard_gather(c->dp, c->d_pcloc, c->d_exchange, c->d_exchange + c->dp.nfree, false, c->stream);
+  FW_TRY(zero_pack(c, 2));
+  fw::launch_dist_pack(c->dp, c->d_pcloc, true, false, c->stream);
   c->launches += 1;
   FW_CUDA(cudaGetLastError());
   FW_CUDA(cudaStreamSynchronize(c->stream));
   return FWGPU_OK;
 }
 
-int fwgpu_shard_first_finish(fwgpu_context *c, int32_t *status) {
-  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
-  if (c->stage < 2 || !c->d_exchange) return set_error(FWGPU_ERR_STATE, "shard_first_finish before shard_first");
-  FW_CUDA(cudaSetDevice(c->opts.device));
-  c->dp.xq = c->d_exchange;
-  c->dp.xpc = c->d_exchange + c->dp.nfree;
+int fwgpu_shard_first_sums(fwgpu_context *c) {
+  FW_TRY(shard_ready(c));
+  if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "shard_first_sums before shard_first");
   fw::launch_set_status(c->d_sc, c->opts.hddm_eps, c->opts.hddm_max_loop, c->stream);
-  fw::launch_cocg_first(c->dp, c->d_pcloc, c->stream);
-  c->dp.xq = nullptr;
-  c->dp.xpc = nullptr;
-  c->launches += 3;
+  fw::launch_dist_first(c->dp, c->d_pcloc, c->stream);
+  c->launches += 2;
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  return FWGPU_OK;
+}
+
+int fwgpu_shard_first_finish(fwgpu_context *c, int32_t *status) {
+  FW_TRY(shard_ready(c));
+  if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "shard_first_finish before shard_first");
+  fw::launch_dist_first_finish(c->dp, c->stream);
+  c->launches += 1;
   FW_CUDA(cudaGetLastError());
   FW_TRY(read_status(c, status));
   c->stage = 3;
@@ -1373,26 +1453,43 @@ int fwgpu_shard_first_finish(fwgpu_context *c, int32_t *status) {
 }
 
 int fwgpu_shard_iterate(fwgpu_context *c) {
-  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  FW_TRY(shard_ready(c));
   if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "shard_iterate outside the interface loop");
-  FW_CUDA(cudaSetDevice(c->opts.device));
   const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
   fw::launch_subsolve(c->dp, fw::kModeIter, fp32, c->stream);
-  fw::launch_shard_gather(c->dp, c->d_pcloc, c->d_exchange, nullptr, true, c->stream);
+  FW_TRY(zero_pack(c, 1));
+  fw::launch_dist_pack(c->dp, c->d_pcloc, false, true, c->stream);
   c->launches += 1 + fw::subsolve_launches(c->dp, fp32);
   FW_CUDA(cudaGetLastError());
   FW_CUDA(cudaStreamSynchronize(c->stream));
   return FWGPU_OK;
 }
 
+int fwgpu_shard_iterate_pq(fwgpu_context *c) {
+  FW_TRY(shard_ready(c));
+  if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "shard_iterate_pq outside the interface loop");
+  fw::launch_dist_pq(c->dp, c->stream);
+  c->launches += 1;
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  return FWGPU_OK;
+}
+
+int fwgpu_shard_iterate_update(fwgpu_context *c) {
+  FW_TRY(shard_ready(c));
+  if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "shard_iterate_update outside the interface loop");
+  fw::launch_dist_update(c->dp, c->stream);
+  c->launches += 1;
+  FW_CUDA(cudaGetLastError());
+  FW_CUDA(cudaStreamSynchronize(c->stream));
+  return FWGPU_OK;
+}
+
 int fwgpu_shard_iterate_finish(fwgpu_context *c, int32_t *status) {
-  if (!c) return set_error(FWGPU_ERR_ARG, "null context");
+  FW_TRY(shard_ready(c));
   if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "shard_iterate_finish outside the interface loop");
-  FW_CUDA(cudaSetDevice(c->opts.device));
-  c->dp.xq = c->d_exchange;
-  fw::launch_cocg_update(c->dp, c->stream);
-  c->dp.xq = nullptr;
-  c->launches += 3;
+  fw::launch_dist_finish(c->dp, c->stream);
+  c->launches += 2;
   FW_CUDA(cudaGetLastError());
   FW_TRY(read_status(c, status));
   return FWGPU_OK;

@@ -1021,22 +1021,12 @@ __device__ __forceinline__ double2 gather_slots(const DevProblem &p, const doubl
   }
   return q;
 }
-__device__ __forceinline__ double2 gather_q(const DevProblem &p, int g) {
-  return p.xq ? p.xq[g] : gather_slots(p, p.qloc, g);
-}
+__device__ __forceinline__ double2 gather_q(const DevProblem &p, int g) { return gather_slots(p, p.qloc, g); }
 
 // A shard's partial interface sums, written to the exchange buffer that the
 // caller sums over ranks: Q (and on the first step the diagonal PC sums)
 // over this shard's subdomains (COM_RES_SP / DIAG_GATHER_S over one part's
 // subdomains, hddm_solver_sp.h:8-25, hddm_pc.h:110-124).
-__global__ void shard_gather_kernel(DevProblem p, const double2 *__restrict__ pcloc, double2 *__restrict__ xq,
-                                    double2 *__restrict__ xpc, int status_check) {
-  if (status_check && p.sc->status != 0) return;
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
-    xq[g] = gather_slots(p, p.qloc, g);
-    if (xpc) xpc[g] = gather_slots(p, pcloc, g);
-  }
-}
 
 // first step: Q and PC gathered over subdomains (hddm_solver_s.h:174-181),
 // PC reciprocal (hddm_pc.h:128-135), r = Q, z = r pc, p = z, max|r|, (r, z)
@@ -1045,7 +1035,7 @@ __global__ void cocg_first_kernel(DevProblem p, const double2 *__restrict__ pclo
   double mx = 0.0, rzr = 0.0, rzi = 0.0, l2 = 0.0;
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
     const double2 q = gather_q(p, g);
-    double2 pc = p.xpc ? p.xpc[g] : gather_slots(p, pcloc, g);
+    double2 pc = gather_slots(p, pcloc, g);
     pc = ciszero(pc) ? make_double2(1.0, 0.0) : cdiv_ref(make_double2(1.0, 0.0), pc);
     p.PC[g] = pc;
     p.Q[g] = q;
@@ -1200,6 +1190,222 @@ __global__ void cocg_pupdate_kernel(DevProblem p) {
   if (st == 2) return;
   const double2 be = p.sc->beta;
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < p.nfree; g += gridDim.x * blockDim.x) {
+    p.P[g] = st == 1 ? p.U[g] : cadd(p.Z[g], cmul(be, p.P[g]));
+  }
+  if (st == 1 && last_cta(&p.sc->ticket[2]) && threadIdx.x == 0) {
+    p.sc->status = 2;
+    p.sc->ticket[2] = 0;
+  }
+}
+
+// ---- sharded solve, exchange packed to the shared interface DOFs -----------
+// Every shard runs the COCG on the interface DOFs its subdomains hold (the
+// same recurrence as the kernels above, on the same summed values, so the
+// shards holding a DOF keep the same bits for it); the dot products and the
+// max-norm run over the DOFs it owns, and the shards add them up (the
+// reference's p-mode: hddm_solver_ph.h:112-131,158-175,199,228-329).  Only
+// the DOFs held by two or more shards cross between the ranks, packed.
+
+__device__ __forceinline__ double2 dist_q(const DevProblem &p, int i, int g) {
+  const int pos = p.dist_pos[i];
+  return pos >= 0 ? p.dist_pack[pos] : gather_slots(p, p.qloc, g);
+}
+
+// this shard's partial Q (and PC diagonal) of its shared DOFs; the host
+// zeroed the packed buffer, so the DOFs it does not hold add nothing
+__global__ void dist_pack_kernel(DevProblem p, const double2 *__restrict__ pcloc, int with_pc, int status_check) {
+  if (status_check && p.sc->status != 0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.dist_n; i += gridDim.x * blockDim.x) {
+    const int pos = p.dist_pos[i];
+    if (pos < 0) continue;
+    const int g = p.dist_dof[i];
+    p.dist_pack[pos] = gather_slots(p, p.qloc, g);
+    if (with_pc) p.dist_pack[p.n_shared + pos] = gather_slots(p, pcloc, g);
+  }
+}
+
+// the first step on the held DOFs (cocg_first_kernel); the last CTA writes the
+// local sums of the owned DOFs: (r, z) and |r|^2 to scal[0..2], max|r| to scal[4]
+__global__ void dist_first_kernel(DevProblem p, const double2 *__restrict__ pcloc) {
+  __shared__ double sh[40];
+  double mx = 0.0, rzr = 0.0, rzi = 0.0, l2 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.dist_n; i += gridDim.x * blockDim.x) {
+    const int g = p.dist_dof[i], pos = p.dist_pos[i];
+    const double2 q = dist_q(p, i, g);
+    double2 pc = pos >= 0 ? p.dist_pack[p.n_shared + pos] : gather_slots(p, pcloc, g);
+    pc = ciszero(pc) ? make_double2(1.0, 0.0) : cdiv_ref(make_double2(1.0, 0.0), pc);
+    p.PC[g] = pc;
+    p.Q[g] = q;
+    p.R[g] = q;
+    const double2 z = cmul(q, pc);
+    p.Z[g] = z;
+    p.P[g] = z;
+    p.U[g] = cz();
+    if (p.dist_own[i]) {
+      mx = fmax(mx, cabs_ref(q));
+      const double2 rz = cmul(q, z);
+      rzr += rz.x;
+      rzi += rz.y;
+      l2 += q.x * q.x + q.y * q.y;
+    }
+  }
+  const int nb = p.n_part_blocks;
+  double r;
+  r = block_max(mx, sh);
+  if (threadIdx.x == 0) p.part[kFMax * nb + blockIdx.x] = r;
+  r = block_sum(rzr, sh);
+  if (threadIdx.x == 0) p.part[kFRzRe * nb + blockIdx.x] = r;
+  r = block_sum(rzi, sh);
+  if (threadIdx.x == 0) p.part[kFRzIm * nb + blockIdx.x] = r;
+  r = block_sum(l2, sh);
+  if (threadIdx.x == 0) p.part[kFL2 * nb + blockIdx.x] = r;
+  if (!last_cta(&p.sc->ticket[0])) return;
+  const double vmx = reduce_partials(p.part, nb, kFMax, true, sh);
+  const double vrr = reduce_partials(p.part, nb, kFRzRe, false, sh);
+  const double vri = reduce_partials(p.part, nb, kFRzIm, false, sh);
+  const double vl2 = reduce_partials(p.part, nb, kFL2, false, sh);
+  if (threadIdx.x == 0) {
+    p.dist_scal[0] = vrr;
+    p.dist_scal[1] = vri;
+    p.dist_scal[2] = vl2;
+    p.dist_scal[4] = vmx;
+    p.sc->ticket[0] = 0;
+  }
+}
+
+// the first step's scalars from the summed values (cocg_first_scalars_kernel)
+__global__ void dist_first_finish_kernel(DevProblem p) {
+  CocgScalars *sc = p.sc;
+  const double mx = p.dist_scal[4], rzr = p.dist_scal[0], rzi = p.dist_scal[1], l2 = p.dist_scal[2];
+  const bool bad = !isfinite(mx) || !isfinite(l2) || !isfinite(rzr) || !isfinite(rzi);
+  sc->norm0 = mx;
+  sc->l2_0 = sqrt(l2);
+  sc->status = (bad || mx < kNearlyZero) ? 1 : 0;
+  sc->r0inv = 1.0 / mx;
+  sc->rz = make_double2(rzr, rzi);
+  sc->resi = 1.0;
+  sc->resi_l2 = 1.0;
+  sc->loop = 1;
+  sc->converged = (!bad && mx < kNearlyZero) ? 1 : 0;
+  sc->nonfinite = bad ? 1 : 0;
+}
+
+// Q on the held DOFs and the local (p, q) of the owned ones -> scal[0..1]
+__global__ void dist_pq_kernel(DevProblem p) {
+  if (p.sc->status != 0) return;
+  __shared__ double sh[40];
+  double re = 0.0, im = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.dist_n; i += gridDim.x * blockDim.x) {
+    const int g = p.dist_dof[i];
+    const double2 q = dist_q(p, i, g);
+    p.Q[g] = q;
+    if (p.dist_own[i]) {
+      const double2 t = cmul(p.P[g], q);
+      re += t.x;
+      im += t.y;
+    }
+  }
+  const int nb = p.n_part_blocks;
+  double r = block_sum(re, sh);
+  if (threadIdx.x == 0) p.part[kFPqRe * nb + blockIdx.x] = r;
+  r = block_sum(im, sh);
+  if (threadIdx.x == 0) p.part[kFPqIm * nb + blockIdx.x] = r;
+  if (!last_cta(&p.sc->ticket[0])) return;
+  const double pr = reduce_partials(p.part, nb, kFPqRe, false, sh);
+  const double pi = reduce_partials(p.part, nb, kFPqIm, false, sh);
+  if (threadIdx.x == 0) {
+    p.dist_scal[0] = pr;
+    p.dist_scal[1] = pi;
+    p.sc->ticket[0] = 0;
+  }
+}
+
+// -alpha from the summed (p, q) (every thread the same), u += -alpha p,
+// r += -alpha q, z on the held DOFs; the local sums of the owned ones
+__global__ void dist_update_kernel(DevProblem p) {
+  if (p.sc->status != 0) return;
+  __shared__ double sh[40];
+  const double2 pq = make_double2(p.dist_scal[0], p.dist_scal[1]);
+  const double2 rz0 = p.sc->rz;
+  const double2 ma =
+      (cabs_ref(rz0) < kNearlyZero && cabs_ref(pq) < kNearlyZero) ? cz() : csub(cz(), cdiv_ref(rz0, pq));
+  double mx = 0.0, rzr = 0.0, rzi = 0.0, l2 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.dist_n; i += gridDim.x * blockDim.x) {
+    const int g = p.dist_dof[i];
+    p.U[g] = cadd(p.U[g], cmul(ma, p.P[g]));
+    const double2 r = cadd(p.R[g], cmul(ma, p.Q[g]));
+    p.R[g] = r;
+    const double2 z = cmul(r, p.PC[g]);
+    p.Z[g] = z;
+    if (p.dist_own[i]) {
+      mx = fmax(mx, cabs_ref(r));
+      const double2 rz = cmul(r, z);
+      rzr += rz.x;
+      rzi += rz.y;
+      l2 += r.x * r.x + r.y * r.y;
+    }
+  }
+  const int nb = p.n_part_blocks;
+  double r;
+  r = block_max(mx, sh);
+  if (threadIdx.x == 0) p.part[kFMax * nb + blockIdx.x] = r;
+  r = block_sum(rzr, sh);
+  if (threadIdx.x == 0) p.part[kFRzRe * nb + blockIdx.x] = r;
+  r = block_sum(rzi, sh);
+  if (threadIdx.x == 0) p.part[kFRzIm * nb + blockIdx.x] = r;
+  r = block_sum(l2, sh);
+  if (threadIdx.x == 0) p.part[kFL2 * nb + blockIdx.x] = r;
+  if (!last_cta(&p.sc->ticket[1])) return;
+  const double vmx = reduce_partials(p.part, nb, kFMax, true, sh);
+  const double vrr = reduce_partials(p.part, nb, kFRzRe, false, sh);
+  const double vri = reduce_partials(p.part, nb, kFRzIm, false, sh);
+  const double vl2 = reduce_partials(p.part, nb, kFL2, false, sh);
+  if (threadIdx.x == 0) {
+    p.sc->malpha = ma;
+    p.dist_scal[0] = vrr;
+    p.dist_scal[1] = vri;
+    p.dist_scal[2] = vl2;
+    p.dist_scal[4] = vmx;
+    p.sc->ticket[1] = 0;
+  }
+}
+
+// resi, beta, the stopping test (the last CTA of cocg_update_kernel) from
+// the summed values
+__global__ void dist_finish_kernel(DevProblem p) {
+  CocgScalars *sc = p.sc;
+  if (sc->status != 0) return;
+  const double rzr_t = p.dist_scal[0], rzi_t = p.dist_scal[1], l2_t = p.dist_scal[2], rmx = p.dist_scal[4];
+  const double resi = rmx * sc->r0inv;
+  sc->resi = resi;
+  sc->resi_l2 = sqrt(l2_t) / sc->l2_0;
+  if (sc->loop - 1 < p.hist_cap) p.hist[sc->loop - 1] = resi;
+  const double2 rz = make_double2(rzr_t, rzi_t);
+  if (cabs_ref(rz) < kNearlyZero && cabs_ref(sc->rz) < kNearlyZero) {
+    sc->beta = cz();
+  } else {
+    sc->beta = cdiv_ref(rz, sc->rz);
+  }
+  sc->rz = rz;
+  if (!isfinite(l2_t) || !isfinite(rzr_t) || !isfinite(rzi_t)) {
+    sc->status = 1;
+    sc->nonfinite = 1;
+  } else if (resi < sc->eps) {
+    sc->status = 1;
+    sc->converged = 1;
+  } else if (sc->loop >= sc->max_loop) {
+    sc->status = 1;
+  }
+  sc->loop += 1;
+}
+
+// p = z + beta p, or p = u after the last iteration, on the held DOFs
+__global__ void dist_pupdate_kernel(DevProblem p) {
+  const int st = p.sc->status;
+  if (st == 2) return;
+  const double2 be = p.sc->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < p.dist_n; i += gridDim.x * blockDim.x) {
+    const int g = p.dist_dof[i];
     p.P[g] = st == 1 ? p.U[g] : cadd(p.Z[g], cmul(be, p.P[g]));
   }
   if (st == 1 && last_cta(&p.sc->ticket[2]) && threadIdx.x == 0) {
@@ -1387,12 +1593,28 @@ void launch_edge_solution(const DevProblem &p, int64_t ne, const int64_t *edge_s
                                                                  p.n_slots);
 }
 
-void launch_shard_gather(const DevProblem &p, const double2 *pcloc, double2 *xq, double2 *xpc, bool status_check,
-                         cudaStream_t stream) {
-  shard_gather_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p, pcloc, xq, xpc, status_check ? 1 : 0);
-}
 
 void launch_profile_reset(CocgScalars *sc, cudaStream_t stream) { profile_reset_kernel<<<1, 1, 0, stream>>>(sc); }
+
+void launch_dist_pack(const DevProblem &p, const double2 *pcloc, bool with_pc, bool status_check, cudaStream_t stream) {
+  dist_pack_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p, pcloc, with_pc ? 1 : 0, status_check ? 1 : 0);
+}
+void launch_dist_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream) {
+  dist_first_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p, pcloc);
+}
+void launch_dist_first_finish(const DevProblem &p, cudaStream_t stream) {
+  dist_first_finish_kernel<<<1, 1, 0, stream>>>(p);
+}
+void launch_dist_pq(const DevProblem &p, cudaStream_t stream) {
+  dist_pq_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
+}
+void launch_dist_update(const DevProblem &p, cudaStream_t stream) {
+  dist_update_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
+}
+void launch_dist_finish(const DevProblem &p, cudaStream_t stream) {
+  dist_finish_kernel<<<1, 1, 0, stream>>>(p);
+  dist_pupdate_kernel<<<p.n_part_blocks, kRedThreads, 0, stream>>>(p);
+}
 
 void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream) {
   set_status_kernel<<<1, 1, 0, stream>>>(sc, eps, max_loop);

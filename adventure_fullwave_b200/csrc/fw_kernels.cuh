@@ -93,8 +93,6 @@ struct DevProblem {
   int64_t slot0, n_slots;        // interface slots of the subdomains this context solves
   // sharded solve: this shard's partial interface sums go to the exchange
   // buffer (summed over ranks by the caller) and the COCG reads them back
-  const double2 *xq;             // summed Q, or null: gather from this context's slots
-  const double2 *xpc;            // summed PC diagonal (first step), or null
   const int64_t *cpl_rowptr;     // n_interior+1 into cpl_val
   const int32_t *cpl_gcol;       // interface DOF (index into P) of each coupling entry
   const int64_t *ifr_rowptr;     // n_slots+1 into ifr_val
@@ -102,6 +100,19 @@ struct DevProblem {
   const int64_t *aii_rowptr;     // n_interior+1 into aii_val
   const int32_t *aii_gcol;       // global interior row of each interior entry
   double2 *Rres;                 // n_interior: refinement residual
+  // sharded solve with the exchange packed to the shared interface DOFs: the
+  // interface DOFs this shard's subdomains hold (ascending), whether it owns
+  // each (every DOF has one owner, so sums over owned DOFs add up once over
+  // the shards), each one's place in the packed exchange (-1: held by this
+  // shard alone), the packed buffer (2 x n_shared complex) and the scalar
+  // buffer ([0..2] summed, [4] maxed over the shards)
+  const int32_t *dist_dof;
+  const uint8_t *dist_own;
+  const int32_t *dist_pos;
+  int32_t dist_n;
+  int32_t n_shared;
+  double2 *dist_pack;
+  double *dist_scal;
 };
 
 // Batched subdomain solve kernels: one warp per subdomain with TMA-staged row
@@ -183,8 +194,6 @@ void launch_cocg_iteration(const DevProblem &p, cudaStream_t stream);
 void launch_cocg_update(const DevProblem &p, cudaStream_t stream);
 void launch_edge_solution(const DevProblem &p, int64_t ne, const int64_t *edge_src, const double2 *Y,
                           const double2 *V, double2 *x, cudaStream_t stream);
-void launch_shard_gather(const DevProblem &p, const double2 *pcloc, double2 *xq, double2 *xpc, bool status_check,
-                         cudaStream_t stream);
 void launch_set_status(CocgScalars *sc, double eps, int32_t max_loop, cudaStream_t stream);
 void launch_element_rhs(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
                         const double *el_sigma, double omega, int32_t n_gaps, const double *gap,
@@ -200,5 +209,15 @@ void launch_adjoint_gradient(int32_t n_design, const int32_t *design_tets, const
                              const int32_t *tet_edges, const double *crd, double omega, const double2 *x,
                              const double2 *lam, double *g_eps, double *g_sigma, cudaStream_t stream);
 void launch_profile_reset(CocgScalars *sc, cudaStream_t stream);
+// sharded solve, packed exchange (DevProblem dist_*): pack the shard's
+// partial Q (and PC diagonal) of its shared DOFs; the first COCG step up to
+// the local sums; its scalars from the exchanged sums; an iteration's (p, q),
+// its update up to the local sums, and its scalars and p
+void launch_dist_pack(const DevProblem &p, const double2 *pcloc, bool with_pc, bool status_check, cudaStream_t stream);
+void launch_dist_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream);
+void launch_dist_first_finish(const DevProblem &p, cudaStream_t stream);
+void launch_dist_pq(const DevProblem &p, cudaStream_t stream);
+void launch_dist_update(const DevProblem &p, cudaStream_t stream);
+void launch_dist_finish(const DevProblem &p, cudaStream_t stream);
 
 }  // namespace fw

@@ -370,12 +370,33 @@ class HddmSolver:
         return ms.value
 
     # -- sharded solve (one context per rank) --------------------------------
-    def shard_set_exchange(self, device_ptr: int) -> None:
-        """Device buffer of 4*total_free doubles for the partial sums."""
-        _lib.check(self._lib.fwgpu_shard_set_exchange(self._h, ctypes.c_void_p(int(device_ptr))))
+    def shard_set_layout(self, shard_first) -> int:
+        """The subdomain ranges of all shards (``shard_first``: n_shards+1
+        boundaries); returns the number of interface DOFs held by two or
+        more shards, the length of the packed exchange."""
+        f = np.ascontiguousarray(shard_first, dtype=np.int32)
+        n = ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_shard_set_layout(self._h, int(f.shape[0] - 1), _ptr(f, ctypes.c_int32),
+                                                     ctypes.byref(n)))
+        return n.value
+
+    def shard_set_exchange(self, pack_ptr: int, scal_ptr: int) -> None:
+        """Device buffers: 4*n_shared doubles (packed Q and diagonal) and 8
+        doubles (scalars)."""
+        _lib.check(self._lib.fwgpu_shard_set_exchange(self._h, ctypes.c_void_p(int(pack_ptr)),
+                                                      ctypes.c_void_p(int(scal_ptr))))
 
     def shard_first(self) -> None:
         _lib.check(self._lib.fwgpu_shard_first(self._h))
+
+    def shard_first_sums(self) -> None:
+        _lib.check(self._lib.fwgpu_shard_first_sums(self._h))
+
+    def shard_iterate_pq(self) -> None:
+        _lib.check(self._lib.fwgpu_shard_iterate_pq(self._h))
+
+    def shard_iterate_update(self) -> None:
+        _lib.check(self._lib.fwgpu_shard_iterate_update(self._h))
 
     def shard_first_finish(self) -> int:
         st = ctypes.c_int32()

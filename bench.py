@@ -581,7 +581,7 @@ def run_sharded_bench(args, rank, world, local, dist):
                 ir_max_steps=args.ir_steps, ir_tol=args.ir_tol, ir_relax=args.ir_relax,
                 solve_kernel=args.solve_kernel, stage_cap=args.stage_cap, stage_warps=args.stage_warps)
     exch = shard.torch_exchange()
-    backend = shard.GpuShard(model, (lo, hi), device=local, **opts)
+    backend = shard.GpuShard(model, (lo, hi), shard.shard_bounds(model, world), device=local, **opts)
     for _ in range(args.warmup):
         shard.run_sharded(backend, exch, 0)
     clocks = ClockSampler(local)

@@ -371,29 +371,54 @@ int fwgpu_adjoint_gradient_multi(fwgpu_context *ctx, int32_t n_probe, const int3
 
 /* A context created with shard_begin < shard_end solves the subdomains of
  * that range only: the reference's "part" (lib/hddm/hddm_solver_ph.h:112-329,
- * one part per rank).  The interface vectors stay global; every iteration the
- * ranks sum their partial interface vector Q, and the first step also the
- * preconditioner diagonal, through a caller-owned device buffer (an NCCL
- * all-reduce in place); every rank then runs the same COCG update on the same
- * sums.  Order per solve:
- *   fwgpu_make_tmp_aij; fwgpu_shard_first; [sum the buffer over ranks];
+ * one part per rank).  Each shard runs the COCG on the interface DOFs its
+ * subdomains hold; every DOF has one owner (the shard of the first subdomain
+ * holding it), and the dot products and the max-norm sum or max the owned
+ * DOFs over the shards.  Only the DOFs held by two or more shards cross
+ * between the ranks, packed in ascending DOF order (the same positions on
+ * every rank).  Per iteration the caller sums, over the ranks, in place on
+ * the context's device: the packed partial Q, then (p, q), then (r, z) and
+ * |r|^2 together with the max of max|r| -- the reference's neighbour exchange
+ * and its scalar all-reduces.  Order per solve:
+ *   fwgpu_shard_set_layout; fwgpu_shard_set_exchange (once per context);
+ *   fwgpu_make_tmp_aij; fwgpu_shard_first; [sum pack];
+ *   fwgpu_shard_first_sums; [sum scal[0..2], max scal[4]];
  *   fwgpu_shard_first_finish; then until *status != 0:
- *   fwgpu_shard_iterate; [sum Q over ranks]; fwgpu_shard_iterate_finish;
+ *     fwgpu_shard_iterate; [sum pack[0 .. 2*n_shared)];
+ *     fwgpu_shard_iterate_pq; [sum scal[0..1]];
+ *     fwgpu_shard_iterate_update; [sum scal[0..2], max scal[4]];
+ *     fwgpu_shard_iterate_finish;
  *   fwgpu_solve_dom_last; fwgpu_get_edge_solution gives this shard's edges
  *   (zero elsewhere): their sum over ranks is the solution.
- * The whole-solve calls (fwgpu_hddm_solve, fwgpu_iteration_s*) refuse a
- * sharded context. */
+ * Every call returns after its kernels finished, so the caller's collective
+ * may read the buffers at once.  The whole-solve calls (fwgpu_hddm_solve,
+ * fwgpu_iteration_s*) refuse a sharded context. */
 
-/* d_exchange: 4*total_free doubles on the context's device: the complex
- * partial Q (2*total_free doubles), then the complex partial diagonal. */
-int fwgpu_shard_set_exchange(fwgpu_context *ctx, double *d_exchange);
-/* solve_dom_1st on this shard; partial Q and diagonal into the buffer */
+/* The subdomain ranges of all n_shards shards: shard k solves subdomains
+ * shard_first[k] .. shard_first[k+1]-1 (shard_first[0] = 0,
+ * shard_first[n_shards] = n_subdomains); this context's range must be one
+ * of them.  *n_shared receives the number of interface DOFs held by two or
+ * more shards, the length of the packed exchange. */
+int fwgpu_shard_set_layout(fwgpu_context *ctx, int32_t n_shards, const int32_t *shard_first, int32_t *n_shared);
+/* Caller-owned device buffers on the context's device: d_pack 4*n_shared
+ * doubles (two packed complex vectors: Q, and on the first step the
+ * preconditioner diagonal), d_scal 8 doubles. */
+int fwgpu_shard_set_exchange(fwgpu_context *ctx, double *d_pack, double *d_scal);
+/* solve_dom_1st on this shard; packed partial Q and diagonal */
 int fwgpu_shard_first(fwgpu_context *ctx);
-/* ITERATION_S_1ST from the summed buffer */
+/* the first step of ITERATION_S_1ST on the held DOFs, from the summed pack;
+ * local sums of the owned DOFs into scal */
+int fwgpu_shard_first_sums(fwgpu_context *ctx);
+/* its scalars from the summed scal; *status as fwgpu_iteration_s_1st */
 int fwgpu_shard_first_finish(fwgpu_context *ctx, int32_t *status);
-/* the subdomain solves of one iteration; partial Q into the buffer */
+/* the subdomain solves of one iteration; packed partial Q */
 int fwgpu_shard_iterate(fwgpu_context *ctx);
-/* the COCG update of ITERATION_S from the summed Q; *status as fwgpu_iteration_s */
+/* Q from the summed pack; the owned DOFs' (p, q) into scal[0..1] */
+int fwgpu_shard_iterate_pq(fwgpu_context *ctx);
+/* alpha from the summed (p, q); u, r, z; the owned DOFs' (r, z), |r|^2, max|r| into scal */
+int fwgpu_shard_iterate_update(fwgpu_context *ctx);
+/* resi, beta and the stopping test from the summed scal, then p;
+ * *status as fwgpu_iteration_s */
 int fwgpu_shard_iterate_finish(fwgpu_context *ctx, int32_t *status);
 
 /* -- batched skyline substitution without device allocation -------------- */

@@ -18,7 +18,7 @@ def test_two_shards_match_unsharded(precision):
     with hddm.HddmSolver(m, **opts) as s:
         r = s.solve(0)
         x_ref = s.edge_solution()
-    backends = [shard.GpuShard(m, rng, device=0, **opts) for rng in shard.shard_ranges(m, 2)]
+    backends = [shard.GpuShard(m, rng, shard.shard_bounds(m, 2), device=0, **opts) for rng in shard.shard_ranges(m, 2)]
     try:
         x, it = shard.run_lockstep(backends, 0)
     finally:

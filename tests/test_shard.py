@@ -41,7 +41,7 @@ def test_cpu_backend_alone_matches_oracle():
     m = _model()
     part = oracle.partition(m)
     xo, _, hist, _ = oracle.hddm(m, part, 1e-10, 5000)
-    x, it = shard.run_sharded(CpuShard(m, (0, m.nsub), hddm_eps=1e-10), lambda buf: None, 0)
+    x, it = shard.run_sharded(CpuShard(m, (0, m.nsub), [0, m.nsub], hddm_eps=1e-10), lambda buf, op: None, 0)
     assert rel_l2(x, xo) <= 1e-8
     assert abs(it - len(hist)) <= max(2, len(hist) // 20)
 
@@ -67,8 +67,10 @@ def _rank_main(rank, world, port, out):
     try:
         m = _model()
         lo, hi = shard.shard_ranges(m, world)[rank]
-        x, it = shard.run_sharded(CpuShard(m, (lo, hi), hddm_eps=1e-10), shard.torch_exchange(), 0)
-        np.savez(f"{out}_{rank}.npz", x=x, it=it, lo=lo, hi=hi)
+        b = CpuShard(m, (lo, hi), shard.shard_bounds(m, world), hddm_eps=1e-10)
+        x, it = shard.run_sharded(b, shard.torch_exchange(), 0)
+        np.savez(f"{out}_{rank}.npz", x=x, it=it, lo=lo, hi=hi, n_shared=b.n_shared, nfree=b.nfree,
+                 held=b.held.shape[0], owned=int(b.owned.sum()))
     finally:
         dist.destroy_process_group()
 
@@ -96,5 +98,10 @@ def test_two_gloo_ranks_match_single_process():
     assert int(res[0]["it"]) == int(res[1]["it"])
     assert np.array_equal(res[0]["x"], res[1]["x"])
     assert int(res[0]["hi"]) == int(res[1]["lo"]) and 0 < int(res[0]["hi"]) < m.nsub
+    # the packed exchange: the same shared DOFs on both ranks, fewer than the
+    # interface; every DOF owned by exactly one rank
+    assert int(res[0]["n_shared"]) == int(res[1]["n_shared"])
+    assert 0 < int(res[0]["n_shared"]) < int(res[0]["nfree"])
+    assert int(res[0]["owned"]) + int(res[1]["owned"]) == int(res[0]["nfree"])
     assert rel_l2(res[0]["x"], xo) <= 1e-8
     assert abs(int(res[0]["it"]) - len(hist)) <= max(2, len(hist) // 20)
