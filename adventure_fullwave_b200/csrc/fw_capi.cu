@@ -497,7 +497,8 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
       return set_error(FWGPU_ERR_ARG, "shard range outside the subdomains");
     s_begin = opts->shard_begin;
     s_end = opts->shard_end;
-    c->sharded = s_begin != 0 || s_end != nsub;
+    // an explicit range, all subdomains included (one rank), runs the shard protocol
+    c->sharded = true;
   }
   // subdomains largest first (by interior DOFs, then local DOFs)
   std::vector<int32_t> order(s_end - s_begin);
