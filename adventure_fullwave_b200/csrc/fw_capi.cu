@@ -441,9 +441,9 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
   c->opts = *opts;
   if (c->opts.graph_iterations <= 0) c->opts.graph_iterations = 16;
   if (c->opts.ir_max_steps <= 0) c->opts.ir_max_steps = 1;
-  if (c->opts.stage_warps < 0 || c->opts.stage_warps > 2) {
+  if (c->opts.stage_warps != 0 && c->opts.stage_warps != 1 && c->opts.stage_warps != 2 && c->opts.stage_warps != 4) {
     delete c;
-    return set_error(FWGPU_ERR_ARG, "stage_warps must be 0, 1 or 2");
+    return set_error(FWGPU_ERR_ARG, "stage_warps must be 0, 1, 2 or 4");
   }
   if (c->opts.solve_kernel < FWGPU_SOLVE_AUTO || c->opts.solve_kernel > FWGPU_SOLVE_GLOBAL) {
     delete c;
@@ -497,7 +497,8 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
       return set_error(FWGPU_ERR_ARG, "shard range outside the subdomains");
     s_begin = opts->shard_begin;
     s_end = opts->shard_end;
-    c->sharded = s_begin != 0 || s_end != nsub;
+    // an explicit range, all subdomains included (one rank), runs the shard protocol
+    c->sharded = true;
   }
   // subdomains largest first (by interior DOFs, then local DOFs)
   std::vector<int32_t> order(s_end - s_begin);
@@ -851,7 +852,7 @@ static int build_stage_blocks(fwgpu_context *c, int cap, int *max_blocks_out) {
   c->dp.blk_tab = c->d_blk_tab;
   c->dp.max_blocks = max_blocks;
   c->dp.stage_cap = cap;
-  if (c->dp.stage_warps < 1) c->dp.stage_warps = c->opts.stage_warps == 2 ? 2 : 1;
+  if (c->dp.stage_warps < 1) c->dp.stage_warps = c->opts.stage_warps > 0 ? c->opts.stage_warps : 1;
   if (max_blocks_out) *max_blocks_out = max_blocks;
   return FWGPU_OK;
 }
@@ -894,7 +895,7 @@ static int setup_stage(fwgpu_context *c) {
 // same bits on every run: AUTO times only variants that sum in the same
 // order.  The staging capacity sets the row blocks, and with them the
 // order of the sums, so AUTO keeps the default capacity (a rule on the
-// model's envelope, setup_stage) and times one against two warps per
+// model's envelope, setup_stage) and times one, two and four warps per
 // subdomain, which share out whole row groups and column chunks and so sum
 // alike.  The CTA kernel sums in another order and runs only when asked
 // for.  An explicit WARP choice times the staging capacities too.
@@ -906,14 +907,14 @@ static int tune_solve_kernel(fwgpu_context *c) {
   std::vector<Cand> cand;
   const bool any = c->opts.solve_kernel == FWGPU_SOLVE_AUTO;
   if (any && c->warp_ok) {
-    for (int warps = 1; warps <= 2; warps++)
+    for (int warps = 1; warps <= 4; warps *= 2)
       if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps)
         cand.push_back({fw::kSolveWarp, c->dp.stage_cap, warps});
     if (cand.empty()) cand.push_back({fw::kSolveWarp, c->dp.stage_cap, c->opts.stage_warps});
   }
   if (c->opts.solve_kernel == FWGPU_SOLVE_WARP && c->warp_ok)
     for (int cap : c->stage_caps)
-      for (int warps = 1; warps <= 2; warps++)
+      for (int warps = 1; warps <= 4; warps *= 2)
         if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps) cand.push_back({fw::kSolveWarp, cap, warps});
   if (any && !c->warp_ok && c->dp.cta_smem > 0) cand.push_back({fw::kSolveCta, 0, 1});
   if (cand.empty()) {

@@ -835,12 +835,12 @@ __device__ bool staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
 }
 
 template <typename T>
-__global__ void __launch_bounds__(64) subsolve_staged_kernel(DevProblem p, int mode, const double2 *rhs, double2 *xout,
+__global__ void __launch_bounds__(128) subsolve_staged_kernel(DevProblem p, int mode, const double2 *rhs, double2 *xout,
                                                              T *zstash, int accumulate, StageLayout lay) {
   if (mode == kModeIter && p.sc->status != 0) return;
   if (accumulate && refine_skipped(p, mode)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[2][2];
+  __shared__ double red[4][2];
   const int tid = threadIdx.x, nt = blockDim.x, nw = nt >> 5;
   const int s = p.sub_order[blockIdx.x];
   const int64_t io = p.int_off[s];

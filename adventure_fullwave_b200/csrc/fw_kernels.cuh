@@ -88,7 +88,7 @@ struct DevProblem {
   const int2 *blk_tab;           // per subdomain nblk+1 x (first row, first envelope element)
   int32_t max_blocks;            // most blocks of one subdomain
   int32_t stage_cap;             // envelope elements per staging buffer
-  int32_t stage_warps;           // warps sharing one subdomain's sweeps (1 or 2)
+  int32_t stage_warps;           // warps sharing one subdomain's sweeps (1, 2 or 4)
   int64_t row0, n_interior;      // interior rows of the subdomains this context solves
   int64_t slot0, n_slots;        // interface slots of the subdomains this context solves
   // sharded solve: this shard's partial interface sums go to the exchange

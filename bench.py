@@ -680,7 +680,7 @@ def main():
     ap.add_argument("--graph-iters", type=int, default=32)
     ap.add_argument("--solve-kernel", default="auto", choices=["auto", "warp", "cta", "global"])
     ap.add_argument("--stage-cap", type=int, default=0, help="staging buffer elements (0: timed choice)")
-    ap.add_argument("--stage-warps", type=int, default=0, help="warps per subdomain, 1 or 2 (0: timed choice)")
+    ap.add_argument("--stage-warps", type=int, default=0, help="warps per subdomain, 1, 2 or 4 (0: timed choice)")
     ap.add_argument("--prof-reps", type=int, default=50)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--ref-iters", type=int, default=1, help="timed reference iterations of the CPU baseline")

@@ -145,8 +145,9 @@ typedef struct {
                             residual is above ir_relax (0 = always); the first and last
                             subdomain solves always refine */
   int32_t shard_begin;   /* sharded solve: this context solves subdomains [shard_begin, shard_end) */
-  int32_t shard_end;     /* (0, 0 = every subdomain); drive it with the fwgpu_shard_* calls */
-  int32_t stage_warps;   /* WARP kernel: warps sharing a subdomain's sweeps, 1 or 2 (0 = timed choice) */
+  int32_t shard_end;     /* (0, 0 = every subdomain, unsharded); a given range, even all of them,
+                            makes a sharded context: drive it with the fwgpu_shard_* calls */
+  int32_t stage_warps;   /* WARP kernel: warps sharing a subdomain's sweeps, 1, 2 or 4 (0 = timed choice) */
   int32_t stall_copy_test; /* test hook, 0 in normal use: 1 makes the staged subdomain solves' first wait
                               for a copy poll a barrier that nothing completes, give up after a few polls
                               and raise FWGPU_ERR_TIMEOUT (each CTA still waits for its copies in flight
