@@ -673,11 +673,12 @@ __host__ __device__ inline StageLayout stage_layout(int max_interior, int max_bl
 // Forward sweep over the row blocks.  Per block of nb <= 32 rows starting at
 // row r0:
 //   - the entries left of the block: eight lanes per row, four rows per
-//     warp step (row groups of four shared out over the warps); lane j of a
-//     row sums the row's entries j, j+8, j+16, ... in order into one
-//     accumulator, and three shuffles add the eight lanes.  The sum of a row
-//     therefore depends on its entries alone, not on the staging capacity or
-//     the number of warps;
+//     row group, two row groups in flight per warp (the groups shared out
+//     over the warps); lane j of a row sums the row's entries j, j+8, j+16,
+//     ... in order into one accumulator, and a three-level tree adds the
+//     eight lanes (real parts in lanes 0-3, imaginary parts in lanes 4-7).
+//     The sum of a row therefore depends on its entries alone, not on the
+//     staging capacity or the number of warps;
 //   - the block's triangle: lane t holds row r0 + t, one broadcast shuffle per
 //     row, the operands of 4 steps loaded ahead;
 //   - the pivot scaling z = y/d goes to the z stash for the backward sweep.
@@ -702,26 +703,45 @@ __device__ bool staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, cons
     const bool late = !stage_wait(st, b);
     if (__syncthreads_or(late)) return false;
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);  // S[e]: entry e of the envelope
-    for (int g = w; 4 * g < nb; g += nw) {
-      const int t = 4 * g + q;
-      const int2 mt = t < nb ? meta[t] : make_int2(r0, 0);
-      const int len = t < nb ? max(0, r0 - mt.x) : 0;
-      int longest = max(len, __shfl_xor_sync(0xffffffffu, len, 8));
-      longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, 16));
-      const T *row = S + mt.y;  // the row's entries from its first column
-      const T *yr = y + mt.x;
-      T acc = czero<T>();
-      for (int k = j; k < longest; k += 16) {
-        const bool i0 = k < len, i1 = k + 8 < len;
-        const T a0 = i0 ? row[k] : czero<T>(), b0 = i0 ? yr[k] : czero<T>();
-        const T a1 = i1 ? row[k + 8] : czero<T>(), b1 = i1 ? yr[k + 8] : czero<T>();
-        acc = cmac(acc, a0, b0);
-        acc = cmac(acc, a1, b1);
+    // two row groups per warp step, so that each warp has two independent
+    // sums in flight
+    for (int g = w; 4 * g < nb; g += 2 * nw) {
+      int len[2], t[2];
+      const T *row[2], *yr[2];
+      T acc[2];
+      int longest = 0;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        t[h] = 4 * (g + h * nw) + q;
+        const int2 mt = t[h] < nb ? meta[t[h]] : make_int2(r0, 0);
+        len[h] = t[h] < nb ? max(0, r0 - mt.x) : 0;
+        row[h] = S + mt.y;  // the row's entries from its first column
+        yr[h] = y + mt.x;
+        acc[h] = czero<T>();
+        longest = max(longest, len[h]);
       }
-      acc = cadd(acc, shfl_xor(acc, 4));
-      acc = cadd(acc, shfl_xor(acc, 2));
-      acc = cadd(acc, shfl_xor(acc, 1));
-      if (j == 0 && t < nb) rectb[t] = acc;
+      longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, 8));
+      longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, 16));
+      for (int k = j; k < longest; k += 16) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const bool i0 = k < len[h], i1 = k + 8 < len[h];
+          const T a0 = i0 ? row[h][k] : czero<T>(), b0 = i0 ? yr[h][k] : czero<T>();
+          const T a1 = i1 ? row[h][k + 8] : czero<T>(), b1 = i1 ? yr[h][k + 8] : czero<T>();
+          acc[h] = cmac(acc[h], a0, b0);
+          acc[h] = cmac(acc[h], a1, b1);
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const auto part = group8_sum_split(acc[h], j);  // real part in lanes 0-3, imaginary in 4-7
+        if ((j & 3) == 0 && t[h] < nb) {
+          if (j == 0)
+            rectb[t[h]].x = part;
+          else
+            rectb[t[h]].y = part;
+        }
+      }
     }
     __syncthreads();
     if (w == 0) {
