@@ -101,6 +101,14 @@ struct fwgpu_context {
   int multi_n = 0;                 // sources of the last batched solve (0: none)
   int32_t *d_blk_off = nullptr;    // staged solve block table (current staging capacity)
   int2 *d_blk_tab = nullptr;
+  // block-inverse layout of the factor (FWGPU_SOLVE_BLOCKINV)
+  bool inv_ok = false;             // its block table is built and its kernel fits in shared memory
+  int64_t inv_len = 0;             // elements of Linv
+  int64_t *d_inv_ptr = nullptr;
+  int32_t *d_inv_blk_off = nullptr;
+  int2 *d_inv_blk_tab = nullptr;
+  double2 *d_Linv64 = nullptr;
+  float2 *d_Linv32 = nullptr;
   std::vector<int> stage_caps;     // staging capacities that fit in shared memory
   std::vector<int32_t> h_order;    // subdomains by interior size, largest first (the device sub_order)
   std::vector<int32_t> h_nblk;     // staged blocks of each subdomain at the current capacity
@@ -445,7 +453,7 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
     delete c;
     return set_error(FWGPU_ERR_ARG, "stage_warps must be 0, 1, 2 or 4");
   }
-  if (c->opts.solve_kernel < FWGPU_SOLVE_AUTO || c->opts.solve_kernel > FWGPU_SOLVE_GLOBAL) {
+  if (c->opts.solve_kernel < FWGPU_SOLVE_AUTO || c->opts.solve_kernel > FWGPU_SOLVE_BLOCKINV) {
     delete c;
     return set_error(FWGPU_ERR_ARG, "unknown solve_kernel");
   }
@@ -651,11 +659,15 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
       case FWGPU_SOLVE_GLOBAL:
         dp.solve_variant = fw::kSolveGlobal;
         break;
+      case FWGPU_SOLVE_BLOCKINV:
+        dp.solve_variant = fw::kSolveInv;
+        break;
       default:
         dp.solve_variant = dp.cta_smem > 0 ? fw::kSolveCta : fw::kSolveGlobal;
     }
-    // AUTO times the warps per subdomain; WARP times its staging capacities too
-    c->solve_tuned = c->opts.solve_kernel != FWGPU_SOLVE_AUTO && c->opts.solve_kernel != FWGPU_SOLVE_WARP;
+    // AUTO and BLOCKINV time the warps per subdomain; WARP times its staging capacities too
+    c->solve_tuned = c->opts.solve_kernel != FWGPU_SOLVE_AUTO && c->opts.solve_kernel != FWGPU_SOLVE_WARP &&
+                     c->opts.solve_kernel != FWGPU_SOLVE_BLOCKINV;
   }
   // per-edge solution source: the first subdomain holding each edge
   std::vector<int64_t> esrc(m.ne, -1);
@@ -857,6 +869,79 @@ static int build_stage_blocks(fwgpu_context *c, int cap, int *max_blocks_out) {
   return FWGPU_OK;
 }
 
+// Block-inverse layout: row blocks of at most 32 rows whose stored elements
+// (the rows' entries left of the block, the block's N = (I + L_bb)^-1 - I as
+// a dense strict lower triangle, and its pivots) fit one staging buffer of
+// `cap` elements, each subdomain's elements from a 16-byte boundary.
+static int build_inv_blocks(fwgpu_context *c, int cap) {
+  const fw::Plan &p = c->p;
+  const int nsub = c->m.nsub;
+  const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
+  std::vector<int32_t> boff(nsub + 1, 0);
+  std::vector<int2> btab;
+  std::vector<int64_t> iptr(p.sub_int_off[nsub], 0);
+  int max_blocks = 0, max_nI = 0;
+  int64_t pos = 0;
+  for (int s = 0; s < nsub; s++) {
+    const int64_t io = p.sub_int_off[s];
+    const int nI = (int)(p.sub_int_off[s + 1] - io);
+    max_nI = std::max(max_nI, nI);
+    pos = (pos + 1) & ~(int64_t)1;
+    const int64_t base = pos;
+    boff[s] = (int32_t)btab.size();
+    auto left = [&](int r, int r0) { return std::max(0, r0 - c->h_env_lo[io + r]); };
+    int r = 0, nb = 0;
+    while (r < nI) {
+      const int r0 = r;
+      int64_t lsum = 0;
+      int rows = 0;
+      while (r < nI && rows < 32) {
+        const int64_t size = lsum + left(r, r0) + (int64_t)(rows + 1) * rows / 2 + rows + 1;
+        if (rows > 0 && size > cap - 2) break;
+        lsum += left(r, r0);
+        r++;
+        rows++;
+      }
+      if (lsum + (int64_t)rows * (rows - 1) / 2 + rows > cap - 2) return set_error(FWGPU_ERR_ARG, "block-inverse layout: a row exceeds the staging capacity");
+      btab.push_back(make_int2(r0, (int)(pos - base)));
+      for (int t = r0; t < r; t++) {
+        iptr[io + t] = pos;
+        pos += left(t, r0);
+      }
+      pos += (int64_t)rows * (rows - 1) / 2 + rows;
+      nb++;
+    }
+    btab.push_back(make_int2(nI, (int)(pos - base)));
+    if (pos - base > INT32_MAX) return set_error(FWGPU_ERR_ARG, "block-inverse layout: a subdomain over 2^31 elements");
+    if (nI > 0) iptr[io] = base;
+    max_blocks = std::max(max_blocks, nb);
+  }
+  boff[nsub] = (int32_t)btab.size();
+  const size_t smem = fw::subsolve_staged_smem_bytes(max_nI, max_blocks, cap, fp32);
+  if (smem > 227 * 1024 || fw::configure_subsolve_inv(smem, fp32) != 0) {
+    c->inv_ok = false;
+    return FWGPU_OK;
+  }
+  FW_TRY(c->upload(&c->d_inv_blk_off, boff));
+  FW_TRY(c->upload(&c->d_inv_blk_tab, btab));
+  FW_TRY(c->upload(&c->d_inv_ptr, iptr));
+  // padding: bulk copies of a block may read up to 16 bytes past its end
+  if (fp32)
+    FW_TRY(c->alloc(&c->d_Linv32, pos + 64));
+  else
+    FW_TRY(c->alloc(&c->d_Linv64, pos + 64));
+  c->inv_len = pos;
+  c->dp.inv_ptr = c->d_inv_ptr;
+  c->dp.inv_blk_off = c->d_inv_blk_off;
+  c->dp.inv_blk_tab = c->d_inv_blk_tab;
+  c->dp.Linv64 = c->d_Linv64;
+  c->dp.Linv32 = c->d_Linv32;
+  c->dp.inv_max_blocks = max_blocks;
+  c->dp.inv_cap = cap;
+  c->inv_ok = true;
+  return FWGPU_OK;
+}
+
 // Staging capacities the staged kernel can run with (shared memory of one
 // warp <= 227 KB), the default one's block table, and the kernel's shared
 // memory limit set for the largest of them.
@@ -917,6 +1002,10 @@ static int tune_solve_kernel(fwgpu_context *c) {
       for (int warps = 1; warps <= 4; warps *= 2)
         if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps) cand.push_back({fw::kSolveWarp, cap, warps});
   if (any && !c->warp_ok && c->dp.cta_smem > 0) cand.push_back({fw::kSolveCta, 0, 1});
+  if (c->opts.solve_kernel == FWGPU_SOLVE_BLOCKINV && c->inv_ok)
+    for (int warps = 1; warps <= 4; warps *= 2)
+      if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps)
+        cand.push_back({fw::kSolveInv, c->dp.inv_cap, warps});
   if (cand.empty()) {
     c->solve_tuned = true;
     return FWGPU_OK;
@@ -1012,6 +1101,10 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     FW_TRY(setup_stage(c));
     if (c->opts.solve_kernel == FWGPU_SOLVE_WARP && !c->warp_ok)
       return set_error(FWGPU_ERR_ARG, "staged solve kernel: subdomains too large for shared memory");
+    if (c->opts.solve_kernel == FWGPU_SOLVE_BLOCKINV) {
+      if (c->warp_ok) FW_TRY(build_inv_blocks(c, c->dp.stage_cap));
+      if (!c->inv_ok) return set_error(FWGPU_ERR_ARG, "block-inverse solve kernel: subdomains too large for shared memory");
+    }
   }
   if (!c->factor_fresh) {
     // envelope values and LDL^T factor (the layout is fixed by the model)
@@ -1027,6 +1120,10 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
       fw::launch_to_fp32(pos + 64, c->d_L64, c->d_L32, c->stream);
       c->dp.L32 = c->d_L32;
       c->dp.L64 = nullptr;
+    }
+    if (c->inv_ok) {
+      fw::launch_inv_relayout(c->dp, c->d_L64, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
+      c->launches += 1;
     }
     int32_t fstat = 0;
     FW_CUDA(cudaMemcpyAsync(&fstat, c->d_mesh_status + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
@@ -1549,8 +1646,11 @@ static int fill_result(fwgpu_context *c, fwgpu_result *res) {
     res->t_last_ms = ms;
     res->kernel_launches = c->launches;
     res->solve_kernel = c->dp.solve_variant + 1;
-    res->stage_cap = c->dp.solve_variant == fw::kSolveWarp ? c->dp.stage_cap : 0;
-    res->stage_warps = c->dp.solve_variant == fw::kSolveWarp ? c->dp.stage_warps : 0;
+    res->stage_cap = c->dp.solve_variant == fw::kSolveWarp  ? c->dp.stage_cap
+                     : c->dp.solve_variant == fw::kSolveInv ? c->dp.inv_cap
+                                                            : 0;
+    res->stage_warps =
+        c->dp.solve_variant == fw::kSolveWarp || c->dp.solve_variant == fw::kSolveInv ? c->dp.stage_warps : 0;
     res->reserved = 0;
   }
   if (sc.nonfinite) return set_error(FWGPU_ERR_NONFINITE, "the interface residual became NaN or infinite");

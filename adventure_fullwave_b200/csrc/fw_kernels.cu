@@ -684,7 +684,7 @@ __host__ __device__ inline StageLayout stage_layout(int max_interior, int max_bl
 //   - the pivot scaling z = y/d goes to the z stash for the backward sweep.
 // Returns false when a staged copy did not arrive (error word raised); the
 // caller drains the copies in flight and stops.
-template <typename T>
+template <typename T, bool kInv>
 __device__ bool staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
                                T *y, int2 *meta, T *zstash, T *rectb, int tid, int nw) {
   const int lane = tid & 31, w = tid >> 5;
@@ -744,7 +744,35 @@ __device__ bool staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, cons
       }
     }
     __syncthreads();
-    if (w == 0) {
+    if (kInv && w == 0) {
+      // y_b = (I + N) v with v = y_b - (the sums left of the block): lane t
+      // sums N_tj v_j over j in four chunks of 8 columns, one accumulator
+      // per chunk, in ascending j; no chain from row to row
+      const int2 ml = meta[nb - 1];
+      const T *N = S + ml.y + max(0, r0 - ml.x);  // after the block's left parts
+      const T *Nr = N + ((lane * (lane - 1)) >> 1);
+      T *vb = rectb + kSB;
+      const T v = lane < nb ? csub(y[r0 + lane], rectb[lane]) : czero<T>();
+      vb[lane] = v;
+      __syncwarp();
+      T acc[4] = {czero<T>(), czero<T>(), czero<T>(), czero<T>()};
+#pragma unroll
+      for (int jj = 0; jj < 8; jj++) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          const int j = 8 * c + jj;
+          if (j < nb - 1) {
+            const T a = (j < lane && lane < nb) ? Nr[j] : czero<T>();
+            acc[c] = cmac(acc[c], a, vb[j]);
+          }
+        }
+      }
+      const T val = cadd(v, cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])));
+      if (lane < nb) {
+        y[r0 + lane] = val;
+        zstash[r0 + lane] = cmul(val, N[((nb * (nb - 1)) >> 1) + lane]);  // the pivots' 1/d after N
+      }
+    } else if (w == 0) {
       const T rect = rectb[lane];
       T val = lane < nb ? csub(y[r0 + lane], rect) : czero<T>();
       const T *mine = S + my_pr - my_lo;  // mine[col]: this lane's row at column col
@@ -777,7 +805,7 @@ __device__ bool staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, cons
 // y_c -= L_tc x_t for the block's rows t from the last to the first, in
 // place, as the reference does (advlas_skyline.c:157-165); a group of eight
 // rows none of which reaches the chunk is skipped.
-template <typename T>
+template <typename T, bool kInv>
 __device__ bool staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, const int64_t *ptr_g, int64_t base,
                                 T *y, T *xb, int2 *meta, int *gmin, int tid, int nw) {
   const int lane = tid & 31, w = tid >> 5;
@@ -802,7 +830,31 @@ __device__ bool staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
     const bool late = !stage_wait(st, b);
     if (__syncthreads_or(late)) return false;
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);
-    if (w == 0) {
+    if (kInv && w == 0) {
+      // x_b = (I + N)^T w with w = y_b: lane j sums N_tj w_t over t in four
+      // chunks of 8 rows, one accumulator per chunk, in ascending t
+      const int2 ml = meta[nb - 1];
+      const T *N = S + ml.y + max(0, r0 - ml.x);
+      const T wv = lane < nb ? y[r0 + lane] : czero<T>();
+      T acc[4] = {czero<T>(), czero<T>(), czero<T>(), czero<T>()};
+#pragma unroll
+      for (int tt = 0; tt < 8; tt++) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          const int t = 8 * c + tt;
+          if (t >= 1 && t < nb) {
+            const T a = lane < t ? N[((t * (t - 1)) >> 1) + lane] : czero<T>();
+            acc[c] = cmac(acc[c], a, y[r0 + t]);
+          }
+        }
+      }
+      const T val = cadd(wv, cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])));
+      __syncwarp();  // every lane has read y_b before it is overwritten
+      if (lane < nb) {
+        y[r0 + lane] = val;
+        xb[lane] = val;
+      }
+    } else if (w == 0) {
       // triangle, lanes over the block's columns; operands of 4 steps loaded ahead
       T val = lane < nb ? y[r0 + lane] : czero<T>();
       const int col = r0 + lane;
@@ -832,7 +884,9 @@ __device__ bool staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
     for (int cb = bmin + 32 * w; cb < r0; cb += 32 * nw) {
       const int c = cb + lane;
       const bool act = c < r0;
-      T yc = act ? y[c] : czero<T>();
+      // four partial sums (rows t with t % 4 = 3, 2, 1, 0), so that four
+      // products are in flight per lane
+      T part[4] = {czero<T>(), czero<T>(), czero<T>(), czero<T>()};
       for (int t0 = (nb - 1) & ~7; t0 >= 0; t0 -= 8) {
         if (gmin[t0 >> 3] >= cb + 32) continue;  // no row of the group reaches this chunk
         T v[8], xv[8];
@@ -845,16 +899,16 @@ __device__ bool staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
           xv[u] = t < nb ? xb[t] : czero<T>();  // xb past the block may hold anything
         }
 #pragma unroll
-        for (int u = 0; u < 8; u++) yc = cmsub(yc, v[u], xv[u]);
+        for (int u = 0; u < 8; u++) part[u & 3] = cmac(part[u & 3], v[u], xv[u]);
       }
-      if (act) y[c] = yc;
+      if (act) y[c] = csub(y[c], cadd(cadd(part[0], part[1]), cadd(part[2], part[3])));
     }
     __syncthreads();
   }
   return true;
 }
 
-template <typename T>
+template <typename T, bool kInv>
 __global__ void __launch_bounds__(128) subsolve_staged_kernel(DevProblem p, int mode, const double2 *rhs, double2 *xout,
                                                              T *zstash, int accumulate, StageLayout lay) {
   if (mode == kModeIter && p.sc->status != 0) return;
@@ -865,8 +919,9 @@ __global__ void __launch_bounds__(128) subsolve_staged_kernel(DevProblem p, int 
   const int s = p.sub_order[blockIdx.x];
   const int64_t io = p.int_off[s];
   const int nI = (int)(p.int_off[s + 1] - io);
-  const int b0 = p.blk_off[s];
-  const int nblk = p.blk_off[s + 1] - b0 - 1;
+  const int32_t *blk_off = kInv ? p.inv_blk_off : p.blk_off;
+  const int b0 = blk_off[s];
+  const int nblk = blk_off[s + 1] - b0 - 1;
   if (nI == 0 || nblk <= 0) return;
   T *y = (T *)(smem_raw + lay.y);
   T *xb = (T *)(smem_raw + lay.xb);
@@ -880,9 +935,14 @@ __global__ void __launch_bounds__(128) subsolve_staged_kernel(DevProblem p, int 
   st.bar = (uint64_t *)(smem_raw + lay.bar);
   st.blk = blk;
   stage_init(st, &p.sc->copy_timeout, p.stall_test);
-  const int64_t base = p.env_ptr[io];
-  st.L = (sizeof(T) == 8 ? (const T *)(const void *)p.L32 : (const T *)(const void *)p.L64) + base;
-  for (int b = tid; b <= nblk; b += nt) blk[b] = p.blk_tab[b0 + b];
+  const int64_t *ptr_all = kInv ? p.inv_ptr : p.env_ptr;
+  const int64_t base = ptr_all[io];
+  if (kInv)
+    st.L = (sizeof(T) == 8 ? (const T *)(const void *)p.Linv32 : (const T *)(const void *)p.Linv64) + base;
+  else
+    st.L = (sizeof(T) == 8 ? (const T *)(const void *)p.L32 : (const T *)(const void *)p.L64) + base;
+  const int2 *blk_tab = kInv ? p.inv_blk_tab : p.blk_tab;
+  for (int b = tid; b <= nblk; b += nt) blk[b] = blk_tab[b0 + b];
   if (tid == 0) {
     mbar_init(&st.bar[0], 1);
     mbar_init(&st.bar[1], 1);
@@ -919,18 +979,18 @@ __global__ void __launch_bounds__(128) subsolve_staged_kernel(DevProblem p, int 
     if (rn <= p.ir_tol * bn) return;  // the same decision in every thread
   }
   const int32_t *lo_g = p.env_lo + io;
-  const int64_t *ptr_g = p.env_ptr + io;
+  const int64_t *ptr_g = ptr_all + io;
   T *z = zstash + io;
   // L2: the forward sweep's blocks are read again by the backward sweep, the
   // backward sweep's reads are the last use
   st.hint = 1;
   st.policy = l2_evict_last();
-  bool ok = staged_forward<T>(st, nblk, lo_g, ptr_g, base, y, meta, z, rectb, tid, nw);
+  bool ok = staged_forward<T, kInv>(st, nblk, lo_g, ptr_g, base, y, meta, z, rectb, tid, nw);
   if (ok) {
     for (int c = tid; c < nI; c += nt) y[c] = z[c];
     __syncthreads();
     st.policy = l2_evict_first();
-    ok = staged_backward<T>(st, nblk, lo_g, ptr_g, base, y, xb, meta, gmin, tid, nw);
+    ok = staged_backward<T, kInv>(st, nblk, lo_g, ptr_g, base, y, xb, meta, gmin, tid, nw);
   }
   // every copy issued into this CTA's shared memory has landed before it exits
   stage_drain(st);
@@ -939,6 +999,59 @@ __global__ void __launch_bounds__(128) subsolve_staged_kernel(DevProblem p, int 
     double2 x = make_double2((double)y[c].x, (double)y[c].y);
     if (accumulate) x = cadd(xout[io + c], x);
     xout[io + c] = x;
+  }
+}
+
+// The block-inverse layout of one subdomain's factor, one warp per
+// subdomain, block by block.  For the block of rows r0..r0+nb-1:
+//   - each row's entries left of the block (columns lo..r0-1), copied;
+//   - N = (I + L_bb)^-1 - I, strictly lower, row-major (row i at i(i-1)/2),
+//     where L_bb is the block's own part of the unit lower factor; row by
+//     row, lane j: N_ij = -(L_ij + sum_{k=j+1}^{i-1} L_ik N_kj), k ascending,
+//     in FP64 (then rounded for the FP32 layout);
+//   - the rows' pivots 1/d (the envelope's diagonal).
+// The sweeps then apply the block's triangle as a product with N instead of
+// a row-by-row substitution.
+template <typename T>
+__global__ void __launch_bounds__(32) inv_relayout_kernel(DevProblem p, const double2 *__restrict__ L64, T *out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2 *M = (double2 *)smem_raw;  // [32][33]: L_bb
+  double2 *Nd = M + 32 * 33;         // [32][33]: N
+  const int s = blockIdx.x, lane = threadIdx.x;
+  const int64_t io = p.int_off[s];
+  const int b0 = p.inv_blk_off[s];
+  const int nblk = p.inv_blk_off[s + 1] - b0 - 1;
+  for (int b = 0; b < nblk; b++) {
+    const int r0 = p.inv_blk_tab[b0 + b].x, nb = p.inv_blk_tab[b0 + b + 1].x - r0;
+    int lo = r0;
+    int64_t ep = 0, ip = 0;
+    if (lane < nb) {
+      lo = p.env_lo[io + r0 + lane];
+      ep = p.env_ptr[io + r0 + lane];
+      ip = p.inv_ptr[io + r0 + lane];
+    }
+    for (int t = 0; t < nb; t++) {
+      const int lo_t = __shfl_sync(0xffffffffu, lo, t);
+      const int64_t ep_t = __shfl_sync(0xffffffffu, ep, t), ip_t = __shfl_sync(0xffffffffu, ip, t);
+      for (int k = lane; k < r0 - lo_t; k += 32) out[ip_t + k] = from_d2<T>(L64[ep_t + k]);
+      const int col = r0 + lane;
+      M[t * 33 + lane] = (lane < t && col >= lo_t) ? L64[ep_t + (col - lo_t)] : make_double2(0.0, 0.0);
+    }
+    __syncwarp();
+    for (int i = 1; i < nb; i++) {
+      if (lane < i) {
+        double2 acc = M[i * 33 + lane];
+        for (int k = lane + 1; k < i; k++) acc = cmac(acc, M[i * 33 + k], Nd[k * 33 + lane]);
+        Nd[i * 33 + lane] = make_double2(-acc.x, -acc.y);  // lane j reads only its own column of N
+      }
+    }
+    const int lo_l = __shfl_sync(0xffffffffu, lo, nb - 1);
+    const int64_t ip_l = __shfl_sync(0xffffffffu, ip, nb - 1);
+    const int64_t tri0 = ip_l + max(0, r0 - lo_l);
+    for (int i = 1; i < nb; i++)
+      if (lane < i) out[tri0 + ((i * (i - 1)) >> 1) + lane] = from_d2<T>(Nd[i * 33 + lane]);
+    if (lane < nb) out[tri0 + ((nb * (nb - 1)) >> 1) + lane] = from_d2<T>(L64[ep + (r0 + lane - lo)]);
+    __syncwarp();  // M and N are rewritten for the next block
   }
 }
 
@@ -1516,27 +1629,37 @@ size_t subsolve_smem_bytes(int max_interior, int max_iface, bool fp32) {
   return cta_smem_bytes(max_interior, max_iface, fp32);
 }
 
+template <bool kInv>
+void launch_staged(const DevProblem &p, int mode, bool fp32, cudaStream_t stream) {
+  const StageLayout lay = kInv ? stage_layout(p.max_interior, p.inv_max_blocks, p.inv_cap, fp32)
+                               : stage_layout(p.max_interior, p.max_blocks, p.stage_cap, fp32);
+  double2 *rhs = fp32 ? p.B : p.Y;
+  // one thread per row for both products: their rows are short (a few to a
+  // few tens of entries) and the loads of several entries in flight per
+  // thread beat lanes sharing a row (timed with 1, 2, 4 and 8 lanes)
+  rhs_kernel<1><<<blocks_min1(p.n_interior, 256), 256, 0, stream>>>(p, mode, rhs);
+  if (fp32) {
+    subsolve_staged_kernel<float2, kInv><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.B, p.Y, p.Y32,
+                                                                                           0, lay);
+    for (int k = 0; k < p.ir_steps; k++) {
+      ir_residual_kernel<4><<<blocks_min1(p.n_interior * 4, 256), 256, 0, stream>>>(p, mode);
+      subsolve_staged_kernel<float2, kInv><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.Rres, p.Y,
+                                                                                             p.Y32, 1, lay);
+    }
+  } else {
+    subsolve_staged_kernel<double2, kInv><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.Y, p.Y, p.Y,
+                                                                                            0, lay);
+  }
+  iface_product_kernel<1><<<blocks_min1(p.n_slots, 256), 256, 0, stream>>>(p, mode);
+}
+
 void launch_subsolve(const DevProblem &p, int mode, bool fp32, cudaStream_t stream) {
   if (p.solve_variant == kSolveWarp) {
-    const StageLayout lay = stage_layout(p.max_interior, p.max_blocks, p.stage_cap, fp32);
-    double2 *rhs = fp32 ? p.B : p.Y;
-    // one thread per row for both products: their rows are short (a few to a
-    // few tens of entries) and the loads of several entries in flight per
-    // thread beat lanes sharing a row (timed with 1, 2, 4 and 8 lanes)
-    rhs_kernel<1><<<blocks_min1(p.n_interior, 256), 256, 0, stream>>>(p, mode, rhs);
-    if (fp32) {
-      subsolve_staged_kernel<float2><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.B, p.Y, p.Y32, 0,
-                                                                                       lay);
-      for (int k = 0; k < p.ir_steps; k++) {
-        ir_residual_kernel<4><<<blocks_min1(p.n_interior * 4, 256), 256, 0, stream>>>(p, mode);
-        subsolve_staged_kernel<float2><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.Rres, p.Y, p.Y32,
-                                                                                         1, lay);
-      }
-    } else {
-      subsolve_staged_kernel<double2><<<p.nsub, 32 * p.stage_warps, lay.total, stream>>>(p, mode, p.Y, p.Y, p.Y, 0,
-                                                                                          lay);
-    }
-    iface_product_kernel<1><<<blocks_min1(p.n_slots, 256), 256, 0, stream>>>(p, mode);
+    launch_staged<false>(p, mode, fp32, stream);
+    return;
+  }
+  if (p.solve_variant == kSolveInv) {
+    launch_staged<true>(p, mode, fp32, stream);
     return;
   }
   if (p.solve_variant == kSolveCta && p.cta_smem > 0) {
@@ -1576,12 +1699,26 @@ int raise_smem_limit(const void *func, int slot, size_t smem) {
 }
 
 int configure_subsolve_staged(size_t smem, bool fp32) {
-  return fp32 ? raise_smem_limit((const void *)subsolve_staged_kernel<float2>, 0, smem)
-              : raise_smem_limit((const void *)subsolve_staged_kernel<double2>, 1, smem);
+  return fp32 ? raise_smem_limit((const void *)subsolve_staged_kernel<float2, false>, 0, smem)
+              : raise_smem_limit((const void *)subsolve_staged_kernel<double2, false>, 1, smem);
+}
+
+int configure_subsolve_inv(size_t smem, bool fp32) {
+  return fp32 ? raise_smem_limit((const void *)subsolve_staged_kernel<float2, true>, 4, smem)
+              : raise_smem_limit((const void *)subsolve_staged_kernel<double2, true>, 5, smem);
+}
+
+void launch_inv_relayout(const DevProblem &p, const double2 *L64, bool fp32, cudaStream_t stream) {
+  if (p.nsub <= 0) return;
+  constexpr size_t smem = 2 * 32 * 33 * sizeof(double2);
+  if (fp32)
+    inv_relayout_kernel<float2><<<p.nsub, 32, smem, stream>>>(p, L64, (float2 *)(void *)p.Linv32);
+  else
+    inv_relayout_kernel<double2><<<p.nsub, 32, smem, stream>>>(p, L64, (double2 *)(void *)p.Linv64);
 }
 
 int subsolve_launches(const DevProblem &p, bool fp32) {
-  if (p.solve_variant == kSolveWarp) return 3 + (fp32 ? 2 * p.ir_steps : 0);
+  if (p.solve_variant == kSolveWarp || p.solve_variant == kSolveInv) return 3 + (fp32 ? 2 * p.ir_steps : 0);
   return 1;
 }
 

@@ -89,6 +89,16 @@ struct DevProblem {
   int32_t max_blocks;            // most blocks of one subdomain
   int32_t stage_cap;             // envelope elements per staging buffer
   int32_t stage_warps;           // warps sharing one subdomain's sweeps (1, 2 or 4)
+  // staged solve on the block-inverse layout (kSolveInv): per block of rows,
+  // the rows' entries left of the block, then N = (I + L_bb)^-1 - I strictly
+  // lower and row-major (row t at t(t-1)/2), then the block's pivots 1/d
+  const int64_t *inv_ptr;        // sum nI: position of each row's left entries in Linv
+  const double2 *Linv64;
+  const float2 *Linv32;
+  const int32_t *inv_blk_off;    // nsub+1
+  const int2 *inv_blk_tab;       // per subdomain nblk+1 x (first row, first element relative to inv_ptr[row 0])
+  int32_t inv_max_blocks;
+  int32_t inv_cap;               // elements per staging buffer
   int64_t row0, n_interior;      // interior rows of the subdomains this context solves
   int64_t slot0, n_slots;        // interface slots of the subdomains this context solves
   // sharded solve: this shard's partial interface sums go to the exchange
@@ -118,7 +128,7 @@ struct DevProblem {
 // Batched subdomain solve kernels: one warp per subdomain with TMA-staged row
 // blocks and grid-wide operator products, one CTA per subdomain, or one warp
 // per subdomain with the vectors in global memory (any size).
-enum SolveVariant { kSolveWarp = 0, kSolveCta = 1, kSolveGlobal = 2 };
+enum SolveVariant { kSolveWarp = 0, kSolveCta = 1, kSolveGlobal = 2, kSolveInv = 3 };
 
 enum SolveMode { kModeFirst = 0, kModeIter = 1, kModeLast = 2 };
 
@@ -183,6 +193,10 @@ size_t subsolve_smem_bytes(int max_interior, int max_iface, bool fp32);
 int configure_subsolve(size_t smem, bool fp32);
 size_t subsolve_staged_smem_bytes(int max_interior, int max_blocks, int cap, bool fp32);
 int configure_subsolve_staged(size_t smem, bool fp32);
+int configure_subsolve_inv(size_t smem, bool fp32);
+// the block-inverse layout (DevProblem inv_*) from the FP64 factor L64 in the
+// envelope layout, in FP32 (Linv32) or FP64 (Linv64)
+void launch_inv_relayout(const DevProblem &p, const double2 *L64, bool fp32, cudaStream_t stream);
 // Raises (never lowers) the dynamic shared-memory limit of kernel `func` on
 // the current device; `slot` names the kernel (0..7).
 int raise_smem_limit(const void *func, int slot, size_t smem);

@@ -27,7 +27,7 @@ from . import _lib
 from ._lib import FwgpuError  # noqa: F401  (re-exported)
 
 # batched subdomain-solve kernels (FWGPU_SOLVE_*); "auto" times the candidates once
-SOLVE_KERNELS = {"auto": 0, "warp": 1, "cta": 2, "global": 3}
+SOLVE_KERNELS = {"auto": 0, "warp": 1, "cta": 2, "global": 3, "blockinv": 4}
 _KERNEL_NAMES = {v: k for k, v in SOLVE_KERNELS.items()}
 
 P = ctypes.POINTER

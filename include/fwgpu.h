@@ -162,6 +162,8 @@ typedef struct {
 #define FWGPU_SOLVE_WARP 1   /* one warp per subdomain, vectors in shared memory */
 #define FWGPU_SOLVE_CTA 2    /* one 256-thread CTA per subdomain */
 #define FWGPU_SOLVE_GLOBAL 3 /* one warp per subdomain, vectors in global memory (any size) */
+#define FWGPU_SOLVE_BLOCKINV 4 /* the WARP kernel on a second layout of the factor: each row block's own
+                                  triangle stored as its inverse, applied as a product */
 
 typedef struct fwgpu_context fwgpu_context;
 

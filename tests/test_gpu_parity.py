@@ -144,7 +144,7 @@ def test_fp32_ir_vs_fp64():
     assert rel_l2(x32, x64) <= 1e-6
 
 
-@pytest.mark.parametrize("kernel", ["warp", "cta", "global"])
+@pytest.mark.parametrize("kernel", ["warp", "blockinv", "cta", "global"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32_ir"])
 def test_solve_kernels_vs_oracle(kernel, precision):
     """Every batched subdomain-solve kernel against the oracle's FP64 HDDM at
