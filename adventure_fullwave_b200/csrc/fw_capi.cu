@@ -902,7 +902,8 @@ static int build_inv_blocks(fwgpu_context *c, int cap) {
         r++;
         rows++;
       }
-      if (lsum + (int64_t)rows * (rows - 1) / 2 + rows > cap - 2) return set_error(FWGPU_ERR_ARG, "block-inverse layout: a row exceeds the staging capacity");
+      if (lsum + (int64_t)rows * (rows - 1) / 2 + rows > cap - 2)
+        return set_error(FWGPU_ERR_ARG, "block-inverse layout: a row exceeds the staging capacity");
       btab.push_back(make_int2(r0, (int)(pos - base)));
       for (int t = r0; t < r; t++) {
         iptr[io + t] = pos;
@@ -982,8 +983,10 @@ static int setup_stage(fwgpu_context *c) {
 // order of the sums, so AUTO keeps the default capacity (a rule on the
 // model's envelope, setup_stage) and times one, two and four warps per
 // subdomain, which share out whole row groups and column chunks and so sum
-// alike.  The CTA kernel sums in another order and runs only when asked
-// for.  An explicit WARP choice times the staging capacities too.
+// alike.  With FP32 factors AUTO runs the block-inverse sweep (a rule, not
+// a timed choice), with FP64 factors the staged sweep.  The CTA kernel sums
+// in another order and runs only when asked for.  An explicit WARP choice
+// times the staging capacities too.
 static int tune_solve_kernel(fwgpu_context *c) {
   const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
   struct Cand {
@@ -991,7 +994,9 @@ static int tune_solve_kernel(fwgpu_context *c) {
   };
   std::vector<Cand> cand;
   const bool any = c->opts.solve_kernel == FWGPU_SOLVE_AUTO;
-  if (any && c->warp_ok) {
+  // AUTO runs the block-inverse sweep where it built that layout (FP32 factors)
+  const bool any_inv = any && c->inv_ok;
+  if (any && c->warp_ok && !any_inv) {
     for (int warps = 1; warps <= 4; warps *= 2)
       if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps)
         cand.push_back({fw::kSolveWarp, c->dp.stage_cap, warps});
@@ -1002,7 +1007,7 @@ static int tune_solve_kernel(fwgpu_context *c) {
       for (int warps = 1; warps <= 4; warps *= 2)
         if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps) cand.push_back({fw::kSolveWarp, cap, warps});
   if (any && !c->warp_ok && c->dp.cta_smem > 0) cand.push_back({fw::kSolveCta, 0, 1});
-  if (c->opts.solve_kernel == FWGPU_SOLVE_BLOCKINV && c->inv_ok)
+  if ((c->opts.solve_kernel == FWGPU_SOLVE_BLOCKINV || any_inv) && c->inv_ok)
     for (int warps = 1; warps <= 4; warps *= 2)
       if (c->opts.stage_warps == 0 || c->opts.stage_warps == warps)
         cand.push_back({fw::kSolveInv, c->dp.inv_cap, warps});
@@ -1101,10 +1106,18 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     FW_TRY(setup_stage(c));
     if (c->opts.solve_kernel == FWGPU_SOLVE_WARP && !c->warp_ok)
       return set_error(FWGPU_ERR_ARG, "staged solve kernel: subdomains too large for shared memory");
-    if (c->opts.solve_kernel == FWGPU_SOLVE_BLOCKINV) {
-      if (c->warp_ok) FW_TRY(build_inv_blocks(c, c->dp.stage_cap));
-      if (!c->inv_ok) return set_error(FWGPU_ERR_ARG, "block-inverse solve kernel: subdomains too large for shared memory");
+    // the block-inverse layout: asked for, or AUTO with FP32 factors, where
+    // it is the faster sweep (C2 12 %, C3 3 %; with FP64 factors the two
+    // sweeps take the same time)
+    const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
+    const bool inv = c->opts.solve_kernel == FWGPU_SOLVE_BLOCKINV || (c->opts.solve_kernel == FWGPU_SOLVE_AUTO && fp32);
+    if (inv && c->warp_ok) {
+      // staging capacity: the caller's, else the staged kernel's, whose rule
+      // was also the fastest of 1, 1.5 and 2 times it for this layout
+      FW_TRY(build_inv_blocks(c, c->opts.stage_cap > 0 ? c->opts.stage_cap : c->dp.stage_cap));
     }
+    if (c->opts.solve_kernel == FWGPU_SOLVE_BLOCKINV && !c->inv_ok)
+      return set_error(FWGPU_ERR_ARG, "block-inverse solve kernel: subdomains too large for shared memory");
   }
   if (!c->factor_fresh) {
     // envelope values and LDL^T factor (the layout is fixed by the model)

@@ -66,26 +66,6 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
-// Sum of a complex value over the eight lanes j = lane & 7 of a lane group,
-// with the component of each lane shuffled once per level: lanes 0-3 keep
-// the real part and lanes 4-7 the imaginary part.  Both end as the tree
-// ((0+4)+(2+6))+((1+5)+(3+7)) over the group's lanes: the real sum in
-// lanes 0-3, the imaginary sum in lanes 4-7.
-__device__ __forceinline__ double group8_sum_split(double2 v, int j) {
-  const bool hi = (j & 4) != 0;
-  double s = (hi ? v.y : v.x) + __shfl_xor_sync(0xffffffffu, hi ? v.x : v.y, 4);
-  s += __shfl_xor_sync(0xffffffffu, s, 2);
-  s += __shfl_xor_sync(0xffffffffu, s, 1);
-  return s;
-}
-__device__ __forceinline__ float group8_sum_split(float2 v, int j) {
-  const bool hi = (j & 4) != 0;
-  float s = (hi ? v.y : v.x) + __shfl_xor_sync(0xffffffffu, hi ? v.x : v.y, 4);
-  s += __shfl_xor_sync(0xffffffffu, s, 2);
-  s += __shfl_xor_sync(0xffffffffu, s, 1);
-  return s;
-}
-
 template <typename T>
 __device__ __forceinline__ T czero();
 template <>

@@ -628,11 +628,14 @@ __global__ void __launch_bounds__(kCtaThreads) subsolve_cta_kernel(DevProblem p,
 //   backward - the triangle with lanes over columns, then the transposed
 //              update of the columns left of the block (lanes over columns,
 //              the block's rows from the last in the inner loop, in place).
-// Several subdomains share an SM and hide each other's dependent chains.  The
-// arithmetic is the reference's row-oriented envelope substitution
+// Several subdomains share an SM and hide each other's dependent chains.
+// With FWGPU_SOLVE_BLOCKINV the factor has a second layout in which each
+// block's triangle is stored as N = (I + L_bb)^-1 - I, and the triangles are
+// products with N (four independent sums per lane) instead of substitutions.
+// The arithmetic is the reference's row-oriented envelope substitution
 // (advlas_skyline.c:134-167) with the forward sums regrouped; the grouping
-// depends on the rows' entries and the block boundaries only, so one or two
-// warps per subdomain give the same bits.  The copies of the forward sweep
+// depends on the rows' entries and the block boundaries only, so one, two or
+// four warps per subdomain give the same bits.  The copies of the forward sweep
 // keep their lines in L2 (evict_last) for the backward sweep, whose copies
 // are the lines' last use (evict_first).  Every mbarrier wait is bounded: on
 // a timeout the CTA raises the error word, issues no further copy, waits for
@@ -673,12 +676,11 @@ __host__ __device__ inline StageLayout stage_layout(int max_interior, int max_bl
 // Forward sweep over the row blocks.  Per block of nb <= 32 rows starting at
 // row r0:
 //   - the entries left of the block: eight lanes per row, four rows per
-//     row group, two row groups in flight per warp (the groups shared out
-//     over the warps); lane j of a row sums the row's entries j, j+8, j+16,
-//     ... in order into one accumulator, and a three-level tree adds the
-//     eight lanes (real parts in lanes 0-3, imaginary parts in lanes 4-7).
-//     The sum of a row therefore depends on its entries alone, not on the
-//     staging capacity or the number of warps;
+//     warp step (row groups of four shared out over the warps); lane j of a
+//     row sums the row's entries j, j+8, j+16, ... in order into one
+//     accumulator, and three shuffles add the eight lanes.  The sum of a row
+//     therefore depends on its entries alone, not on the staging capacity or
+//     the number of warps;
 //   - the block's triangle: lane t holds row r0 + t, one broadcast shuffle per
 //     row, the operands of 4 steps loaded ahead;
 //   - the pivot scaling z = y/d goes to the z stash for the backward sweep.
@@ -703,45 +705,26 @@ __device__ bool staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, cons
     const bool late = !stage_wait(st, b);
     if (__syncthreads_or(late)) return false;
     const T *S = ((b & 1) ? st.buf1 : st.buf0) - stage_a0(st, b);  // S[e]: entry e of the envelope
-    // two row groups per warp step, so that each warp has two independent
-    // sums in flight
-    for (int g = w; 4 * g < nb; g += 2 * nw) {
-      int len[2], t[2];
-      const T *row[2], *yr[2];
-      T acc[2];
-      int longest = 0;
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        t[h] = 4 * (g + h * nw) + q;
-        const int2 mt = t[h] < nb ? meta[t[h]] : make_int2(r0, 0);
-        len[h] = t[h] < nb ? max(0, r0 - mt.x) : 0;
-        row[h] = S + mt.y;  // the row's entries from its first column
-        yr[h] = y + mt.x;
-        acc[h] = czero<T>();
-        longest = max(longest, len[h]);
-      }
-      longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, 8));
+    for (int g = w; 4 * g < nb; g += nw) {
+      const int t = 4 * g + q;
+      const int2 mt = t < nb ? meta[t] : make_int2(r0, 0);
+      const int len = t < nb ? max(0, r0 - mt.x) : 0;
+      int longest = max(len, __shfl_xor_sync(0xffffffffu, len, 8));
       longest = max(longest, __shfl_xor_sync(0xffffffffu, longest, 16));
+      const T *row = S + mt.y;  // the row's entries from its first column
+      const T *yr = y + mt.x;
+      T acc = czero<T>();
       for (int k = j; k < longest; k += 16) {
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const bool i0 = k < len[h], i1 = k + 8 < len[h];
-          const T a0 = i0 ? row[h][k] : czero<T>(), b0 = i0 ? yr[h][k] : czero<T>();
-          const T a1 = i1 ? row[h][k + 8] : czero<T>(), b1 = i1 ? yr[h][k + 8] : czero<T>();
-          acc[h] = cmac(acc[h], a0, b0);
-          acc[h] = cmac(acc[h], a1, b1);
-        }
+        const bool i0 = k < len, i1 = k + 8 < len;
+        const T a0 = i0 ? row[k] : czero<T>(), b0 = i0 ? yr[k] : czero<T>();
+        const T a1 = i1 ? row[k + 8] : czero<T>(), b1 = i1 ? yr[k + 8] : czero<T>();
+        acc = cmac(acc, a0, b0);
+        acc = cmac(acc, a1, b1);
       }
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const auto part = group8_sum_split(acc[h], j);  // real part in lanes 0-3, imaginary in 4-7
-        if ((j & 3) == 0 && t[h] < nb) {
-          if (j == 0)
-            rectb[t[h]].x = part;
-          else
-            rectb[t[h]].y = part;
-        }
-      }
+      acc = cadd(acc, shfl_xor(acc, 4));
+      acc = cadd(acc, shfl_xor(acc, 2));
+      acc = cadd(acc, shfl_xor(acc, 1));
+      if (j == 0 && t < nb) rectb[t] = acc;
     }
     __syncthreads();
     if (kInv && w == 0) {
@@ -760,11 +743,9 @@ __device__ bool staged_forward(Stage<T> &st, int nblk, const int32_t *lo_g, cons
       for (int jj = 0; jj < 8; jj++) {
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-          const int j = 8 * c + jj;
-          if (j < nb - 1) {
-            const T a = (j < lane && lane < nb) ? Nr[j] : czero<T>();
-            acc[c] = cmac(acc[c], a, vb[j]);
-          }
+          const int j = 8 * c + jj;  // straight-line code: the loads go ahead of the sums
+          const T a = (j < lane && lane < nb) ? Nr[j] : czero<T>();
+          acc[c] = cmac(acc[c], a, vb[j]);
         }
       }
       const T val = cadd(v, cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])));
@@ -842,10 +823,8 @@ __device__ bool staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
 #pragma unroll
         for (int c = 0; c < 4; c++) {
           const int t = 8 * c + tt;
-          if (t >= 1 && t < nb) {
-            const T a = lane < t ? N[((t * (t - 1)) >> 1) + lane] : czero<T>();
-            acc[c] = cmac(acc[c], a, y[r0 + t]);
-          }
+          const T a = (lane < t && t < nb) ? N[((t * (t - 1)) >> 1) + lane] : czero<T>();
+          acc[c] = cmac(acc[c], a, y[r0 + min(t, nb - 1)]);
         }
       }
       const T val = cadd(wv, cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])));
@@ -884,9 +863,7 @@ __device__ bool staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
     for (int cb = bmin + 32 * w; cb < r0; cb += 32 * nw) {
       const int c = cb + lane;
       const bool act = c < r0;
-      // four partial sums (rows t with t % 4 = 3, 2, 1, 0), so that four
-      // products are in flight per lane
-      T part[4] = {czero<T>(), czero<T>(), czero<T>(), czero<T>()};
+      T yc = act ? y[c] : czero<T>();
       for (int t0 = (nb - 1) & ~7; t0 >= 0; t0 -= 8) {
         if (gmin[t0 >> 3] >= cb + 32) continue;  // no row of the group reaches this chunk
         T v[8], xv[8];
@@ -899,9 +876,9 @@ __device__ bool staged_backward(Stage<T> &st, int nblk, const int32_t *lo_g, con
           xv[u] = t < nb ? xb[t] : czero<T>();  // xb past the block may hold anything
         }
 #pragma unroll
-        for (int u = 0; u < 8; u++) part[u & 3] = cmac(part[u & 3], v[u], xv[u]);
+        for (int u = 0; u < 8; u++) yc = cmsub(yc, v[u], xv[u]);
       }
-      if (act) y[c] = csub(y[c], cadd(cadd(part[0], part[1]), cadd(part[2], part[3])));
+      if (act) y[c] = yc;
     }
     __syncthreads();
   }
@@ -1017,7 +994,7 @@ __global__ void __launch_bounds__(32) inv_relayout_kernel(DevProblem p, const do
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2 *M = (double2 *)smem_raw;  // [32][33]: L_bb
   double2 *Nd = M + 32 * 33;         // [32][33]: N
-  const int s = blockIdx.x, lane = threadIdx.x;
+  const int s = p.sub_order[blockIdx.x], lane = threadIdx.x;  // the subdomains this context solves
   const int64_t io = p.int_off[s];
   const int b0 = p.inv_blk_off[s];
   const int nblk = p.inv_blk_off[s + 1] - b0 - 1;

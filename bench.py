@@ -349,6 +349,7 @@ def run_ours(args):
     achieved = alg / (prof["subsolve_ms"] * 1e-3) / 1e9
     traffic = ncu_traffic(args.config, args.precision)
     kname = {"warp": "rhs_kernel + subsolve_staged_kernel + iface_product_kernel",
+             "blockinv": "rhs_kernel + subsolve_staged_kernel (block-inverse layout) + iface_product_kernel",
              "cta": "subsolve_cta_kernel", "global": "subsolve_kernel"}.get(results[-1].solve_kernel,
                                                                            results[-1].solve_kernel)
     roofline = {"bound": "hbm", "kernel": f"{kname} (one batched subdomain solve of an interface iteration)",
@@ -537,6 +538,10 @@ def run_c5(args):
             res = s.solve_multi(srcs)
             times.append((res[0].t_setup_ms + res[0].t_iterate_ms + res[0].t_last_ms) / 1e3)
             iters.append([r.iterations for r in res])
+            # the forward result goes to stderr at once: the batched adjoint
+            # that follows takes about as long again
+            print(json.dumps({"c5_forward_s": times[-1], "iterations_per_source": iters[-1],
+                              "converged": [bool(r.converged) for r in res]}), file=sys.stderr, flush=True)
             if not args.no_adjoint:
                 t0 = time.perf_counter()
                 J, ge, gs, ares = s.adjoint_gradient_multi()

@@ -154,10 +154,11 @@ typedef struct {
                               before it exits) */
 } fwgpu_options;
 
-/* Batched subdomain-solve kernels.  AUTO times one launch of each candidate
- * (the WARP kernel with each staging capacity that fits in shared memory)
- * after the factorisation and keeps the fastest; WARP times only its
- * staging capacities. */
+/* Batched subdomain-solve kernels.  AUTO runs the WARP kernel (FP64
+ * factors) or the BLOCKINV kernel (FP32 factors) at the staging capacity
+ * that a rule on the envelope gives, and times 1, 2 and 4 warps per
+ * subdomain, which sum in the same order; WARP also times its staging
+ * capacities, which changes the order of the sums. */
 #define FWGPU_SOLVE_AUTO 0
 #define FWGPU_SOLVE_WARP 1   /* one warp per subdomain, vectors in shared memory */
 #define FWGPU_SOLVE_CTA 2    /* one 256-thread CTA per subdomain */
