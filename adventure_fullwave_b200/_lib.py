@@ -135,6 +135,11 @@ SIGNATURES = {
     "fwgpu_skyline_solve_noalloc": [c_i32, c_i32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                     ctypes.c_void_p],
+    "fwgpu_cojo_create": [P(FwMesh), c_i32, ctypes.c_void_p, P(FwOptions), P(ctypes.c_void_p)],
+    "fwgpu_cojo_solve": [ctypes.c_void_p, P(c_dbl), P(FwResult), P(c_dbl)],
+    "fwgpu_cojo_subdomains": [ctypes.c_void_p, P(c_i32), P(c_i32)],
+    "fwgpu_cojo_partition_build": [P(FwMesh), c_i32, ctypes.c_void_p, P(ctypes.c_void_p)],
+    "fwgpu_cojo_partition_subdomains": [ctypes.c_void_p, P(c_i32)],
     "fwgpu_get_edge_solution": [ctypes.c_void_p, P(c_dbl)],
     "fwgpu_get_history": [ctypes.c_void_p, P(c_dbl), c_i32, P(c_i32)],
     "fwgpu_get_subdomain_maps": [ctypes.c_void_p, c_i32, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32),

@@ -53,6 +53,8 @@ struct Scratch {
   std::vector<int32_t> count;
 };
 
+void build_lists(SubHost &h, SubLists &L, Scratch &w, int64_t e0, int nel, int nd);
+
 void build_sub(const Model &m, const Plan &p, const std::vector<int32_t> &iface_of_edge, int s, SubHost &h,
                SubLists &L, Scratch &w) {
   const int64_t e0 = p.sub_el_off[s], e1 = p.sub_el_off[s + 1];
@@ -122,7 +124,15 @@ void build_sub(const Model &m, const Plan &p, const std::vector<int32_t> &iface_
   for (int i = 0; i < h.nmp; i++)
     if (!h.isbc[i]) h.cidx[i] = nI++;
   h.nI = nI;
+  build_lists(h, L, w, e0, nel, 6);
+}
 
+// The lower-row structure, the element contributions of every lower entry
+// and the per-iteration operator lists of one subdomain whose element k
+// holds the nd local DOFs h.nop[10k+4 .. 10k+4+nd-1] (nd = 6 edges, or 4
+// vertices for the correction-Jo problem); the element matrix of slot e0+k
+// is stored as 6x6 complex entries from (e0+k)*36, DOF pair (i, j) at i*6+j.
+void build_lists(SubHost &h, SubLists &L, Scratch &w, int64_t e0, int nel, int nd) {
   // structural lower rows: entry (row = larger DOF, col = smaller DOF) of
   // every element, value M[slot(row)][slot(col)] (aij_matrix_func.h:278-322);
   // contributions stay in element order inside every (row, col): two stable
@@ -132,8 +142,8 @@ void build_sub(const Model &m, const Plan &p, const std::vector<int32_t> &iface_
   for (int k = 0; k < nel; k++) {
     const int32_t *d = &h.nop[10 * k + 4];
     int64_t base = (e0 + k) * 36;
-    for (int i = 0; i < 6; i++)
-      for (int j = 0; j < 6; j++)
+    for (int i = 0; i < nd; i++)
+      for (int j = 0; j < nd; j++)
         if (d[i] >= d[j]) ents.push_back({d[i], d[j], base + i * 6 + j});
   }
   w.tmp.resize(ents.size());
@@ -237,80 +247,10 @@ void build_sub(const Model &m, const Plan &p, const std::vector<int32_t> &iface_
   }
 }
 
-}  // namespace
-
-std::string build_plan(const Model &m, Plan &p) {
-  const int nsub = m.nsub;
-  if (nsub <= 0 || m.nt <= 0 || m.ne <= 0 || m.nv <= 0) return "empty model";
-  p = Plan();
-  p.subs.resize(nsub);
-
-  // elements of each subdomain in ascending global id (counting sort)
-  std::vector<int64_t> cnt(nsub + 1, 0);
-  for (int t = 0; t < m.nt; t++) {
-    int s = m.sub_of_tet[t];
-    if (s < 0 || s >= nsub) return "sub_of_tet out of range";
-    cnt[s + 1]++;
-  }
-  for (int s = 0; s < nsub; s++) {
-    if (cnt[s + 1] == 0) return "empty subdomain " + std::to_string(s);
-    cnt[s + 1] += cnt[s];
-  }
-  p.sub_el_off = cnt;
-  p.el_order.resize(m.nt);
-  {
-    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
-    for (int t = 0; t < m.nt; t++) p.el_order[pos[m.sub_of_tet[t]]++] = t;
-  }
-
-  // how many subdomains hold each edge; the first one is its owner
-  std::vector<int32_t> ecount(m.ne, 0), eowner(m.ne, -1), mark(m.ne, -1);
-  for (int s = 0; s < nsub; s++) {
-    for (int64_t k = p.sub_el_off[s]; k < p.sub_el_off[s + 1]; k++) {
-      int t = p.el_order[k];
-      for (int i = 0; i < 6; i++) {
-        int e = m.te[6 * (int64_t)t + i];
-        if (e < 0 || e >= m.ne) return "tet_edges out of range";
-        if (mark[e] != s) {
-          mark[e] = s;
-          ecount[e]++;
-          if (eowner[e] < 0) eowner[e] = s;
-        }
-      }
-    }
-  }
-  for (int64_t k = 0; k < 4 * (int64_t)m.nt; k++)
-    if (m.tv[k] < 0 || m.tv[k] >= m.nv) return "tet_vertices out of range";
-  // part-level interface DOFs in ascending global edge id
-  std::vector<int32_t> iface_of_edge(m.ne, -1);
-  for (int e = 0; e < m.ne; e++) {
-    if (ecount[e] >= 2 && !m.pec[e]) {
-      iface_of_edge[e] = (int32_t)p.iface_gid.size();
-      p.iface_gid.push_back(e);
-      p.iface_owner_sub.push_back(eowner[e]);
-    }
-  }
-  p.total_free = (int32_t)p.iface_gid.size();
-
-  // the subdomains are independent: built on all host threads
-  std::vector<SubLists> lists(nsub);
-  {
-    const int nthreads = std::max(1, std::min<int>(nsub, (int)std::thread::hardware_concurrency()));
-    std::atomic<int> next(0);
-    auto worker = [&]() {
-      Scratch w;
-      w.eloc.assign(m.ne, -1);
-      w.vloc.assign(m.nv, -1);
-      for (int s = next++; s < nsub; s = next++) build_sub(m, p, iface_of_edge, s, p.subs[s], lists[s], w);
-    };
-    std::vector<std::thread> pool;
-    for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
-    worker();
-    for (auto &t : pool) t.join();
-  }
-  for (int s = 0; s < nsub; s++)
-    if (!lists[s].err.empty()) return lists[s].err;
-
+// Concatenates the subdomains' lists in subdomain order (offsets first, then
+// every subdomain's slice on all host threads) and builds the gather of Q.
+void finish_plan(Plan &p, const std::vector<SubLists> &lists) {
+  const int nsub = (int)p.subs.size();
   // concatenated in subdomain order: offsets first, then every subdomain's
   // slice written on all host threads
   p.sub_dof_off.assign(nsub + 1, 0);
@@ -418,6 +358,231 @@ std::string build_plan(const Model &m, Plan &p) {
       for (int k = 0; k < h.nG; k++) p.gq_slot[fill[h.inbc_ln[k]]++] = p.sub_if_off[s] + k;
     }
   }
+}
+
+}  // namespace
+
+std::string build_plan(const Model &m, Plan &p) {
+  const int nsub = m.nsub;
+  if (nsub <= 0 || m.nt <= 0 || m.ne <= 0 || m.nv <= 0) return "empty model";
+  p = Plan();
+  p.subs.resize(nsub);
+
+  // elements of each subdomain in ascending global id (counting sort)
+  std::vector<int64_t> cnt(nsub + 1, 0);
+  for (int t = 0; t < m.nt; t++) {
+    int s = m.sub_of_tet[t];
+    if (s < 0 || s >= nsub) return "sub_of_tet out of range";
+    cnt[s + 1]++;
+  }
+  for (int s = 0; s < nsub; s++) {
+    if (cnt[s + 1] == 0) return "empty subdomain " + std::to_string(s);
+    cnt[s + 1] += cnt[s];
+  }
+  p.sub_el_off = cnt;
+  p.el_order.resize(m.nt);
+  {
+    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+    for (int t = 0; t < m.nt; t++) p.el_order[pos[m.sub_of_tet[t]]++] = t;
+  }
+
+  // how many subdomains hold each edge; the first one is its owner
+  std::vector<int32_t> ecount(m.ne, 0), eowner(m.ne, -1), mark(m.ne, -1);
+  for (int s = 0; s < nsub; s++) {
+    for (int64_t k = p.sub_el_off[s]; k < p.sub_el_off[s + 1]; k++) {
+      int t = p.el_order[k];
+      for (int i = 0; i < 6; i++) {
+        int e = m.te[6 * (int64_t)t + i];
+        if (e < 0 || e >= m.ne) return "tet_edges out of range";
+        if (mark[e] != s) {
+          mark[e] = s;
+          ecount[e]++;
+          if (eowner[e] < 0) eowner[e] = s;
+        }
+      }
+    }
+  }
+  for (int64_t k = 0; k < 4 * (int64_t)m.nt; k++)
+    if (m.tv[k] < 0 || m.tv[k] >= m.nv) return "tet_vertices out of range";
+  // part-level interface DOFs in ascending global edge id
+  std::vector<int32_t> iface_of_edge(m.ne, -1);
+  for (int e = 0; e < m.ne; e++) {
+    if (ecount[e] >= 2 && !m.pec[e]) {
+      iface_of_edge[e] = (int32_t)p.iface_gid.size();
+      p.iface_gid.push_back(e);
+      p.iface_owner_sub.push_back(eowner[e]);
+    }
+  }
+  p.total_free = (int32_t)p.iface_gid.size();
+
+  // the subdomains are independent: built on all host threads
+  std::vector<SubLists> lists(nsub);
+  {
+    const int nthreads = std::max(1, std::min<int>(nsub, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next(0);
+    auto worker = [&]() {
+      Scratch w;
+      w.eloc.assign(m.ne, -1);
+      w.vloc.assign(m.nv, -1);
+      for (int s = next++; s < nsub; s = next++) build_sub(m, p, iface_of_edge, s, p.subs[s], lists[s], w);
+    };
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+  }
+  for (int s = 0; s < nsub; s++)
+    if (!lists[s].err.empty()) return lists[s].err;
+
+  finish_plan(p, lists);
+  return "";
+}
+
+
+// The correction-Jo problem of one antenna (main/fullwave/main.c:92-98):
+// nodal unknowns at the vertices of the antenna's elements, with the
+// integer setup the reference makes in make_PartMesh_FW:
+//   - a subdomain's DOFs are the vertices of its elements whose flag is the
+//     antenna's, in the subdomain's vertex order (ap order), numbered
+//     0, 1, ... in that order (enf, make_PartMesh_make_ANTENNA_make_enf,
+//     lib/hddm/make_PartMesh.c:973-983 with make_MESH.c:459-500);
+//   - interface DOFs are the antenna vertices held by two or more subdomains
+//     (make_PartMesh_FW_change_innerbc_ANTENNA with its make_nf,
+//     make_PartMesh.c:1288-1340,1546-1575), numbered in ascending global
+//     vertex id;
+//   - the Dirichlet list is the sorted PEC antenna DOFs, then the interface
+//     DOFs in ascending local id; a subdomain with neither holds its DOF 0 at
+//     zero (make_PartMesh_make_ANTENNA_change_bc / _add_inbc,
+//     make_PartMesh.c:986-1063).
+// Only subdomains with antenna elements enter the problem: sub_map gives
+// the original subdomain id of each.  A vertex that is PEC and interface at
+// once is listed twice, as the reference lists it, and is solved as an
+// interface DOF.
+std::string build_plan_cojo(const Model &m, int32_t antenna_flag, const std::vector<uint8_t> &pec_vertex, Plan &p,
+                            std::vector<int32_t> &sub_map) {
+  const int nsub_all = m.nsub;
+  if (nsub_all <= 0 || m.nt <= 0 || m.nv <= 0) return "empty model";
+  if (!pec_vertex.empty() && (int64_t)pec_vertex.size() != m.nv) return "pec_vertex must hold one flag per vertex";
+  p = Plan();
+  p.el_dofs = 4;
+  sub_map.clear();
+  for (int64_t k = 0; k < 4 * (int64_t)m.nt; k++)
+    if (m.tv[k] < 0 || m.tv[k] >= m.nv) return "tet_vertices out of range";
+  // antenna elements of each subdomain, ascending global id
+  std::vector<int64_t> cnt(nsub_all + 1, 0);
+  for (int t = 0; t < m.nt; t++) {
+    const int s = m.sub_of_tet[t];
+    if (s < 0 || s >= nsub_all) return "sub_of_tet out of range";
+    if (m.flag[t] == antenna_flag) cnt[s + 1]++;
+  }
+  std::vector<int32_t> rs_of(nsub_all, -1);
+  for (int s = 0; s < nsub_all; s++)
+    if (cnt[s + 1] > 0) {
+      rs_of[s] = (int32_t)sub_map.size();
+      sub_map.push_back(s);
+    }
+  const int nsub = (int)sub_map.size();
+  if (nsub == 0) return "no element carries the antenna flag";
+  p.sub_el_off.assign(nsub + 1, 0);
+  for (int r = 0; r < nsub; r++) p.sub_el_off[r + 1] = p.sub_el_off[r] + cnt[sub_map[r] + 1];
+  p.el_order.resize(p.sub_el_off[nsub]);
+  {
+    std::vector<int64_t> pos(p.sub_el_off.begin(), p.sub_el_off.end() - 1);
+    for (int t = 0; t < m.nt; t++)
+      if (m.flag[t] == antenna_flag) p.el_order[pos[rs_of[m.sub_of_tet[t]]]++] = t;
+  }
+  // each subdomain's antenna vertices in its vertex order
+  std::vector<std::vector<int32_t>> dofs(nsub);
+  std::vector<int32_t> vcount(m.nv, 0), mark(m.nv, -1);
+  for (int r = 0; r < nsub; r++) {
+    std::vector<int32_t> &d = dofs[r];
+    for (int64_t k = p.sub_el_off[r]; k < p.sub_el_off[r + 1]; k++)
+      for (int i = 0; i < 4; i++) {
+        const int v = m.tv[4 * (int64_t)p.el_order[k] + i];
+        if (mark[v] != r) {
+          mark[v] = r;
+          d.push_back(v);
+          vcount[v]++;
+        }
+      }
+    if (!m.sub_vptr.empty()) {
+      const int s = sub_map[r];
+      std::vector<int32_t> ord;
+      ord.reserve(d.size());
+      for (int64_t q = m.sub_vptr[s]; q < m.sub_vptr[s + 1]; q++)
+        if (mark[m.sub_vord[q]] == r) ord.push_back(m.sub_vord[q]);
+      if (ord.size() != d.size())
+        return "subdomain " + std::to_string(s) + ": the given vertex order misses an antenna vertex";
+      d.swap(ord);
+    } else {
+      std::sort(d.begin(), d.end());
+    }
+  }
+  std::vector<int32_t> iface_of_vertex(m.nv, -1), vowner(m.nv, -1);
+  for (int r = 0; r < nsub; r++)
+    for (int v : dofs[r])
+      if (vowner[v] < 0) vowner[v] = r;
+  for (int v = 0; v < m.nv; v++)
+    if (vcount[v] >= 2) {
+      iface_of_vertex[v] = (int32_t)p.iface_gid.size();
+      p.iface_gid.push_back(v);
+      p.iface_owner_sub.push_back(vowner[v]);
+    }
+  p.total_free = (int32_t)p.iface_gid.size();
+
+  p.subs.resize(nsub);
+  std::vector<SubLists> lists(nsub);
+  Scratch w;
+  w.vloc.assign(m.nv, -1);
+  for (int r = 0; r < nsub; r++) {
+    SubHost &h = p.subs[r];
+    const std::vector<int32_t> &d = dofs[r];
+    const int64_t e0 = p.sub_el_off[r];
+    const int nel = (int)(p.sub_el_off[r + 1] - e0);
+    h.els.assign(p.el_order.begin() + e0, p.el_order.begin() + p.sub_el_off[r + 1]);
+    h.nmp = h.nap = (int32_t)d.size();
+    h.edge_gid = d;
+    for (int i = 0; i < h.nmp; i++) w.vloc[d[i]] = i;
+    h.nop.assign((size_t)nel * 10, -1);
+    for (int k = 0; k < nel; k++)
+      for (int i = 0; i < 4; i++) {
+        const int32_t loc = w.vloc[m.tv[4 * (int64_t)h.els[k] + i]];
+        h.nop[10 * k + i] = loc;
+        h.nop[10 * k + 4 + i] = loc;
+      }
+    for (int i = 0; i < h.nmp; i++) w.vloc[d[i]] = -1;
+    h.isbc.assign(h.nmp, 0);
+    h.cidx.assign(h.nmp, -1);
+    h.slot.assign(h.nmp, -1);
+    std::vector<int32_t> pecl;
+    for (int i = 0; i < h.nmp; i++) {
+      const int v = d[i];
+      if (!pec_vertex.empty() && pec_vertex[v]) {
+        pecl.push_back(i);
+        h.isbc[i] = 1;
+      }
+      if (iface_of_vertex[v] >= 0) {
+        h.slot[i] = (int32_t)h.inbc_nfid.size();
+        h.inbc_nfid.push_back(i);
+        h.inbc_ln.push_back(iface_of_vertex[v]);
+        h.isbc[i] = 1;
+      }
+    }
+    if (pecl.empty() && h.inbc_nfid.empty() && h.nmp > 0) {
+      pecl.push_back(0);  // the pinned DOF: zero, like a PEC DOF
+      h.isbc[0] = 1;
+    }
+    h.npec = (int32_t)pecl.size();
+    h.ibc = pecl;
+    h.ibc.insert(h.ibc.end(), h.inbc_nfid.begin(), h.inbc_nfid.end());
+    h.nG = (int32_t)h.inbc_nfid.size();
+    int nI = 0;
+    for (int i = 0; i < h.nmp; i++)
+      if (!h.isbc[i]) h.cidx[i] = nI++;
+    h.nI = nI;
+    build_lists(h, lists[r], w, e0, nel, 4);
+  }
+  finish_plan(p, lists);
   return "";
 }
 

@@ -132,6 +132,14 @@ struct fwgpu_context {
   uint8_t *d_el_has_nu = nullptr;
   double2 *d_post = nullptr;       // 3 x 3 complex per element (B, E, Je), when the caller's buffers are on the host
   double2 *d_post_x = nullptr;     // the caller's edge solution, when it is on the host
+  // per-entity solution: edges, or vertices of the correction-Jo problem
+  int64_t n_out = 0;
+  // correction-Jo problem of one antenna (fwgpu_cojo_*): its element flag
+  // (-1: the full-wave problem), the original subdomain id of each of its
+  // subdomains and the current of the pass (3 per vertex)
+  int32_t cojo_flag = -1;
+  std::vector<int32_t> cojo_sub;
+  double *d_cojo_J = nullptr;
 
   template <typename T>
   int alloc(T **ptr, size_t count) {
@@ -209,6 +217,8 @@ int resolve_material(fw::Model &m, const fwgpu_mesh *mesh, const fwgpu_material 
 }
 
 int build_rhs(fwgpu_context *c, const fwgpu_source *src) {
+  if (c->cojo_flag >= 0 && src && src->n_entries > 0)
+    return set_error(FWGPU_ERR_ARG, "a correction-Jo context takes its right-hand side from the antenna current");
   const fw::Plan &p = c->p;
   const int nsub = c->m.nsub;
   std::vector<double2> fI(p.sub_int_off[nsub], make_double2(0.0, 0.0));
@@ -280,12 +290,47 @@ int build_rhs(fwgpu_context *c, const fwgpu_source *src) {
   return FWGPU_OK;
 }
 
+// Gather lists of the element right-hand side: local DOF -> (element slot *
+// 6 + element DOF), elements in subdomain order, and the local DOF of every
+// interior and interface entry; built once per context.
+int build_rhs_lists(fwgpu_context *c) {
+  if (c->d_rhs_ptr) return FWGPU_OK;
+  const fw::Plan &p = c->p;
+  const int nsub = c->m.nsub;
+  const int nd = p.el_dofs;
+  const int64_t ndof = p.sub_dof_off[nsub];
+  std::vector<int64_t> ptr(ndof + 1, 0);
+  for (int s = 0; s < nsub; s++) {
+    const fw::SubHost &h = p.subs[s];
+    for (size_t e = 0; e < h.els.size(); e++)
+      for (int i = 0; i < nd; i++) ptr[p.sub_dof_off[s] + h.nop[10 * e + 4 + i] + 1]++;
+  }
+  for (int64_t r = 0; r < ndof; r++) ptr[r + 1] += ptr[r];
+  std::vector<int32_t> src(ptr[ndof]);
+  std::vector<int64_t> fill(ptr.begin(), ptr.end() - 1);
+  for (int s = 0; s < nsub; s++) {
+    const fw::SubHost &h = p.subs[s];
+    for (size_t e = 0; e < h.els.size(); e++)
+      for (int i = 0; i < nd; i++)
+        src[fill[p.sub_dof_off[s] + h.nop[10 * e + 4 + i]]++] = (int32_t)(6 * (p.sub_el_off[s] + (int64_t)e) + i);
+  }
+  std::vector<int64_t> int_pos(p.sub_int_off[nsub]), if_pos(p.sub_if_off[nsub]);
+  for (int s = 0; s < nsub; s++) {
+    for (int64_t k = p.sub_int_off[s]; k < p.sub_int_off[s + 1]; k++) int_pos[k] = p.sub_dof_off[s] + p.int_local[k];
+    for (int64_t k = p.sub_if_off[s]; k < p.sub_if_off[s + 1]; k++) if_pos[k] = p.sub_dof_off[s] + p.if_local[k];
+  }
+  FW_TRY(c->upload(&c->d_rhs_ptr, ptr));
+  FW_TRY(c->upload(&c->d_rhs_src, src));
+  FW_TRY(c->upload(&c->d_int_pos, int_pos));
+  FW_TRY(c->upload(&c->d_if_pos, if_pos));
+  FW_TRY(c->alloc(&c->d_elrhs, 6 * std::max<size_t>(1, p.el_order.size())));
+  return FWGPU_OK;
+}
+
 // Element sources: the per-element right-hand side is computed once (it
 // depends on the geometry, the conductivity and the source only) and the
 // gather lists from local DOFs to element contributions are built.
 int set_element_source(fwgpu_context *c, const fwgpu_element_source *es) {
-  const fw::Plan &p = c->p;
-  const int nsub = c->m.nsub;
   const int64_t nv = c->m.nv, nt = c->m.nt;
   if (es->n_gaps < 0 || es->n_antennas < 0) return set_error(FWGPU_ERR_ARG, "negative count");
   if (es->n_gaps > 0 && (!es->gap_box || !es->gap_volt)) return set_error(FWGPU_ERR_ARG, "gaps without boxes");
@@ -319,35 +364,7 @@ int set_element_source(fwgpu_context *c, const fwgpu_element_source *es) {
     FW_CUDA(cudaMemcpyAsync(c->d_Jo, es->antenna_Jo, nj * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     FW_CUDA(cudaMemcpyAsync(c->d_Jor, es->antenna_Jor, nj * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   }
-  if (!c->d_rhs_ptr) {
-    // local DOF -> (element slot * 6 + edge), elements in subdomain order
-    const int64_t ndof = p.sub_dof_off[nsub];
-    std::vector<int64_t> ptr(ndof + 1, 0);
-    for (int s = 0; s < nsub; s++) {
-      const fw::SubHost &h = p.subs[s];
-      for (size_t e = 0; e < h.els.size(); e++)
-        for (int i = 0; i < 6; i++) ptr[p.sub_dof_off[s] + h.nop[10 * e + 4 + i] + 1]++;
-    }
-    for (int64_t r = 0; r < ndof; r++) ptr[r + 1] += ptr[r];
-    std::vector<int32_t> src(ptr[ndof]);
-    std::vector<int64_t> fill(ptr.begin(), ptr.end() - 1);
-    for (int s = 0; s < nsub; s++) {
-      const fw::SubHost &h = p.subs[s];
-      for (size_t e = 0; e < h.els.size(); e++)
-        for (int i = 0; i < 6; i++)
-          src[fill[p.sub_dof_off[s] + h.nop[10 * e + 4 + i]]++] = (int32_t)(6 * (p.sub_el_off[s] + (int64_t)e) + i);
-    }
-    std::vector<int64_t> int_pos(p.sub_int_off[nsub]), if_pos(p.sub_if_off[nsub]);
-    for (int s = 0; s < nsub; s++) {
-      for (int64_t k = p.sub_int_off[s]; k < p.sub_int_off[s + 1]; k++) int_pos[k] = p.sub_dof_off[s] + p.int_local[k];
-      for (int64_t k = p.sub_if_off[s]; k < p.sub_if_off[s + 1]; k++) if_pos[k] = p.sub_dof_off[s] + p.if_local[k];
-    }
-    FW_TRY(c->upload(&c->d_rhs_ptr, ptr));
-    FW_TRY(c->upload(&c->d_rhs_src, src));
-    FW_TRY(c->upload(&c->d_int_pos, int_pos));
-    FW_TRY(c->upload(&c->d_if_pos, if_pos));
-    FW_TRY(c->alloc(&c->d_elrhs, 6 * (size_t)std::max<int64_t>(1, nt)));
-  }
+  FW_TRY(build_rhs_lists(c));
   fw::launch_element_rhs(nt, c->d_el_order, c->d_tv, c->d_crd, c->d_el_sigma, c->m.omega, es->n_gaps, c->d_gap,
                          c->d_el_ant, c->d_Jo, c->d_Jor, nv, c->d_elrhs, c->stream);
   c->launches += 1;
@@ -378,6 +395,7 @@ int read_status(fwgpu_context *c, int32_t *status) {
 struct fwgpu_partition {
   fw::Model m;
   fw::Plan p;
+  std::vector<int32_t> cojo_sub;  // correction-Jo partition: original id of each subdomain
 };
 
 static int copy_maps(const fw::Plan &p, int32_t s, int32_t *nel, int32_t *nmp, int32_t *nbc, int32_t *ninbc,
@@ -432,46 +450,12 @@ static int model_from_mesh(const fwgpu_mesh *mesh, fw::Model &m) {
   return FWGPU_OK;
 }
 
-extern "C" {
-
-const char *fwgpu_last_error(void) { return g_last_error.c_str(); }
-int fwgpu_abi_version(void) { return FWGPU_ABI_VERSION; }
-
-int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_options *opts, fwgpu_context **out) {
-  if (!mesh || !mt || !opts || !out) return set_error(FWGPU_ERR_ARG, "null argument");
-  *out = nullptr;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
-    return set_error(FWGPU_ERR_CUDA, "no CUDA device");
-  if (opts->device < 0 || opts->device >= ndev) return set_error(FWGPU_ERR_ARG, "bad device ordinal");
-
-  fwgpu_context *c = new fwgpu_context();
-  c->opts = *opts;
-  if (c->opts.graph_iterations <= 0) c->opts.graph_iterations = 16;
-  if (c->opts.ir_max_steps <= 0) c->opts.ir_max_steps = 1;
-  if (c->opts.stage_warps != 0 && c->opts.stage_warps != 1 && c->opts.stage_warps != 2 && c->opts.stage_warps != 4) {
-    delete c;
-    return set_error(FWGPU_ERR_ARG, "stage_warps must be 0, 1, 2 or 4");
-  }
-  if (c->opts.solve_kernel < FWGPU_SOLVE_AUTO || c->opts.solve_kernel > FWGPU_SOLVE_BLOCKINV) {
-    delete c;
-    return set_error(FWGPU_ERR_ARG, "unknown solve_kernel");
-  }
+// The device side of a context whose model and plan are built: stream,
+// uploads, operator structures, vectors and the per-entity solution map over
+// c->n_out entities (edges, or vertices of the correction-Jo problem).  On a
+// failure after the stream exists the context is handed out for release.
+static int setup_device(fwgpu_context *c, const fwgpu_options *opts, fwgpu_context **out) {
   fw::Model &m = c->m;
-  {
-    int rc = model_from_mesh(mesh, m);
-    if (rc != FWGPU_OK) {
-      delete c;
-      return rc;
-    }
-  }
-  m.omega = mt->omega;
-  resolve_material(m, mesh, mt);
-  std::string err = fw::build_plan(m, c->p);
-  if (!err.empty()) {
-    delete c;
-    return set_error(FWGPU_ERR_ARG, err);
-  }
   cudaError_t e = cudaSetDevice(opts->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
@@ -669,9 +653,9 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
     c->solve_tuned = c->opts.solve_kernel != FWGPU_SOLVE_AUTO && c->opts.solve_kernel != FWGPU_SOLVE_WARP &&
                      c->opts.solve_kernel != FWGPU_SOLVE_BLOCKINV;
   }
-  // per-edge solution source: the first subdomain holding each edge
-  std::vector<int64_t> esrc(m.ne, -1);
-  std::vector<uint8_t> seen(m.ne, 0);
+  // per-entity solution source: the first subdomain holding each edge (vertex)
+  std::vector<int64_t> esrc(c->n_out, -1);
+  std::vector<uint8_t> seen(c->n_out, 0);
   for (int s = 0; s < nsub; s++) {
     const fw::SubHost &h = p.subs[s];
     for (int r = 0; r < h.nmp; r++) {
@@ -687,9 +671,53 @@ int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_o
     }
   }
   FW_TRY(c->upload(&c->d_edge_src, esrc));
-  FW_TRY(c->alloc(&c->d_xedge, m.ne));
+  FW_TRY(c->alloc(&c->d_xedge, c->n_out));
   FW_CUDA(cudaStreamSynchronize(c->stream));
   return FWGPU_OK;
+}
+
+extern "C" {
+
+const char *fwgpu_last_error(void) { return g_last_error.c_str(); }
+int fwgpu_abi_version(void) { return FWGPU_ABI_VERSION; }
+
+int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_options *opts, fwgpu_context **out) {
+  if (!mesh || !mt || !opts || !out) return set_error(FWGPU_ERR_ARG, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(FWGPU_ERR_CUDA, "no CUDA device");
+  if (opts->device < 0 || opts->device >= ndev) return set_error(FWGPU_ERR_ARG, "bad device ordinal");
+
+  fwgpu_context *c = new fwgpu_context();
+  c->opts = *opts;
+  if (c->opts.graph_iterations <= 0) c->opts.graph_iterations = 16;
+  if (c->opts.ir_max_steps <= 0) c->opts.ir_max_steps = 1;
+  if (c->opts.stage_warps != 0 && c->opts.stage_warps != 1 && c->opts.stage_warps != 2 && c->opts.stage_warps != 4) {
+    delete c;
+    return set_error(FWGPU_ERR_ARG, "stage_warps must be 0, 1, 2 or 4");
+  }
+  if (c->opts.solve_kernel < FWGPU_SOLVE_AUTO || c->opts.solve_kernel > FWGPU_SOLVE_BLOCKINV) {
+    delete c;
+    return set_error(FWGPU_ERR_ARG, "unknown solve_kernel");
+  }
+  fw::Model &m = c->m;
+  {
+    int rc = model_from_mesh(mesh, m);
+    if (rc != FWGPU_OK) {
+      delete c;
+      return rc;
+    }
+  }
+  m.omega = mt->omega;
+  resolve_material(m, mesh, mt);
+  std::string err = fw::build_plan(m, c->p);
+  if (!err.empty()) {
+    delete c;
+    return set_error(FWGPU_ERR_ARG, err);
+  }
+  c->n_out = m.ne;
+  return setup_device(c, opts, out);
 }
 
 int fwgpu_partition_build(const fwgpu_mesh *mesh, fwgpu_partition **out) {
@@ -707,6 +735,107 @@ int fwgpu_partition_build(const fwgpu_mesh *mesh, fwgpu_partition **out) {
     return set_error(FWGPU_ERR_ARG, err);
   }
   *out = part;
+  return FWGPU_OK;
+}
+
+// -- correction-Jo problem (main/fullwave/main.c:92-98) ------------------------
+
+int fwgpu_cojo_create(const fwgpu_mesh *mesh, int32_t antenna_flag, const uint8_t *pec_vertex,
+                      const fwgpu_options *opts, fwgpu_context **out) {
+  if (!mesh || !opts || !out) return set_error(FWGPU_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (opts->precision != FWGPU_PREC_FP64) return set_error(FWGPU_ERR_ARG, "the correction-Jo problem is solved in FP64");
+  if (opts->shard_begin != 0 || opts->shard_end != 0)
+    return set_error(FWGPU_ERR_ARG, "the correction-Jo problem is not sharded");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(FWGPU_ERR_CUDA, "no CUDA device");
+  if (opts->device < 0 || opts->device >= ndev) return set_error(FWGPU_ERR_ARG, "bad device ordinal");
+  if (opts->stage_warps != 0 && opts->stage_warps != 1 && opts->stage_warps != 2 && opts->stage_warps != 4)
+    return set_error(FWGPU_ERR_ARG, "stage_warps must be 0, 1, 2 or 4");
+  if (opts->solve_kernel < FWGPU_SOLVE_AUTO || opts->solve_kernel > FWGPU_SOLVE_BLOCKINV)
+    return set_error(FWGPU_ERR_ARG, "unknown solve_kernel");
+  fwgpu_context *c = new fwgpu_context();
+  c->opts = *opts;
+  if (c->opts.graph_iterations <= 0) c->opts.graph_iterations = 16;
+  c->opts.ir_max_steps = 1;
+  fw::Model &m = c->m;
+  int rc = model_from_mesh(mesh, m);
+  if (rc != FWGPU_OK) {
+    delete c;
+    return rc;
+  }
+  std::vector<uint8_t> pv;
+  if (pec_vertex) pv.assign(pec_vertex, pec_vertex + m.nv);
+  std::string err = fw::build_plan_cojo(m, antenna_flag, pv, c->p, c->cojo_sub);
+  if (!err.empty()) {
+    delete c;
+    return set_error(FWGPU_ERR_ARG, err);
+  }
+  m.nsub = (int32_t)c->cojo_sub.size();  // the problem's own subdomains from here on
+  c->cojo_flag = antenna_flag;
+  c->n_out = m.nv;
+  return setup_device(c, &c->opts, out);
+}
+
+int fwgpu_cojo_solve(fwgpu_context *c, const double *current, fwgpu_result *res, double *potential) {
+  if (!c || !current) return set_error(FWGPU_ERR_ARG, "null argument");
+  if (c->cojo_flag < 0) return set_error(FWGPU_ERR_STATE, "not a correction-Jo context");
+  FW_CUDA(cudaSetDevice(c->opts.device));
+  const int64_t nv = c->m.nv;
+  if (!c->d_cojo_J) FW_TRY(c->alloc(&c->d_cojo_J, 3 * (size_t)nv));
+  FW_CUDA(cudaMemcpyAsync(c->d_cojo_J, current, 3 * (size_t)nv * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FW_TRY(build_rhs_lists(c));
+  fw::launch_cojo_element_rhs((int64_t)c->p.el_order.size(), c->d_el_order, c->d_tv, c->d_crd, c->d_cojo_J,
+                              c->d_elrhs, c->stream);
+  FW_CUDA(cudaGetLastError());
+  c->el_src = true;
+  // the matrix does not depend on the current: the second pass reuses the factors
+  const int rc = c->stage >= 2 && c->factor_fresh ? fwgpu_hddm_resolve(c, nullptr, res)
+                                                   : fwgpu_hddm_solve(c, nullptr, res);
+  if (rc != FWGPU_OK && rc != FWGPU_ERR_NOT_CONVERGED) return rc;
+  if (potential) {
+    std::vector<double2> x(nv);
+    FW_CUDA(cudaMemcpy(x.data(), c->d_xedge, nv * sizeof(double2), cudaMemcpyDeviceToHost));
+    for (int64_t v = 0; v < nv; v++) potential[v] = x[v].x;
+  }
+  if (res) res->kernel_launches += 1;
+  return rc;
+}
+
+int fwgpu_cojo_subdomains(const fwgpu_context *c, int32_t *n, int32_t *sub_ids) {
+  if (!c || !n) return set_error(FWGPU_ERR_ARG, "null argument");
+  if (c->cojo_flag < 0) return set_error(FWGPU_ERR_STATE, "not a correction-Jo context");
+  *n = (int32_t)c->cojo_sub.size();
+  if (sub_ids) std::copy(c->cojo_sub.begin(), c->cojo_sub.end(), sub_ids);
+  return FWGPU_OK;
+}
+
+int fwgpu_cojo_partition_build(const fwgpu_mesh *mesh, int32_t antenna_flag, const uint8_t *pec_vertex,
+                               fwgpu_partition **out) {
+  if (!out) return set_error(FWGPU_ERR_ARG, "null argument");
+  *out = nullptr;
+  fwgpu_partition *part = new fwgpu_partition();
+  int rc = model_from_mesh(mesh, part->m);
+  if (rc != FWGPU_OK) {
+    delete part;
+    return rc;
+  }
+  std::vector<uint8_t> pv;
+  if (pec_vertex) pv.assign(pec_vertex, pec_vertex + part->m.nv);
+  std::string err = fw::build_plan_cojo(part->m, antenna_flag, pv, part->p, part->cojo_sub);
+  if (!err.empty()) {
+    delete part;
+    return set_error(FWGPU_ERR_ARG, err);
+  }
+  part->m.nsub = (int32_t)part->cojo_sub.size();
+  *out = part;
+  return FWGPU_OK;
+}
+
+int fwgpu_cojo_partition_subdomains(const fwgpu_partition *part, int32_t *sub_ids) {
+  if (!part || !sub_ids) return set_error(FWGPU_ERR_ARG, "null argument");
+  if (part->cojo_sub.empty()) return set_error(FWGPU_ERR_STATE, "not a correction-Jo partition");
+  std::copy(part->cojo_sub.begin(), part->cojo_sub.end(), sub_ids);
   return FWGPU_OK;
 }
 
@@ -765,6 +894,7 @@ int fwgpu_get_sizes(const fwgpu_context *c, fwgpu_sizes *sz) {
 }
 
 int fwgpu_set_element_source(fwgpu_context *c, const fwgpu_element_source *es) {
+  if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (!es) {
     c->el_src = false;
@@ -780,7 +910,7 @@ int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
   const fw::Plan &p = c->p;
   FW_CUDA(cudaEventRecord(c->ev[0], c->stream));
   if (!c->d_elmat) {
-    FW_TRY(c->alloc(&c->d_elmat, (size_t)c->m.nt * 72));
+    FW_TRY(c->alloc(&c->d_elmat, p.el_order.size() * 72));
     FW_TRY(c->alloc(&c->d_aval, p.nnz_total));
     FW_TRY(c->upload(&c->d_cpl_src, p.cpl_src));
     FW_TRY(c->upload(&c->d_ifr_src, p.ifr_src));
@@ -788,8 +918,12 @@ int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
     FW_TRY(c->upload(&c->d_diag_src, p.if_diag_src));
   }
   c->launches += 2;
-  fw::launch_element_matrices(c->m.nt, c->d_el_order, c->d_tv, c->d_crd, c->d_el_eps, c->d_el_sigma, c->m.omega,
-                              c->d_elmat, c->d_mesh_status, c->stream);
+  if (c->cojo_flag >= 0)
+    fw::launch_cojo_element_matrices((int64_t)p.el_order.size(), c->d_el_order, c->d_tv, c->d_crd, c->d_elmat,
+                                     c->d_mesh_status, c->stream);
+  else
+    fw::launch_element_matrices(c->m.nt, c->d_el_order, c->d_tv, c->d_crd, c->d_el_eps, c->d_el_sigma, c->m.omega,
+                                c->d_elmat, c->d_mesh_status, c->stream);
   fw::launch_gather_values(p.nnz_total, c->d_cptr, c->d_contrib, (const double2 *)c->d_elmat, c->d_aval, c->stream);
   FW_CUDA(cudaGetLastError());
   FW_CUDA(cudaStreamSynchronize(c->stream));
@@ -1348,6 +1482,7 @@ static int multi_run(fwgpu_context *c, int32_t n_src, const fwgpu_source *srcs, 
 }
 
 int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *srcs, fwgpu_result *res) {
+  if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c || !srcs || !res) return set_error(FWGPU_ERR_ARG, "null argument");
   if (n_src < 1 || n_src > fw::kMaxRhs) return set_error(FWGPU_ERR_ARG, "n_src outside 1..FWGPU_MAX_RHS");
   if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
@@ -1362,6 +1497,7 @@ int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *
 int fwgpu_adjoint_gradient_multi(fwgpu_context *c, int32_t n_probe, const int32_t *probe_edges, int32_t n_design,
                                  const int32_t *design_tets, double *J, double *grad_eps, double *grad_sigma,
                                  fwgpu_result *adjoint_results) {
+  if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c || n_probe < 0 || n_design < 0 || (n_probe > 0 && !probe_edges) || (n_design > 0 && !design_tets))
     return set_error(FWGPU_ERR_ARG, "bad argument");
   const int n_src = c->multi_n;
@@ -1453,6 +1589,7 @@ int fwgpu_get_edge_solution_multi(fwgpu_context *c, int32_t k, double *x) {
 }
 
 int fwgpu_shard_set_layout(fwgpu_context *c, int32_t n_shards, const int32_t *shard_first, int32_t *n_shared) {
+  if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c || !shard_first || n_shards < 1) return set_error(FWGPU_ERR_ARG, "bad argument");
   if (!c->sharded) return set_error(FWGPU_ERR_STATE, "not a sharded context");
   const fw::Plan &p = c->p;
@@ -1611,7 +1748,7 @@ int fwgpu_solve_dom_last(fwgpu_context *c) {
   if (c->stage < 3) return set_error(FWGPU_ERR_STATE, "solve_dom_last before the interface loop");
   FW_CUDA(cudaSetDevice(c->opts.device));
   fw::launch_subsolve(c->dp, fw::kModeLast, c->opts.precision == FWGPU_PREC_FP32_IR, c->stream);
-  fw::launch_edge_solution(c->dp, c->m.ne, c->d_edge_src, c->dp.Y, c->dp.V, c->d_xedge, c->stream);
+  fw::launch_edge_solution(c->dp, c->n_out, c->d_edge_src, c->dp.Y, c->dp.V, c->d_xedge, c->stream);
   c->launches += 1 + fw::subsolve_launches(c->dp, c->opts.precision == FWGPU_PREC_FP32_IR);
   FW_CUDA(cudaGetLastError());
   c->stage = 4;
@@ -1713,6 +1850,7 @@ int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *
 int fwgpu_adjoint_gradient(fwgpu_context *c, int32_t n_probe, const int32_t *probe_edges, int32_t n_design,
                            const int32_t *design_tets, double *J, double *grad_eps, double *grad_sigma,
                            fwgpu_result *adjoint_result) {
+  if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c || n_probe < 0 || n_design < 0 || (n_probe > 0 && !probe_edges) || (n_design > 0 && !design_tets))
     return set_error(FWGPU_ERR_ARG, "bad argument");
   if (c->stage < 4) return set_error(FWGPU_ERR_STATE, "adjoint needs a forward solve");
@@ -1794,6 +1932,7 @@ int post_static_data(fwgpu_context *c) {
 }  // namespace
 
 int fwgpu_post_em_E(fwgpu_context *c, const double *x, double *el_B, double *el_E, double *el_Je) {
+  if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (!x && !c->xedge_ok)
     return set_error(FWGPU_ERR_STATE, c->sharded ? "a sharded context needs the whole edge solution x"
@@ -1918,7 +2057,7 @@ int fwgpu_profile_iteration(fwgpu_context *c, int32_t reps, fwgpu_kernel_profile
 int fwgpu_get_edge_solution(fwgpu_context *c, double *x) {
   if (!c || !x) return set_error(FWGPU_ERR_ARG, "null argument");
   if (c->stage < 4) return set_error(FWGPU_ERR_STATE, "no solution yet");
-  FW_CUDA(cudaMemcpy(x, c->d_xedge, (size_t)c->m.ne * sizeof(double2), cudaMemcpyDeviceToHost));
+  FW_CUDA(cudaMemcpy(x, c->d_xedge, (size_t)c->n_out * sizeof(double2), cudaMemcpyDeviceToHost));
   return FWGPU_OK;
 }
 

@@ -36,9 +36,9 @@ struct TetGeom {
   bool bad;
 };
 
-__device__ __forceinline__ void tet_geometry(const double *x, const double *y, const double *z, TetGeom &G) {
-  G.bad = false;
-  // 6 x volume, summed term by term in the reference's order
+// 6 x the signed volume (tet_Volume6, lib/fem/tetrahedral.c:44-61), summed term
+// by term in the reference's order
+__device__ __forceinline__ double tet_volume6(const double *x, const double *y, const double *z) {
   double D = -x[0] * y[1] * z[2];
   D = D + x[0] * y[1] * z[3];
   D = D + x[0] * y[2] * z[1];
@@ -63,6 +63,12 @@ __device__ __forceinline__ void tet_geometry(const double *x, const double *y, c
   D = D + x[3] * y[1] * z[2];
   D = D + x[3] * y[2] * z[0];
   D = D - x[3] * y[2] * z[1];
+  return D;
+}
+
+__device__ __forceinline__ void tet_geometry(const double *x, const double *y, const double *z, TetGeom &G) {
+  G.bad = false;
+  const double D = tet_volume6(x, y, z);
   if (!(D > 0.0)) G.bad = true;
   G.D = D;
   for (int i = 0; i < 6; i++) {
@@ -608,6 +614,90 @@ void launch_adjoint_gradient(int32_t n_design, const int32_t *design_tets, const
   if (n_design <= 0) return;
   adjoint_gradient_kernel<<<(n_design + 127) / 128, 128, 0, stream>>>(n_design, design_tets, tet_vertices, tet_edges,
                                                                       crd, omega, x, lam, g_eps, g_sigma);
+}
+
+
+// ---------------------------------------------------------------------------
+// The correction-Jo problem of an antenna (tet_MakeElement_correct_Jo,
+// lib/fem/make_elem.c:10-66): conventional linear tetrahedra on the
+// antenna's elements, element matrix (grad N_i, grad N_j)
+// (tet_simple_gradgrad, lib/fem/tetrahedral.c:188-202) and element vector
+// (J, grad N_i) of the vertex currents J (tet_simple_be_apgrad :206-220),
+// with the determinants b, c, d of tet_simple_b/c/d (:122-184) over the
+// vertex table tet_m (tetrahedral.h:14-17).  Reference operation order,
+// contraction off, as for the edge elements.
+__constant__ int c_tet_m[4][4] = {{0, 1, 2, 3}, {1, 3, 2, 0}, {2, 3, 0, 1}, {3, 1, 0, 2}};
+
+__device__ __forceinline__ void tet_simple_bcd(const double *x, const double *y, const double *z, double *b, double *c,
+                                               double *d) {
+  for (int i = 0; i < 4; i++) {
+    const int ii = c_tet_m[i][1], jj = c_tet_m[i][2], kk = c_tet_m[i][3];
+    b[i] = -1.0 * (y[ii] * (z[jj] - z[kk]) + y[jj] * (z[kk] - z[ii]) + y[kk] * (z[ii] - z[jj]));
+    c[i] = -1.0 * (z[ii] * (x[jj] - x[kk]) + z[jj] * (x[kk] - x[ii]) + z[kk] * (x[ii] - x[jj]));
+    d[i] = -1.0 * (x[ii] * (y[jj] - y[kk]) + x[jj] * (y[kk] - y[ii]) + x[kk] * (y[ii] - y[jj]));
+  }
+}
+
+// One thread per element slot k (el_order[k] a global element): its 4x4 real
+// matrix is stored in the 6x6 complex slot layout of the edge elements,
+// entry (i, j) at out[k*72 + 2*(i*6+j)], imaginary parts and the unused
+// rows and columns zero.  status[0] is raised for a non-positive volume.
+__global__ void cojo_element_matrices_kernel(int64_t n_el, const int32_t *__restrict__ el_order,
+                                             const int32_t *__restrict__ tet_vertices,
+                                             const double *__restrict__ crd, double *__restrict__ out,
+                                             int32_t *__restrict__ status) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_el) return;
+  double x[4], y[4], z[4], b[4], c[4], d[4];
+  load_tet(el_order[k], tet_vertices, crd, x, y, z);
+  const double D = tet_volume6(x, y, z);
+  if (!(D > 0.0)) atomicMax(status, 1);
+  tet_simple_bcd(x, y, z, b, c, d);
+  const double dd = 1.0 / (6.0 * D);
+  double *o = out + k * 72;
+  for (int q = 0; q < 72; q++) o[q] = 0.0;
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) o[2 * (i * 6 + j)] = (b[i] * b[j] + c[i] * c[j] + d[i] * d[j]) * dd;
+}
+
+// One thread per element slot: be_i = sum_j (b_i J_j,x + c_i J_j,y + d_i J_j,z) / 24
+// with J (3 per global vertex) the pass's currents, written as 6 complex
+// per slot (entries 0..3, imaginary parts and entries 4, 5 zero).
+__global__ void cojo_element_rhs_kernel(int64_t n_el, const int32_t *__restrict__ el_order,
+                                        const int32_t *__restrict__ tet_vertices, const double *__restrict__ crd,
+                                        const double *__restrict__ J, double2 *__restrict__ be) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_el) return;
+  const int t = el_order[k];
+  double x[4], y[4], z[4], b[4], c[4], d[4], u[4][3];
+  load_tet(t, tet_vertices, crd, x, y, z);
+  tet_simple_bcd(x, y, z, b, c, d);
+  for (int i = 0; i < 4; i++) {
+    const int64_t v = tet_vertices[4 * (int64_t)t + i];
+    for (int j = 0; j < 3; j++) u[i][j] = J[3 * v + j];
+  }
+  const double dd = 1.0 / 24.0;
+  for (int i = 0; i < 4; i++) {
+    double ag = 0.0;
+    for (int j = 0; j < 4; j++) ag += (b[i] * u[j][0] + c[i] * u[j][1] + d[i] * u[j][2]) * dd;
+    be[6 * k + i] = make_double2(ag, 0.0);
+  }
+  be[6 * k + 4] = make_double2(0.0, 0.0);
+  be[6 * k + 5] = make_double2(0.0, 0.0);
+}
+
+void launch_cojo_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices,
+                                  const double *crd, double *out, int32_t *status, cudaStream_t stream) {
+  if (n_el <= 0) return;
+  cojo_element_matrices_kernel<<<(unsigned)((n_el + 127) / 128), 128, 0, stream>>>(n_el, el_order, tet_vertices, crd,
+                                                                                   out, status);
+}
+
+void launch_cojo_element_rhs(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
+                             const double *J, double2 *be, cudaStream_t stream) {
+  if (n_el <= 0) return;
+  cojo_element_rhs_kernel<<<(unsigned)((n_el + 127) / 128), 128, 0, stream>>>(n_el, el_order, tet_vertices, crd, J,
+                                                                              be);
 }
 
 }  // namespace fw

@@ -99,10 +99,16 @@ struct Plan {
   std::vector<int64_t> gq_slot;      // global slot index (sub_if_off + k)
   int64_t nnz_total = 0;
   int64_t nlen_reference = 0;
+  int32_t el_dofs = 6;               // DOFs per element: 6 edges, or 4 vertices (correction-Jo problem)
   int32_t max_local = 0, max_interior = 0, max_iface = 0;
 };
 
 // Builds the plan; returns an empty string on success or an error message.
 std::string build_plan(const Model &m, Plan &p);
+// The plan of one antenna's correction-Jo problem (vertex DOFs of the
+// elements carrying antenna_flag); sub_map receives the original subdomain id
+// of each of its subdomains.  pec_vertex: one flag per vertex, or empty.
+std::string build_plan_cojo(const Model &m, int32_t antenna_flag, const std::vector<uint8_t> &pec_vertex, Plan &p,
+                            std::vector<int32_t> &sub_map);
 
 }  // namespace fw

@@ -177,6 +177,12 @@ int multi_iteration_launches(bool fp32, int ir_steps, int n_buckets);
 void launch_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
                              const double *el_eps, const double *el_sigma, double omega, double *out,
                              int32_t *status, cudaStream_t stream);
+// correction-Jo problem: linear-tetrahedron (grad, grad) matrices in the
+// 6x6 slot layout, and element vectors (J, grad N_i) from vertex currents J
+void launch_cojo_element_matrices(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices,
+                                  const double *crd, double *out, int32_t *status, cudaStream_t stream);
+void launch_cojo_element_rhs(int64_t n_el, const int32_t *el_order, const int32_t *tet_vertices, const double *crd,
+                             const double *J, double2 *be, cudaStream_t stream);
 void launch_gather_values(int64_t nnz, const int64_t *contrib_ptr, const int64_t *contrib, const double2 *elmat,
                           double2 *aval, cudaStream_t stream);
 void launch_profile(int32_t nsub, const int64_t *dof_off, const int64_t *nnz_off, const int32_t *row_ptr_rel,

@@ -496,3 +496,152 @@ def hddm_solver_CS(model, source=0, **opts) -> Tuple[np.ndarray, HddmResult]:
     with HddmSolver(model, **opts) as s:
         r = s.solve(source)
         return s.edge_solution(), r
+
+
+# -- correction-Jo pre-solve ---------------------------------------------------
+
+def _pec_vertex(model, pec_vertex):
+    if pec_vertex is None:
+        return None, None
+    a = np.ascontiguousarray(pec_vertex, dtype=np.uint8)
+    if a.shape != (int(model.n_vertices),):
+        raise ValueError("pec_vertex must hold one flag per vertex")
+    return a, a.ctypes.data_as(ctypes.c_void_p)
+
+
+class CorrectJoPartition:
+    """Host-only integer setup of one antenna's correction-Jo problem (the
+    ANTENNA part of the reference's make_PartMesh_FW,
+    lib/hddm/make_PartMesh.c:973-1063,1288-1340,1546-1575): per subdomain
+    holding antenna elements, its vertex DOFs, Dirichlet list and interface
+    entries.  Needs no GPU."""
+
+    def __init__(self, model, antenna_flag: int, pec_vertex=None):
+        self._lib = _lib.load()
+        mesh, keep = _mesh_struct(model)
+        pv, pv_ptr = _pec_vertex(model, pec_vertex)
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.fwgpu_cojo_partition_build(ctypes.byref(mesh), int(antenna_flag), pv_ptr,
+                                                        ctypes.byref(h)))
+        self._h = h
+        ns, tf = ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_partition_info(h, ctypes.byref(ns), ctypes.byref(tf)))
+        self.n_subdomains = ns.value
+        self.total_free = tf.value
+        ids = np.zeros(max(1, ns.value), np.int32)
+        _lib.check(self._lib.fwgpu_cojo_partition_subdomains(h, _ptr(ids, ctypes.c_int32)))
+        self.subdomain_ids = ids[: ns.value]
+
+    def maps(self, s: int) -> dict:
+        """Maps of the problem's subdomain s: ``edge_gid`` holds the global
+        vertex of each local DOF (the reference's enf order)."""
+        return _maps(self._lib.fwgpu_partition_maps, self._h, s)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.fwgpu_partition_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CorrectJoSolver:
+    """The correction-Jo pre-solve of one antenna on one GPU: the reference's
+    ``hddm_solver_RS`` with ``set_hddm_func_correct_Jor`` and then
+    ``set_hddm_func_correct_Joi`` (main/fullwave/main.c:92-98,
+    lib/hddm/set_hddm_func.c:90-233).  A real-symmetric HDDM for a potential
+    at the vertices of the antenna's elements, stiffness (grad, grad) and
+    right-hand side (J, grad N_i) of the vertex currents J
+    (lib/fem/make_elem.c:10-66), interface PCG with the diagonal
+    preconditioner.  ``hddm_eps`` and ``hddm_max_loop`` are the reference's
+    coJo-hddm-eps (1e-10) and coJo-hddm-max-loop (4000).  One ``solve`` per
+    pass; the second reuses the factors."""
+
+    def __init__(self, model, antenna_flag: int, hddm_eps: float = 1e-10, hddm_max_loop: int = 4000,
+                 pec_vertex=None, graph_iterations: int = 16, device: int = 0, solve_kernel: str = "auto"):
+        lib = _lib.load()
+        self._lib = lib
+        self.model = model
+        self.antenna_flag = int(antenna_flag)
+        self.n_vertices = int(model.n_vertices)
+        mesh, keep = _mesh_struct(model)
+        pv, pv_ptr = _pec_vertex(model, pec_vertex)
+        opts = _lib.FwOptions(float(hddm_eps), int(hddm_max_loop), _lib.PREC_FP64, 1, 0.0, int(graph_iterations),
+                              int(device), SOLVE_KERNELS[solve_kernel], 0, 0.0, 0, 0, 0, 0)
+        handle = ctypes.c_void_p()
+        rc = lib.fwgpu_cojo_create(ctypes.byref(mesh), self.antenna_flag, pv_ptr, ctypes.byref(opts),
+                                   ctypes.byref(handle))
+        if rc != 0 and handle.value:
+            lib.fwgpu_destroy(handle)
+        _lib.check(rc)
+        self._h = handle
+
+    def solve(self, current, raise_not_converged: bool = False) -> Tuple[np.ndarray, HddmResult]:
+        """One pass with the vertex currents ``current`` (n_vertices x 3):
+        the potential at every vertex (0 off the antenna) and the result."""
+        j = np.ascontiguousarray(current, dtype=np.float64)
+        if j.shape != (self.n_vertices, 3):
+            raise ValueError("current must be n_vertices x 3")
+        phi = np.zeros(self.n_vertices, np.float64)
+        r = _lib.FwResult()
+        rc = self._lib.fwgpu_cojo_solve(self._h, _ptr(j, ctypes.c_double), ctypes.byref(r), _ptr(phi, ctypes.c_double))
+        _lib.check(rc, () if raise_not_converged else (_lib.ERR_NOT_CONVERGED,))
+        return phi, HddmSolver._result(r)
+
+    def history(self) -> np.ndarray:
+        return HddmSolver.history(self)
+
+    def sizes(self) -> dict:
+        return HddmSolver.sizes(self)
+
+    def subdomain_ids(self) -> np.ndarray:
+        n = ctypes.c_int32()
+        _lib.check(self._lib.fwgpu_cojo_subdomains(self._h, ctypes.byref(n), None))
+        ids = np.zeros(max(1, n.value), np.int32)
+        _lib.check(self._lib.fwgpu_cojo_subdomains(self._h, ctypes.byref(n), _ptr(ids, ctypes.c_int32)))
+        return ids[: n.value]
+
+    def subdomain_maps(self, s: int) -> dict:
+        return _maps(self._lib.fwgpu_get_subdomain_maps, self._h, s)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.fwgpu_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def correct_jo_log_section(part: str, antenna: int, total_free: int, initial_norm: float, history) -> str:
+    """One correction-Jo section of the reference's convergence log: title
+    "Correction Jo : Real part" or "Imaginary part"
+    (HDDM_set_HDDM_Opt_correct_Jor/Joi, lib/hddm/set_hddm_func.c:266-298),
+    the antenna number, then the lines calc_log_section writes."""
+    body = calc_log_section(total_free, initial_norm, history).split("\n")[3:]
+    lines = ["", "", f"# Correction Jo : {part} part", "", f"#   Antenna number = {int(antenna)}"] + body
+    return "\n".join(lines)
+
+
+def hddm_solver_RS_correct_jo(model, k: int = 0, **opts):
+    """main()'s pre-solve for antenna k of ``model.element_source``: the pass
+    on the real part of the currents (Jor), then on the imaginary part (Jo).
+    Returns (Ihr, Ihi) per vertex and the two results."""
+    es = model.element_source
+    with CorrectJoSolver(model, int(es.antenna_flag[k]), **opts) as s:
+        ihr, rr = s.solve(es.antenna_Jor[k])
+        ihi, ri = s.solve(es.antenna_Jo[k])
+    return ihr, ihi, (rr, ri)

@@ -279,6 +279,50 @@ int fwgpu_hddm_solve(fwgpu_context *ctx, const fwgpu_source *src, fwgpu_result *
  * on the existing factors (multi-source runs). */
 int fwgpu_hddm_resolve(fwgpu_context *ctx, const fwgpu_source *src, fwgpu_result *result);
 
+/* -- correction-Jo pre-solve of an antenna ------------------------------- */
+
+/* The real-symmetric HDDM that main() runs for every antenna before the
+ * full-wave solve (main/fullwave/main.c:92-98: hddm_solver_RS with
+ * set_hddm_func_correct_Jor, then set_hddm_func_correct_Joi,
+ * lib/hddm/set_hddm_func.c:90-233).  Its unknown is a potential at the
+ * vertices of the antenna's elements, its element matrix (grad N_i, grad N_j)
+ * and its element vector (J, grad N_i) of the vertex currents J
+ * (tet_MakeElement_correct_Jo, lib/fem/make_elem.c:10-66); interface DOFs
+ * are the antenna vertices two or more subdomains hold, and a subdomain with
+ * no Dirichlet or interface DOF holds its first DOF at zero
+ * (make_PartMesh.c:973-1063,1288-1340,1546-1575).  The interface problem is
+ * solved by the same batched kernels as the full-wave one (the reference's
+ * RS and CS drivers are one template, hddm_solver.h and hddm_solver_s.h,
+ * here with real values), the subdomain systems by the envelope LDL^T
+ * factor where the reference iterates (mymt_RS_AIJ_Solver_CG with ICC to
+ * coJo-l-sol-eps 1e-12).  Pass the reference's coJo options in opts:
+ * hddm_eps = coJo-hddm-eps (1e-10), hddm_max_loop = coJo-hddm-max-loop
+ * (4000); precision must be FWGPU_PREC_FP64.
+ *
+ * fwgpu_cojo_create: the integer setup of the antenna with element flag
+ * antenna_flag (only subdomains with antenna elements take part) and the
+ * device context.  pec_vertex: one flag per vertex marking vertex nodes of
+ * the Dirichlet (DirichletBCs_Axn0) lists, or NULL for none. */
+int fwgpu_cojo_create(const fwgpu_mesh *mesh, int32_t antenna_flag, const uint8_t *pec_vertex,
+                      const fwgpu_options *opts, fwgpu_context **out);
+/* One pass: current = 3 doubles per global vertex (the real part Jor for the
+ * first pass, the imaginary part Jo for the second); potential receives one
+ * double per global vertex (Ihr / Ihi of every subdomain holding it; 0 off
+ * the antenna).  The first call assembles and factors, later calls reuse the
+ * factors.  Returns FWGPU_ERR_NOT_CONVERGED (result and potential filled)
+ * at hddm_max_loop. */
+int fwgpu_cojo_solve(fwgpu_context *ctx, const double *current, fwgpu_result *result, double *potential);
+/* The original subdomain id of each of the problem's subdomains (n first;
+ * sub_ids may be NULL to query n). */
+int fwgpu_cojo_subdomains(const fwgpu_context *ctx, int32_t *n, int32_t *sub_ids);
+/* The integer setup alone, without a GPU; fwgpu_partition_info and
+ * fwgpu_partition_maps then describe the problem's subdomains (edge_gid
+ * holds the global vertex of each local DOF, nop the local DOFs of each
+ * antenna element in slots 0-3 and 4-7, -1 in 8-9). */
+int fwgpu_cojo_partition_build(const fwgpu_mesh *mesh, int32_t antenna_flag, const uint8_t *pec_vertex,
+                               fwgpu_partition **out);
+int fwgpu_cojo_partition_subdomains(const fwgpu_partition *part, int32_t *sub_ids);
+
 /* -- adjoint ------------------------------------------------------------- */
 
 /* Backward of fwgpu_hddm_solve (the forward).  No reference counterpart.

@@ -24,12 +24,15 @@
  *
  * With FW_HARNESS_MAIN=1 the model is read by the reference's own hddm_Init
  * and the correction-Jo pre-solve of main.c:92-98 runs first, as in main();
- * the antenna currents it leaves are dumped to <prefix>.jo.  This runs a
+ * the antenna currents it leaves are dumped to <prefix>.jo, and the
+ * pre-solve's own systems and potentials to <prefix>.cojo.  This runs a
  * model directory of the reference as its main() would.
  *
  * Usage: fw_ref_harness [reference options] <model_dir>
  * Environment:
  *   FW_HARNESS_OUT   output prefix (default <model_dir>/ref)
+ *   FW_HARNESS_COJO_ONLY  1 (with FW_HARNESS_MAIN=1): stop after the
+ *                    correction-Jo pre-solve and its dumps
  *   FW_HARNESS_DUMP  0: timings + solution, 1: + integer maps and the
  *                    element results of the post step,
  *                    2: + assembled TMP_AIJ and skyline factors
@@ -375,6 +378,49 @@ static void dump_jo(PartMesh *pms, int nparts) {
   fclose(f);
 }
 
+/* The correction-Jo pre-solve's systems and results (main.c:92-98 with
+   lib/hddm/set_hddm_func.c:90-233): per antenna, per subdomain in part
+   order, "nf nbc ninbc", the global node id of each antenna DOF
+   (enf order), the Dirichlet list dbc.ibc, the interface entries (nfid,
+   ln_part) and the potentials Ihr and Ihi the two real-symmetric HDDM runs
+   leave (HDDM_get_result_sp_correct_Jor/Joi, set_hddm_func.c:626-667). */
+static void dump_cojo(PartMesh *pms, int nparts) {
+  char path[FILENAME_MAX];
+  snprintf(path, sizeof(path), "%s.cojo", g_prefix);
+  FILE *f = fopen(path, "w");
+  if (!f) return;
+  const int nant = pms[0].mtrl.nantenna;
+  int nsub = 0;
+  for (int q = 0; q < nparts; q++) nsub += pms[q].ndomain;
+  fprintf(f, "%d %d\n", nant, nsub);
+  for (int k = 0; k < nant; k++) {
+    fprintf(f, "%d %d\n", pms[0].mtrl.antenna_def[k].flag, pms[0].pantenna ? pms[0].pantenna[k].total_free : 0);
+    for (int q = 0; q < nparts; q++)
+      for (int d = 0; d < pms[q].ndomain; d++) {
+        PartMesh *pm = &pms[q];
+        DomMesh *dm = &pm->dm[d];
+        ANTENNA *a = &dm->antenna[k];
+        const int nf = a->enf ? a->nf : 0;
+        fprintf(f, "%d %d %d\n", nf, nf ? a->dbc.nbc : 0, nf ? a->ninbc : 0);
+        if (!nf) continue;
+        int *gid = (int *)calloc(nf, sizeof(int));
+        for (int v = 0; v < dm->nap; v++)
+          if (a->enf[v] >= 0) gid[a->enf[v]] = pm->pnid2gnid[dm->snid2pnid[dm->apid2snid[v]]];
+        for (int i = 0; i < nf; i++) fprintf(f, "%d%c", gid[i], i + 1 < nf ? ' ' : '\n');
+        free(gid);
+        for (int i = 0; i < a->dbc.nbc; i++) fprintf(f, "%d ", a->dbc.ibc[i]);
+        fprintf(f, "\n");
+        for (int i = 0; i < a->ninbc; i++) fprintf(f, "%d %d ", a->inbc[i].nfid, a->inbc[i].ln_part);
+        fprintf(f, "\n");
+        for (int i = 0; i < nf; i++) fprintf(f, "%.17e ", a->Ihr ? a->Ihr[i] : 0.0);
+        fprintf(f, "\n");
+        for (int i = 0; i < nf; i++) fprintf(f, "%.17e ", a->Ihi ? a->Ihi[i] : 0.0);
+        fprintf(f, "\n");
+      }
+  }
+  fclose(f);
+}
+
 /* every part's subdomains, parts in order; the header counts all of them and
    gives the first part's interface sizes */
 static void dump_ints(PartMesh *pms, int nparts) {
@@ -518,6 +564,10 @@ int main(int argc, char **argv) {
       hddm_solver_RS(g_pm, options, set_hddm_func_correct_Joi);
     }
     dump_jo(g_pm, nrepeat);
+    dump_cojo(g_pm, nrepeat);
+    /* FW_HARNESS_COJO_ONLY=1: stop after the pre-solve */
+    const char *cojo_only = getenv("FW_HARNESS_COJO_ONLY");
+    if (cojo_only && atoi(cojo_only) == 1) return 0;
   } else {
   /* hddm_Init (lib/hddm/make_PartMesh.c:58-117) in s-mode, calling
      make_PartMesh_FW directly: make_PartMesh's material check

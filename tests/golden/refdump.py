@@ -173,3 +173,72 @@ def run_harness(model, hddm_eps: float, hddm_max_loop: int, dump: int = 2, workd
         out["fac"] = read_fac(os.path.join(mdir, "ref.fac"))
     out["workdir"] = wd
     return out
+
+
+def read_cojo(path: str):
+    """The correction-Jo dump of the harness in main() mode (<prefix>.cojo):
+    per antenna its flag, interface size and, per subdomain of every part in
+    order, the global node id of each antenna DOF (enf order), the Dirichlet
+    list, the interface entries (nfid, ln_part) and the potentials Ihr, Ihi."""
+    lines = open(path).read().split("\n")
+    pos = 0
+
+    def nxt():
+        nonlocal pos
+        pos += 1
+        return lines[pos - 1]
+
+    nant, nsub = (int(t) for t in nxt().split())
+    out = []
+    for _ in range(nant):
+        flag, tfree = (int(t) for t in nxt().split())
+        subs = []
+        for _ in range(nsub):
+            nf, nbc, ninbc = (int(t) for t in nxt().split())
+            d = dict(nf=nf)
+            if nf:
+                d["gid"] = np.array(nxt().split(), np.int64)
+                d["ibc"] = np.array(nxt().split(), np.int64)
+                ib = np.array(nxt().split(), np.int64).reshape(-1, 2)
+                d["inbc_nfid"], d["inbc_ln"] = ib[:, 0], ib[:, 1]
+                d["ihr"] = np.array(nxt().split(), np.float64)
+                d["ihi"] = np.array(nxt().split(), np.float64)
+                assert d["gid"].shape[0] == nf and d["ibc"].shape[0] == nbc and ib.shape[0] == ninbc
+            subs.append(d)
+        out.append(dict(flag=flag, total_free=tfree, subs=subs))
+    return out
+
+
+def read_log_sections(path: str):
+    """Every section of a reference calc_log: title, interface DOFs, initial
+    max-norm and the residual per iteration (7 digits)."""
+    secs = []
+    for line in open(path):
+        t = line.split()
+        if line.startswith("# ") and not line.startswith("# DOF") and not line.startswith("#   "):
+            secs.append(dict(title=line[2:].strip(), dof=None, norm0=None, hist=[]))
+        elif line.startswith("# DOF on interface"):
+            secs[-1]["dof"] = int(t[-1])
+        elif len(t) >= 5 and t[0] == "0" and t[2] == "#" and t[3] == "Norm":
+            secs[-1]["norm0"] = float(t[4])
+        elif len(t) == 2 and not line.startswith("#"):
+            secs[-1]["hist"].append(float(t[1]))
+    for sec in secs:
+        sec["hist"] = np.array(sec["hist"])
+    return secs
+
+
+def run_cojo(model_dir: str, workdir: str, timeout=600):
+    """Run main()'s correction-Jo pre-solve of the reference on a model
+    directory (copied into workdir/MODEL) and return the parsed dump and the
+    log sections."""
+    import shutil
+
+    mdir = os.path.join(workdir, "MODEL")
+    if os.path.abspath(model_dir) != os.path.abspath(mdir):
+        shutil.copytree(model_dir, mdir, ignore=shutil.ignore_patterns("calc_log", "result"))
+    env = dict(os.environ, FW_HARNESS_MAIN="1", FW_HARNESS_COJO_ONLY="1", FW_HARNESS_OUT=os.path.join(mdir, "ref"))
+    subprocess.run([HARNESS, "-memlimit", "60000", "MODEL"], cwd=workdir, env=env, check=True,
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=timeout)
+    return read_cojo(os.path.join(mdir, "ref.cojo")), read_log_sections(
+        os.path.join(mdir, "calc_log", "log_g_HDDM_Full_Wave"))
