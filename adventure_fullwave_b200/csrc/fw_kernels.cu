@@ -1661,28 +1661,36 @@ size_t subsolve_staged_smem_bytes(int max_interior, int max_blocks, int cap, boo
 // The dynamic shared-memory limit of a kernel is process-wide (per device):
 // it is only ever raised, so that a context configured later with smaller
 // subdomains cannot break the launches of an earlier one.
+// Each kernel has a slot of its own (SmemSlot): two kernels sharing one would
+// see the other's limit as theirs and launch above their own.  A failed
+// attribute call is cleared from the runtime's last error, so that a later
+// check of a launch does not report it.
 int raise_smem_limit(const void *func, int slot, size_t smem) {
-  constexpr int kDevs = 64, kSlots = 8;
+  constexpr int kDevs = 64;
   static std::mutex mu;
-  static size_t current[kDevs][kSlots] = {};
+  static size_t current[kDevs][kSmemSlots] = {};
   if (smem > 227 * 1024) return -1;
+  if (slot < 0 || slot >= kSmemSlots) return -2;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) return -2;
   std::lock_guard<std::mutex> lock(mu);
   if (smem <= current[dev][slot]) return 0;
-  if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -2;
+  if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return -2;
+  }
   current[dev][slot] = smem;
   return 0;
 }
 
 int configure_subsolve_staged(size_t smem, bool fp32) {
-  return fp32 ? raise_smem_limit((const void *)subsolve_staged_kernel<float2, false>, 0, smem)
-              : raise_smem_limit((const void *)subsolve_staged_kernel<double2, false>, 1, smem);
+  return fp32 ? raise_smem_limit((const void *)subsolve_staged_kernel<float2, false>, kSlotStaged32, smem)
+              : raise_smem_limit((const void *)subsolve_staged_kernel<double2, false>, kSlotStaged64, smem);
 }
 
 int configure_subsolve_inv(size_t smem, bool fp32) {
-  return fp32 ? raise_smem_limit((const void *)subsolve_staged_kernel<float2, true>, 4, smem)
-              : raise_smem_limit((const void *)subsolve_staged_kernel<double2, true>, 5, smem);
+  return fp32 ? raise_smem_limit((const void *)subsolve_staged_kernel<float2, true>, kSlotInv32, smem)
+              : raise_smem_limit((const void *)subsolve_staged_kernel<double2, true>, kSlotInv64, smem);
 }
 
 void launch_inv_relayout(const DevProblem &p, const double2 *L64, bool fp32, cudaStream_t stream) {
@@ -1700,8 +1708,8 @@ int subsolve_launches(const DevProblem &p, bool fp32) {
 }
 
 int configure_subsolve(size_t smem, bool fp32) {
-  return fp32 ? raise_smem_limit((const void *)subsolve_cta_kernel<true>, 2, smem)
-              : raise_smem_limit((const void *)subsolve_cta_kernel<false>, 3, smem);
+  return fp32 ? raise_smem_limit((const void *)subsolve_cta_kernel<true>, kSlotCta32, smem)
+              : raise_smem_limit((const void *)subsolve_cta_kernel<false>, kSlotCta64, smem);
 }
 
 void launch_cocg_first(const DevProblem &p, const double2 *pcloc, cudaStream_t stream) {

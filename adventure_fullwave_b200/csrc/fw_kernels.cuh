@@ -205,6 +205,19 @@ int configure_subsolve_inv(size_t smem, bool fp32);
 void launch_inv_relayout(const DevProblem &p, const double2 *L64, bool fp32, cudaStream_t stream);
 // Raises (never lowers) the dynamic shared-memory limit of kernel `func` on
 // the current device; `slot` names the kernel (0..7).
+// Slots of the process-wide dynamic shared-memory limits (raise_smem_limit):
+// one per kernel instantiation that runs above the 48 KB default.
+enum SmemSlot {
+  kSlotStaged32 = 0,
+  kSlotStaged64 = 1,
+  kSlotCta32 = 2,
+  kSlotCta64 = 3,
+  kSlotInv32 = 4,
+  kSlotInv64 = 5,
+  kSlotMulti32 = 6,
+  kSlotMulti64 = 7,
+  kSmemSlots = 8
+};
 int raise_smem_limit(const void *func, int slot, size_t smem);
 // kernels one launch_subsolve call issues
 int subsolve_launches(const DevProblem &p, bool fp32);

@@ -542,8 +542,8 @@ size_t multi_smem_bytes(int max_interior, int max_blocks, int cap, bool fp32) {
 }
 
 int configure_multi(size_t smem, bool fp32) {
-  return fp32 ? raise_smem_limit((const void *)multi_sweep_kernel<float2, kRwFp32>, 4, smem)
-              : raise_smem_limit((const void *)multi_sweep_kernel<double2, kRwFp64>, 5, smem);
+  return fp32 ? raise_smem_limit((const void *)multi_sweep_kernel<float2, kRwFp32>, kSlotMulti32, smem)
+              : raise_smem_limit((const void *)multi_sweep_kernel<double2, kRwFp64>, kSlotMulti64, smem);
 }
 
 // The sweep, one launch per size bucket, each with the shared memory of its

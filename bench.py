@@ -19,7 +19,8 @@ solve, download of the edge solution) timed per step.
 refinement to the same tolerance: time, iterations and relative L2 distance
 to the FP64 solution, ``--mixed-steps`` timed solves), ``adjoint`` (the C4
 design-region model: one forward solve and the backward call on its
-factors), ``c2`` (the C2 model, FP64), ``sample`` (the reference's shipped
+factors), ``c2`` (the C2 model, FP64), ``correct_jo`` (the correction-Jo
+pre-solve of the sample's antenna), ``sample`` (the reference's shipped
 model) and ``accuracy`` (C1 solved in FP64 and FP32+IR, each solution's
 relative L2 error against the FP64 sparse direct solve of the global system
 kept in tests/golden/direct_c1.npz).
@@ -154,6 +155,7 @@ def algorithmic_bytes(sz: dict, precision: str, ir_steps: int) -> int:
 
 
 SAMPLE_FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "ref_sample.npz")
+COJO_FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "ref_cojo.npz")
 
 
 def sample_model():
@@ -444,6 +446,32 @@ def run_ours(args):
                   "rel_l2_vs_reference": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)),
                   "timing": "device events of one solve (second of two)"}
 
+    # the correction-Jo pre-solve of the sample's antenna (main.c:92-98), both
+    # passes, against the reference's own pre-solve kept in tests/golden/ref_cojo.npz
+    correct_jo = None
+    if not args.no_sample and os.path.exists(SAMPLE_FIXTURE) and os.path.exists(COJO_FIXTURE):
+        try:
+            cz = np.load(COJO_FIXTURE)
+            es = sm.element_source
+            t0 = time.perf_counter()
+            with hddm.CorrectJoSolver(sm, int(cz["sample_flag"][0]), device=local) as cs:
+                t1 = time.perf_counter()
+                ihr, rr = cs.solve(es.antenna_Jor[0])
+                ihi, ri = cs.solve(es.antenna_Jo[0])
+                t2 = time.perf_counter()
+            want = cz["sample_ihr"]
+            got = ihr[cz["sample_vertex"]]
+            correct_jo = {"model": "the sample's antenna: 7 subdomains, 26 interface DOFs (vertices)",
+                          "iterations": [rr.iterations, ri.iterations],
+                          "reference_iterations": [int(cz["sample_hist_r"].shape[0]), int(cz["sample_hist_i"].shape[0])],
+                          "device_ms": [rr.t_setup_ms + rr.t_iterate_ms + rr.t_last_ms,
+                                        ri.t_setup_ms + ri.t_iterate_ms + ri.t_last_ms],
+                          "host_s": {"context": t1 - t0, "two_passes": t2 - t1},
+                          "rel_l2_vs_reference_Ihr": float(np.linalg.norm(got - want) / np.linalg.norm(want)),
+                          "Ihi_max_abs": float(np.abs(ihi).max())}
+        except Exception as exc:  # reported, never fatal to the headline line
+            correct_jo = {"error": repr(exc)}
+
     # C1 against the exact discrete solution (FP64 sparse direct solve)
     accuracy = None
     if not args.no_accuracy and os.path.exists(DIRECT_FIXTURE):
@@ -507,7 +535,7 @@ def run_ours(args):
         "solution_check": {"finite": bool(np.all(np.isfinite(x_check))), "final_resi": results[-1].final_resi},
     }
     for k, v in (("mixed_precision", mixed), ("adjoint", adjoint), ("c2", c2), ("post", post), ("sample", sample),
-                 ("accuracy", accuracy)):
+                 ("correct_jo", correct_jo), ("accuracy", accuracy)):
         if v is not None:
             line[k] = v
     print(json.dumps(line))
