@@ -137,6 +137,7 @@ SIGNATURES = {
                                     ctypes.c_void_p],
     "fwgpu_cojo_create": [P(FwMesh), c_i32, ctypes.c_void_p, P(FwOptions), P(ctypes.c_void_p)],
     "fwgpu_cojo_solve": [ctypes.c_void_p, P(c_dbl), P(FwResult), P(c_dbl)],
+    "fwgpu_cojo_set_current": [ctypes.c_void_p, P(c_dbl)],
     "fwgpu_cojo_subdomains": [ctypes.c_void_p, P(c_i32), P(c_i32)],
     "fwgpu_cojo_partition_build": [P(FwMesh), c_i32, ctypes.c_void_p, P(ctypes.c_void_p)],
     "fwgpu_cojo_partition_subdomains": [ctypes.c_void_p, P(c_i32)],

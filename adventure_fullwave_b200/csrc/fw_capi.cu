@@ -777,7 +777,7 @@ int fwgpu_cojo_create(const fwgpu_mesh *mesh, int32_t antenna_flag, const uint8_
   return setup_device(c, &c->opts, out);
 }
 
-int fwgpu_cojo_solve(fwgpu_context *c, const double *current, fwgpu_result *res, double *potential) {
+int fwgpu_cojo_set_current(fwgpu_context *c, const double *current) {
   if (!c || !current) return set_error(FWGPU_ERR_ARG, "null argument");
   if (c->cojo_flag < 0) return set_error(FWGPU_ERR_STATE, "not a correction-Jo context");
   FW_CUDA(cudaSetDevice(c->opts.device));
@@ -789,6 +789,12 @@ int fwgpu_cojo_solve(fwgpu_context *c, const double *current, fwgpu_result *res,
                               c->d_elrhs, c->stream);
   FW_CUDA(cudaGetLastError());
   c->el_src = true;
+  return FWGPU_OK;
+}
+
+int fwgpu_cojo_solve(fwgpu_context *c, const double *current, fwgpu_result *res, double *potential) {
+  FW_TRY(fwgpu_cojo_set_current(c, current));
+  const int64_t nv = c->m.nv;
   // the matrix does not depend on the current: the second pass reuses the factors
   const int rc = c->stage >= 2 && c->factor_fresh ? fwgpu_hddm_resolve(c, nullptr, res)
                                                    : fwgpu_hddm_solve(c, nullptr, res);

@@ -312,6 +312,12 @@ int fwgpu_cojo_create(const fwgpu_mesh *mesh, int32_t antenna_flag, const uint8_
  * factors.  Returns FWGPU_ERR_NOT_CONVERGED (result and potential filled)
  * at hddm_max_loop. */
 int fwgpu_cojo_solve(fwgpu_context *ctx, const double *current, fwgpu_result *result, double *potential);
+/* The current of the next right-hand side, without solving: with it the
+ * slot-by-slot calls (fwgpu_make_tmp_aij with a NULL or empty source,
+ * fwgpu_solve_dom_1st, fwgpu_iteration_s_1st, fwgpu_iteration_s,
+ * fwgpu_solve_dom_last) run a pass behind the reference's own hddm_solver_RS
+ * loop, and fwgpu_get_edge_solution then gives 2 doubles per vertex. */
+int fwgpu_cojo_set_current(fwgpu_context *ctx, const double *current);
 /* The original subdomain id of each of the problem's subdomains (n first;
  * sub_ids may be NULL to query n). */
 int fwgpu_cojo_subdomains(const fwgpu_context *ctx, int32_t *n, int32_t *sub_ids);

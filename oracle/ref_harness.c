@@ -90,6 +90,8 @@ static double *g_srcv = NULL;
 /* adventure_fullwave_b200/dropin/set_hddm_func_gpu.c: the reference's table
    with the subdomain and interface slots on the GPU library */
 void set_hddm_func_fullwave_gpu(HDDM_FUNC *f, OPTIONS options);
+void set_hddm_func_correct_Jor_gpu(HDDM_FUNC *f, OPTIONS options);
+void set_hddm_func_correct_Joi_gpu(HDDM_FUNC *f, OPTIONS options);
 void hddm_gpu_set_edge_source(int n, const int *mid_gnid, const double *re_im);
 #endif
 
@@ -560,8 +562,14 @@ int main(int argc, char **argv) {
     hddm_sw.t_loop = -2;
     for (int i = 0; i < g_pm[0].mtrl.nantenna; i++) {
       hddm_sw.antenna = i;
+#ifdef FW_HARNESS_GPU
+      /* the pre-solve's slots on the GPU library */
+      hddm_solver_RS(g_pm, options, set_hddm_func_correct_Jor_gpu);
+      hddm_solver_RS(g_pm, options, set_hddm_func_correct_Joi_gpu);
+#else
       hddm_solver_RS(g_pm, options, set_hddm_func_correct_Jor);
       hddm_solver_RS(g_pm, options, set_hddm_func_correct_Joi);
+#endif
     }
     dump_jo(g_pm, nrepeat);
     dump_cojo(g_pm, nrepeat);

@@ -228,17 +228,17 @@ def read_log_sections(path: str):
     return secs
 
 
-def run_cojo(model_dir: str, workdir: str, timeout=600):
+def run_cojo(model_dir: str, workdir: str, timeout=600, binary: str = HARNESS):
     """Run main()'s correction-Jo pre-solve of the reference on a model
     directory (copied into workdir/MODEL) and return the parsed dump and the
-    log sections."""
+    log sections.  binary=HARNESS_GPU runs it through the GPU tables."""
     import shutil
 
     mdir = os.path.join(workdir, "MODEL")
     if os.path.abspath(model_dir) != os.path.abspath(mdir):
         shutil.copytree(model_dir, mdir, ignore=shutil.ignore_patterns("calc_log", "result"))
     env = dict(os.environ, FW_HARNESS_MAIN="1", FW_HARNESS_COJO_ONLY="1", FW_HARNESS_OUT=os.path.join(mdir, "ref"))
-    subprocess.run([HARNESS, "-memlimit", "60000", "MODEL"], cwd=workdir, env=env, check=True,
+    subprocess.run([binary, "-memlimit", "60000", "MODEL"], cwd=workdir, env=env, check=True,
                    stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=timeout)
     return read_cojo(os.path.join(mdir, "ref.cojo")), read_log_sections(
         os.path.join(mdir, "calc_log", "log_g_HDDM_Full_Wave"))
