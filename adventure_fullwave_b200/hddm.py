@@ -598,6 +598,14 @@ class CorrectJoSolver:
     def sizes(self) -> dict:
         return HddmSolver.sizes(self)
 
+    def write_calc_log(self, path: str, result: HddmResult, part: str, antenna: int = 0, mode: str = "a") -> None:
+        """Append (or write, mode "w") the last pass's residual history as
+        the reference's correction-Jo log section; part is "Real" or
+        "Imaginary" (correct_jo_log_section)."""
+        with open(path, mode) as f:
+            f.write(correct_jo_log_section(part, antenna, self.sizes()["total_free"], result.initial_norm,
+                                           self.history()))
+
     def subdomain_ids(self) -> np.ndarray:
         n = ctypes.c_int32()
         _lib.check(self._lib.fwgpu_cojo_subdomains(self._h, ctypes.byref(n), None))
