@@ -10,8 +10,22 @@
 #include <unordered_map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "fw_internal.h"
 #include "fw_kernels.cuh"
+
+namespace {
+// An NVTX range over one library call, so that a profiler's timeline (nsys,
+// or ncu --nvtx) shows the reference's slots; without a tool attached a
+// range costs a call into a no-op.
+struct Trace {
+  explicit Trace(const char *name) { nvtxRangePushA(name); }
+  ~Trace() { nvtxRangePop(); }
+  Trace(const Trace &) = delete;
+  Trace &operator=(const Trace &) = delete;
+};
+}  // namespace
 
 namespace {
 
@@ -682,6 +696,7 @@ const char *fwgpu_last_error(void) { return g_last_error.c_str(); }
 int fwgpu_abi_version(void) { return FWGPU_ABI_VERSION; }
 
 int fwgpu_create(const fwgpu_mesh *mesh, const fwgpu_material *mt, const fwgpu_options *opts, fwgpu_context **out) {
+  Trace trace("fwgpu_create");
   if (!mesh || !mt || !opts || !out) return set_error(FWGPU_ERR_ARG, "null argument");
   *out = nullptr;
   int ndev = 0;
@@ -742,6 +757,7 @@ int fwgpu_partition_build(const fwgpu_mesh *mesh, fwgpu_partition **out) {
 
 int fwgpu_cojo_create(const fwgpu_mesh *mesh, int32_t antenna_flag, const uint8_t *pec_vertex,
                       const fwgpu_options *opts, fwgpu_context **out) {
+  Trace trace("fwgpu_cojo_create");
   if (!mesh || !opts || !out) return set_error(FWGPU_ERR_ARG, "null argument");
   *out = nullptr;
   if (opts->precision != FWGPU_PREC_FP64) return set_error(FWGPU_ERR_ARG, "the correction-Jo problem is solved in FP64");
@@ -793,6 +809,7 @@ int fwgpu_cojo_set_current(fwgpu_context *c, const double *current) {
 }
 
 int fwgpu_cojo_solve(fwgpu_context *c, const double *current, fwgpu_result *res, double *potential) {
+  Trace trace("hddm_solver_RS correct_Jo");
   FW_TRY(fwgpu_cojo_set_current(c, current));
   const int64_t nv = c->m.nv;
   // the matrix does not depend on the current: the second pass reuses the factors
@@ -911,6 +928,7 @@ int fwgpu_set_element_source(fwgpu_context *c, const fwgpu_element_source *es) {
 }
 
 int fwgpu_make_tmp_aij(fwgpu_context *c, const fwgpu_source *src) {
+  Trace trace("make_TMP_AIJ");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   FW_CUDA(cudaSetDevice(c->opts.device));
   const fw::Plan &p = c->p;
@@ -1182,6 +1200,7 @@ static int tune_solve_kernel(fwgpu_context *c) {
 }
 
 int fwgpu_solve_dom_1st(fwgpu_context *c) {
+  Trace trace("solve_dom_1st");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (c->stage < 1) return set_error(FWGPU_ERR_STATE, "solve_dom_1st before make_tmp_aij");
   FW_CUDA(cudaSetDevice(c->opts.device));
@@ -1301,6 +1320,7 @@ static int64_t iteration_launches(const fwgpu_context *c) {
 }
 
 int fwgpu_iteration_s_1st(fwgpu_context *c, int32_t *status) {
+  Trace trace("iteration_s_1st");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
   if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "iteration_s_1st before solve_dom_1st");
@@ -1315,6 +1335,7 @@ int fwgpu_iteration_s_1st(fwgpu_context *c, int32_t *status) {
 }
 
 int fwgpu_iteration_s(fwgpu_context *c, int32_t *status) {
+  Trace trace("iteration_s");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
   if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "iteration_s outside the interface loop");
@@ -1488,6 +1509,7 @@ static int multi_run(fwgpu_context *c, int32_t n_src, const fwgpu_source *srcs, 
 }
 
 int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *srcs, fwgpu_result *res) {
+  Trace trace("hddm_solve_multi");
   if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c || !srcs || !res) return set_error(FWGPU_ERR_ARG, "null argument");
   if (n_src < 1 || n_src > fw::kMaxRhs) return set_error(FWGPU_ERR_ARG, "n_src outside 1..FWGPU_MAX_RHS");
@@ -1503,6 +1525,7 @@ int fwgpu_hddm_solve_multi(fwgpu_context *c, int32_t n_src, const fwgpu_source *
 int fwgpu_adjoint_gradient_multi(fwgpu_context *c, int32_t n_probe, const int32_t *probe_edges, int32_t n_design,
                                  const int32_t *design_tets, double *J, double *grad_eps, double *grad_sigma,
                                  fwgpu_result *adjoint_results) {
+  Trace trace("adjoint_gradient_multi");
   if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c || n_probe < 0 || n_design < 0 || (n_probe > 0 && !probe_edges) || (n_design > 0 && !design_tets))
     return set_error(FWGPU_ERR_ARG, "bad argument");
@@ -1707,6 +1730,7 @@ int fwgpu_shard_first_finish(fwgpu_context *c, int32_t *status) {
 }
 
 int fwgpu_shard_iterate(fwgpu_context *c) {
+  Trace trace("shard iterate");
   FW_TRY(shard_ready(c));
   if (c->stage != 3) return set_error(FWGPU_ERR_STATE, "shard_iterate outside the interface loop");
   const bool fp32 = c->opts.precision == FWGPU_PREC_FP32_IR;
@@ -1750,6 +1774,7 @@ int fwgpu_shard_iterate_finish(fwgpu_context *c, int32_t *status) {
 }
 
 int fwgpu_solve_dom_last(fwgpu_context *c) {
+  Trace trace("solve_dom_last");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (c->stage < 3) return set_error(FWGPU_ERR_STATE, "solve_dom_last before the interface loop");
   FW_CUDA(cudaSetDevice(c->opts.device));
@@ -1764,6 +1789,7 @@ int fwgpu_solve_dom_last(fwgpu_context *c) {
 }
 
 static int run_loop(fwgpu_context *c, fwgpu_result *res) {
+  Trace trace("interface iterations");
   // interface iterations captured in a CUDA graph, graph_iterations per launch
   if (!c->graph) {
     cudaGraph_t g;
@@ -1814,6 +1840,7 @@ static int fill_result(fwgpu_context *c, fwgpu_result *res) {
 }
 
 int fwgpu_hddm_solve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *res) {
+  Trace trace("hddm_solver_CS");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
   if (c->opts.hddm_max_loop == 0) return set_error(FWGPU_ERR_ARG, "hddm_max_loop is 0");
@@ -1832,6 +1859,7 @@ int fwgpu_hddm_solve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *re
 }
 
 int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *res) {
+  Trace trace("hddm_resolve");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (c->sharded) return set_error(FWGPU_ERR_STATE, "sharded context: use the fwgpu_shard_* calls");
   if (c->stage < 2) return set_error(FWGPU_ERR_STATE, "resolve before the factors exist");
@@ -1856,6 +1884,7 @@ int fwgpu_hddm_resolve(fwgpu_context *c, const fwgpu_source *src, fwgpu_result *
 int fwgpu_adjoint_gradient(fwgpu_context *c, int32_t n_probe, const int32_t *probe_edges, int32_t n_design,
                            const int32_t *design_tets, double *J, double *grad_eps, double *grad_sigma,
                            fwgpu_result *adjoint_result) {
+  Trace trace("adjoint_gradient");
   if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c || n_probe < 0 || n_design < 0 || (n_probe > 0 && !probe_edges) || (n_design > 0 && !design_tets))
     return set_error(FWGPU_ERR_ARG, "bad argument");
@@ -1938,6 +1967,7 @@ int post_static_data(fwgpu_context *c) {
 }  // namespace
 
 int fwgpu_post_em_E(fwgpu_context *c, const double *x, double *el_B, double *el_E, double *el_Je) {
+  Trace trace("post_em_E");
   if (c && c->cojo_flag >= 0) return set_error(FWGPU_ERR_STATE, "a correction-Jo context solves only fwgpu_cojo_solve");
   if (!c) return set_error(FWGPU_ERR_ARG, "null context");
   if (!x && !c->xedge_ok)
