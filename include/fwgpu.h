@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define FWGPU_ABI_VERSION 3
+#define FWGPU_ABI_VERSION 4
 
 enum {
   FWGPU_OK = 0,

@@ -41,7 +41,10 @@ def test_binding_covers_header():
 def test_abi_version():
     from adventure_fullwave_b200 import _lib
 
-    assert _lib.load().fwgpu_abi_version() == 3
+    txt = open(os.path.join(REPO, "include", "fwgpu.h")).read()
+    declared = int(re.search(r"^#define FWGPU_ABI_VERSION (\d+)", txt, flags=re.M).group(1))
+    assert declared == 4  # 4: the correction-Jo entry points (fwgpu_cojo_*)
+    assert _lib.load().fwgpu_abi_version() == declared
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")
