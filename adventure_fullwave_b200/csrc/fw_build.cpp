@@ -299,7 +299,7 @@ void finish_plan(Plan &p, const std::vector<SubLists> &lists) {
   {
     auto copy_to = [](auto &dst, int64_t at, const auto &src) { std::copy(src.begin(), src.end(), dst.begin() + at); };
     // src positions are local to the subdomain; -1 (no diagonal) stays -1
-    auto copy_src = [](std::vector<int64_t> &dst, int64_t at, const std::vector<int64_t> &src, int64_t nnz0) {
+    auto copy_src = [](HostVec<int64_t> &dst, int64_t at, const std::vector<int64_t> &src, int64_t nnz0) {
       for (size_t i = 0; i < src.size(); i++) dst[at + i] = src[i] < 0 ? src[i] : src[i] + nnz0;
     };
     std::atomic<int> next(0);

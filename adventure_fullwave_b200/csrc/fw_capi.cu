@@ -167,8 +167,8 @@ struct fwgpu_context {
     *ptr = (T *)raw;
     return FWGPU_OK;
   }
-  template <typename T>
-  int upload(T **ptr, const std::vector<T> &v) {
+  template <typename T, typename A>
+  int upload(T **ptr, const std::vector<T, A> &v) {
     int rc = alloc(ptr, v.size());
     if (rc) return rc;
     if (!v.empty()) FW_CUDA(cudaMemcpyAsync(*ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
@@ -192,7 +192,7 @@ namespace {
     if (rc_ != FWGPU_OK) return rc_; \
   } while (0)
 
-std::vector<int64_t> offsets_from_rel(const std::vector<int32_t> &rel_ptr, const std::vector<int64_t> &count_off,
+std::vector<int64_t> offsets_from_rel(const fw::HostVec<int32_t> &rel_ptr, const std::vector<int64_t> &count_off,
                                       int nsub) {
   // rel_ptr holds (n_s + 1) relative entries per subdomain; returns the
   // cumulative base of each subdomain's entry arrays

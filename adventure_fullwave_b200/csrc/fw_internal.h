@@ -2,12 +2,41 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../../include/fwgpu.h"
 
 namespace fw {
+
+// The plan's concatenated host arrays (gigabytes on the largest models) are
+// written once, slice by slice, on all host threads.  This allocator leaves
+// new elements uninitialised, so that resize() does not first zero-fill them
+// on one thread; every element is then written by exactly one worker.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <typename U>
+  NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+  template <typename U>
+  void construct(U *p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new (static_cast<void *>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U *p, Args &&...args) {
+    ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
+  }
+};
+template <typename T>
+using HostVec = std::vector<T, NoInitAlloc<T>>;
 
 // Element edge table of the reference (lib/fem/tetrahedral.h:19-24):
 // slot i joins vertices kTetN[i][0] and kTetN[i][1]; kTetN[i][2..3] is the
@@ -69,34 +98,34 @@ struct Plan {
   std::vector<int64_t> sub_int_off;  // nsub+1, offsets of interior arrays
   std::vector<int64_t> sub_if_off;   // nsub+1, offsets of interface slot arrays
   // lower CSR (local rows, concatenated), row_ptr relative to sub_nnz_off
-  std::vector<int32_t> csr_row_ptr;  // sum(nmp+1)
-  std::vector<int32_t> csr_col;      // local col
-  std::vector<int64_t> contrib_ptr;  // nnz_total+1
-  std::vector<int64_t> contrib;      // element-slot*36 + (i*6+j)
-  std::vector<uint8_t> isbc;         // sum(nmp)
+  HostVec<int32_t> csr_row_ptr;  // sum(nmp+1)
+  HostVec<int32_t> csr_col;      // local col
+  HostVec<int64_t> contrib_ptr;  // nnz_total+1
+  HostVec<int64_t> contrib;      // element-slot*36 + (i*6+j)
+  HostVec<uint8_t> isbc;         // sum(nmp)
   // per-iteration operators (positions into the global lower-CSR value array)
   // coupling: interior row c -> interface slots   (b_I = -A_IG v)
-  std::vector<int32_t> cpl_ptr;      // sum(nI+1), relative
-  std::vector<int32_t> cpl_col;      // interface slot
-  std::vector<int64_t> cpl_src;      // lower-CSR position
+  HostVec<int32_t> cpl_ptr;      // sum(nI+1), relative
+  HostVec<int32_t> cpl_col;      // interface slot
+  HostVec<int64_t> cpl_src;      // lower-CSR position
   // interface rows: slot k -> (interior c) or (interface slot)
-  std::vector<int32_t> ifr_ptr;      // sum(nG+1), relative
-  std::vector<int32_t> ifr_col;      // >=0 interior index, <0: -(slot+1)
-  std::vector<int64_t> ifr_src;
+  HostVec<int32_t> ifr_ptr;      // sum(nG+1), relative
+  HostVec<int32_t> ifr_col;      // >=0 interior index, <0: -(slot+1)
+  HostVec<int64_t> ifr_src;
   // interior operator (both triangles), for FP64 refinement residuals
-  std::vector<int32_t> aii_ptr;      // sum(nI+1), relative
-  std::vector<int32_t> aii_col;
-  std::vector<int64_t> aii_src;
+  HostVec<int32_t> aii_ptr;      // sum(nI+1), relative
+  HostVec<int32_t> aii_col;
+  HostVec<int64_t> aii_src;
   // interface slot data
-  std::vector<int32_t> if_ln;        // sum(nG): global interface id
-  std::vector<int64_t> if_diag_src;  // sum(nG): lower-CSR position of the diagonal, -1 if absent
-  std::vector<int32_t> if_local;     // sum(nG): local DOF id
+  HostVec<int32_t> if_ln;        // sum(nG): global interface id
+  HostVec<int64_t> if_diag_src;  // sum(nG): lower-CSR position of the diagonal, -1 if absent
+  HostVec<int32_t> if_local;     // sum(nG): local DOF id
   // interior data
-  std::vector<int32_t> int_local;    // sum(nI): local DOF id
-  std::vector<int64_t> int_diag_src; // sum(nI): lower-CSR position of the diagonal
+  HostVec<int32_t> int_local;    // sum(nI): local DOF id
+  HostVec<int64_t> int_diag_src; // sum(nI): lower-CSR position of the diagonal
   // gather of q into Q: for each interface DOF g, the (sub-major) slots in sub order
   std::vector<int32_t> gq_ptr;       // total_free+1
-  std::vector<int64_t> gq_slot;      // global slot index (sub_if_off + k)
+  HostVec<int64_t> gq_slot;      // global slot index (sub_if_off + k)
   int64_t nnz_total = 0;
   int64_t nlen_reference = 0;
   int32_t el_dofs = 6;               // DOFs per element: 6 edges, or 4 vertices (correction-Jo problem)
