@@ -586,4 +586,120 @@ std::string build_plan_cojo(const Model &m, int32_t antenna_flag, const std::vec
   return "";
 }
 
+
+namespace {
+
+// fn(s) for every subdomain s, on all host threads (each call writes slices
+// of its own).
+template <typename F>
+void for_each_subdomain(int nsub, F fn) {
+  const int nthreads = std::max(1, std::min<int>(nsub, (int)std::thread::hardware_concurrency()));
+  std::atomic<int> next(0);
+  auto worker = [&]() {
+    for (int s = next++; s < nsub; s = next++) fn(s);
+  };
+  std::vector<std::thread> pool;
+  for (int i = 1; i < nthreads; i++) pool.emplace_back(worker);
+  worker();
+  for (auto &t : pool) t.join();
+}
+
+// per-subdomain offsets of lists whose per-row pointers are stored per
+// subdomain (rows + 1 entries each, concatenated)
+std::vector<int64_t> offsets_from_rel(const HostVec<int32_t> &rel_ptr, const std::vector<int64_t> &count_off,
+                                      int nsub) {
+  std::vector<int64_t> off(nsub + 1, 0);
+  for (int s = 0; s < nsub; s++) off[s + 1] = off[s] + rel_ptr[count_off[s + 1] + s];
+  return off;
+}
+
+}  // namespace
+
+void global_rows(const Plan &p, GlobalRows &g) {
+  const int nsub = (int)p.subs.size();
+  g.cpl_off = offsets_from_rel(p.cpl_ptr, p.sub_int_off, nsub);
+  g.ifr_off = offsets_from_rel(p.ifr_ptr, p.sub_if_off, nsub);
+  g.aii_off = offsets_from_rel(p.aii_ptr, p.sub_int_off, nsub);
+  const int64_t nI_all = p.sub_int_off[nsub], nG_all = p.sub_if_off[nsub];
+  g.cpl_rowptr.resize(nI_all + 1);
+  g.aii_rowptr.resize(nI_all + 1);
+  g.ifr_rowptr.resize(nG_all + 1);
+  g.cpl_gcol.resize(p.cpl_col.size());
+  g.ifr_gcol.resize(p.ifr_col.size());
+  g.aii_gcol.resize(p.aii_col.size());
+  for_each_subdomain(nsub, [&](int s) {
+    const int64_t io = p.sub_int_off[s], go = p.sub_if_off[s];
+    const int nI = (int)(p.sub_int_off[s + 1] - io), nG = (int)(p.sub_if_off[s + 1] - go);
+    for (int cI = 0; cI < nI; cI++) {
+      g.cpl_rowptr[io + cI] = g.cpl_off[s] + p.cpl_ptr[io + s + cI];
+      g.aii_rowptr[io + cI] = g.aii_off[s] + p.aii_ptr[io + s + cI];
+    }
+    for (int k = 0; k < nG; k++) g.ifr_rowptr[go + k] = g.ifr_off[s] + p.ifr_ptr[go + s + k];
+    for (int64_t q = g.cpl_off[s]; q < g.cpl_off[s + 1]; q++) g.cpl_gcol[q] = p.if_ln[go + p.cpl_col[q]];
+    for (int64_t q = g.ifr_off[s]; q < g.ifr_off[s + 1]; q++) {
+      const int col = p.ifr_col[q];
+      g.ifr_gcol[q] = col >= 0 ? (int32_t)(io + col) : -p.if_ln[go + (-col - 1)] - 1;
+    }
+    for (int64_t q = g.aii_off[s]; q < g.aii_off[s + 1]; q++) g.aii_gcol[q] = (int32_t)(io + p.aii_col[q]);
+  });
+  // every subdomain's rows end where the next one's begin
+  g.cpl_rowptr[nI_all] = g.cpl_off[nsub];
+  g.aii_rowptr[nI_all] = g.aii_off[nsub];
+  g.ifr_rowptr[nG_all] = g.ifr_off[nsub];
+}
+
+void envelope_layout(const Plan &p, const int32_t *idx1, EnvelopeLayout &e) {
+  const int nsub = (int)p.subs.size();
+  const int64_t nI_tot = p.sub_int_off[nsub];
+  e.env_lo.assign(nI_tot, 0);
+  e.env_ptr.assign(nI_tot, 0);
+  e.dst.resize(p.nnz_total);
+  // per subdomain: its interior envelope length and the reference's skyline length
+  std::vector<int64_t> len(nsub), ref(nsub), start(nsub);
+  for_each_subdomain(nsub, [&](int s) {
+    const SubHost &h = p.subs[s];
+    const int32_t *i1 = idx1 + p.sub_dof_off[s];
+    int64_t idx2 = 0;
+    for (int i = 1; i < h.nmp; i++) idx2 += i - i1[i];
+    ref[s] = idx2 + h.nmp;
+    int64_t n = 0;
+    for (int r = 0; r < h.nmp; r++) {
+      const int cI = h.cidx[r];
+      if (cI >= 0) n += cI - h.cidx[i1[r]] + 1;
+    }
+    len[s] = n;
+  });
+  int64_t pos = 0, nref = 0;
+  for (int s = 0; s < nsub; s++) {
+    pos = (pos + 1) & ~(int64_t)1;  // every subdomain's envelope starts 16-byte aligned in FP32 too
+    start[s] = pos;
+    pos += len[s];
+    nref += ref[s];
+  }
+  e.nlen = pos;
+  e.nlen_ref = nref;
+  for_each_subdomain(nsub, [&](int s) {
+    const SubHost &h = p.subs[s];
+    const int32_t *i1 = idx1 + p.sub_dof_off[s];
+    const int64_t io = p.sub_int_off[s], z0 = p.sub_nnz_off[s];
+    int64_t at = start[s];
+    for (int r = 0; r < h.nmp; r++) {
+      const int cI = h.cidx[r];
+      if (cI < 0) continue;
+      const int lo = h.cidx[i1[r]];
+      e.env_lo[io + cI] = lo;
+      e.env_ptr[io + cI] = at;
+      at += cI - lo + 1;
+    }
+    for (int r = 0; r < h.nmp; r++) {
+      const int cI = h.cidx[r];
+      const int lo = cI >= 0 ? e.env_lo[io + cI] : 0;
+      for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++) {
+        const int cj = h.cidx[h.col[q]];
+        e.dst[z0 + q] = (cI < 0 || cj < 0 || cj < lo) ? -1 : e.env_ptr[io + cI] + (cj - lo);
+      }
+    }
+  });
+}
+
 }  // namespace fw

@@ -192,17 +192,6 @@ namespace {
     if (rc_ != FWGPU_OK) return rc_; \
   } while (0)
 
-std::vector<int64_t> offsets_from_rel(const fw::HostVec<int32_t> &rel_ptr, const std::vector<int64_t> &count_off,
-                                      int nsub) {
-  // rel_ptr holds (n_s + 1) relative entries per subdomain; returns the
-  // cumulative base of each subdomain's entry arrays
-  std::vector<int64_t> off(nsub + 1, 0);
-  for (int s = 0; s < nsub; s++) {
-    const int64_t n = count_off[s + 1] - count_off[s];
-    off[s + 1] = off[s] + rel_ptr[count_off[s] + s + n];
-  }
-  return off;
-}
 
 int resolve_material(fw::Model &m, const fwgpu_mesh *mesh, const fwgpu_material *mt) {
   m.el_eps.assign(m.nt, 0.0);
@@ -525,27 +514,27 @@ static int setup_device(fwgpu_context *c, const fwgpu_options *opts, fwgpu_conte
   dp.sub_order = d_order;
   dp.int_off = d_int_off;
   dp.if_off = d_if_off;
-  // operator structures
-  auto cpl_off = offsets_from_rel(p.cpl_ptr, p.sub_int_off, nsub);
-  auto ifr_off = offsets_from_rel(p.ifr_ptr, p.sub_if_off, nsub);
-  auto aii_off = offsets_from_rel(p.aii_ptr, p.sub_int_off, nsub);
+  // operator structures, and the global row pointers and column maps of the
+  // grid-wide products of the staged solve
+  fw::GlobalRows g;
+  fw::global_rows(p, g);
   int32_t *ip = nullptr;
   int64_t *lp = nullptr;
   FW_TRY(c->upload(&ip, p.cpl_ptr));
   dp.cpl_ptr = ip;
-  FW_TRY(c->upload(&lp, cpl_off));
+  FW_TRY(c->upload(&lp, g.cpl_off));
   dp.cpl_off = lp;
   FW_TRY(c->upload(&ip, p.cpl_col));
   dp.cpl_col = ip;
   FW_TRY(c->upload(&ip, p.ifr_ptr));
   dp.ifr_ptr = ip;
-  FW_TRY(c->upload(&lp, ifr_off));
+  FW_TRY(c->upload(&lp, g.ifr_off));
   dp.ifr_off = lp;
   FW_TRY(c->upload(&ip, p.ifr_col));
   dp.ifr_col = ip;
   FW_TRY(c->upload(&ip, p.aii_ptr));
   dp.aii_ptr = ip;
-  FW_TRY(c->upload(&lp, aii_off));
+  FW_TRY(c->upload(&lp, g.aii_off));
   dp.aii_off = lp;
   FW_TRY(c->upload(&ip, p.aii_col));
   dp.aii_col = ip;
@@ -556,39 +545,18 @@ static int setup_device(fwgpu_context *c, const fwgpu_options *opts, fwgpu_conte
   FW_TRY(c->upload(&lp, p.gq_slot));
   dp.gq_slot = lp;
   {
-    // global row pointers and column maps of the grid-wide products of the staged solve
-    const int64_t nI_all = p.sub_int_off[nsub], nG_all = p.sub_if_off[nsub];
-    std::vector<int64_t> crp(nI_all + 1, 0), irp(nG_all + 1, 0), arp(nI_all + 1, 0);
-    std::vector<int32_t> cg(p.cpl_col.size()), ig(p.ifr_col.size()), ag(p.aii_col.size());
-    for (int s = 0; s < nsub; s++) {
-      const int64_t io = p.sub_int_off[s], go = p.sub_if_off[s];
-      const int nI = (int)(p.sub_int_off[s + 1] - io), nG = (int)(p.sub_if_off[s + 1] - go);
-      for (int cI = 0; cI <= nI; cI++) {
-        crp[io + cI] = cpl_off[s] + p.cpl_ptr[io + s + cI];
-        arp[io + cI] = aii_off[s] + p.aii_ptr[io + s + cI];
-      }
-      for (int k = 0; k <= nG; k++) irp[go + k] = ifr_off[s] + p.ifr_ptr[go + s + k];
-      for (int64_t q = cpl_off[s]; q < cpl_off[s + 1]; q++) cg[q] = p.if_ln[go + p.cpl_col[q]];
-      for (int64_t q = ifr_off[s]; q < ifr_off[s + 1]; q++) {
-        const int col = p.ifr_col[q];
-        ig[q] = col >= 0 ? (int32_t)(io + col) : -p.if_ln[go + (-col - 1)] - 1;
-      }
-      for (int64_t q = aii_off[s]; q < aii_off[s + 1]; q++) ag[q] = (int32_t)(io + p.aii_col[q]);
-    }
-    FW_TRY(c->upload(&lp, crp));
+    FW_TRY(c->upload(&lp, g.cpl_rowptr));
     dp.cpl_rowptr = lp;
-    FW_TRY(c->upload(&ip, cg));
+    FW_TRY(c->upload(&ip, g.cpl_gcol));
     dp.cpl_gcol = ip;
-    FW_TRY(c->upload(&lp, irp));
+    FW_TRY(c->upload(&lp, g.ifr_rowptr));
     dp.ifr_rowptr = lp;
-    FW_TRY(c->upload(&ip, ig));
+    FW_TRY(c->upload(&ip, g.ifr_gcol));
     dp.ifr_gcol = ip;
-    FW_TRY(c->upload(&lp, arp));
+    FW_TRY(c->upload(&lp, g.aii_rowptr));
     dp.aii_rowptr = lp;
-    FW_TRY(c->upload(&ip, ag));
+    FW_TRY(c->upload(&ip, g.aii_gcol));
     dp.aii_gcol = ip;
-    (void)nI_all;
-    (void)nG_all;
     dp.row0 = p.sub_int_off[s_begin];
     dp.n_interior = p.sub_int_off[s_end] - p.sub_int_off[s_begin];
     dp.slot0 = p.sub_if_off[s_begin];
@@ -1217,46 +1185,17 @@ int fwgpu_solve_dom_1st(fwgpu_context *c) {
     c->h_idx1.resize(ndof);
     FW_CUDA(cudaMemcpyAsync(c->h_idx1.data(), c->d_idx1, ndof * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     FW_CUDA(cudaStreamSynchronize(c->stream));
-    const int64_t nI_tot = p.sub_int_off[nsub];
-    c->h_env_lo.assign(nI_tot, 0);
-    c->h_env_ptr.assign(nI_tot, 0);
-    std::vector<int64_t> dst(p.nnz_total, -1);
-    int64_t pos = 0, nref = 0;
-    for (int s = 0; s < nsub; s++) {
-      const fw::SubHost &h = p.subs[s];
-      const int32_t *idx1 = c->h_idx1.data() + p.sub_dof_off[s];
-      pos = (pos + 1) & ~(int64_t)1;  // every subdomain's envelope starts 16-byte aligned in FP32 too
-      // reference skyline length (advlas_skyline.c:20-24)
-      int64_t idx2 = 0;
-      for (int i = 1; i < h.nmp; i++) idx2 += i - idx1[i];
-      nref += idx2 + h.nmp;
-      const int64_t io = p.sub_int_off[s];
-      for (int r = 0; r < h.nmp; r++) {
-        const int cI = h.cidx[r];
-        if (cI < 0) continue;
-        const int lo = h.cidx[idx1[r]];
-        c->h_env_lo[io + cI] = lo;
-        c->h_env_ptr[io + cI] = pos;
-        pos += cI - lo + 1;
-      }
-      const int64_t z0 = p.sub_nnz_off[s];
-      for (int r = 0; r < h.nmp; r++) {
-        const int cI = h.cidx[r];
-        if (cI < 0) continue;
-        const int lo = c->h_env_lo[io + cI];
-        for (int q = h.row_ptr[r]; q < h.row_ptr[r + 1]; q++) {
-          const int j = h.col[q];
-          const int cj = h.cidx[j];
-          if (cj < 0 || cj < lo) continue;
-          dst[z0 + q] = c->h_env_ptr[io + cI] + (cj - lo);
-        }
-      }
-    }
-    c->nlen_int = pos;
-    c->nlen_ref = nref;
+    // the interior envelope of every subdomain, laid out on all host threads
+    fw::EnvelopeLayout env;
+    fw::envelope_layout(p, c->h_idx1.data(), env);
+    c->h_env_lo.swap(env.env_lo);
+    c->h_env_ptr.swap(env.env_ptr);
+    const int64_t pos = env.nlen;
+    c->nlen_int = env.nlen;
+    c->nlen_ref = env.nlen_ref;
     FW_TRY(c->upload(&c->d_env_lo, c->h_env_lo));
     FW_TRY(c->upload(&c->d_env_ptr, c->h_env_ptr));
-    FW_TRY(c->upload(&c->d_env_dst, dst));
+    FW_TRY(c->upload(&c->d_env_dst, env.dst));
     // padding: bulk copies of a block may read up to 16 bytes past its end
     FW_TRY(c->alloc(&c->d_L64, pos + 64));
     c->dp.env_lo = c->d_env_lo;

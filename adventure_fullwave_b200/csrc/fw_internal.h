@@ -134,6 +134,32 @@ struct Plan {
 
 // Builds the plan; returns an empty string on success or an error message.
 std::string build_plan(const Model &m, Plan &p);
+
+// Row pointers and column maps of the grid-wide products over all
+// subdomains' rows at once (the concatenated interior rows and interface
+// slots): cpl (interior row -> interface DOF), ifr (interface slot -> global
+// interior row, or -(interface DOF)-1), aii (interior row -> global interior
+// row); *_off are the per-subdomain offsets of the lists (nsub+1).
+struct GlobalRows {
+  std::vector<int64_t> cpl_off, ifr_off, aii_off;
+  HostVec<int64_t> cpl_rowptr, ifr_rowptr, aii_rowptr;
+  HostVec<int32_t> cpl_gcol, ifr_gcol, aii_gcol;
+};
+void global_rows(const Plan &p, GlobalRows &g);
+
+// The interior envelope of every subdomain from the reference's skyline
+// profile idx1 (one entry per local DOF, concatenated): the first interior
+// column env_lo and the position env_ptr of every interior row (each
+// subdomain from an even position), the envelope position of every lower
+// entry (dst, -1 outside the interior envelope), the total length nlen and
+// the reference's skyline length nlen_ref (advlas_skyline.c:20-24).
+struct EnvelopeLayout {
+  std::vector<int32_t> env_lo;
+  std::vector<int64_t> env_ptr;
+  HostVec<int64_t> dst;
+  int64_t nlen = 0, nlen_ref = 0;
+};
+void envelope_layout(const Plan &p, const int32_t *idx1, EnvelopeLayout &e);
 // The plan of one antenna's correction-Jo problem (vertex DOFs of the
 // elements carrying antenna_flag); sub_map receives the original subdomain id
 // of each of its subdomains.  pec_vertex: one flag per vertex, or empty.
