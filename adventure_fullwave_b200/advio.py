@@ -463,7 +463,9 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
     Subdomains are numbered part by part.  Vertices and edges are numbered
     in ascending global node id; each subdomain keeps its local order, the
     part file's node order, in ``model.sub_order``.  An edge is on the PEC wall when its
-    mid-node is in a subdomain's DirichletBCs_Axn0 list.  A ``volt.dat``
+    mid-node is in a subdomain's DirichletBCs_Axn0 list; vertex nodes of those
+    lists go to ``model.pec_vertex`` (the correction-Jo problem's Dirichlet
+    vertices).  A ``volt.dat``
     with gaps becomes the model's delta-gap source; otherwise the antennas
     of ``mtrl.dat`` become its antenna source, with the vertex currents the
     reference builds: from shape definitions (``md``, ``antenna_currents``)
@@ -525,10 +527,12 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
         edges[tet_edges[:, q], 0] = lo
         edges[tet_edges[:, q], 1] = hi
     pec = np.zeros(mid_g.shape[0], bool)
+    pec_vertex = np.zeros(vert_g.shape[0], bool)
     if pec_gnid:
         g = np.concatenate(pec_gnid)
-        g = g[eidx[g] >= 0]
-        pec[eidx[g]] = True
+        pec[eidx[g[eidx[g] >= 0]]] = True
+        # vertex nodes of the lists: the correction-Jo problem's Dirichlet vertices
+        pec_vertex[vidx[g[vidx[g] >= 0]]] = True
     crd = g_crd[vert_g]
     # each subdomain's local order: its vertices, then its mid-nodes, in the
     # part file's node order (make_MESH_make_ap / make_MESH_change_ap)
@@ -557,7 +561,7 @@ def load_model(model_dir: str, name: Optional[str] = None) -> LoadedModel:
         mat_sigma=np.array([sig_of.get(f, 0.0) for f in flags.tolist()]), omega=mat.omega, pec_edge=pec,
         sub_of_tet=el_sub, nsub=sub, sources=[],
         eps_table=(mat.eps_flag.copy(), mat.eps.copy()), sigma_table=(mat.sigma_flag.copy(), mat.sigma.copy()),
-        sub_order=sub_order)
+        sub_order=sub_order, pec_vertex=pec_vertex if pec_vertex.any() else None)
     vpath = os.path.join(model_dir, "volt.dat")
     boxes, volts = read_volt(vpath) if os.path.exists(vpath) else (np.zeros((0, 6)), np.zeros(0))
     if volts.shape[0] > 0:

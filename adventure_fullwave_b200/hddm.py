@@ -502,6 +502,9 @@ def hddm_solver_CS(model, source=0, **opts) -> Tuple[np.ndarray, HddmResult]:
 
 def _pec_vertex(model, pec_vertex):
     if pec_vertex is None:
+        # the model's own Dirichlet vertices (advio.load_model reads them)
+        pec_vertex = getattr(model, "pec_vertex", None)
+    if pec_vertex is None:
         return None, None
     a = np.ascontiguousarray(pec_vertex, dtype=np.uint8)
     if a.shape != (int(model.n_vertices),):

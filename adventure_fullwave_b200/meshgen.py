@@ -96,6 +96,10 @@ class Model:
     # (its node order): (vertex ptr, vertex ids, edge ptr, edge ids), or None
     # for ascending global id
     sub_order: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]] = None
+    # vertex nodes of the Dirichlet (DirichletBCs_Axn0) lists, one flag per
+    # vertex, or None: the full-wave problem ignores them, the correction-Jo
+    # problem of an antenna holds its vertices there at zero
+    pec_vertex: Optional[np.ndarray] = None
 
     @property
     def n_vertices(self) -> int:
@@ -541,6 +545,8 @@ def write_hddm_model(model: Model, directory: str, source_index: Optional[int] =
     ln_of[iface] = np.arange(iface.shape[0])
     pec_node = np.zeros(nnd, dtype=bool)
     pec_node[nv + np.nonzero(model.pec_edge)[0]] = True
+    if getattr(model, "pec_vertex", None) is not None:
+        pec_node[:nv] = np.asarray(model.pec_vertex, bool)
     tag = "HDDM_Part[0]:0:5EED0000"
     docs = []
     mid_crd = 0.5 * (model.vertex_crd[model.edges[:, 0]] + model.vertex_crd[model.edges[:, 1]])

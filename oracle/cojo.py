@@ -64,6 +64,8 @@ class CojoPartition:
 
 def partition(model, antenna_flag: int, pec_vertex: Optional[np.ndarray] = None) -> CojoPartition:
     nv = model.n_vertices
+    if pec_vertex is None:
+        pec_vertex = getattr(model, "pec_vertex", None)
     order = np.argsort(model.sub_of_tet, kind="stable")
     counts = np.bincount(model.sub_of_tet, minlength=model.nsub)
     starts = np.concatenate([[0], np.cumsum(counts)])

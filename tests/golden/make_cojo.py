@@ -5,13 +5,16 @@ in main() mode (FW_HARNESS_MAIN=1, FW_HARNESS_COJO_ONLY=1):
     make -f oracle/Makefile.ref
     python tests/golden/make_cojo.py
 
-Two models:
+Three models:
   * ``sample``: the reference's shipped model directory (main/fullwave/MODEL,
     6 parts x 73 subdomains, one parallelepiped antenna);
   * ``cyl``: the synthetic ``antenna`` golden model written in the
     reference's layout with a double sectorial cylinder antenna (md) whose
     currents have real and imaginary parts (``cylinder_model`` rebuilds it
-    through the package's own writer and reader).
+    through the package's own writer and reader);
+  * ``cylp``: the same with vertex nodes in its Dirichlet lists
+    (``pec_vertices``: antenna vertices one subdomain holds, on the
+    antenna's lowest plane), which the pre-solve holds at zero.
 For each, per subdomain holding antenna elements: its id, the model vertex of
 each antenna DOF (enf order), the Dirichlet list, the interface entries
 (nfid, ln_part) and the potentials Ihr, Ihi the reference leaves; the
@@ -39,14 +42,27 @@ SAMPLE = os.path.join(os.environ.get("FW_REFERENCE", "/root/reference"), "main",
 CYLINDER = "Full-Wave\nDoubleSectorialCylinder\n0.75 0.75 0.5 z 0.5\ndeg 30 270\n0.1 0.3\n2.0 -1.0\n"
 
 
-def write_cylinder_model(mdir: str):
+def pec_vertices(model, flag):
+    """Dirichlet vertices for the ``cylp`` model: the antenna's vertices on
+    its lowest plane (z = 0.5) that one antenna subdomain alone holds."""
+    held = np.zeros(model.n_vertices, np.int64)
+    for s in range(model.nsub):
+        els = np.nonzero((model.sub_of_tet == s) & (model.flag == flag))[0]
+        held[np.unique(model.tets[els])] += 1
+    return (held == 1) & (model.vertex_crd[:, 2] == 0.5)
+
+
+def write_cylinder_model(mdir: str, with_pec_vertices: bool = False):
     """The ``antenna`` golden model with an md cylinder antenna, in the
-    reference's model-directory layout."""
+    reference's model-directory layout; with_pec_vertices adds vertex nodes
+    to its Dirichlet lists (pec_vertices)."""
     from helpers import golden
 
     z, params, model = golden("antenna")
     flag = int(model.element_source.antenna_flag[0])
     model.element_source = None
+    if with_pec_vertices:
+        model.pec_vertex = pec_vertices(model, flag)
     meshgen.write_hddm_model(model, mdir)
     os.remove(os.path.join(mdir, "source.txt"))
     with open(os.path.join(mdir, "mtrl.dat"), "a") as f:
@@ -55,11 +71,11 @@ def write_cylinder_model(mdir: str):
         f.write(CYLINDER)
 
 
-def cylinder_model():
+def cylinder_model(with_pec_vertices: bool = False):
     """The cylinder model as the package reads it (advio.load_model)."""
     with tempfile.TemporaryDirectory() as wd:
         mdir = os.path.join(wd, "MODEL")
-        write_cylinder_model(mdir)
+        write_cylinder_model(mdir, with_pec_vertices)
         return advio.load_model(mdir)
 
 
@@ -101,6 +117,13 @@ def main():
         cj, secs = refdump.run_cojo(mdir, wd)
     vidx = {int(g): k for k, g in enumerate(np.asarray(ld.vertex_gnid).tolist())}
     out.update(pack("cyl", cj, secs, vidx))
+    with tempfile.TemporaryDirectory() as wd:
+        mdir = os.path.join(wd, "MODEL")
+        write_cylinder_model(mdir, with_pec_vertices=True)
+        ld = advio.load_model(mdir)
+        cj, secs = refdump.run_cojo(mdir, wd)
+    vidx = {int(g): k for k, g in enumerate(np.asarray(ld.vertex_gnid).tolist())}
+    out.update(pack("cylp", cj, secs, vidx))
     path = os.path.join(HERE, "ref_cojo.npz")
     np.savez_compressed(path, **out)
     print(path, {k: v.shape for k, v in out.items()})

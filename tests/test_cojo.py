@@ -3,7 +3,9 @@ on the CPU: the library's integer setup (fwgpu_cojo_partition_build, no GPU)
 and the oracle (oracle/cojo.py) against the reference's own run of the
 pre-solve (fixture tests/golden/ref_cojo.npz, made by
 tests/golden/make_cojo.py) on the shipped sample model and on a synthetic
-single-part model with a cylinder antenna."""
+single-part model with a cylinder antenna, also with vertex nodes in its
+Dirichlet lists (which advio reads into model.pec_vertex and the pre-solve
+holds at zero)."""
 import os
 import sys
 
@@ -29,7 +31,8 @@ def models():
     import bench
 
     m, _ = bench.sample_model()
-    return {"sample": m, "cyl": make_cojo.cylinder_model().model}
+    return {"sample": m, "cyl": make_cojo.cylinder_model().model,
+            "cylp": make_cojo.cylinder_model(with_pec_vertices=True).model}
 
 
 def ref_subs(z, key):
@@ -47,7 +50,7 @@ def ref_subs(z, key):
     return out
 
 
-@pytest.mark.parametrize("key", ["sample", "cyl"])
+@pytest.mark.parametrize("key", ["sample", "cyl", "cylp"])
 def test_integer_setup_matches_the_reference(key):
     """Subdomains, antenna DOFs in enf order, Dirichlet lists and interface
     DOFs bit-exact; interface numbers too on the single-part model (the
@@ -66,7 +69,7 @@ def test_integer_setup_matches_the_reference(key):
         assert np.array_equal(mp["edge_gid"], verts), s
         assert np.array_equal(mp["ibc"], ibc), s
         assert np.array_equal(mp["inbc_nfid"], nfid), s
-        if key == "cyl":
+        if key != "sample":
             assert np.array_equal(mp["inbc_ln_part"], ln), s
         for n, g in zip(mp["inbc_ln_part"].tolist(), mp["edge_gid"][mp["inbc_nfid"]].tolist()):
             assert gid_of_ln.setdefault(n, g) == g
@@ -77,7 +80,7 @@ def test_integer_setup_matches_the_reference(key):
         assert np.array_equal(sb.gid, r[1]) and np.array_equal(sb.ibc, r[2]) and np.array_equal(sb.inbc_nfid, r[3])
 
 
-@pytest.mark.parametrize("key", ["sample", "cyl"])
+@pytest.mark.parametrize("key", ["sample", "cyl", "cylp"])
 def test_oracle_matches_the_reference(key):
     """Both passes (currents Jor, then Jo): the same iteration count, the
     residual history to the 7 printed digits (the first 15 above 1e-12), and
@@ -131,6 +134,22 @@ def test_pinned_dof_without_interface():
     assert op.subs[0].pinned and op.subs[0].ibc.tolist() == [0]
     phi, per_sub, hist, _ = cojo.hddm(m, op, m.element_source.antenna_Jor[0])
     assert hist.shape[0] == 0 and per_sub[0][0] == 0.0 and np.any(per_sub[0])
+
+
+def test_dirichlet_vertices_are_read_and_held():
+    """advio reads the vertex nodes of the Dirichlet lists; the pre-solve's
+    Dirichlet lists then start with them (the reference's order)."""
+    ms = models()
+    assert ms["cyl"].pec_vertex is None
+    pv = ms["cylp"].pec_vertex
+    assert pv is not None and pv.any()
+    z = fixture()
+    ref = ref_subs(z, "cylp")
+    n_pec = sum(int(pv[r[1]].sum()) for r in ref)
+    assert n_pec == int(pv.sum())
+    for r in ref:
+        k = int(pv[r[1]].sum())
+        assert np.array_equal(r[2][:k], np.nonzero(pv[r[1]])[0])
 
 
 def test_no_antenna_element_is_an_error():

@@ -1,9 +1,9 @@
 """The correction-Jo pre-solve of an antenna (main/fullwave/main.c:92-98) on
 the GPU through the C ABI (fwgpu_cojo_create / fwgpu_cojo_solve), against
 the reference's own run (fixture tests/golden/ref_cojo.npz) and the oracle
-(oracle/cojo.py): the shipped sample model and a synthetic cylinder antenna,
-both passes, plus PEC vertices and a single subdomain checked against the
-oracle."""
+(oracle/cojo.py): the shipped sample model and a synthetic cylinder antenna
+(also with Dirichlet vertices), both passes, plus PEC vertices on interface
+DOFs and a single subdomain checked against the oracle."""
 import numpy as np
 import pytest
 
@@ -18,7 +18,7 @@ def rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-@pytest.mark.parametrize("key", ["sample", "cyl"])
+@pytest.mark.parametrize("key", ["sample", "cyl", "cylp"])
 def test_gpu_matches_the_reference_and_the_oracle(key):
     z = fixture()
     m = models()[key]
