@@ -448,16 +448,15 @@ std::string build_plan(const Model &m, Plan &p) {
 //     lib/hddm/make_PartMesh.c:973-983 with make_MESH.c:459-500);
 //   - interface DOFs are the antenna vertices held by two or more subdomains
 //     (make_PartMesh_FW_change_innerbc_ANTENNA with its make_nf,
-//     make_PartMesh.c:1288-1340,1546-1575), numbered in ascending global
-//     vertex id;
+//     make_PartMesh.c:1288-1340,1546-1575) that are not on a Dirichlet list
+//     (the pass that excludes essential BCs, :393-421), numbered in ascending
+//     global vertex id;
 //   - the Dirichlet list is the sorted PEC antenna DOFs, then the interface
 //     DOFs in ascending local id; a subdomain with neither holds its DOF 0 at
 //     zero (make_PartMesh_make_ANTENNA_change_bc / _add_inbc,
 //     make_PartMesh.c:986-1063).
 // Only subdomains with antenna elements enter the problem: sub_map gives
-// the original subdomain id of each.  A vertex that is PEC and interface at
-// once is listed twice, as the reference lists it, and is solved as an
-// interface DOF.
+// the original subdomain id of each.
 std::string build_plan_cojo(const Model &m, int32_t antenna_flag, const std::vector<uint8_t> &pec_vertex, Plan &p,
                             std::vector<int32_t> &sub_map) {
   const int nsub_all = m.nsub;
@@ -523,7 +522,7 @@ std::string build_plan_cojo(const Model &m, int32_t antenna_flag, const std::vec
     for (int v : dofs[r])
       if (vowner[v] < 0) vowner[v] = r;
   for (int v = 0; v < m.nv; v++)
-    if (vcount[v] >= 2) {
+    if (vcount[v] >= 2 && (pec_vertex.empty() || !pec_vertex[v])) {
       iface_of_vertex[v] = (int32_t)p.iface_gid.size();
       p.iface_gid.push_back(v);
       p.iface_owner_sub.push_back(vowner[v]);

@@ -288,7 +288,8 @@ int fwgpu_hddm_resolve(fwgpu_context *ctx, const fwgpu_source *src, fwgpu_result
  * vertices of the antenna's elements, its element matrix (grad N_i, grad N_j)
  * and its element vector (J, grad N_i) of the vertex currents J
  * (tet_MakeElement_correct_Jo, lib/fem/make_elem.c:10-66); interface DOFs
- * are the antenna vertices two or more subdomains hold, and a subdomain with
+ * are the antenna vertices two or more subdomains hold that are on no
+ * Dirichlet list (make_PartMesh.c:393-421), and a subdomain with
  * no Dirichlet or interface DOF holds its first DOF at zero
  * (make_PartMesh.c:973-1063,1288-1340,1546-1575).  The interface problem is
  * solved by the same batched kernels as the full-wave one (the reference's

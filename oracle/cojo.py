@@ -14,7 +14,8 @@ module restates them in numpy:
   vertex order (``make_PartMesh_make_ANTENNA_make_enf``,
   ``lib/hddm/make_PartMesh.c:973-983``), interface DOFs the antenna vertices
   two or more subdomains hold (``make_PartMesh_FW_change_innerbc_ANTENNA``
-  with its ``make_nf``, ``:1288-1340,1546-1575``), the Dirichlet list the
+  with its ``make_nf``, ``:1288-1340,1546-1575``) that are on no Dirichlet
+  list (``:393-421``), the Dirichlet list the
   sorted PEC DOFs then the interface DOFs, or DOF 0 alone when a subdomain
   has neither (``make_PartMesh_make_ANTENNA_change_bc`` / ``_add_inbc``,
   ``:986-1063``);
@@ -84,7 +85,10 @@ def partition(model, antenna_flag: int, pec_vertex: Optional[np.ndarray] = None)
             v = vord[np.isin(vord, v)]
         held[v] += 1
         per.append((s, els, v))
-    iface_gid = np.nonzero(held >= 2)[0]
+    # vertices on a Dirichlet list stay out of the interface (the pass that
+    # excludes essential BCs, make_PartMesh.c:393-421)
+    pec = np.zeros(nv, bool) if pec_vertex is None else np.asarray(pec_vertex, bool)
+    iface_gid = np.nonzero((held >= 2) & ~pec)[0]
     ln_of = np.full(nv, -1, np.int64)
     ln_of[iface_gid] = np.arange(iface_gid.shape[0])
     subs = []

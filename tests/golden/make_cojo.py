@@ -13,8 +13,9 @@ Three models:
     currents have real and imaginary parts (``cylinder_model`` rebuilds it
     through the package's own writer and reader);
   * ``cylp``: the same with vertex nodes in its Dirichlet lists
-    (``pec_vertices``: antenna vertices one subdomain holds, on the
-    antenna's lowest plane), which the pre-solve holds at zero.
+    (``pec_vertices``: the antenna's vertices on its lowest plane, some of
+    them shared by subdomains), which the pre-solve holds at zero and keeps
+    out of its interface.
 For each, per subdomain holding antenna elements: its id, the model vertex of
 each antenna DOF (enf order), the Dirichlet list, the interface entries
 (nfid, ln_part) and the potentials Ihr, Ihi the reference leaves; the
@@ -44,12 +45,10 @@ CYLINDER = "Full-Wave\nDoubleSectorialCylinder\n0.75 0.75 0.5 z 0.5\ndeg 30 270\
 
 def pec_vertices(model, flag):
     """Dirichlet vertices for the ``cylp`` model: the antenna's vertices on
-    its lowest plane (z = 0.5) that one antenna subdomain alone holds."""
-    held = np.zeros(model.n_vertices, np.int64)
-    for s in range(model.nsub):
-        els = np.nonzero((model.sub_of_tet == s) & (model.flag == flag))[0]
-        held[np.unique(model.tets[els])] += 1
-    return (held == 1) & (model.vertex_crd[:, 2] == 0.5)
+    its lowest plane (z = 0.5), some of them shared by subdomains."""
+    on_antenna = np.zeros(model.n_vertices, bool)
+    on_antenna[np.unique(model.tets[model.flag == flag])] = True
+    return on_antenna & (model.vertex_crd[:, 2] == 0.5)
 
 
 def write_cylinder_model(mdir: str, with_pec_vertices: bool = False):

@@ -137,19 +137,25 @@ def test_pinned_dof_without_interface():
 
 
 def test_dirichlet_vertices_are_read_and_held():
-    """advio reads the vertex nodes of the Dirichlet lists; the pre-solve's
-    Dirichlet lists then start with them (the reference's order)."""
+    """advio reads the vertex nodes of the Dirichlet lists.  In the
+    reference's pre-solve they lead each subdomain's Dirichlet list and stay
+    out of the interface, shared ones too (make_PartMesh.c:393-421)."""
     ms = models()
     assert ms["cyl"].pec_vertex is None
     pv = ms["cylp"].pec_vertex
     assert pv is not None and pv.any()
     z = fixture()
     ref = ref_subs(z, "cylp")
-    n_pec = sum(int(pv[r[1]].sum()) for r in ref)
-    assert n_pec == int(pv.sum())
+    seen = np.zeros_like(pv)
+    shared = 0
     for r in ref:
         k = int(pv[r[1]].sum())
         assert np.array_equal(r[2][:k], np.nonzero(pv[r[1]])[0])
+        assert not pv[r[1][r[3]]].any()  # no interface DOF on a Dirichlet list
+        shared += int(seen[r[1]][pv[r[1]]].sum())
+        seen[r[1][pv[r[1]]]] = True
+    assert np.array_equal(seen, pv) and shared > 0
+    assert int(z["cylp_tfree"][0]) < int(z["cyl_tfree"][0])
 
 
 def test_no_antenna_element_is_an_error():
