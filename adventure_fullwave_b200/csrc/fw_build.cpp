@@ -60,18 +60,30 @@ void build_sub(const Model &m, const Plan &p, const std::vector<int32_t> &iface_
   const int64_t e0 = p.sub_el_off[s], e1 = p.sub_el_off[s + 1];
   const int nel = (int)(e1 - e0);
   h.els.assign(p.el_order.begin() + e0, p.el_order.begin() + e1);
+  // the subdomain's edges and vertices once each (the scratch maps mark
+  // them; the marks are overwritten by the local ids below), ascending
   std::vector<int32_t> ve, vv;
   ve.reserve(nel * 2);
   vv.reserve(nel);
   for (int k = 0; k < nel; k++) {
     int t = h.els[k];
-    for (int i = 0; i < 6; i++) ve.push_back(m.te[6 * (int64_t)t + i]);
-    for (int i = 0; i < 4; i++) vv.push_back(m.tv[4 * (int64_t)t + i]);
+    for (int i = 0; i < 6; i++) {
+      const int32_t e = m.te[6 * (int64_t)t + i];
+      if (w.eloc[e] < 0) {
+        w.eloc[e] = 0;
+        ve.push_back(e);
+      }
+    }
+    for (int i = 0; i < 4; i++) {
+      const int32_t v = m.tv[4 * (int64_t)t + i];
+      if (w.vloc[v] < 0) {
+        w.vloc[v] = 0;
+        vv.push_back(v);
+      }
+    }
   }
   std::sort(ve.begin(), ve.end());
-  ve.erase(std::unique(ve.begin(), ve.end()), ve.end());
   std::sort(vv.begin(), vv.end());
-  vv.erase(std::unique(vv.begin(), vv.end()), vv.end());
   if (!m.sub_eptr.empty()) {
     // the caller's local order (the part file's node order): the same sets
     std::vector<int32_t> ge(m.sub_eord.begin() + m.sub_eptr[s], m.sub_eord.begin() + m.sub_eptr[s + 1]);
@@ -81,6 +93,8 @@ void build_sub(const Model &m, const Plan &p, const std::vector<int32_t> &iface_
     std::sort(sv.begin(), sv.end());
     if (se != ve || sv != vv) {
       L.err = "subdomain " + std::to_string(s) + ": the given local order does not list its vertices and edges once each";
+      for (int32_t e : ve) w.eloc[e] = -1;
+      for (int32_t v : vv) w.vloc[v] = -1;
       return;
     }
     ve.swap(ge);
