@@ -180,3 +180,37 @@ def test_fixture_is_the_reference_run():
     got = make_cojo.pack("cyl", cj, secs, vidx)
     for k, v in got.items():
         assert np.array_equal(v, z[k]), k
+
+
+def test_entry_points_refuse_bad_arguments_before_any_device_work():
+    """The C ABI's argument checks of the pre-solve's entry points, which run
+    before any CUDA call: FP32 factors and shard ranges are refused, null
+    handles and currents too, and a context that is not a pre-solve's is
+    turned away by the pre-solve's calls."""
+    import ctypes
+
+    lib = _lib.load()
+    m = models()["cyl"]
+    mesh, keep = hddm._mesh_struct(m)
+    flag = int(m.element_source.antenna_flag[0])
+    out = ctypes.c_void_p()
+    fp32 = _lib.FwOptions(1e-10, 4000, _lib.PREC_FP32_IR, 1, 0.0, 16, 0, 0, 0, 0.0, 0, 0, 0, 0)
+    assert lib.fwgpu_cojo_create(ctypes.byref(mesh), flag, None, ctypes.byref(fp32), ctypes.byref(out)) == _lib.ERR_ARG
+    assert not out.value
+    shard = _lib.FwOptions(1e-10, 4000, _lib.PREC_FP64, 1, 0.0, 16, 0, 0, 0, 0.0, 0, 2, 0, 0)
+    assert lib.fwgpu_cojo_create(ctypes.byref(mesh), flag, None, ctypes.byref(shard), ctypes.byref(out)) == _lib.ERR_ARG
+    cur = np.zeros(3 * m.n_vertices)
+    p = cur.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert lib.fwgpu_cojo_solve(None, p, None, None) == _lib.ERR_ARG
+    assert lib.fwgpu_cojo_set_current(None, p) == _lib.ERR_ARG
+    n = ctypes.c_int32()
+    assert lib.fwgpu_cojo_subdomains(None, ctypes.byref(n), None) == _lib.ERR_ARG
+    with pytest.raises(ValueError):
+        hddm.CorrectJoPartition(m, flag, pec_vertex=np.zeros(3, bool))
+
+
+@pytest.mark.skipif(__import__("conftest").has_gpu(), reason="checks the no-device error path")
+def test_no_device_fails_loudly():
+    with pytest.raises(_lib.FwgpuError) as e:
+        hddm.CorrectJoSolver(models()["cyl"], 4)
+    assert e.value.code == _lib.ERR_CUDA
